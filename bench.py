@@ -1,0 +1,405 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 block-iterative reconstruction path.
+
+Workload (one "step" = one full SART iteration over the tilt series):
+  volume 1024 x 1024 x 256 float32, ellipsoid phantom (200 ellipsoids, semi-axes
+  8-128 voxels, densities 0.05-1.0, scaled by 0.01 per voxel so line integrals
+  stay in the range where 100-count Poisson noise is informative);
+  61 parallel-beam views -60..+60 deg step 2, detector 1024 x 1024, pitch 1;
+  Poisson noise at 100 counts/pixel then -log; SART (block 1), lambda 0.3,
+  identity order, zero initial volume.  Synthetic data, seeded per rank.
+
+  metric  "SART s to reach plain 30-iter residual": the plain-SART time to
+          run 30 iterations = 30 x measured seconds per iteration (lower is better).
+  value   device-resident inputs (projections and volume in HBM), one CUDA
+          graph per iteration, CUDA events on the library stream, max over ranks.
+  e2e     the same metric through the one-call C ABI etcu_reconstruct with host
+          buffers: pinned host projections + volume in, 30 iterations, volume out.
+
+Multi-GPU: one process per GPU, each reconstructs its own independent tilt
+series (weak scaling); the only collective is the timing max over ranks.
+`--impl reference` times the CPU restatement of the reference's kernels
+(the reference's OpenCL build cannot run here) on a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_VIEWS = 61
+RES = (1024, 1024, 256)  # x, y, z
+DET = (1024, 1024)
+LAMBDA = 0.3
+I0 = 100.0
+MU_SCALE = 0.01
+TARGET_ITERS = 30
+WORKLOAD = "SART parallel beam, 1024x1024x256 f32 volume, 61 views +-60 deg step 2, 1024^2 detector, Poisson I0=100"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-reps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ distributed plumbing
+def dist_init():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        cmd = ["nvidia-smi", "-i", str(self.device),
+               "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+               "--format=csv,noheader,nounits", "-lms", "200"]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.lines:
+            return None
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = max(mx, float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ workload
+def make_phantom_torch(seed: int, device):
+    """200 ellipsoids (centres uniform, semi-axes U(8,128), uniform rotation,
+    density U(0.05,1.0), additive), scaled by MU_SCALE; built on the GPU."""
+    import torch
+    rng = np.random.Generator(np.random.PCG64(seed))
+    X, Y, Z = RES
+    vol = torch.zeros((Z, Y, X), dtype=torch.float32, device=device)
+    for _ in range(200):
+        c = rng.uniform([0, 0, 0], [X, Y, Z])
+        a = rng.uniform(8.0, 128.0, 3)
+        q = rng.normal(size=4)
+        q /= np.linalg.norm(q)
+        w, x, y, z = q
+        R = np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
+                      [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
+                      [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)]])
+        d = rng.uniform(0.05, 1.0)
+        r = int(np.ceil(a.max())) + 1
+        x0, x1 = max(0, int(c[0]) - r), min(X, int(c[0]) + r + 1)
+        y0, y1 = max(0, int(c[1]) - r), min(Y, int(c[1]) + r + 1)
+        z0, z1 = max(0, int(c[2]) - r), min(Z, int(c[2]) + r + 1)
+        if x0 >= x1 or y0 >= y1 or z0 >= z1:
+            continue
+        zz = torch.arange(z0, z1, device=device, dtype=torch.float32) + 0.5 - float(c[2])
+        yy = torch.arange(y0, y1, device=device, dtype=torch.float32) + 0.5 - float(c[1])
+        xx = torch.arange(x0, x1, device=device, dtype=torch.float32) + 0.5 - float(c[0])
+        Rt = torch.tensor(R, dtype=torch.float32, device=device)
+        p = (xx[None, None, :, None] * Rt[0] + yy[None, :, None, None] * Rt[1] + zz[:, None, None, None] * Rt[2])
+        at = torch.tensor(a, dtype=torch.float32, device=device)
+        inside = ((p / at) ** 2).sum(-1) <= 1.0
+        vol[z0:z1, y0:y1, x0:x1] += float(d * MU_SCALE) * inside.float()
+    return vol
+
+
+def make_problem(ctx, seed: int):
+    """Phantom, tilt geometry and noisy projections (forward projected by the CUDA path)."""
+    import torch
+    from ettention_b200.operators import ForwardProjectionOperator, GPUMappedVolume, mrc_base_geometry
+    dev = torch.device("cuda", ctx.device)
+    phantom = make_phantom_torch(seed, dev)
+    torch.cuda.synchronize(dev)
+    angles = np.linspace(-60.0, 60.0, N_VIEWS)
+    geoms = [mrc_base_geometry(*DET).rotated(float(a)) for a in angles]
+    vol = GPUMappedVolume(ctx, RES)
+    vol.upload(phantom.cpu().numpy())
+    del phantom
+    fp = ForwardProjectionOperator(vol, 1)
+    projs = torch.zeros((N_VIEWS, DET[1], DET[0]), dtype=torch.float32, device=dev)
+    scratch = torch.zeros((DET[1], DET[0]), dtype=torch.float32, device=dev)
+    for i, g in enumerate(geoms):
+        fp.setScannerGeometry(g)
+        fp.SetOutput(projs[i], scratch)
+        fp.Execute(0)
+    vol.close()
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed)
+    counts = torch.poisson(I0 * torch.exp(-projs), generator=gen)
+    b = -torch.log(torch.clamp(counts, min=1.0) / I0)
+    torch.cuda.synchronize(dev)
+    return geoms, b.contiguous()
+
+
+# ------------------------------------------------------------------ byte model
+def algorithmic_bytes():
+    """Per launch, FP32 storage: forward projection of one view reads the volume once,
+    reads b and writes (r, L); back projection of a one-view block read-modify-writes
+    the volume and reads (r, L)."""
+    V = RES[0] * RES[1] * RES[2]
+    P = DET[0] * DET[1]
+    fp = V * 4 + P * 4 + P * 8
+    bp = 2 * V * 4 + P * 8
+    return fp, bp
+
+
+# ------------------------------------------------------------------ CPU baseline (oracle)
+def cpu_sample_seconds(threads: int, views: int = 1):
+    """Times the FP32 CPU restatement of the reference kernels (oracle/) on `views` views
+    of the same workload: forward projection + residual + back projection per view."""
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    from oracle import oracle as O
+    X, Y, Z = RES
+    rng = np.random.Generator(np.random.PCG64(5))
+    vol = (rng.uniform(0, 1, size=(Z, Y, X)).astype(np.float32) * MU_SCALE)
+    vg = O.VolumeGeometry.centered(RES)
+    base = O.mrc_base_geometry(*DET)
+    angles = np.linspace(-60.0, 60.0, N_VIEWS)[: views]
+    b = rng.uniform(0, 3, size=(DET[1], DET[0])).astype(np.float32)
+    t0 = time.perf_counter()
+    for a in angles:
+        g = O.rotate_geometry(base, float(a))
+        p, l = O.forward_project(vol, vg, g, 1, 32)
+        r = b - p
+        O.back_project(vol, vg, g, r, l, LAMBDA, 1, 32, O.WEIGHTS_EXACT)
+    return time.perf_counter() - t0
+
+
+def run_reference(args, rank, world):
+    """Reference arm: the CPU restatement of the reference's path on all host cores."""
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    for _ in range(args.warmup):
+        cpu_sample_seconds(threads, 1)
+    ts = [cpu_sample_seconds(threads, 1) for _ in range(args.steps)]
+    per_view = statistics.mean(ts)
+    value = per_view * N_VIEWS * TARGET_ITERS
+    sample = "1 of 61 views (FP + residual + BP) per step at full size, scaled x61 views x30 iterations"
+    line = {"impl": "reference", "metric": "SART s to reach plain 30-iter residual", "value": value, "unit": "s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_view * 1e3,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "step": "one view of one SART iteration",
+                                            "host_threads": threads},
+            "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference's OpenCL build cannot be compiled or run on this box; this arm times the "
+                    "FP32 CPU restatement of its kernels (oracle/) on all host threads"}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ ours
+def run_ours(args, rank, world, local):
+    import torch
+    from ettention_b200 import _abi
+    from ettention_b200._abi import ReconParams, View, VolumeDesc, check, lib
+    from ettention_b200.operators import (AlgebraicParameterSet, BlockIterativeReconstructionOperator, Context,
+                                          GPUMappedVolume)
+    torch.cuda.set_device(local)
+    ctx = Context(local)
+    geoms, b = make_problem(ctx, 2000 + rank)
+    params = AlgebraicParameterSet(algorithm="sart", block_size=1, iterations=TARGET_ITERS, lam=LAMBDA,
+                                   order=_abi.ORDER_IDENTITY)
+    vol = GPUMappedVolume(ctx, RES)
+    rec = BlockIterativeReconstructionOperator(vol, geoms, b, params, use_graph=True)
+    launches_per_iter = rec.launches_per_iteration
+    d0 = rec.data_residual_sq()
+    for _ in range(args.warmup):
+        rec.runNiterations(1)
+    ctx.synchronize()
+    # ---- timed region: K iterations, CUDA events on the library stream ----
+    cudart = torch.cuda.cudart()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    lib_stream = torch.cuda.ExternalStream(ctx.stream_handle)  # events on the stream the kernels run on
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        ev0.record(lib_stream)
+        rec.runNiterations(args.steps)
+        ev1.record(lib_stream)
+        ctx.synchronize()
+        torch.cuda.synchronize()
+    barrier(world)
+    ms_total = ev0.elapsed_time(ev1)
+    ms_total = max_over_ranks(ms_total, world)
+    ms_per_step = ms_total / args.steps
+    value = TARGET_ITERS * ms_per_step / 1e3
+    d1 = rec.data_residual_sq()
+    # ---- per-kernel device times (one more real iteration, launch by launch) ----
+    fp_ms, bp_ms, nf, nb = rec.profile_iteration()
+    fp_bytes, bp_bytes = algorithmic_bytes()
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    fp_avg, bp_avg = fp_ms / max(nf, 1), bp_ms / max(nb, 1)
+    fp_gbs = fp_bytes / (fp_avg * 1e-3) / 1e9
+    bp_gbs = bp_bytes / (bp_avg * 1e-3) / 1e9
+    dominant = "back_project" if bp_ms >= fp_ms else "forward_project"
+    ach = bp_gbs if dominant == "back_project" else fp_gbs
+    roofline = {"bound": "hbm", "kernel": dominant, "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
+                "frac": ach / hbm_peak, "peak_source": peak_src, "traffic": None,
+                "per_kernel": {"forward_project": {"avg_ms": fp_avg, "launches": nf, "algorithmic_bytes": fp_bytes,
+                                                   "gbs": fp_gbs, "frac": fp_gbs / hbm_peak},
+                               "back_project": {"avg_ms": bp_avg, "launches": nb, "algorithmic_bytes": bp_bytes,
+                                                "gbs": bp_gbs, "frac": bp_gbs / hbm_peak}}}
+    rec.close()
+    vol.close()
+    # ---- e2e: one-call host-buffer reconstruction through the C ABI ----
+    host_proj = torch.empty(b.shape, dtype=torch.float32, pin_memory=True)
+    host_proj.copy_(b.cpu())
+    X, Y, Z = RES
+    host_vol = torch.zeros((Z, Y, X), dtype=torch.float32, pin_memory=True)
+    views = (View * N_VIEWS)(*[g.to_view() for g in geoms])
+    desc = VolumeDesc()
+    for i in range(3):
+        desc.resolution[i] = RES[i]
+        desc.bbox_min[i] = -0.5 * RES[i]
+        desc.bbox_max[i] = 0.5 * RES[i]
+    desc.subvolume_count = 1
+    rp = params.recon_params(True)
+    del b
+    torch.cuda.empty_cache()
+    e2e_times = []
+    for rep in range(1 + args.e2e_reps):
+        host_vol.zero_()
+        barrier(world)
+        ctx.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(lib_stream)
+        ctx.check(lib().etcu_reconstruct(ctx.handle, ctypes.byref(desc), _abi.VOXEL_FLOAT32, views, N_VIEWS,
+                                         host_proj.data_ptr(), ctypes.byref(rp), TARGET_ITERS, host_vol.data_ptr()))
+        e1.record(lib_stream)
+        torch.cuda.synchronize()
+        if rep > 0:
+            e2e_times.append(e0.elapsed_time(e1))
+    e2e_ms = max_over_ranks(statistics.mean(e2e_times), world)
+    h2d = host_proj.numel() * 4 + host_vol.numel() * 4
+    d2h = host_vol.numel() * 4
+    # ---- CPU baseline (rank 0, N = 1 only) ----
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        t = cpu_sample_seconds(threads, 1)
+        cpu = {"value": t * N_VIEWS * TARGET_ITERS, "unit": "s", "cores": threads, "kind": "port",
+               "sample": "1 of 61 views (FP + residual + BP) at full size, FP32 oracle, scaled x61 views x30 "
+                         "iterations"}
+    if rank == 0:
+        line = {"metric": "SART s to reach plain 30-iter residual", "value": value, "unit": "s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+                "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded ellipsoid phantom, CUDA-forward-projected, Poisson noise)",
+                "config": {"workload": WORKLOAD, "step": "one SART iteration (61 views, one CUDA graph)",
+                           "volume": list(RES), "views": N_VIEWS, "detector": list(DET), "lambda": LAMBDA,
+                           "storage": "f32", "l2": "inputs larger than L2 (1 GiB volume)",
+                           "parallelism": f"independent series per GPU x{world}"},
+                "e2e": {"value": e2e_ms * 1e-3, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                "gpu_launches": launches_per_iter * args.steps,
+                "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks.summary(),
+                "residual_sq": {"before": d0, "after_warmup_and_timed": d1},
+                "learned_warm_start": "not built: plain SART only"}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_init()
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

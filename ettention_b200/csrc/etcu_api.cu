@@ -1,0 +1,1111 @@
+// C ABI of the B200 block-iterative reconstruction path: contexts, device
+// volumes, the projector operators and the block-iterative driver.
+//
+// Reference host code replaced here (LR = ettention/libReconstruction/src):
+//   LR/gpu/opencl/CLAbstractionLayer.cpp, LR/gpu/GPUMapped.cpp   -> context, device buffers
+//   LR/algorithm/projections/forward/ForwardProjectionKernel.cpp   -> etcu_forward_project
+//   LR/algorithm/projections/back/BackProjectionKernel.cpp         -> etcu_back_project
+//   LR/algorithm/reconstruction/blockiterative/*.cpp               -> etcu_recon_*
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "ettention_b200.h"
+#include "geometry.hpp"
+#include "kernels.cuh"
+
+using namespace etcu;
+
+struct etcu_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    std::string err;
+    size_t bytes = 0;
+    size_t tex_align = 512, tex_pitch_align = 32;
+    // scratch of the single-view back projector: interleaved (residual, length) image
+    float2* pair = nullptr;
+    void* pair_raw = nullptr;
+    size_t pair_pitch = 0;  // float2 units
+    uint32_t pair_w = 0, pair_h = 0;
+    cudaTextureObject_t pair_tex = 0;
+};
+
+struct etcu_volume {
+    etcu_context* ctx = nullptr;
+    etcu_volume_desc desc{};
+    etcu_voxel_type type = ETCU_VOXEL_FLOAT32;
+    float* master = nullptr;  // FP32 volume / FP32 master
+    void* low = nullptr;      // half volume (HALF16) or 16-bit shadow (*_MASTER)
+    uint8_t* mask = nullptr;
+    std::vector<SlabConst> slabs;
+    int use_min = 0, use_max = 0;
+    float vmin = 0.f, vmax = 0.f;
+};
+
+struct etcu_recon {
+    etcu_volume* vol = nullptr;
+    etcu_context* ctx = nullptr;
+    etcu_recon_params params{};
+    uint32_t n_input = 0, W = 0, H = 0;
+    std::vector<uint32_t> order;
+    uint32_t block = 1, nblocks = 0;
+    float* d_proj = nullptr;
+    bool own_proj = false;
+    ViewConst* d_views = nullptr;
+    uint32_t* d_order = nullptr;
+    float4* d_samples = nullptr;
+    uint32_t nsamples = 1;
+    float2* rl = nullptr;
+    void* rl_raw = nullptr;
+    size_t rl_pitch = 0, rl_slot = 0;  // float2 units
+    uint32_t slots = 0;
+    std::vector<cudaTextureObject_t> texs;
+    cudaTextureObject_t* d_texs = nullptr;
+    double* d_resid = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint32_t launches = 0;
+    bool persp = false;
+};
+
+namespace {
+
+thread_local std::string g_create_error;
+
+etcu_status fail(etcu_context* ctx, etcu_status st, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (ctx) ctx->err = buf;
+    else g_create_error = buf;
+    return st;
+}
+
+#define CK(ctx, call)                                                                                   \
+    do {                                                                                                \
+        cudaError_t e_ = (call);                                                                        \
+        if (e_ != cudaSuccess)                                                                          \
+            return fail(ctx, e_ == cudaErrorMemoryAllocation ? ETCU_ERR_OUT_OF_MEMORY : ETCU_ERR_CUDA, \
+                        "%s failed: %s", #call, cudaGetErrorString(e_));                                \
+    } while (0)
+
+#define CKL(ctx) CK(ctx, cudaGetLastError())
+
+etcu_status dalloc(etcu_context* ctx, void** p, size_t bytes) {
+    *p = nullptr;
+    if (bytes == 0) return ETCU_OK;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ctx, ETCU_ERR_OUT_OF_MEMORY, "device allocation of %zu bytes failed: %s", bytes,
+                    cudaGetErrorString(e));
+    }
+    ctx->bytes += bytes;
+    return ETCU_OK;
+}
+
+// Texture-bound images must start on cudaDeviceProp::textureAlignment; the raw
+// allocation is over-sized by that much and the aligned base returned.
+etcu_status dalloc_aligned(etcu_context* ctx, void** raw, void** aligned, size_t bytes, size_t align) {
+    etcu_status s = dalloc(ctx, raw, bytes + align);
+    if (s != ETCU_OK) return s;
+    uintptr_t a = ((uintptr_t)*raw + align - 1) / align * align;
+    *aligned = (void*)a;
+    return ETCU_OK;
+}
+
+void dfree(etcu_context* ctx, void* p, size_t bytes) {
+    if (p) {
+        cudaFree(p);
+        ctx->bytes -= std::min(ctx->bytes, bytes);
+    }
+}
+
+size_t voxel_count(const etcu_volume_desc& d) {
+    return (size_t)d.resolution[0] * d.resolution[1] * d.resolution[2];
+}
+
+float4 f4(const float* p) { return make_float4(p[0], p[1], p[2], 0.f); }
+
+// VolumeProperties::init / setSubVolumeCount (LR/model/volume/VolumeProperties.cpp:21-98).
+bool make_slabs(const etcu_volume_desc& d, std::vector<SlabConst>& out, std::string& err) {
+    uint32_t cnt = d.subvolume_count == 0 ? 1 : d.subvolume_count;
+    if (d.resolution[2] < cnt) {
+        char b[256];
+        snprintf(b, sizeof b, "Volume of size %u in z direction cannot be split into %u subvolumes!", d.resolution[2],
+                 cnt);
+        err = b;
+        return false;
+    }
+    float vs[3], ivs[3];
+    for (int i = 0; i < 3; ++i) {
+        vs[i] = (d.bbox_max[i] - d.bbox_min[i]) / (float)d.resolution[i];
+        ivs[i] = 1.0f / vs[i];
+    }
+    uint32_t base = d.resolution[2] / cnt, rem = d.resolution[2] - cnt * base;
+    float next_min[3] = {d.bbox_min[0], d.bbox_min[1], d.bbox_min[2]};
+    uint32_t z0 = 0;
+    out.clear();
+    for (uint32_t i = 0; i < cnt; ++i) {
+        SlabConst s{};
+        s.rx = (int)d.resolution[0];
+        s.ry = (int)d.resolution[1];
+        s.rz = (int)(i < rem ? base + 1 : base);
+        s.z0 = (int)z0;
+        float smax[3] = {next_min[0] + (float)s.rx * vs[0], next_min[1] + (float)s.ry * vs[1],
+                         next_min[2] + (float)s.rz * vs[2]};
+        s.bmin = f4(next_min);
+        s.bmax = f4(smax);
+        s.cmin = f4(d.bbox_min);
+        s.cmax = f4(d.bbox_max);
+        s.vs = f4(vs);
+        s.ivs = f4(ivs);
+        next_min[2] = smax[2];
+        z0 += (uint32_t)s.rz;
+        out.push_back(s);
+    }
+    return true;
+}
+
+// Host packing of the per-view kernel constants (LR/model/geometry/ScannerGeometry.cpp:95-103).
+ViewConst make_view_const(const etcu_view& v, const SlabConst& slab, float loc_length) {
+    ViewConst c{};
+    Vec3 r = ray_direction(v);
+    c.ray = make_float4(r.x, r.y, r.z, 0.f);
+    float inv[3] = {1.0f / r.x, 1.0f / r.y, 1.0f / r.z};
+    if (r.x == 0.f) inv[0] = -FLT_MAX;
+    if (r.y == 0.f) inv[1] = -FLT_MAX;
+    if (r.z == 0.f) inv[2] = -FLT_MAX;
+    c.inv = make_float4(inv[0], inv[1], inv[2], 0.f);
+    c.source = f4(v.source);
+    c.detector = f4(v.detector);
+    c.hpitch = f4(v.hpitch);
+    c.vpitch = f4(v.vpitch);
+    projection_matrix(v, c.mat);
+    c.loc_length = loc_length;
+    c.perspective = v.perspective ? 1 : 0;
+    // The xz walk is exact when y never steps (ray.y == 0) and every step
+    // difference vs * inv * sign(ray) is finite (DDARaytracer.hl:79).
+    auto sdf = [](float vs, float iv, float rr) {
+        float sg = rr > 0.f ? 1.f : (rr < 0.f ? -1.f : rr);
+        volatile float a = vs * iv;
+        return a * sg;
+    };
+    float sdx = sdf(slab.vs.x, inv[0], r.x), sdy = sdf(slab.vs.y, inv[1], r.y), sdz = sdf(slab.vs.z, inv[2], r.z);
+    c.fast2d = (!v.perspective && r.y == 0.f && std::isfinite(sdx) && std::isfinite(sdy) && std::isfinite(sdz)) ? 1 : 0;
+    return c;
+}
+
+etcu_status check_view(etcu_context* ctx, const etcu_view* v) {
+    if (!v) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "view is NULL");
+    if (v->width == 0 || v->height == 0)
+        return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "projection resolution must be non-zero");
+    float m[16];
+    if (!projection_matrix(*v, m)) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "matrix not invertible");
+    return ETCU_OK;
+}
+
+size_t slab_offset_elems(const etcu_volume* vol, const SlabConst& s) {
+    return (size_t)s.z0 * (size_t)s.rx * (size_t)s.ry;
+}
+
+// ------------------------------------------------------------- launches
+template <typename VoxT, bool kMask, bool kPersp>
+void launch_fp_t(const FpArgs& a, uint32_t nviews, cudaStream_t st) {
+    dim3 block(128);
+    dim3 grid;
+    if (kPersp) grid = dim3((a.W + 15) / 16, (a.H + 7) / 8, nviews);
+    else grid = dim3((a.W + 127) / 128, a.H, nviews);
+    forward_project_kernel<VoxT, kMask, kPersp><<<grid, block, 0, st>>>(a);
+}
+
+template <typename VoxT>
+void launch_fp_v(const FpArgs& a, bool mask, bool persp, uint32_t nviews, cudaStream_t st) {
+    if (persp) {
+        if (mask) launch_fp_t<VoxT, true, true>(a, nviews, st);
+        else launch_fp_t<VoxT, false, true>(a, nviews, st);
+    } else {
+        if (mask) launch_fp_t<VoxT, true, false>(a, nviews, st);
+        else launch_fp_t<VoxT, false, false>(a, nviews, st);
+    }
+}
+
+void launch_fp(const etcu_volume* vol, const FpArgs& a, bool persp, uint32_t nviews, cudaStream_t st) {
+    bool mask = a.mask != nullptr;
+    switch (vol->type) {
+    case ETCU_VOXEL_FLOAT32: launch_fp_v<float>(a, mask, persp, nviews, st); break;
+    case ETCU_VOXEL_HALF16:
+    case ETCU_VOXEL_F16_MASTER: launch_fp_v<__half>(a, mask, persp, nviews, st); break;
+    case ETCU_VOXEL_BF16_MASTER: launch_fp_v<__nv_bfloat16>(a, mask, persp, nviews, st); break;
+    }
+}
+
+template <bool kPersp, bool kMask, int kStore, bool kExact>
+void launch_bp_t(const BpArgs& a, cudaStream_t st) {
+    dim3 block(64, 4, 1);
+    dim3 grid((a.slab.rx + 63) / 64, (a.slab.ry + 3) / 4, a.slab.rz);
+    back_project_kernel<kPersp, kMask, kStore, kExact><<<grid, block, 0, st>>>(a);
+}
+
+template <bool kPersp, bool kMask, int kStore>
+void launch_bp_s(const BpArgs& a, bool exact, cudaStream_t st) {
+    if (exact) launch_bp_t<kPersp, kMask, kStore, true>(a, st);
+    else launch_bp_t<kPersp, kMask, kStore, false>(a, st);
+}
+
+template <bool kPersp, bool kMask>
+void launch_bp_m(const BpArgs& a, etcu_voxel_type t, bool exact, cudaStream_t st) {
+    switch (t) {
+    case ETCU_VOXEL_FLOAT32: launch_bp_s<kPersp, kMask, 0>(a, exact, st); break;
+    case ETCU_VOXEL_HALF16: launch_bp_s<kPersp, kMask, 1>(a, exact, st); break;
+    case ETCU_VOXEL_F16_MASTER: launch_bp_s<kPersp, kMask, 2>(a, exact, st); break;
+    case ETCU_VOXEL_BF16_MASTER: launch_bp_s<kPersp, kMask, 3>(a, exact, st); break;
+    }
+}
+
+void launch_bp(const etcu_volume* vol, const BpArgs& a, bool persp, bool exact, cudaStream_t st) {
+    bool mask = a.mask != nullptr;
+    if (persp) {
+        if (mask) launch_bp_m<true, true>(a, vol->type, exact, st);
+        else launch_bp_m<true, false>(a, vol->type, exact, st);
+    } else {
+        if (mask) launch_bp_m<false, true>(a, vol->type, exact, st);
+        else launch_bp_m<false, false>(a, vol->type, exact, st);
+    }
+}
+
+void fill_bp_volume_ptrs(const etcu_volume* vol, const SlabConst& s, BpArgs& a) {
+    size_t off = slab_offset_elems(vol, s);
+    if (vol->type == ETCU_VOXEL_HALF16) {
+        a.vol = (__half*)vol->low + off;
+        a.shadow = nullptr;
+    } else {
+        a.vol = vol->master + off;
+        a.shadow = vol->type == ETCU_VOXEL_FLOAT32 ? nullptr : (void*)((uint16_t*)vol->low + off);
+    }
+    a.mask = vol->mask ? vol->mask + off : nullptr;
+}
+
+void fill_fp_volume_ptrs(const etcu_volume* vol, const SlabConst& s, FpArgs& a) {
+    size_t off = slab_offset_elems(vol, s);
+    if (vol->type == ETCU_VOXEL_FLOAT32) a.vol = vol->master + off;
+    else a.vol = (const uint16_t*)vol->low + off;
+    a.mask = vol->mask ? vol->mask + off : nullptr;
+}
+
+etcu_status make_pair_texture(etcu_context* ctx, float2* base, size_t pitch_elems, uint32_t W, uint32_t H,
+                              cudaTextureObject_t* out) {
+    cudaResourceDesc rd{};
+    rd.resType = cudaResourceTypePitch2D;
+    rd.res.pitch2D.devPtr = base;
+    rd.res.pitch2D.desc = cudaCreateChannelDesc<float2>();
+    rd.res.pitch2D.width = W;
+    rd.res.pitch2D.height = H;
+    rd.res.pitch2D.pitchInBytes = pitch_elems * sizeof(float2);
+    cudaTextureDesc td{};
+    td.addressMode[0] = cudaAddressModeBorder;
+    td.addressMode[1] = cudaAddressModeBorder;
+    td.filterMode = cudaFilterModeLinear;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 0;
+    CK(ctx, cudaCreateTextureObject(out, &rd, &td, nullptr));
+    return ETCU_OK;
+}
+
+size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+etcu_status ensure_pair_scratch(etcu_context* ctx, uint32_t W, uint32_t H) {
+    if (ctx->pair && ctx->pair_w == W && ctx->pair_h == H) return ETCU_OK;
+    if (ctx->pair_tex) cudaDestroyTextureObject(ctx->pair_tex);
+    ctx->pair_tex = 0;
+    dfree(ctx, ctx->pair_raw, ctx->pair_pitch * sizeof(float2) * ctx->pair_h + ctx->tex_align);
+    ctx->pair = nullptr;
+    ctx->pair_raw = nullptr;
+    size_t pitch_bytes = round_up((size_t)W * sizeof(float2), ctx->tex_pitch_align);
+    etcu_status s = dalloc_aligned(ctx, &ctx->pair_raw, (void**)&ctx->pair, pitch_bytes * H, ctx->tex_align);
+    if (s != ETCU_OK) return s;
+    ctx->pair_pitch = pitch_bytes / sizeof(float2);
+    ctx->pair_w = W;
+    ctx->pair_h = H;
+    return make_pair_texture(ctx, ctx->pair, ctx->pair_pitch, W, H, &ctx->pair_tex);
+}
+
+etcu_status upload_host_float(etcu_context* ctx, float* dst, const float* host, size_t n) {
+    CK(ctx, cudaMemcpyAsync(dst, host, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    return ETCU_OK;
+}
+
+void launch_1d_dims(size_t n, dim3& g, dim3& b) {
+    b = dim3(256);
+    g = dim3((unsigned)((n + 255) / 256));
+}
+
+etcu_status refresh_low_from_master(etcu_volume* vol) {
+    etcu_context* ctx = vol->ctx;
+    size_t n = voxel_count(vol->desc);
+    dim3 g, b;
+    launch_1d_dims(n, g, b);
+    if (vol->type == ETCU_VOXEL_F16_MASTER)
+        convert_from_float_kernel<__half><<<g, b, 0, ctx->stream>>>(vol->master, (__half*)vol->low, n);
+    else if (vol->type == ETCU_VOXEL_BF16_MASTER)
+        convert_from_float_kernel<__nv_bfloat16><<<g, b, 0, ctx->stream>>>(vol->master, (__nv_bfloat16*)vol->low, n);
+    CKL(ctx);
+    return ETCU_OK;
+}
+
+}  // namespace
+
+// =============================================================== context
+extern "C" int etcu_abi_version(void) { return ETCU_ABI_VERSION; }
+
+extern "C" etcu_status etcu_context_create(int device, etcu_context** out) {
+    if (!out) return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return fail(nullptr, ETCU_ERR_NO_DEVICE, "no CUDA device available (%s)", cudaGetErrorString(e));
+    }
+    if (device < 0 || device >= n) return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT, "device %d out of range", device);
+    std::unique_ptr<etcu_context> c(new etcu_context());
+    c->device = device;
+    if (cudaSetDevice(device) != cudaSuccess) return fail(nullptr, ETCU_ERR_CUDA, "cudaSetDevice failed");
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess)
+        return fail(nullptr, ETCU_ERR_CUDA, "cudaGetDeviceProperties failed");
+    if (prop.major < 10) return fail(nullptr, ETCU_ERR_UNSUPPORTED, "device %s (sm_%d%d) is not sm_100", prop.name,
+                                     prop.major, prop.minor);
+    c->tex_align = prop.textureAlignment;
+    c->tex_pitch_align = prop.texturePitchAlignment;
+    // A blocking stream: work on the legacy default stream (which other CUDA
+    // users in the process write device images on) is ordered before and after it.
+    if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamDefault) != cudaSuccess)
+        return fail(nullptr, ETCU_ERR_CUDA, "cudaStreamCreate failed");
+    c->stream = c->own_stream;
+    *out = c.release();
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_context_destroy(etcu_context* ctx) {
+    if (!ctx) return ETCU_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    if (ctx->pair_tex) cudaDestroyTextureObject(ctx->pair_tex);
+    if (ctx->pair_raw) cudaFree(ctx->pair_raw);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return ETCU_OK;
+}
+
+extern "C" const char* etcu_last_error(const etcu_context* ctx) {
+    return ctx ? ctx->err.c_str() : g_create_error.c_str();
+}
+
+extern "C" etcu_status etcu_synchronize(etcu_context* ctx) {
+    if (!ctx) return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    CKL(ctx);
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_set_stream(etcu_context* ctx, void* stream) {
+    if (!ctx) return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+    return ETCU_OK;
+}
+
+extern "C" size_t etcu_device_bytes(const etcu_context* ctx) { return ctx ? ctx->bytes : 0; }
+
+extern "C" void* etcu_context_stream(const etcu_context* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+// =============================================================== geometry
+extern "C" etcu_status etcu_view_rotate(const etcu_view* base, float tilt, float xtilt, etcu_view* out) {
+    if (!base || !out) return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL view");
+    *out = rotate_view(*base, tilt, xtilt);
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_view_projection_matrix(const etcu_view* view, float out16[16]) {
+    if (!view || !out16) return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (!projection_matrix(*view, out16)) return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT, "matrix not invertible");
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_view_sample_pattern(const etcu_view* view, const float vs[3], uint32_t samples,
+                                                float* out4) {
+    if (!view || !vs || !out4) return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    std::string err;
+    if (!sample_pattern(*view, vs, samples, out4, &err)) return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT, "%s", err.c_str());
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_view_traversal_length(const etcu_view* view, const float bmin[3], const float bmax[3],
+                                                  float* out) {
+    if (!view || !bmin || !bmax || !out) return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (view->perspective)
+        return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT,
+                    "Calculation of traversal length is only supported for parallel scanner geometry!");
+    *out = traversal_length(*view, bmin, bmax);
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_projection_order(etcu_order order, uint32_t n, const uint32_t* skip, uint32_t nskip,
+                                             uint32_t* out, uint32_t* count) {
+    if (!out || !count) return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    if ((int)order < 0 || (int)order > 3) return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT, "Illegal ProjectionSetType!");
+    std::vector<uint32_t> o = projection_order(order, n, skip, skip ? nskip : 0);
+    for (size_t i = 0; i < o.size(); ++i) out[i] = o[i];
+    *count = (uint32_t)o.size();
+    return ETCU_OK;
+}
+
+// =============================================================== volume
+extern "C" etcu_status etcu_volume_create(etcu_context* ctx, const etcu_volume_desc* desc, etcu_voxel_type type,
+                                          float init_value, etcu_volume** out) {
+    if (!ctx || !desc || !out) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    if (desc->resolution[0] == 0 || desc->resolution[1] == 0 || desc->resolution[2] == 0)
+        return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "volume resolution must be non-zero");
+    if ((int)type < 0 || (int)type > 3)
+        return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "UChar is not supported as a valid internal voxel storage data type.");
+    for (int i = 0; i < 3; ++i)
+        if (!(desc->bbox_max[i] > desc->bbox_min[i]))
+            return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "volume bounding box is empty along axis %d", i);
+    std::unique_ptr<etcu_volume> v(new etcu_volume());
+    v->ctx = ctx;
+    v->desc = *desc;
+    v->type = type;
+    std::string err;
+    if (!make_slabs(*desc, v->slabs, err)) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "%s", err.c_str());
+    CK(ctx, cudaSetDevice(ctx->device));
+    size_t n = voxel_count(*desc);
+    etcu_status s;
+    if (type != ETCU_VOXEL_HALF16) {
+        if ((s = dalloc(ctx, (void**)&v->master, n * sizeof(float))) != ETCU_OK) return s;
+    }
+    if (type != ETCU_VOXEL_FLOAT32) {
+        if ((s = dalloc(ctx, &v->low, n * 2)) != ETCU_OK) {
+            dfree(ctx, v->master, n * sizeof(float));
+            return s;
+        }
+    }
+    dim3 g, b;
+    launch_1d_dims(n, g, b);
+    if (v->master) {
+        fill_kernel<<<g, b, 0, ctx->stream>>>(v->master, init_value, n);
+        CKL(ctx);
+        if (type != ETCU_VOXEL_FLOAT32 && (s = refresh_low_from_master(v.get())) != ETCU_OK) return s;
+    } else {
+        float* tmp = nullptr;
+        if ((s = dalloc(ctx, (void**)&tmp, n * sizeof(float))) != ETCU_OK) return s;
+        fill_kernel<<<g, b, 0, ctx->stream>>>(tmp, init_value, n);
+        convert_from_float_kernel<__half><<<g, b, 0, ctx->stream>>>(tmp, (__half*)v->low, n);
+        cudaStreamSynchronize(ctx->stream);
+        dfree(ctx, tmp, n * sizeof(float));
+        CKL(ctx);
+    }
+    *out = v.release();
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_volume_destroy(etcu_volume* vol) {
+    if (!vol) return ETCU_OK;
+    etcu_context* ctx = vol->ctx;
+    cudaStreamSynchronize(ctx->stream);
+    size_t n = voxel_count(vol->desc);
+    dfree(ctx, vol->master, n * sizeof(float));
+    dfree(ctx, vol->low, n * 2);
+    dfree(ctx, vol->mask, n);
+    delete vol;
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_volume_upload(etcu_volume* vol, const float* host) {
+    if (!vol || !host) return fail(vol ? vol->ctx : nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    etcu_context* ctx = vol->ctx;
+    size_t n = voxel_count(vol->desc);
+    etcu_status s;
+    if (vol->master) {
+        if ((s = upload_host_float(ctx, vol->master, host, n)) != ETCU_OK) return s;
+        if (vol->type != ETCU_VOXEL_FLOAT32) return refresh_low_from_master(vol);
+        return ETCU_OK;
+    }
+    float* tmp = nullptr;
+    if ((s = dalloc(ctx, (void**)&tmp, n * sizeof(float))) != ETCU_OK) return s;
+    s = upload_host_float(ctx, tmp, host, n);
+    if (s == ETCU_OK) {
+        dim3 g, b;
+        launch_1d_dims(n, g, b);
+        convert_from_float_kernel<__half><<<g, b, 0, ctx->stream>>>(tmp, (__half*)vol->low, n);
+        cudaStreamSynchronize(ctx->stream);
+    }
+    dfree(ctx, tmp, n * sizeof(float));
+    CKL(ctx);
+    return s;
+}
+
+extern "C" etcu_status etcu_volume_download(etcu_volume* vol, float* host) {
+    if (!vol || !host) return fail(vol ? vol->ctx : nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    etcu_context* ctx = vol->ctx;
+    size_t n = voxel_count(vol->desc);
+    if (vol->master) {
+        CK(ctx, cudaMemcpyAsync(host, vol->master, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(ctx, cudaStreamSynchronize(ctx->stream));
+        return ETCU_OK;
+    }
+    float* tmp = nullptr;
+    etcu_status s;
+    if ((s = dalloc(ctx, (void**)&tmp, n * sizeof(float))) != ETCU_OK) return s;
+    dim3 g, b;
+    launch_1d_dims(n, g, b);
+    convert_to_float_kernel<__half><<<g, b, 0, ctx->stream>>>((const __half*)vol->low, tmp, n);
+    cudaError_t e = cudaMemcpyAsync(host, tmp, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+    dfree(ctx, tmp, n * sizeof(float));
+    CK(ctx, e);
+    CKL(ctx);
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_volume_set_mask(etcu_volume* vol, const uint8_t* host_mask) {
+    if (!vol) return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL volume");
+    etcu_context* ctx = vol->ctx;
+    size_t n = voxel_count(vol->desc);
+    if (!host_mask) {
+        cudaStreamSynchronize(ctx->stream);
+        dfree(ctx, vol->mask, n);
+        vol->mask = nullptr;
+        return ETCU_OK;
+    }
+    etcu_status s;
+    if (!vol->mask && (s = dalloc(ctx, (void**)&vol->mask, n)) != ETCU_OK) return s;
+    CK(ctx, cudaMemcpyAsync(vol->mask, host_mask, n, cudaMemcpyHostToDevice, ctx->stream));
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    return ETCU_OK;
+}
+
+extern "C" void* etcu_volume_device_ptr(etcu_volume* vol) {
+    if (!vol) return nullptr;
+    return vol->master ? (void*)vol->master : vol->low;
+}
+
+extern "C" etcu_status etcu_volume_set_intensity_clamp(etcu_volume* vol, int use_min, float vmin, int use_max,
+                                                       float vmax) {
+    if (!vol) return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL volume");
+    vol->use_min = use_min;
+    vol->vmin = vmin;
+    vol->use_max = use_max;
+    vol->vmax = vmax;
+    return ETCU_OK;
+}
+
+// =============================================================== operators
+extern "C" etcu_status etcu_forward_project(etcu_volume* vol, const etcu_view* view, uint32_t subvolume,
+                                            uint32_t samples, float* d_virtual, float* d_traversal) {
+    if (!vol) return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL volume");
+    etcu_context* ctx = vol->ctx;
+    etcu_status s;
+    if ((s = check_view(ctx, view)) != ETCU_OK) return s;
+    if (!d_virtual ^ !d_traversal)
+        return fail(ctx, ETCU_ERR_INVALID_ARGUMENT,
+                    "Virtual projection and traversal length must either be set both or none of them!");
+    if (!d_virtual)
+        return fail(ctx, ETCU_ERR_STATE,
+                    "ForwardProjectionKernel cannot be run without setting output images! Be sure to call setOutput() "
+                    "before with non-null parameters.");
+    if (subvolume >= vol->slabs.size())
+        return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "Tried to get resolution of subvolume %u while there are only %zu!",
+                    subvolume, vol->slabs.size());
+    const SlabConst& slab = vol->slabs[subvolume];
+    FpArgs a{};
+    fill_fp_volume_ptrs(vol, slab, a);
+    a.slab = slab;
+    a.views = nullptr;
+    a.inline_view = make_view_const(*view, slab, 0.f);
+    a.order = nullptr;
+    a.first = 0;
+    a.W = (int)view->width;
+    a.H = (int)view->height;
+    a.samples = samples == 0 ? 1 : (int)samples;  // ForwardProjectionKernel.cpp:65-68
+    a.mode = kFpSeparateAccumulate;
+    a.out_v = d_virtual;
+    a.out_l = d_traversal;
+    launch_fp(vol, a, view->perspective != 0, 1, ctx->stream);
+    CKL(ctx);
+    return ETCU_OK;
+}
+
+namespace {
+etcu_status bp_one_slab(etcu_volume* vol, const etcu_view* view, const SlabConst& slab, uint32_t samples,
+                        float lambda_eff, const float4* pattern, etcu_sampling sampling) {
+    etcu_context* ctx = vol->ctx;
+    BpArgs a{};
+    fill_bp_volume_ptrs(vol, slab, a);
+    a.slab = slab;
+    a.views = nullptr;
+    a.inline_view = make_view_const(*view, slab, 0.f);
+    a.order = nullptr;
+    a.first = 0;
+    a.nviews = 1;
+    a.texs = nullptr;
+    a.inline_tex = ctx->pair_tex;
+    a.rl = ctx->pair;
+    a.rl_pitch = ctx->pair_pitch;
+    a.rl_slot = 0;
+    a.W = (int)view->width;
+    a.H = (int)view->height;
+    a.lambda = lambda_eff;
+    a.samples = nullptr;
+    if (!view->perspective) {
+        a.nsamples = (int)samples;
+        for (uint32_t k = 0; k < samples; ++k) a.inline_samples[k] = pattern[k];
+    } else {
+        a.nsamples = 0;
+        uint32_t res[3] = {(uint32_t)slab.rx, (uint32_t)slab.ry, (uint32_t)slab.rz};
+        a.persp_n = (int)perspective_sampling_factor(view->width, view->height, res, samples);
+    }
+    a.use_min = vol->use_min;
+    a.use_max = vol->use_max;
+    a.vmin = vol->vmin;
+    a.vmax = vol->vmax;
+    launch_bp(vol, a, view->perspective != 0, sampling == ETCU_SAMPLING_EXACT, ctx->stream);
+    CKL(ctx);
+    return ETCU_OK;
+}
+}  // namespace
+
+extern "C" etcu_status etcu_back_project(etcu_volume* vol, const etcu_view* view, uint32_t subvolume,
+                                         uint32_t samples, float lambda, uint32_t block_size, const float* d_residual,
+                                         const float* d_traversal, etcu_sampling sampling) {
+    if (!vol) return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL volume");
+    etcu_context* ctx = vol->ctx;
+    etcu_status s;
+    if ((s = check_view(ctx, view)) != ETCU_OK) return s;
+    if (!d_residual ^ !d_traversal)
+        return fail(ctx, ETCU_ERR_INVALID_ARGUMENT,
+                    "Either residual and traversalLength images must be provided both or none of them!");
+    if (!d_residual)
+        return fail(ctx, ETCU_ERR_STATE,
+                    "Residual and traversalLength images must both be provided via SetInput() before kernel launch!");
+    if (block_size == 0) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "Illegal ProjectionBlockSize!");
+    if (subvolume != ETCU_ALL_SUBVOLUMES && subvolume >= vol->slabs.size())
+        return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "Tried to get resolution of subvolume %u while there are only %zu!",
+                    subvolume, vol->slabs.size());
+    std::vector<float> pattern;
+    if (!view->perspective) {
+        float vs[3] = {vol->slabs[0].vs.x, vol->slabs[0].vs.y, vol->slabs[0].vs.z};
+        pattern.resize(4 * (size_t)std::max(samples, 1u));
+        std::string err;
+        if (!sample_pattern(*view, vs, samples, pattern.data(), &err))
+            return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "%s", err.c_str());
+        if (samples > (uint32_t)kMaxInlineSamples)
+            return fail(ctx, ETCU_ERR_UNSUPPORTED, "at most %d back-projection samples per voxel", kMaxInlineSamples);
+    }
+    if ((s = ensure_pair_scratch(ctx, view->width, view->height)) != ETCU_OK) return s;
+    dim3 b(128), g((view->width + 127) / 128, view->height);
+    pack_pair_kernel<<<g, b, 0, ctx->stream>>>(d_residual, d_traversal, ctx->pair, ctx->pair_pitch, (int)view->width,
+                                               (int)view->height);
+    CKL(ctx);
+    const float lam = lambda / (float)block_size;  // BackProjectionKernel.cpp:94
+    const float4* pat = (const float4*)pattern.data();
+    if (subvolume == ETCU_ALL_SUBVOLUMES) {  // BackProjectionOperator.cpp:43-57
+        for (const SlabConst& sl : vol->slabs)
+            if ((s = bp_one_slab(vol, view, sl, samples, lam, pat, sampling)) != ETCU_OK) return s;
+    } else if ((s = bp_one_slab(vol, view, vol->slabs[subvolume], samples, lam, pat, sampling)) != ETCU_OK) {
+        return s;
+    }
+    if (vol->type == ETCU_VOXEL_F16_MASTER || vol->type == ETCU_VOXEL_BF16_MASTER) {
+        // the kernel already wrote the shadow of every updated voxel
+    }
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_compare(etcu_context* ctx, const float* d_real, const float* d_virtual,
+                                    float* d_residual, size_t n) {
+    if (!ctx || !d_real || !d_virtual || !d_residual) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (n == 0) return ETCU_OK;
+    dim3 g, b;
+    launch_1d_dims(n, g, b);
+    compare_kernel<<<g, b, 0, ctx->stream>>>(d_real, d_virtual, d_residual, n);
+    CKL(ctx);
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_long_object_compensation(etcu_context* ctx, float* d_virtual, float* d_traversal,
+                                                     float constant_length, size_t n) {
+    if (!ctx || !d_virtual || !d_traversal) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (n == 0) return ETCU_OK;
+    dim3 g, b;
+    launch_1d_dims(n, g, b);
+    loc_kernel<<<g, b, 0, ctx->stream>>>(d_virtual, d_traversal, constant_length, n);
+    CKL(ctx);
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_compute_ray_length(etcu_volume* vol, const etcu_view* view, float* d_out) {
+    if (!vol || !d_out) return fail(vol ? vol->ctx : nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    etcu_context* ctx = vol->ctx;
+    etcu_status s;
+    if ((s = check_view(ctx, view)) != ETCU_OK) return s;
+    ViewConst vc = make_view_const(*view, vol->slabs[0], 0.f);
+    dim3 b(128), g((view->width + 127) / 128, view->height);
+    ray_length_kernel<<<g, b, 0, ctx->stream>>>(vc, vol->slabs[0], (int)view->width, (int)view->height, d_out);
+    CKL(ctx);
+    return ETCU_OK;
+}
+
+// =============================================================== reconstruction
+namespace {
+
+void recon_free(etcu_recon* r) {
+    etcu_context* ctx = r->ctx;
+    cudaStreamSynchronize(ctx->stream);
+    if (r->exec) cudaGraphExecDestroy(r->exec);
+    if (r->graph) cudaGraphDestroy(r->graph);
+    for (auto t : r->texs) cudaDestroyTextureObject(t);
+    size_t N = r->n_input;
+    if (r->own_proj) dfree(ctx, r->d_proj, N * (size_t)r->W * r->H * sizeof(float));
+    dfree(ctx, r->d_views, N * sizeof(ViewConst) * r->vol->slabs.size());
+    dfree(ctx, r->d_order, r->order.size() * sizeof(uint32_t));
+    dfree(ctx, r->d_samples, N * r->nsamples * sizeof(float4));
+    dfree(ctx, r->rl_raw, r->rl_slot * r->slots * sizeof(float2) + ctx->tex_align);
+    dfree(ctx, r->d_texs, r->slots * sizeof(cudaTextureObject_t));
+    dfree(ctx, r->d_resid, sizeof(double));
+}
+
+// Forward projection of `count` views starting at order position `first`
+// into slots 0..count-1: every slab in turn, the first overwriting and the
+// last writing (residual, length) plus the FP64 sum of residual^2.
+uint32_t issue_forward(etcu_recon* r, uint32_t first, uint32_t count, cudaStream_t st) {
+    etcu_volume* vol = r->vol;
+    const uint32_t S = (uint32_t)vol->slabs.size();
+    for (uint32_t s = 0; s < S; ++s) {
+        const SlabConst& slab = vol->slabs[s];
+        FpArgs a{};
+        fill_fp_volume_ptrs(vol, slab, a);
+        a.slab = slab;
+        a.views = r->d_views + (size_t)s * r->n_input;
+        a.order = r->d_order;
+        a.first = first;
+        a.W = (int)r->W;
+        a.H = (int)r->H;
+        a.samples = r->params.fp_samples == 0 ? 1 : (int)r->params.fp_samples;
+        a.mode = (s == S - 1) ? kFpPairResidual : kFpPairAccumulate;
+        a.overwrite = (s == 0) ? 1 : 0;
+        a.loc = r->params.use_long_object_compensation ? 1 : 0;
+        a.rl = r->rl;
+        a.rl_pitch = r->rl_pitch;
+        a.rl_slot = r->rl_slot;
+        a.real = r->d_proj;
+        a.resid_sq = r->d_resid;
+        launch_fp(vol, a, r->persp, count, st);
+    }
+    return S;
+}
+
+// Back projection of the block's views, slabs in reverse order
+// (BlockIterativeReconstructionOperator.cpp:130-142), lambda / blockSize.
+uint32_t issue_backward(etcu_recon* r, uint32_t first, uint32_t count, cudaStream_t st) {
+    etcu_volume* vol = r->vol;
+    const uint32_t S = (uint32_t)vol->slabs.size();
+    for (int s = (int)S - 1; s >= 0; --s) {
+        const SlabConst& slab = vol->slabs[s];
+        BpArgs a{};
+        fill_bp_volume_ptrs(vol, slab, a);
+        a.slab = slab;
+        a.views = r->d_views + (size_t)s * r->n_input;
+        a.order = r->d_order;
+        a.first = first;
+        a.nviews = (int)count;
+        a.texs = r->d_texs;
+        a.rl = r->rl;
+        a.rl_pitch = r->rl_pitch;
+        a.rl_slot = r->rl_slot;
+        a.W = (int)r->W;
+        a.H = (int)r->H;
+        a.lambda = r->params.lambda / (float)count;  // BackProjectionKernel.cpp:94
+        a.samples = r->d_samples;
+        a.nsamples = (int)r->nsamples;
+        uint32_t res[3] = {(uint32_t)slab.rx, (uint32_t)slab.ry, (uint32_t)slab.rz};
+        a.persp_n = (int)perspective_sampling_factor(r->W, r->H, res, r->params.bp_samples);
+        a.use_min = vol->use_min;
+        a.use_max = vol->use_max;
+        a.vmin = vol->vmin;
+        a.vmax = vol->vmax;
+        launch_bp(vol, a, r->persp, r->params.sampling == ETCU_SAMPLING_EXACT, st);
+    }
+    return S;
+}
+
+// One iteration (BlockIterativeReconstructionOperator.cpp:92-103).
+etcu_status issue_iteration(etcu_recon* r, cudaStream_t st, uint32_t* launches) {
+    etcu_context* ctx = r->ctx;
+    const uint32_t M = (uint32_t)r->order.size();
+    uint32_t n = 0;
+    CK(ctx, cudaMemsetAsync(r->d_resid, 0, sizeof(double), st));
+    for (uint32_t b = 0; b < r->nblocks; ++b) {
+        const uint32_t first = b * r->block;
+        const uint32_t bs = (b < r->nblocks - 1) ? r->block : M - first;  // BlockIterativeProjectionAccess.cpp:55-70
+        n += issue_forward(r, first, bs, st);
+        n += issue_backward(r, first, bs, st);
+    }
+    CKL(ctx);
+    if (launches) *launches = n;
+    return ETCU_OK;
+}
+
+etcu_status recon_build(etcu_volume* vol, const etcu_view* views, uint32_t n_views, const float* host_proj,
+                        const float* dev_proj, const etcu_recon_params* params, etcu_recon** out) {
+    etcu_context* ctx = vol ? vol->ctx : nullptr;
+    if (!vol || !views || !params || !out || (!host_proj && !dev_proj))
+        return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    if (n_views == 0) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "No projections given!");
+    if (params->block_size == 0) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "Illegal ProjectionBlockSize!");
+    if ((int)params->order < 0 || (int)params->order > 3)
+        return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "Illegal ProjectionSetType!");
+    const uint32_t W = views[0].width, H = views[0].height;
+    const bool persp = views[0].perspective != 0;
+    for (uint32_t i = 0; i < n_views; ++i) {
+        etcu_status s = check_view(ctx, &views[i]);
+        if (s != ETCU_OK) return s;
+        if (views[i].width != W || views[i].height != H)
+            return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "all projections must share one resolution");
+        if ((views[i].perspective != 0) != persp)
+            return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "all projections must share one beam geometry");
+    }
+    if (persp && params->use_long_object_compensation)
+        return fail(ctx, ETCU_ERR_INVALID_ARGUMENT,
+                    "Calculation of traversal length is only supported for parallel scanner geometry!");
+    std::unique_ptr<etcu_recon, void (*)(etcu_recon*)> r(new etcu_recon(), [](etcu_recon* p) {
+        recon_free(p);
+        delete p;
+    });
+    r->vol = vol;
+    r->ctx = ctx;
+    r->params = *params;
+    r->n_input = n_views;
+    r->W = W;
+    r->H = H;
+    r->persp = persp;
+    r->order = projection_order(params->order, n_views, params->skip, params->skip ? params->skip_count : 0);
+    const uint32_t M = (uint32_t)r->order.size();
+    if (M == 0) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "After applying SkipProjectionList no projections are left!");
+    r->block = params->block_size == ETCU_BLOCK_ALL ? M : std::min(params->block_size, M);
+    r->nblocks = (M + r->block - 1) / r->block;  // BlockIterativeProjectionAccess.cpp:46
+    r->slots = r->block;
+    etcu_status s;
+    const size_t P = (size_t)W * H;
+    // tilt series, device-resident for the whole reconstruction
+    if (dev_proj) {
+        r->d_proj = const_cast<float*>(dev_proj);
+    } else {
+        if ((s = dalloc(ctx, (void**)&r->d_proj, P * n_views * sizeof(float))) != ETCU_OK) return s;
+        r->own_proj = true;
+        CK(ctx, cudaMemcpyAsync(r->d_proj, host_proj, P * n_views * sizeof(float), cudaMemcpyHostToDevice,
+                                ctx->stream));
+    }
+    // view constants per slab (fast-path flags depend on the voxel size)
+    const size_t S = vol->slabs.size();
+    std::vector<ViewConst> vc(S * n_views);
+    for (size_t sl = 0; sl < S; ++sl)
+        for (uint32_t i = 0; i < n_views; ++i) {
+            float loc = 0.f;
+            if (params->use_long_object_compensation)
+                loc = traversal_length(views[i], vol->desc.bbox_min, vol->desc.bbox_max);
+            vc[sl * n_views + i] = make_view_const(views[i], vol->slabs[sl], loc);
+        }
+    if ((s = dalloc(ctx, (void**)&r->d_views, vc.size() * sizeof(ViewConst))) != ETCU_OK) return s;
+    CK(ctx, cudaMemcpyAsync(r->d_views, vc.data(), vc.size() * sizeof(ViewConst), cudaMemcpyHostToDevice, ctx->stream));
+    if ((s = dalloc(ctx, (void**)&r->d_order, M * sizeof(uint32_t))) != ETCU_OK) return s;
+    CK(ctx, cudaMemcpyAsync(r->d_order, r->order.data(), M * sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
+    // back-projection sample patterns
+    if (!persp) {
+        r->nsamples = params->bp_samples;
+        std::vector<float> pat(4 * (size_t)std::max(1u, params->bp_samples) * n_views);
+        float vs[3] = {vol->slabs[0].vs.x, vol->slabs[0].vs.y, vol->slabs[0].vs.z};
+        for (uint32_t i = 0; i < n_views; ++i) {
+            std::string err;
+            if (!sample_pattern(views[i], vs, params->bp_samples, pat.data() + 4 * (size_t)params->bp_samples * i, &err))
+                return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "%s", err.c_str());
+        }
+        if ((s = dalloc(ctx, (void**)&r->d_samples, pat.size() * sizeof(float))) != ETCU_OK) return s;
+        CK(ctx, cudaMemcpyAsync(r->d_samples, pat.data(), pat.size() * sizeof(float), cudaMemcpyHostToDevice,
+                                ctx->stream));
+    } else {
+        r->nsamples = 0;
+    }
+    // per-slot interleaved (residual, length) images and their textures
+    size_t pitch_bytes = round_up((size_t)W * sizeof(float2), ctx->tex_pitch_align);
+    size_t slot_bytes = round_up(pitch_bytes * H, std::max<size_t>(ctx->tex_align, 256));
+    r->rl_pitch = pitch_bytes / sizeof(float2);
+    r->rl_slot = slot_bytes / sizeof(float2);
+    if ((s = dalloc_aligned(ctx, &r->rl_raw, (void**)&r->rl, slot_bytes * r->slots, ctx->tex_align)) != ETCU_OK)
+        return s;
+    CK(ctx, cudaMemsetAsync(r->rl, 0, slot_bytes * r->slots, ctx->stream));
+    r->texs.resize(r->slots);
+    for (uint32_t p = 0; p < r->slots; ++p)
+        if ((s = make_pair_texture(ctx, r->rl + p * r->rl_slot, r->rl_pitch, W, H, &r->texs[p])) != ETCU_OK) return s;
+    if ((s = dalloc(ctx, (void**)&r->d_texs, r->slots * sizeof(cudaTextureObject_t))) != ETCU_OK) return s;
+    CK(ctx, cudaMemcpyAsync(r->d_texs, r->texs.data(), r->slots * sizeof(cudaTextureObject_t), cudaMemcpyHostToDevice,
+                            ctx->stream));
+    if ((s = dalloc(ctx, (void**)&r->d_resid, sizeof(double))) != ETCU_OK) return s;
+    CK(ctx, cudaMemsetAsync(r->d_resid, 0, sizeof(double), ctx->stream));
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    if (params->use_graph) {
+        // The launch sequence of one iteration never changes: capture it once.
+        cudaStream_t cs = ctx->stream;
+        CK(ctx, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        uint32_t n = 0;
+        etcu_status is = issue_iteration(r.get(), cs, &n);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(cs, &g);
+        if (is != ETCU_OK) {
+            if (g) cudaGraphDestroy(g);
+            return is;
+        }
+        CK(ctx, e);
+        r->graph = g;
+        CK(ctx, cudaGraphInstantiate(&r->exec, g, 0));
+        r->launches = n;
+    } else {
+        r->launches = (uint32_t)(2 * S * r->nblocks);
+    }
+    *out = r.release();
+    return ETCU_OK;
+}
+
+}  // namespace
+
+extern "C" etcu_status etcu_recon_create(etcu_volume* vol, const etcu_view* views, uint32_t n_views,
+                                         const float* host_projections, const etcu_recon_params* params,
+                                         etcu_recon** out) {
+    return recon_build(vol, views, n_views, host_projections, nullptr, params, out);
+}
+
+extern "C" etcu_status etcu_recon_create_device(etcu_volume* vol, const etcu_view* views, uint32_t n_views,
+                                                const float* d_projections, const etcu_recon_params* params,
+                                                etcu_recon** out) {
+    if (!d_projections) return fail(vol ? vol->ctx : nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL projections");
+    return recon_build(vol, views, n_views, nullptr, d_projections, params, out);
+}
+
+extern "C" etcu_status etcu_recon_destroy(etcu_recon* rec) {
+    if (!rec) return ETCU_OK;
+    recon_free(rec);
+    delete rec;
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_recon_run(etcu_recon* r, uint32_t iterations) {
+    if (!r) return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL reconstruction");
+    etcu_context* ctx = r->ctx;
+    for (uint32_t it = 0; it < iterations; ++it) {
+        if (r->exec) {
+            CK(ctx, cudaGraphLaunch(r->exec, ctx->stream));
+        } else {
+            etcu_status s = issue_iteration(r, ctx->stream, nullptr);
+            if (s != ETCU_OK) return s;
+        }
+    }
+    CKL(ctx);
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_recon_last_residual_sq(etcu_recon* r, double* out) {
+    if (!r || !out) return fail(r ? r->ctx : nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    etcu_context* ctx = r->ctx;
+    CK(ctx, cudaMemcpyAsync(out, r->d_resid, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_recon_data_residual_sq(etcu_recon* r, double* out) {
+    if (!r || !out) return fail(r ? r->ctx : nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    etcu_context* ctx = r->ctx;
+    const uint32_t M = (uint32_t)r->order.size();
+    CK(ctx, cudaMemsetAsync(r->d_resid, 0, sizeof(double), ctx->stream));
+    for (uint32_t first = 0; first < M; first += r->slots)
+        issue_forward(r, first, std::min(r->slots, M - first), ctx->stream);
+    CKL(ctx);
+    CK(ctx, cudaMemcpyAsync(out, r->d_resid, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_recon_view_order(const etcu_recon* r, uint32_t* out, uint32_t capacity, uint32_t* count) {
+    if (!r || !count) return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    *count = (uint32_t)r->order.size();
+    if (out)
+        for (uint32_t i = 0; i < std::min(capacity, *count); ++i) out[i] = r->order[i];
+    return ETCU_OK;
+}
+
+extern "C" uint32_t etcu_recon_launches_per_iteration(const etcu_recon* r) { return r ? r->launches : 0; }
+
+extern "C" etcu_status etcu_recon_profile_iteration(etcu_recon* r, float* fp_ms, float* bp_ms, uint32_t* fp_n,
+                                                    uint32_t* bp_n) {
+    if (!r || !fp_ms || !bp_ms || !fp_n || !bp_n) return fail(r ? r->ctx : nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    etcu_context* ctx = r->ctx;
+    cudaStream_t st = ctx->stream;
+    const uint32_t M = (uint32_t)r->order.size();
+    std::vector<cudaEvent_t> ev(4 * r->nblocks);
+    for (auto& e : ev) CK(ctx, cudaEventCreate(&e));
+    CK(ctx, cudaMemsetAsync(r->d_resid, 0, sizeof(double), st));
+    uint32_t nf = 0, nb = 0;
+    for (uint32_t b = 0; b < r->nblocks; ++b) {
+        const uint32_t first = b * r->block;
+        const uint32_t bs = (b < r->nblocks - 1) ? r->block : M - first;
+        cudaEventRecord(ev[4 * b + 0], st);
+        nf += issue_forward(r, first, bs, st);
+        cudaEventRecord(ev[4 * b + 1], st);
+        cudaEventRecord(ev[4 * b + 2], st);
+        nb += issue_backward(r, first, bs, st);
+        cudaEventRecord(ev[4 * b + 3], st);
+    }
+    CKL(ctx);
+    CK(ctx, cudaStreamSynchronize(st));
+    float tf = 0.f, tb = 0.f;
+    for (uint32_t b = 0; b < r->nblocks; ++b) {
+        float a = 0.f, c = 0.f;
+        cudaEventElapsedTime(&a, ev[4 * b + 0], ev[4 * b + 1]);
+        cudaEventElapsedTime(&c, ev[4 * b + 2], ev[4 * b + 3]);
+        tf += a;
+        tb += c;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    *fp_ms = tf;
+    *bp_ms = tb;
+    *fp_n = nf;
+    *bp_n = nb;
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_reconstruct(etcu_context* ctx, const etcu_volume_desc* desc, etcu_voxel_type type,
+                                        const etcu_view* views, uint32_t n_views, const float* host_projections,
+                                        const etcu_recon_params* params, uint32_t iterations,
+                                        float* host_volume_inout) {
+    if (!ctx || !host_volume_inout) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    etcu_volume* vol = nullptr;
+    etcu_status s = etcu_volume_create(ctx, desc, type, 0.f, &vol);
+    if (s != ETCU_OK) return s;
+    etcu_recon* rec = nullptr;
+    if ((s = etcu_volume_upload(vol, host_volume_inout)) == ETCU_OK &&
+        (s = etcu_recon_create(vol, views, n_views, host_projections, params, &rec)) == ETCU_OK &&
+        (s = etcu_recon_run(rec, iterations)) == ETCU_OK) {
+        s = etcu_volume_download(vol, host_volume_inout);
+    }
+    etcu_recon_destroy(rec);
+    etcu_volume_destroy(vol);
+    return s;
+}

@@ -1,0 +1,542 @@
+// Device kernels of the B200 block-iterative reconstruction path (sm_100a).
+//
+// Reference semantics (paths relative to ettention/libReconstruction):
+//   forward projection  ocl_src/ParallelBeamsForwardProjection.cl:12-57,
+//                       ocl_src/PerspectiveBeamsForwardProjection.cl:13-52,
+//                       ocl_src/DDARaytracer.hl:20-110, ocl_src/RayUtils.hl:7-35
+//   back projection     ocl_src/ParallelBeamsBackProjection.cl:9-52,
+//                       ocl_src/PerspectiveBeamsBackProjection.cl:10-71
+//   residual / LOC      ocl_src/Compare.cl:1-9, ocl_src/VirtualProjection.cl:3-10
+//   ray length          ocl_src/ComputeRayLength.cl:21-34
+//
+// Layout in HBM: volume x-fastest [z][y][x] (ocl_src/Math.hl:8-11), projection
+// images row-major [v][u]; the per-block residual / ray-length pairs are one
+// interleaved float2 image per block slot with a texture-aligned row pitch, so a
+// single bilinear texture fetch returns both values.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <cfloat>
+#include <stdint.h>
+
+namespace etcu {
+
+constexpr float kEps = 1e-4f;           // ocl_src/Math.hl:4
+constexpr int kMaxDdaIterations = 2048; // DDARaytracer.hl:85-107: counter < 4096, bumped twice per step
+constexpr int kMaxInlineSamples = 64;
+
+struct ViewConst {
+    float4 ray;       // normalised ray direction (parallel) / central direction (perspective)
+    float4 inv;       // invertVectorSafely(ray)
+    float4 source;
+    float4 detector;
+    float4 hpitch;
+    float4 vpitch;
+    float mat[16];    // column-major projection matrix
+    float loc_length; // long-object constant length
+    int perspective;
+    int fast2d;       // parallel view with ray.y == 0 and finite step differences
+    int pad;
+};
+
+struct SlabConst {
+    int rx, ry, rz;   // sub-volume resolution
+    int z0;           // first z plane of the sub-volume in the full volume
+    float4 bmin, bmax;  // sub-volume bounding box
+    float4 cmin, cmax;  // complete bounding box
+    float4 vs, ivs;     // voxel size and its reciprocal
+};
+
+// ---------------------------------------------------------------- helpers
+// Setup arithmetic uses explicit round-to-nearest intrinsics so that no
+// multiply-add is contracted; the result then matches the operation order of
+// the OpenCL source step by step.
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ float clsign(float x) { return x > 0.f ? 1.f : (x < 0.f ? -1.f : x); }
+__device__ __forceinline__ float clclamp(float x, float lo, float hi) { return fminf(fmaxf(x, lo), hi); }
+
+template <typename T> __device__ __forceinline__ float load_voxel(const T* p);
+template <> __device__ __forceinline__ float load_voxel<float>(const float* p) { return __ldg(p); }
+template <> __device__ __forceinline__ float load_voxel<__half>(const __half* p) { return __half2float(__ldg(p)); }
+template <> __device__ __forceinline__ float load_voxel<__nv_bfloat16>(const __nv_bfloat16* p) {
+    return __bfloat162float(__ldg(p));
+}
+
+template <typename T> __device__ __forceinline__ T store_cast(float v);
+template <> __device__ __forceinline__ float store_cast<float>(float v) { return v; }
+template <> __device__ __forceinline__ __half store_cast<__half>(float v) { return __float2half_rn(v); }
+template <> __device__ __forceinline__ __nv_bfloat16 store_cast<__nv_bfloat16>(float v) {
+    return __float2bfloat16_rn(v);
+}
+
+__device__ __forceinline__ float mask_weight(const uint8_t* m) { return fdiv((float)__ldg(m), 255.0f); }
+
+// RayUtils.hl:7-16
+__device__ __forceinline__ void slab_test(float3 bmin, float3 bmax, float3 s, float3 inv, float& tin, float& tout) {
+    float t0x = fmul(fsub(bmin.x, s.x), inv.x), t1x = fmul(fsub(bmax.x, s.x), inv.x);
+    float t0y = fmul(fsub(bmin.y, s.y), inv.y), t1y = fmul(fsub(bmax.y, s.y), inv.y);
+    float t0z = fmul(fsub(bmin.z, s.z), inv.z), t1z = fmul(fsub(bmax.z, s.z), inv.z);
+    tin = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fminf(t0z, t1z));
+    tout = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fmaxf(t0z, t1z));
+}
+
+__device__ __forceinline__ float3 inv_safe(float3 r) {
+    float3 o = make_float3(fdiv(1.f, r.x), fdiv(1.f, r.y), fdiv(1.f, r.z));
+    if (r.x == 0.f) o.x = -FLT_MAX;
+    if (r.y == 0.f) o.y = -FLT_MAX;
+    if (r.z == 0.f) o.z = -FLT_MAX;
+    return o;
+}
+
+struct DdaStart {
+    int ix, iy, iz;
+    float3 res;  // remaining distance to the next border per axis
+    float3 sd;   // step difference per axis
+    int sx, sy, sz;
+};
+
+// DDARaytracer.hl:64-83: entry point, initial voxel, step differences and
+// initial remaining distances.  Returns false when the ray misses the box.
+__device__ __forceinline__ bool dda_setup(float3 src, float3 ray, float3 inv, const SlabConst& g, DdaStart& st) {
+    float3 bmin = make_float3(g.bmin.x, g.bmin.y, g.bmin.z), bmax = make_float3(g.bmax.x, g.bmax.y, g.bmax.z);
+    float tin, tout;
+    slab_test(bmin, bmax, src, inv, tin, tout);
+    if (!(fsub(tout, tin) > kEps)) return false;
+    float px = clclamp(fadd(src.x, fmul(tin, ray.x)), bmin.x, bmax.x);
+    float py = clclamp(fadd(src.y, fmul(tin, ray.y)), bmin.y, bmax.y);
+    float pz = clclamp(fadd(src.z, fmul(tin, ray.z)), bmin.z, bmax.z);
+    int ix = (int)fmul(fsub(px, bmin.x), g.ivs.x);
+    int iy = (int)fmul(fsub(py, bmin.y), g.ivs.y);
+    int iz = (int)fmul(fsub(pz, bmin.z), g.ivs.z);
+    st.ix = min(max(ix, 0), g.rx - 1);
+    st.iy = min(max(iy, 0), g.ry - 1);
+    st.iz = min(max(iz, 0), g.rz - 1);
+    float sgx = clsign(ray.x), sgy = clsign(ray.y), sgz = clsign(ray.z);
+    st.sd = make_float3(fmul(fmul(g.vs.x, inv.x), sgx), fmul(fmul(g.vs.y, inv.y), sgy),
+                        fmul(fmul(g.vs.z, inv.z), sgz));
+    st.sx = (int)sgx; st.sy = (int)sgy; st.sz = (int)sgz;
+    float rx = fmul(floorf(fmul(px, g.ivs.x)), g.vs.x);
+    float ry = fmul(floorf(fmul(py, g.ivs.y)), g.vs.y);
+    float rz = fmul(floorf(fmul(pz, g.ivs.z)), g.vs.z);
+    rx = (ray.x > 0.f) ? fmul(fsub(fadd(rx, g.vs.x), px), inv.x) : fmul(fsub(rx, px), inv.x);
+    ry = (ray.y > 0.f) ? fmul(fsub(fadd(ry, g.vs.y), py), inv.y) : fmul(fsub(ry, py), inv.y);
+    rz = (ray.z > 0.f) ? fmul(fsub(fadd(rz, g.vs.z), pz), inv.z) : fmul(fsub(rz, pz), inv.z);
+    if (ray.x == 0.f) rx = FLT_MAX;
+    if (ray.y == 0.f) ry = FLT_MAX;
+    if (ray.z == 0.f) rz = FLT_MAX;
+    if (rx == 0.f) rx = st.sd.x;
+    if (ry == 0.f) ry = st.sd.y;
+    if (rz == 0.f) rz = st.sd.z;
+    st.res = make_float3(rx, ry, rz);
+    return true;
+}
+
+// General 3-D Amanatides-Woo walk (DDARaytracer.hl:84-108).  kLiteral keeps the
+// reference's arithmetic step update step*sd + (1-step)*(res-dt) so that
+// non-finite step differences propagate as in the reference; otherwise the
+// update is an exact select.
+template <typename VoxT, bool kMask, bool kLiteral>
+__device__ __forceinline__ void dda_walk3(const DdaStart& st, const SlabConst& g, const VoxT* __restrict__ vol,
+                                         const uint8_t* __restrict__ mask, float& acc, float& accl) {
+    int ix = st.ix, iy = st.iy, iz = st.iz;
+    float rx = st.res.x, ry = st.res.y, rz = st.res.z;
+    const size_t plane = (size_t)g.rx * (size_t)g.ry;
+    for (int it = 0; it < kMaxDdaIterations; ++it) {
+        if ((unsigned)ix >= (unsigned)g.rx || (unsigned)iy >= (unsigned)g.ry || (unsigned)iz >= (unsigned)g.rz) break;
+        float dt = fminf(fminf(rx, ry), rz);
+        size_t idx = (size_t)iz * plane + (size_t)iy * (size_t)g.rx + (size_t)ix;
+        acc = fmaf(dt, load_voxel(vol + idx), acc);
+        if (kMask) accl = fmaf(dt, mask_weight(mask + idx), accl);
+        else accl += dt;
+        bool bx = rx <= ry && rx <= rz;
+        bool by = ry < rx && ry <= rz;
+        bool bz = rz < rx && rz < ry;
+        if (kLiteral) {
+            float fx = bx ? 1.f : 0.f, fy = by ? 1.f : 0.f, fz = bz ? 1.f : 0.f;
+            rx = fadd(fmul(fx, st.sd.x), fmul(fsub(1.f, fx), fsub(rx, dt)));
+            ry = fadd(fmul(fy, st.sd.y), fmul(fsub(1.f, fy), fsub(ry, dt)));
+            rz = fadd(fmul(fz, st.sd.z), fmul(fsub(1.f, fz), fsub(rz, dt)));
+        } else {
+            rx = bx ? st.sd.x : fsub(rx, dt);
+            ry = by ? st.sd.y : fsub(ry, dt);
+            rz = bz ? st.sd.z : fsub(rz, dt);
+        }
+        ix += bx ? st.sx : 0;
+        iy += by ? st.sy : 0;
+        iz += bz ? st.sz : 0;
+    }
+}
+
+// Parallel-beam walk for views tilted about y: ray.y == 0, so the y
+// component stays FLT_MAX and never wins; the walk stays in one xz plane of
+// the volume.  Valid (and bit-identical to dda_walk3) when the x and z step
+// differences are finite.
+template <typename VoxT, bool kMask>
+__device__ __forceinline__ void dda_walk_xz(const DdaStart& st, const SlabConst& g, const VoxT* __restrict__ vol,
+                                           const uint8_t* __restrict__ mask, float& acc, float& accl) {
+    int ix = st.ix, iz = st.iz;
+    float rx = st.res.x, rz = st.res.z;
+    const int plane = g.rx * g.ry;
+    const VoxT* row = vol + (size_t)st.iy * (size_t)g.rx;
+    const uint8_t* mrow = kMask ? mask + (size_t)st.iy * (size_t)g.rx : nullptr;
+    const float sdx = st.sd.x, sdz = st.sd.z;
+    const int six = st.sx, siz = st.sz;
+    for (int it = 0; it < kMaxDdaIterations; ++it) {
+        if ((unsigned)ix >= (unsigned)g.rx || (unsigned)iz >= (unsigned)g.rz) break;
+        float dt = fminf(rx, rz);
+        size_t off = (size_t)iz * (size_t)plane + (size_t)ix;
+        acc = fmaf(dt, load_voxel(row + off), acc);
+        if (kMask) accl = fmaf(dt, mask_weight(mrow + off), accl);
+        else accl += dt;
+        bool bx = rx <= rz;
+        rx = bx ? sdx : fsub(rx, dt);
+        rz = bx ? fsub(rz, dt) : sdz;
+        ix += bx ? six : 0;
+        iz += bx ? 0 : siz;
+    }
+}
+
+template <typename VoxT, bool kMask>
+__device__ __forceinline__ void trace_ray(float3 src, float3 ray, float3 inv, bool fast2d, const SlabConst& g,
+                                          const VoxT* vol, const uint8_t* mask, float& v, float& l) {
+    v = 0.f;
+    l = 0.f;
+    DdaStart st;
+    if (!dda_setup(src, ray, inv, g, st)) return;
+    if (fast2d) {
+        dda_walk_xz<VoxT, kMask>(st, g, vol, mask, v, l);
+    } else if (isfinite(st.sd.x) && isfinite(st.sd.y) && isfinite(st.sd.z)) {
+        dda_walk3<VoxT, kMask, false>(st, g, vol, mask, v, l);
+    } else {
+        dda_walk3<VoxT, kMask, true>(st, g, vol, mask, v, l);
+    }
+}
+
+// ---------------------------------------------------------------- forward projection
+enum FpMode : int {
+    kFpSeparateAccumulate = 0,  // d_virtual += ..., d_traversal += ...   (ForwardProjectionKernel semantics)
+    kFpPairAccumulate = 1,      // rl = (first ? 0 : rl) + (proj, len)    (non-final slab of a block)
+    kFpPairResidual = 2         // rl = (b - ((first ? 0 : rl.x) + proj) [LOC], len)  (final slab)
+};
+
+struct FpArgs {
+    const void* vol;            // sub-volume base (element type VoxT)
+    const uint8_t* mask;        // sub-volume mask base or nullptr
+    SlabConst slab;
+    const ViewConst* views;     // device view table (nullptr: use inline_view)
+    ViewConst inline_view;
+    const uint32_t* order;      // iteration order (view ids), may be nullptr
+    uint32_t first;             // order position of grid.z == 0
+    int W, H, samples;
+    int mode, overwrite, loc;
+    float* out_v;               // mode 0
+    float* out_l;
+    float2* rl;                 // modes 1/2: slot p at rl + p * rl_slot, row pitch rl_pitch (float2 units)
+    size_t rl_pitch, rl_slot;
+    const float* real;          // mode 2: measured projections, view id * W * H
+    double* resid_sq;           // mode 2: optional sum of residual^2 (FP64)
+};
+
+template <typename VoxT, bool kMask, bool kPerspective>
+__global__ void __launch_bounds__(128) forward_project_kernel(const __grid_constant__ FpArgs a) {
+    int gx, gy;
+    if (kPerspective) {
+        gx = blockIdx.x * 16 + (threadIdx.x & 15);
+        gy = blockIdx.y * 8 + (threadIdx.x >> 4);
+    } else {
+        gx = blockIdx.x * blockDim.x + threadIdx.x;
+        gy = blockIdx.y;
+    }
+    const int p = blockIdx.z;
+    const uint32_t vid = a.order ? a.order[a.first + p] : (a.first + p);
+    const ViewConst& vc = a.views ? a.views[vid] : a.inline_view;
+    const bool active = gx < a.W && gy < a.H;
+    const VoxT* vol = (const VoxT*)a.vol;
+    const int S = a.samples;
+    float accv = 0.f, accl = 0.f, total;
+    if (active) {
+        if (!kPerspective) {
+            // ParallelBeamsForwardProjection.cl:12-24 sub-ray origins, :37-57 accumulation
+            const float3 ray = make_float3(vc.ray.x, vc.ray.y, vc.ray.z);
+            const float3 inv = make_float3(vc.inv.x, vc.inv.y, vc.inv.z);
+            const float sdist = fdiv(1.f, (float)S), off = fdiv(sdist, 2.f);
+            total = (float)(S * S);
+            for (int sx = 0; sx < S; ++sx) {
+                for (int sy = 0; sy < S; ++sy) {
+                    float fx = fadd(fadd((float)gx, off), fmul(sdist, (float)sx));
+                    float fy = fadd(fadd((float)gy, off), fmul(sdist, (float)sy));
+                    float3 s = make_float3(fadd(fadd(vc.source.x, fmul(vc.hpitch.x, fx)), fmul(vc.vpitch.x, fy)),
+                                           fadd(fadd(vc.source.y, fmul(vc.hpitch.y, fx)), fmul(vc.vpitch.y, fy)),
+                                           fadd(fadd(vc.source.z, fmul(vc.hpitch.z, fx)), fmul(vc.vpitch.z, fy)));
+                    float v, l;
+                    trace_ray<VoxT, kMask>(s, ray, inv, vc.fast2d != 0, a.slab, vol, a.mask, v, l);
+                    accv += v;
+                    accl += l;
+                }
+            }
+        } else {
+            // PerspectiveBeamsForwardProjection.cl:13-52
+            const unsigned tot = (unsigned)(S * S);
+            total = (float)tot;
+            const float3 src = make_float3(vc.source.x, vc.source.y, vc.source.z);
+            for (unsigned k = 0; k < tot; ++k) {
+                float bx = fadd(fadd(vc.detector.x, fmul((float)gx, vc.hpitch.x)), fmul((float)gy, vc.vpitch.x));
+                float by = fadd(fadd(vc.detector.y, fmul((float)gx, vc.hpitch.y)), fmul((float)gy, vc.vpitch.y));
+                float bz = fadd(fadd(vc.detector.z, fmul((float)gx, vc.hpitch.z)), fmul((float)gy, vc.vpitch.z));
+                unsigned dh = k % (unsigned)S, dv = k / (unsigned)S;
+                float fh = fdiv(fadd((float)dh, 0.5f), (float)S), fv = fdiv(fadd((float)dv, 0.5f), (float)S);
+                float px = fadd(fadd(bx, fmul(fh, vc.hpitch.x)), fmul(fv, vc.vpitch.x));
+                float py = fadd(fadd(by, fmul(fh, vc.hpitch.y)), fmul(fv, vc.vpitch.y));
+                float pz = fadd(fadd(bz, fmul(fh, vc.hpitch.z)), fmul(fv, vc.vpitch.z));
+                float dx = fsub(px, src.x), dy = fsub(py, src.y), dz = fsub(pz, src.z);
+                float n = __fsqrt_rn(fadd(fadd(fmul(dx, dx), fmul(dy, dy)), fmul(dz, dz)));
+                float3 d = make_float3(fdiv(dx, n), fdiv(dy, n), fdiv(dz, n));
+                float v, l;
+                trace_ray<VoxT, kMask>(src, d, inv_safe(d), false, a.slab, vol, a.mask, v, l);
+                accv += v;
+                accl += l;
+            }
+        }
+    }
+    double r2 = 0.0;
+    if (active) {
+        float pv = fdiv(accv, total), pl = fdiv(accl, total);
+        const size_t i = (size_t)gy * (size_t)a.W + (size_t)gx;
+        if (a.mode == kFpSeparateAccumulate) {
+            a.out_v[i] = fadd(a.out_v[i], pv);
+            a.out_l[i] = fadd(a.out_l[i], pl);
+        } else {
+            float2* slot = a.rl + (size_t)p * a.rl_slot + (size_t)gy * a.rl_pitch + (size_t)gx;
+            float2 prev = a.overwrite ? make_float2(0.f, 0.f) : *slot;
+            float vv = fadd(prev.x, pv), ll = fadd(prev.y, pl);
+            if (a.mode == kFpPairAccumulate) {
+                *slot = make_float2(vv, ll);
+            } else {
+                if (a.loc) {  // VirtualProjection.cl:8-9
+                    vv = ll > kEps ? fdiv(fmul(vv, vc.loc_length), ll) : 0.f;
+                    ll = vc.loc_length;
+                }
+                float r = fsub(a.real[(size_t)vid * (size_t)a.W * (size_t)a.H + i], vv);  // Compare.cl:8
+                *slot = make_float2(r, ll);
+                r2 = (double)r * (double)r;
+            }
+        }
+    }
+    if (a.mode == kFpPairResidual && a.resid_sq) {
+        // FP64 block reduction of the squared residuals, one atomic per block.
+        for (int o = 16; o > 0; o >>= 1) r2 += __shfl_down_sync(0xffffffffu, r2, o);
+        __shared__ double part[4];
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        if (lane == 0) part[warp] = r2;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double s = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += part[w];
+            atomicAdd(a.resid_sq, s);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- back projection
+struct BpArgs {
+    void* vol;                     // FP32 master / FP32 volume / half volume (sub-volume base)
+    void* shadow;                  // 16-bit shadow written after the block (or nullptr)
+    const uint8_t* mask;
+    SlabConst slab;
+    const ViewConst* views;
+    ViewConst inline_view;
+    const uint32_t* order;
+    uint32_t first;
+    int nviews;                    // views of the block, applied in order
+    const cudaTextureObject_t* texs;  // per slot, float2 (residual, length), linear filter, border 0
+    cudaTextureObject_t inline_tex;
+    const float2* rl;              // exact sampling source
+    size_t rl_pitch, rl_slot;
+    int W, H;
+    float lambda;                  // lambda / blockSize (BackProjectionKernel.cpp:94)
+    const float4* samples;         // parallel: per view id, nsamples (x, y, z, chord); nullptr -> inline
+    float4 inline_samples[kMaxInlineSamples];
+    int nsamples;
+    int persp_n;                   // perspective samples per dimension
+    int use_min, use_max;
+    float vmin, vmax;
+};
+
+__device__ __forceinline__ float2 sample_exact(const float2* __restrict__ img, size_t pitch, int W, int H, float u,
+                                               float v) {
+    // ImageHandler.hl:20-40 (buffer path): fract(c - 0.5), zero outside, mix in x then y.
+    float xb = floorf(fsub(u, 0.5f)), yb = floorf(fsub(v, 0.5f));
+    float ax = fminf(fsub(fsub(u, 0.5f), xb), 0x1.fffffep-1f), ay = fminf(fsub(fsub(v, 0.5f), yb), 0x1.fffffep-1f);
+    int x0 = (int)xb, y0 = (int)yb;
+    float2 r0 = make_float2(0.f, 0.f), r1 = make_float2(0.f, 0.f);
+    auto texel = [&](int x, int y) -> float2 {
+        return (x >= 0 && x < W) ? __ldg(img + (size_t)y * pitch + (size_t)x) : make_float2(0.f, 0.f);
+    };
+    if (y0 >= 0 && y0 < H) {
+        float2 p = texel(x0, y0), q = texel(x0 + 1, y0);
+        r0 = make_float2(fadd(p.x, fmul(fsub(q.x, p.x), ax)), fadd(p.y, fmul(fsub(q.y, p.y), ax)));
+    }
+    if (y0 + 1 >= 0 && y0 + 1 < H) {
+        float2 p = texel(x0, y0 + 1), q = texel(x0 + 1, y0 + 1);
+        r1 = make_float2(fadd(p.x, fmul(fsub(q.x, p.x), ax)), fadd(p.y, fmul(fsub(q.y, p.y), ax)));
+    }
+    return make_float2(fadd(r0.x, fmul(fsub(r1.x, r0.x), ay)), fadd(r0.y, fmul(fsub(r1.y, r0.y), ay)));
+}
+
+__device__ __forceinline__ void project_point(const float* m, float px, float py, float pz, float& u, float& v) {
+    // Matrix4x4.hl:38-58 MultiplyG + TransformCoordG
+    float x = fadd(fadd(fadd(fmul(m[0], px), fmul(m[4], py)), fmul(m[8], pz)), m[12]);
+    float y = fadd(fadd(fadd(fmul(m[1], px), fmul(m[5], py)), fmul(m[9], pz)), m[13]);
+    float w = fadd(fadd(fadd(fmul(m[3], px), fmul(m[7], py)), fmul(m[11], pz)), m[15]);
+    u = fdiv(x, w);
+    v = fdiv(y, w);
+}
+
+// PerspectiveBeamsBackProjection.cl:10-17 getRayLengthInVoxel
+__device__ __forceinline__ float chord_in_voxel(float3 o, float3 dir, float3 c, float3 vs) {
+    float3 bmin = make_float3(fsub(c.x, fmul(0.5f, vs.x)), fsub(c.y, fmul(0.5f, vs.y)), fsub(c.z, fmul(0.5f, vs.z)));
+    float3 bmax = make_float3(fadd(c.x, fmul(0.5f, vs.x)), fadd(c.y, fmul(0.5f, vs.y)), fadd(c.z, fmul(0.5f, vs.z)));
+    float n = __fsqrt_rn(fadd(fadd(fmul(dir.x, dir.x), fmul(dir.y, dir.y)), fmul(dir.z, dir.z)));
+    float3 inv = make_float3(fdiv(1.f, fdiv(dir.x, n)), fdiv(1.f, fdiv(dir.y, n)), fdiv(1.f, fdiv(dir.z, n)));
+    float tin, tout;
+    slab_test(bmin, bmax, o, inv, tin, tout);
+    return fmaxf(0.f, fsub(tout, tin));
+}
+
+// Storage of the updated volume: kStore = 0 FP32 volume, 1 half volume
+// re-rounded after every view (reference half mode), 2 FP32 master + half
+// shadow, 3 FP32 master + bf16 shadow.
+template <bool kPerspective, bool kMask, int kStore, bool kExact>
+__global__ void __launch_bounds__(256) back_project_kernel(const __grid_constant__ BpArgs a) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z = blockIdx.z;
+    const SlabConst& g = a.slab;
+    if (x >= g.rx || y >= g.ry || z >= g.rz) return;
+    const size_t idx = ((size_t)z * (size_t)g.ry + (size_t)y) * (size_t)g.rx + (size_t)x;
+    // VolumeGeometry.hl:17-20 GetVoxelCenter
+    const float cx = fadd(g.bmin.x, fmul(fadd((float)x, 0.5f), g.vs.x));
+    const float cy = fadd(g.bmin.y, fmul(fadd((float)y, 0.5f), g.vs.y));
+    const float cz = fadd(g.bmin.z, fmul(fadd((float)z, 0.5f), g.vs.z));
+    float val;
+    if (kStore == 1) val = __half2float(((const __half*)a.vol)[idx]);
+    else val = ((const float*)a.vol)[idx];
+    const float mw = kMask ? mask_weight(a.mask + idx) : 1.f;
+
+    for (int p = 0; p < a.nviews; ++p) {
+        const uint32_t vid = a.order ? a.order[a.first + p] : (a.first + p);
+        const ViewConst& vc = a.views ? a.views[vid] : a.inline_view;
+        const cudaTextureObject_t tex = a.texs ? a.texs[p] : a.inline_tex;
+        const float2* img = a.rl + (size_t)p * a.rl_slot;
+        if (!kPerspective) {
+            // ParallelBeamsBackProjection.cl:26-51
+            const float4* smp = a.samples ? a.samples + (size_t)vid * (size_t)a.nsamples : a.inline_samples;
+            float pv = 0.f;
+            unsigned used = 0;
+            for (int k = 0; k < a.nsamples; ++k) {
+                const float4 s = smp[k];
+                float u, v;
+                project_point(vc.mat, fadd(cx, s.x), fadd(cy, s.y), fadd(cz, s.z), u, v);
+                float2 rl = kExact ? sample_exact(img, a.rl_pitch, a.W, a.H, u, v) : tex2D<float2>(tex, u, v);
+                float w = fdiv(s.w, rl.y);
+                float contrib = fmul(fmul(rl.x, a.lambda), w);
+                if (rl.y > kEps) {
+                    pv = fadd(pv, contrib);
+                    used += 1;
+                }
+            }
+            if (used != 0) val = fadd(val, fdiv(fmul(mw, pv), (float)used));
+        } else {
+            // PerspectiveBeamsBackProjection.cl:42-69
+            const int n = a.persp_n;
+            const unsigned count = (unsigned)(n * n * n);
+            float value = 0.f;
+            const float3 c = make_float3(cx, cy, cz);
+            const float3 vs = make_float3(g.vs.x, g.vs.y, g.vs.z);
+            const float bxv = fsub(cx, fmul(0.5f, g.vs.x)), byv = fsub(cy, fmul(0.5f, g.vs.y)),
+                        bzv = fsub(cz, fmul(0.5f, g.vs.z));
+            for (unsigned k = 0; k < count; ++k) {
+                unsigned dx = k % (unsigned)n, dy = (k / (unsigned)n) % (unsigned)n, dz = k / (unsigned)(n * n);
+                float px = fadd(bxv, fdiv(fmul(g.vs.x, fadd((float)dx, 0.5f)), (float)n));
+                float py = fadd(byv, fdiv(fmul(g.vs.y, fadd((float)dy, 0.5f)), (float)n));
+                float pz = fadd(bzv, fdiv(fmul(g.vs.z, fadd((float)dz, 0.5f)), (float)n));
+                float u, v;
+                project_point(vc.mat, px, py, pz, u, v);
+                float2 rl = kExact ? sample_exact(img, a.rl_pitch, a.W, a.H, u, v) : tex2D<float2>(tex, u, v);
+                if (rl.y >= kEps) {
+                    float3 dir = make_float3(fsub(px, vc.source.x), fsub(py, vc.source.y), fsub(pz, vc.source.z));
+                    float l = chord_in_voxel(make_float3(px, py, pz), dir, c, vs);
+                    value = fadd(value, fdiv(fmul(rl.x, l), rl.y));
+                }
+            }
+            val = fadd(val, fdiv(fmul(fmul(a.lambda, value), mw), (float)count));
+            if (a.use_min) val = fmaxf(a.vmin, val);
+            if (a.use_max) val = fminf(a.vmax, val);
+        }
+        if (kStore == 1) val = __half2float(__float2half_rn(val));  // vstore_half after every view
+    }
+    if (kStore == 1) ((__half*)a.vol)[idx] = __float2half_rn(val);
+    else ((float*)a.vol)[idx] = val;
+    if (kStore == 2) ((__half*)a.shadow)[idx] = __float2half_rn(val);
+    if (kStore == 3) ((__nv_bfloat16*)a.shadow)[idx] = __float2bfloat16_rn(val);
+}
+
+// ---------------------------------------------------------------- small kernels
+__global__ void compare_kernel(const float* real, const float* virt, float* res, size_t n) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) res[i] = fsub(real[i], virt[i]);
+}
+
+__global__ void loc_kernel(float* proj, float* len, float c, size_t n) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        float l = len[i];
+        proj[i] = l > kEps ? fdiv(fmul(proj[i], c), l) : 0.f;
+        len[i] = c;
+    }
+}
+
+__global__ void ray_length_kernel(ViewConst vc, SlabConst g, int W, int H, float* out) {
+    int gx = blockIdx.x * blockDim.x + threadIdx.x, gy = blockIdx.y;
+    if (gx >= W || gy >= H) return;
+    float fx = fadd((float)gx, 0.5f), fy = fadd((float)gy, 0.5f);
+    float3 s = make_float3(fadd(fadd(vc.source.x, fmul(vc.hpitch.x, fx)), fmul(vc.vpitch.x, fy)),
+                           fadd(fadd(vc.source.y, fmul(vc.hpitch.y, fx)), fmul(vc.vpitch.y, fy)),
+                           fadd(fadd(vc.source.z, fmul(vc.hpitch.z, fx)), fmul(vc.vpitch.z, fy)));
+    float tin, tout;
+    slab_test(make_float3(g.cmin.x, g.cmin.y, g.cmin.z), make_float3(g.cmax.x, g.cmax.y, g.cmax.z), s,
+              make_float3(vc.inv.x, vc.inv.y, vc.inv.z), tin, tout);
+    out[(size_t)gy * W + gx] = fmaxf(fsub(tout, tin), 0.f);
+}
+
+// Interleave separate residual / ray-length images into a pitched float2 image.
+__global__ void pack_pair_kernel(const float* r, const float* l, float2* out, size_t pitch, int W, int H) {
+    int gx = blockIdx.x * blockDim.x + threadIdx.x, gy = blockIdx.y;
+    if (gx >= W || gy >= H) return;
+    size_t i = (size_t)gy * W + gx;
+    out[(size_t)gy * pitch + gx] = make_float2(r[i], l[i]);
+}
+
+template <typename T>
+__global__ void convert_from_float_kernel(const float* in, T* out, size_t n) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = store_cast<T>(in[i]);
+}
+
+template <typename T>
+__global__ void convert_to_float_kernel(const T* in, float* out, size_t n) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = load_voxel(in + i);
+}
+
+__global__ void fill_kernel(float* out, float v, size_t n) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = v;
+}
+
+}  // namespace etcu

@@ -1,0 +1,531 @@
+"""Python face of the CUDA path, mirroring libReconstruction's operator surface.
+
+Names, argument meaning and error behaviour follow the reference
+(LR = ettention/libReconstruction/src):
+
+  ScannerGeometry / rotate          LR/model/geometry/{Parallel,Perspective}ScannerGeometry.cpp,
+                                    LR/model/geometry/SingleAxisTiltRotator.cpp
+  GPUMappedVolume                   LR/model/volume/GPUMappedVolume.cpp (device-resident here)
+  ForwardProjectionOperator         LR/algorithm/projections/forward/ForwardProjectionOperator.cpp
+  BackProjectionOperator            LR/algorithm/projections/back/BackProjectionOperator.cpp
+  BlockIterativeReconstructionOperator
+                                    LR/algorithm/reconstruction/blockiterative/
+                                    BlockIterativeReconstructionOperator.cpp
+  AlgebraicParameterSet.from_config LR/setup/parameterset/*ParameterSet.cpp (same config keys)
+
+Every compute call goes through ``libettention_b200.so``; device images are
+CUDA ``torch.Tensor`` objects (float32, contiguous) used as plain device
+memory.
+"""
+from __future__ import annotations
+
+import ctypes
+import weakref
+from dataclasses import dataclass, field
+from typing import Dict, Iterable, List, Optional, Sequence
+
+import numpy as np
+
+from . import _abi
+from ._abi import EttentionError, View, VolumeDesc, ReconParams, check, lib
+
+
+# ----------------------------------------------------------------------------- geometry
+@dataclass
+class ScannerGeometry:
+    """LR/model/geometry/ScannerGeometry.cpp:39-46 (+ Parallel/Perspective subclass)."""
+    source: Sequence[float]
+    detector: Sequence[float]
+    hpitch: Sequence[float]
+    vpitch: Sequence[float]
+    width: int
+    height: int
+    perspective: bool = False
+
+    def to_view(self) -> View:
+        v = View()
+        for name in ("source", "detector", "hpitch", "vpitch"):
+            arr = getattr(v, name)
+            val = getattr(self, name)
+            for i in range(3):
+                arr[i] = float(val[i])
+        v.width, v.height, v.perspective = int(self.width), int(self.height), int(bool(self.perspective))
+        return v
+
+    @classmethod
+    def from_view(cls, v: View) -> "ScannerGeometry":
+        return cls(list(v.source), list(v.detector), list(v.hpitch), list(v.vpitch), v.width, v.height,
+                   bool(v.perspective))
+
+    def rotated(self, tilt_deg: float, xaxis_tilt_deg: float = 0.0) -> "ScannerGeometry":
+        """SingleAxisTiltRotator::createRotatedScannerGeometry."""
+        out = View()
+        check(lib().etcu_view_rotate(ctypes.byref(self.to_view()), float(tilt_deg), float(xaxis_tilt_deg),
+                                     ctypes.byref(out)))
+        return ScannerGeometry.from_view(out)
+
+    def projection_matrix(self) -> np.ndarray:
+        m = np.zeros(16, np.float32)
+        check(lib().etcu_view_projection_matrix(ctypes.byref(self.to_view()), m.ctypes.data))
+        return m
+
+    def sample_pattern(self, voxel_size: Sequence[float], samples: int) -> np.ndarray:
+        """ParallelBeamsBackProjectionKernel::setSamples + generateSamplingPatternForPerVoxelSampling."""
+        vs = np.asarray(voxel_size, np.float32)
+        out = np.zeros((max(int(samples), 1), 4), np.float32)
+        check(lib().etcu_view_sample_pattern(ctypes.byref(self.to_view()), vs.ctypes.data, int(samples),
+                                             out.ctypes.data))
+        return out
+
+    def traversal_length(self, bbox_min: Sequence[float], bbox_max: Sequence[float]) -> float:
+        lo = np.asarray(bbox_min, np.float32)
+        hi = np.asarray(bbox_max, np.float32)
+        r = ctypes.c_float()
+        check(lib().etcu_view_traversal_length(ctypes.byref(self.to_view()), lo.ctypes.data, hi.ctypes.data,
+                                               ctypes.byref(r)))
+        return float(r.value)
+
+
+def mrc_base_geometry(nx: int, ny: int) -> ScannerGeometry:
+    """LR/io/datasource/MRCStack.cpp:250-261: base parallel geometry of an MRC tilt series."""
+    return ScannerGeometry([-0.5 * nx, -0.5 * ny, float(nx)], [-0.5 * nx, -0.5 * ny, -float(nx)],
+                           [1.0, 0.0, 0.0], [0.0, 1.0, 0.0], nx, ny, False)
+
+
+def tilt_series(base: ScannerGeometry, angles: Iterable[float], xaxis_tilt_deg: float = 0.0) -> List[ScannerGeometry]:
+    return [base.rotated(a, xaxis_tilt_deg) for a in angles]
+
+
+def projection_order(order: int, n: int, skip: Sequence[int] = ()) -> List[int]:
+    """LR/model/projectionset/factory/ProjectionIteratorFactory.cpp:11-22 orderings."""
+    sk = np.asarray(list(skip), np.uint32)
+    out = np.zeros(max(n, 1), np.uint32)
+    cnt = ctypes.c_uint32()
+    check(lib().etcu_projection_order(int(order), int(n), sk.ctypes.data if len(sk) else None, len(sk),
+                                      out.ctypes.data, ctypes.byref(cnt)))
+    return [int(i) for i in out[: cnt.value]]
+
+
+ORDERS = {"identity": _abi.ORDER_IDENTITY, "random": _abi.ORDER_RANDOM, "maxangle": _abi.ORDER_MAXANGLE,
+          "buckets": _abi.ORDER_BUCKETS}
+VOXEL_TYPES = {"float": _abi.VOXEL_FLOAT32, "float32": _abi.VOXEL_FLOAT32, "half": _abi.VOXEL_HALF16,
+               "half_master": _abi.VOXEL_F16_MASTER, "bf16_master": _abi.VOXEL_BF16_MASTER}
+
+
+# ----------------------------------------------------------------------------- context / volume
+class Context:
+    """One device, one stream (replaces CLAbstractionLayer's context and queue)."""
+
+    def __init__(self, device: int = 0):
+        h = ctypes.c_void_p()
+        check(lib().etcu_context_create(int(device), ctypes.byref(h)))
+        self.handle = h
+        self.device = device
+        self._children = weakref.WeakSet()
+
+    def _adopt(self, obj) -> None:
+        self._children.add(obj)
+
+    def close(self) -> None:
+        """Destroys the context after every volume / reconstruction created on it."""
+        if self.handle:
+            for child in [c for c in self._children if not isinstance(c, GPUMappedVolume)]:
+                child.close()
+            for child in list(self._children):
+                child.close()
+            lib().etcu_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def synchronize(self) -> None:
+        check(lib().etcu_synchronize(self.handle), self.handle)
+
+    def set_stream(self, stream_ptr: Optional[int]) -> None:
+        check(lib().etcu_set_stream(self.handle, stream_ptr), self.handle)
+
+    @property
+    def stream_handle(self) -> int:
+        """cudaStream_t of the library's work on this context (for CUDA events)."""
+        return int(lib().etcu_context_stream(self.handle) or 0)
+
+    @property
+    def device_bytes(self) -> int:
+        return int(lib().etcu_device_bytes(self.handle))
+
+    def check(self, status: int) -> None:
+        check(status, self.handle)
+
+
+def _dptr(t) -> int:
+    """Device address of a CUDA tensor (float32, contiguous).  The tensor's pending
+    writes on torch's stream are completed first, so the library's stream sees them."""
+    import torch
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise EttentionError(_abi.ERR_INVALID_ARGUMENT, "device images must be CUDA tensors")
+    if t.dtype != torch.float32 or not t.is_contiguous():
+        raise EttentionError(_abi.ERR_INVALID_ARGUMENT, "device images must be contiguous float32")
+    torch.cuda.current_stream(t.device).synchronize()
+    return t.data_ptr()
+
+
+class GPUMappedVolume:
+    """Device-resident volume (LR/model/volume/GPUMappedVolume.cpp:9-41)."""
+
+    def __init__(self, ctx: Context, resolution: Sequence[int], bbox_min: Optional[Sequence[float]] = None,
+                 bbox_max: Optional[Sequence[float]] = None, voxel_type: int = _abi.VOXEL_FLOAT32,
+                 init_value: float = 0.0, subvolume_count: int = 1):
+        self.ctx = ctx
+        res = [int(r) for r in resolution]
+        if bbox_min is None:  # VolumeParameterSet.cpp:40-46: dimension = resolution, origin 0
+            bbox_min = [-0.5 * r for r in res]
+            bbox_max = [0.5 * r for r in res]
+        d = VolumeDesc()
+        for i in range(3):
+            d.resolution[i] = res[i]
+            d.bbox_min[i] = float(bbox_min[i])
+            d.bbox_max[i] = float(bbox_max[i])
+        d.subvolume_count = int(subvolume_count)
+        self.desc = d
+        self.resolution = tuple(res)
+        self.bbox_min = tuple(float(np.float32(b)) for b in bbox_min)
+        self.bbox_max = tuple(float(np.float32(b)) for b in bbox_max)
+        self.voxel_type = voxel_type
+        h = ctypes.c_void_p()
+        ctx.check(lib().etcu_volume_create(ctx.handle, ctypes.byref(d), int(voxel_type), float(init_value),
+                                           ctypes.byref(h)))
+        self.handle = h
+        ctx._adopt(self)
+
+    @property
+    def voxel_size(self) -> np.ndarray:
+        return ((np.asarray(self.bbox_max, np.float32) - np.asarray(self.bbox_min, np.float32))
+                / np.asarray(self.resolution, np.float32)).astype(np.float32)
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib().etcu_volume_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, data: np.ndarray) -> None:
+        """data: (z, y, x) float32 array, x fastest."""
+        X, Y, Z = self.resolution
+        a = np.ascontiguousarray(data, np.float32)
+        if a.size != X * Y * Z:
+            raise EttentionError(_abi.ERR_INVALID_ARGUMENT, "volume data has the wrong size")
+        self.ctx.check(lib().etcu_volume_upload(self.handle, a.ctypes.data))
+
+    def download(self) -> np.ndarray:
+        X, Y, Z = self.resolution
+        out = np.empty((Z, Y, X), np.float32)
+        self.ctx.check(lib().etcu_volume_download(self.handle, out.ctypes.data))
+        return out
+
+    def set_mask(self, mask: Optional[np.ndarray]) -> None:
+        if mask is None:
+            self.ctx.check(lib().etcu_volume_set_mask(self.handle, None))
+            return
+        m = np.ascontiguousarray(mask, np.uint8)
+        self.ctx.check(lib().etcu_volume_set_mask(self.handle, m.ctypes.data))
+
+    def set_intensity_clamp(self, vmin: Optional[float] = None, vmax: Optional[float] = None) -> None:
+        self.ctx.check(lib().etcu_volume_set_intensity_clamp(self.handle, int(vmin is not None), float(vmin or 0.0),
+                                                              int(vmax is not None), float(vmax or 0.0)))
+
+    def device_ptr(self) -> int:
+        return int(lib().etcu_volume_device_ptr(self.handle) or 0)
+
+
+# ----------------------------------------------------------------------------- operators
+class ForwardProjectionOperator:
+    """ForwardProjectionOperator (ForwardProjectionOperator.cpp:11-55): SetOutput + Execute(subVolume).
+    The outputs are ACCUMULATED (+=), as in the reference."""
+
+    def __init__(self, volume: GPUMappedVolume, samples: int = 1):
+        self.volume = volume
+        self.samples = samples
+        self.geometry: Optional[ScannerGeometry] = None
+        self.virtual = None
+        self.traversal = None
+
+    def setScannerGeometry(self, g: ScannerGeometry) -> None:
+        self.geometry = g
+
+    def SetOutput(self, virtual_projection, traversal_length) -> None:
+        if (virtual_projection is None) != (traversal_length is None):
+            raise EttentionError(_abi.ERR_INVALID_ARGUMENT,
+                                 "Virtual projection and traversal length must either be set both or none of them!")
+        if virtual_projection is not None and tuple(virtual_projection.shape) != tuple(traversal_length.shape):
+            raise EttentionError(_abi.ERR_INVALID_ARGUMENT,
+                                 "Virtual projection and traversal length images differ in size!")
+        self.virtual, self.traversal = virtual_projection, traversal_length
+
+    def Execute(self, subvolume: int = 0) -> None:
+        if self.virtual is None:
+            raise EttentionError(_abi.ERR_STATE, "ForwardProjectionKernel cannot be run without setting output "
+                                 "images! Be sure to call setOutput() before with non-null parameters.")
+        g = self.geometry
+        if tuple(self.virtual.shape) != (g.height, g.width):
+            raise EttentionError(_abi.ERR_INVALID_ARGUMENT, "output image does not match the detector resolution")
+        v = g.to_view()
+        self.volume.ctx.check(lib().etcu_forward_project(self.volume.handle, ctypes.byref(v), int(subvolume),
+                                                         int(self.samples), _dptr(self.virtual),
+                                                         _dptr(self.traversal)))
+        self.volume.ctx.synchronize()  # the reference waits after every launch (CLKernel.cpp:177-179)
+
+
+class BackProjectionOperator:
+    """BackProjectionOperator (BackProjectionOperator.cpp:13-98): setInput(residual, traversal,
+    blockSize) + execute(subVolume | ALL_SUB_VOLUMES); lambda / blockSize per update."""
+
+    ALL_SUB_VOLUMES = _abi.ALL_SUBVOLUMES
+
+    def __init__(self, volume: GPUMappedVolume, lam: float, samples: int = 1,
+                 sampling: int = _abi.SAMPLING_TEXTURE):
+        self.volume = volume
+        self.lam = float(lam)
+        self.samples = int(samples)
+        self.sampling = sampling
+        self.geometry: Optional[ScannerGeometry] = None
+        self.residual = None
+        self.traversal = None
+        self.block_size = 1
+
+    def setScannerGeometry(self, g: ScannerGeometry) -> None:
+        self.geometry = g
+
+    def setInput(self, residual, traversal_length, block_size: int = 1) -> None:
+        if (residual is None) != (traversal_length is None):
+            raise EttentionError(_abi.ERR_INVALID_ARGUMENT,
+                                 "Either residual and traversalLength images must be provided both or none of them!")
+        if residual is not None and tuple(residual.shape) != tuple(traversal_length.shape):
+            raise EttentionError(_abi.ERR_INVALID_ARGUMENT, "Residual and traversalLength differ in size!")
+        self.residual, self.traversal, self.block_size = residual, traversal_length, int(block_size)
+
+    def execute(self, subvolume: int = _abi.ALL_SUBVOLUMES) -> None:
+        if self.residual is None:
+            raise EttentionError(_abi.ERR_STATE, "Residual and traversalLength images must both be provided via "
+                                 "SetInput() before kernel launch!")
+        v = self.geometry.to_view()
+        self.volume.ctx.check(lib().etcu_back_project(self.volume.handle, ctypes.byref(v), int(subvolume),
+                                                      self.samples, self.lam, self.block_size,
+                                                      _dptr(self.residual), _dptr(self.traversal),
+                                                      int(self.sampling)))
+        self.volume.ctx.synchronize()
+
+
+def compare(ctx: Context, real, virtual, residual) -> None:
+    """CompareKernel (ocl_src/Compare.cl): residual = real - virtual."""
+    ctx.check(lib().etcu_compare(ctx.handle, _dptr(real), _dptr(virtual), _dptr(residual), real.numel()))
+    ctx.synchronize()
+
+
+def long_object_compensation(ctx: Context, virtual, traversal, constant_length: float) -> None:
+    """VirtualProjectionKernel (ocl_src/VirtualProjection.cl), in place."""
+    ctx.check(lib().etcu_long_object_compensation(ctx.handle, _dptr(virtual), _dptr(traversal),
+                                                  float(constant_length), virtual.numel()))
+    ctx.synchronize()
+
+
+def compute_ray_length(volume: GPUMappedVolume, g: ScannerGeometry, out) -> None:
+    """ComputeRayLengthKernel (ocl_src/ComputeRayLength.cl)."""
+    v = g.to_view()
+    volume.ctx.check(lib().etcu_compute_ray_length(volume.handle, ctypes.byref(v), _dptr(out)))
+    volume.ctx.synchronize()
+
+
+# ----------------------------------------------------------------------------- parameters
+@dataclass
+class AlgebraicParameterSet:
+    """The hot-path keys of AlgorithmParameterSet, OptimizationParameterSet,
+    Forward/BackProjectionParameterSet, HardwareParameterSet, VolumeParameterSet,
+    InputParameterSet and PriorKnowledgeParameterSet (LR/setup/parameterset)."""
+    algorithm: str = "sart"
+    block_size: int = 1
+    iterations: int = 1
+    lam: float = 1.0
+    use_long_object_compensation: bool = False
+    fp_samples: int = 1
+    bp_samples: int = 1
+    voxel_type: int = _abi.VOXEL_FLOAT32
+    order: int = _abi.ORDER_RANDOM
+    subvolume_count: int = 1
+    dimension: Optional[Sequence[float]] = None
+    resolution: Optional[Sequence[int]] = None
+    origin: Sequence[float] = (0.0, 0.0, 0.0)
+    init_value: float = 0.0
+    skip: Sequence[int] = ()
+    xaxis_tilt: float = 0.0
+    vmin: Optional[float] = None
+    vmax: Optional[float] = None
+    sampling: int = _abi.SAMPLING_TEXTURE
+
+    @classmethod
+    def from_config(cls, cfg: Dict[str, str]) -> "AlgebraicParameterSet":
+        def vec(s):
+            return [float(x) for x in str(s).replace(",", " ").split()]
+
+        p = cls()
+        if "algorithm" not in cfg:
+            raise EttentionError(_abi.ERR_INVALID_ARGUMENT, "missing parameter algorithm")
+        p.algorithm = cfg["algorithm"]
+        # AlgorithmParameterSet.cpp:10-23
+        p.block_size = _abi.BLOCK_ALL
+        if p.algorithm == "sart":
+            p.block_size = 1
+        elif p.algorithm == "sirt":
+            p.block_size = _abi.BLOCK_ALL
+        elif "algorithm.blockSize" in cfg:
+            p.block_size = int(cfg["algorithm.blockSize"])
+        p.iterations = int(cfg["algorithm.numberOfIterations"])
+        p.lam = float(cfg["algorithm.lambda"])
+        p.use_long_object_compensation = str(cfg.get("algorithm.useLongObjectCompensation", "false")).lower() in (
+            "true", "1", "yes")
+        basis = cfg.get("algorithm.basisFunctions", "voxels")
+        if basis == "blobs":
+            raise EttentionError(_abi.ERR_UNSUPPORTED, "blob basis functions are not part of the voxel hot path")
+        if basis != "voxels":
+            raise EttentionError(_abi.ERR_INVALID_ARGUMENT,
+                                 f'Illegal value for parameter "algorithm.basisFunctions": {basis}!')
+        p.fp_samples = int(cfg.get("forwardProjection.samples", 1))
+        p.bp_samples = int(cfg.get("backProjection.samples", 1))
+        vt = cfg.get("optimization.internalVoxelRepresentationType", "float")
+        if vt not in VOXEL_TYPES:
+            raise EttentionError(_abi.ERR_INVALID_ARGUMENT,
+                                 "UChar is not supported as a valid internal voxel storage data type.")
+        p.voxel_type = VOXEL_TYPES[vt]
+        order = cfg.get("optimization.projectionIteration", "random")
+        if order not in ORDERS:
+            raise EttentionError(_abi.ERR_INVALID_ARGUMENT, "Illegal ProjectionSetType!")
+        p.order = ORDERS[order]
+        p.subvolume_count = int(cfg.get("hardware.subVolumeCount", 1))
+        if "volume.dimension" in cfg:
+            p.dimension = vec(cfg["volume.dimension"])
+            p.resolution = [int(x) for x in p.dimension]
+        if "volume.resolution" in cfg:
+            p.resolution = [int(x) for x in vec(cfg["volume.resolution"])]
+        if "volume.origin" in cfg:
+            p.origin = vec(cfg["volume.origin"])
+        p.init_value = float(cfg.get("volume.initValue", 0.0))
+        if "input.skipProjections" in cfg:
+            p.skip = [int(x) for x in vec(cfg["input.skipProjections"])]
+        p.xaxis_tilt = float(cfg.get("input.xAxisTilt", 0.0))
+        if "priorknowledge.volumeMinimumIntensity" in cfg:
+            p.vmin = float(cfg["priorknowledge.volumeMinimumIntensity"])
+        if "priorknowledge.volumeMaximumIntensity" in cfg:
+            p.vmax = float(cfg["priorknowledge.volumeMaximumIntensity"])
+        if p.block_size == 0:
+            raise EttentionError(_abi.ERR_INVALID_ARGUMENT, "Illegal ProjectionBlockSize!")
+        return p
+
+    def bbox(self):
+        dim = np.asarray(self.dimension if self.dimension is not None else self.resolution, np.float64)
+        o = np.asarray(self.origin, np.float64)
+        return list(o - 0.5 * dim), list(o + 0.5 * dim)
+
+    def recon_params(self, use_graph: bool = True) -> ReconParams:
+        rp = ReconParams()
+        rp.lam = float(self.lam)
+        rp.block_size = int(self.block_size)
+        rp.fp_samples = int(self.fp_samples)
+        rp.bp_samples = int(self.bp_samples)
+        rp.use_long_object_compensation = int(bool(self.use_long_object_compensation))
+        rp.order = int(self.order)
+        rp.sampling = int(self.sampling)
+        rp.use_graph = int(bool(use_graph))
+        return rp
+
+
+class BlockIterativeReconstructionOperator:
+    """BlockIterativeReconstructionOperator (BlockIterativeReconstructionOperator.cpp:26-185):
+    SART (blockSize 1), SIRT (one block of every view) and general block sizes.
+
+    ``projections`` is an (N, H, W) float32 NumPy array (uploaded once) or a CUDA
+    tensor already in device memory."""
+
+    def __init__(self, volume: GPUMappedVolume, geometries: Sequence[ScannerGeometry], projections,
+                 params: AlgebraicParameterSet, use_graph: bool = True):
+        self.volume = volume
+        self.params = params
+        self._views = (View * len(geometries))(*[g.to_view() for g in geometries])
+        rp = params.recon_params(use_graph)
+        self._skip = (ctypes.c_uint32 * max(1, len(params.skip)))(*[int(s) for s in params.skip])
+        if len(params.skip):
+            rp.skip = ctypes.cast(self._skip, ctypes.POINTER(ctypes.c_uint32))
+            rp.skip_count = len(params.skip)
+        self._rp = rp
+        if params.vmin is not None or params.vmax is not None:
+            volume.set_intensity_clamp(params.vmin, params.vmax)
+        h = ctypes.c_void_p()
+        if isinstance(projections, np.ndarray):
+            self._host = np.ascontiguousarray(projections, np.float32)
+            volume.ctx.check(lib().etcu_recon_create(volume.handle, self._views, len(geometries),
+                                                     self._host.ctypes.data, ctypes.byref(rp), ctypes.byref(h)))
+        else:
+            self._dev = projections
+            volume.ctx.check(lib().etcu_recon_create_device(volume.handle, self._views, len(geometries),
+                                                            _dptr(projections), ctypes.byref(rp), ctypes.byref(h)))
+        self.handle = h
+        volume.ctx._adopt(self)
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib().etcu_recon_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def runNiterations(self, n: int = 1) -> None:
+        self.volume.ctx.check(lib().etcu_recon_run(self.handle, int(n)))
+
+    def run(self) -> None:
+        self.runNiterations(self.params.iterations)
+
+    def runSingleIteration(self) -> None:
+        self.runNiterations(1)
+
+    def getReconstructedVolume(self) -> np.ndarray:
+        return self.volume.download()
+
+    def last_residual_sq(self) -> float:
+        r = ctypes.c_double()
+        self.volume.ctx.check(lib().etcu_recon_last_residual_sq(self.handle, ctypes.byref(r)))
+        return float(r.value)
+
+    def data_residual_sq(self) -> float:
+        r = ctypes.c_double()
+        self.volume.ctx.check(lib().etcu_recon_data_residual_sq(self.handle, ctypes.byref(r)))
+        return float(r.value)
+
+    def view_order(self) -> List[int]:
+        n = len(self._views)
+        out = np.zeros(n, np.uint32)
+        cnt = ctypes.c_uint32()
+        self.volume.ctx.check(lib().etcu_recon_view_order(self.handle, out.ctypes.data, n, ctypes.byref(cnt)))
+        return [int(i) for i in out[: cnt.value]]
+
+    @property
+    def launches_per_iteration(self) -> int:
+        return int(lib().etcu_recon_launches_per_iteration(self.handle))
+
+    def profile_iteration(self):
+        """Runs one iteration with per-launch CUDA events: (fp_ms, bp_ms, fp_launches, bp_launches)."""
+        f, b = ctypes.c_float(), ctypes.c_float()
+        nf, nb = ctypes.c_uint32(), ctypes.c_uint32()
+        self.volume.ctx.check(lib().etcu_recon_profile_iteration(self.handle, ctypes.byref(f), ctypes.byref(b),
+                                                                 ctypes.byref(nf), ctypes.byref(nb)))
+        return float(f.value), float(b.value), int(nf.value), int(nb.value)

@@ -1,0 +1,241 @@
+/*
+ * ettention_b200 -- C ABI of the B200 (sm_100a) block-iterative reconstruction
+ * path (SART / SIRT / general block size) of Ettention's libReconstruction.
+ *
+ * Plain pointers, sizes and status codes only: no C++ or CUDA types cross this
+ * boundary, so the reference's C++ host code (or any FFI) can bind it.  All
+ * device memory is owned by the library behind opaque handles; host buffers
+ * are only read or written inside explicit upload / download calls.  Calls on
+ * one context are stream-ordered on that context's CUDA stream and are not
+ * thread-safe (one host thread per context, as the reference's single in-order
+ * OpenCL queue, LR = ettention/libReconstruction/src):
+ *   LR/gpu/opencl/CLKernel.cpp:177-179.
+ *
+ * Errors: every call returns ETCU_OK or an error code and never throws; the
+ * message of the last failure on a context is read with etcu_last_error().
+ * The validation messages repeat the reference's exception texts.
+ *
+ * Each entry point names the reference interface it replaces.
+ */
+#ifndef ETTENTION_B200_H
+#define ETTENTION_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ETCU_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define ETCU_API __attribute__((visibility("default")))
+#else
+#define ETCU_API
+#endif
+
+typedef enum {
+    ETCU_OK = 0,
+    ETCU_ERR_INVALID_ARGUMENT = 1, /* reference: ettention::Exception from validation */
+    ETCU_ERR_CUDA = 2,             /* reference: GPUException from CL_ASSERT */
+    ETCU_ERR_OUT_OF_MEMORY = 3,
+    ETCU_ERR_STATE = 4,            /* call order violated (e.g. outputs not set) */
+    ETCU_ERR_UNSUPPORTED = 5,
+    ETCU_ERR_NO_DEVICE = 6
+} etcu_status;
+
+/* Voxel storage of the volume the projectors read.
+ * FLOAT32: one FP32 volume (reference default, optimization.internalVoxelRepresentationType=float).
+ * HALF16:  one IEEE-half volume re-rounded after every view's update
+ *          (reference "half", LR/model/volume/HalfFloatVolume.cpp:38-89).
+ * F16_MASTER / BF16_MASTER: FP32 master volume updated by back projection plus
+ *          a 16-bit shadow copy that forward projection reads; the shadow is
+ *          re-quantised once per block. */
+typedef enum {
+    ETCU_VOXEL_FLOAT32 = 0,
+    ETCU_VOXEL_HALF16 = 1,
+    ETCU_VOXEL_F16_MASTER = 2,
+    ETCU_VOXEL_BF16_MASTER = 3
+} etcu_voxel_type;
+
+/* Bilinear sampling of residual / ray-length images in back projection.
+ * TEXTURE: GPU texture filtering (1/256 weights), the reference's image path
+ *          (LR/algorithm/projections/back/BackProjectionKernel.cpp:146-163).
+ * EXACT:   FP32 weights, the reference's buffer path
+ *          (ettention/libReconstruction/ocl_src/ImageHandler.hl:20-40). */
+typedef enum { ETCU_SAMPLING_TEXTURE = 0, ETCU_SAMPLING_EXACT = 1 } etcu_sampling;
+
+/* Projection iteration order, optimization.projectionIteration
+ * (LR/model/projectionset/factory/ProjectionIteratorFactory.cpp:11-22). */
+typedef enum {
+    ETCU_ORDER_IDENTITY = 0,
+    ETCU_ORDER_RANDOM = 1,
+    ETCU_ORDER_MAXANGLE = 2,
+    ETCU_ORDER_BUCKETS = 3
+} etcu_order;
+
+/* Scanner geometry of one view: LR/model/geometry/ScannerGeometry.cpp:39-46
+ * (source base, detector base, horizontal / vertical pitch, resolution) and
+ * the Parallel / Perspective subclass. */
+typedef struct {
+    float source[3];
+    float detector[3];
+    float hpitch[3];
+    float vpitch[3];
+    uint32_t width, height;
+    int32_t perspective;
+} etcu_view;
+
+/* Volume geometry: LR/setup/parameterset/VolumeParameterSet.cpp:7-71 and the
+ * z-slab sub-volume split of LR/model/volume/VolumeProperties.cpp:74-98. */
+typedef struct {
+    uint32_t resolution[3];  /* x, y, z */
+    float bbox_min[3];       /* world bounding box (origin -+ dimension/2) */
+    float bbox_max[3];
+    uint32_t subvolume_count; /* 0 or 1: one slab */
+} etcu_volume_desc;
+
+typedef struct etcu_context etcu_context;
+typedef struct etcu_volume etcu_volume;
+typedef struct etcu_recon etcu_recon;
+
+/* ---------------------------------------------------------------- context */
+/* Replaces the OpenCL context / queue of LR/gpu/opencl/CLAbstractionLayer.cpp:41-107. */
+ETCU_API int etcu_abi_version(void);
+ETCU_API etcu_status etcu_context_create(int device, etcu_context** out);
+ETCU_API etcu_status etcu_context_destroy(etcu_context* ctx);
+/* Message of the last failed call on ctx (or of the last failed context creation when ctx is NULL). */
+ETCU_API const char* etcu_last_error(const etcu_context* ctx);
+ETCU_API etcu_status etcu_synchronize(etcu_context* ctx);
+/* Make the context issue its work on an existing CUDA stream (cudaStream_t passed as void*; NULL = own stream). */
+ETCU_API etcu_status etcu_set_stream(etcu_context* ctx, void* cuda_stream);
+/* The CUDA stream (cudaStream_t as void*) the context issues its work on, for
+ * callers that record CUDA events around library calls. */
+ETCU_API void* etcu_context_stream(const etcu_context* ctx);
+/* Sum of device bytes the context currently holds. */
+ETCU_API size_t etcu_device_bytes(const etcu_context* ctx);
+
+/* ---------------------------------------------------------------- geometry */
+/* SingleAxisTiltRotator::createRotatedScannerGeometry
+ * (LR/model/geometry/SingleAxisTiltRotator.cpp:42-78): rotate the base geometry
+ * by -tilt about +y (about the x-pre-tilted y axis when xaxis_tilt_deg != 0). */
+ETCU_API etcu_status etcu_view_rotate(const etcu_view* base, float tilt_deg, float xaxis_tilt_deg, etcu_view* out);
+/* ParallelScannerGeometry::getProjectionMatrix (LR/model/geometry/ParallelScannerGeometry.cpp:49-62)
+ * and PerspectiveScannerGeometry::getProjectionMatrix (.../PerspectiveScannerGeometry.cpp:47-50),
+ * 16 floats, column-major (Matrix4x4 layout). */
+ETCU_API etcu_status etcu_view_projection_matrix(const etcu_view* view, float out16[16]);
+/* ParallelBeamsBackProjectionKernel::generateSamplingPatternForPerVoxelSampling
+ * (LR/algorithm/projections/back/parallel/ParallelBeamsBackProjectionKernel.cpp:55-98):
+ * samples x {offset x, y, z, chord}; samples must be a perfect square. */
+ETCU_API etcu_status etcu_view_sample_pattern(const etcu_view* view, const float voxel_size[3], uint32_t samples,
+                                     float* out4);
+/* ParallelScannerGeometry::getTraversalLengthThroughBoundingBox (ParallelScannerGeometry.cpp:64-69). */
+ETCU_API etcu_status etcu_view_traversal_length(const etcu_view* view, const float bbox_min[3], const float bbox_max[3],
+                                       float* out);
+
+/* ---------------------------------------------------------------- volume */
+/* GPUMappedVolume over Float/HalfFloatVolume (LR/model/volume/GPUMappedVolume.cpp:9-41),
+ * device-resident for its whole life.  init_value fills every voxel. */
+ETCU_API etcu_status etcu_volume_create(etcu_context* ctx, const etcu_volume_desc* desc, etcu_voxel_type type,
+                               float init_value, etcu_volume** out);
+ETCU_API etcu_status etcu_volume_destroy(etcu_volume* vol);
+/* Host float32 volume (x fastest, z slowest) <-> device; converts to / from the storage type. */
+ETCU_API etcu_status etcu_volume_upload(etcu_volume* vol, const float* host);
+ETCU_API etcu_status etcu_volume_download(etcu_volume* vol, float* host);
+/* Prior-knowledge mask (UCHAR_8 volume, value/255 weights; LR/algorithm/projections/
+ * forward/ForwardProjectionKernel.cpp:21 USE_PRIOR_KNOWLEDGE_MASK).  NULL removes it. */
+ETCU_API etcu_status etcu_volume_set_mask(etcu_volume* vol, const uint8_t* host_mask);
+/* Device address of the volume (FP32 master, or the half volume) for zero-copy consumers. */
+ETCU_API void* etcu_volume_device_ptr(etcu_volume* vol);
+
+/* ---------------------------------------------------------------- operators */
+/* ForwardProjectionOperator::SetOutput + Execute(subVolume)
+ * (LR/algorithm/projections/forward/ForwardProjectionOperator.cpp:31-55 over
+ * ParallelBeamsForwardProjection.cl / PerspectiveBeamsForwardProjection.cl):
+ * ADDS the sub-volume's line integrals of volume and mask into the device
+ * images d_virtual and d_traversal (width x height floats each, row-major). */
+ETCU_API etcu_status etcu_forward_project(etcu_volume* vol, const etcu_view* view, uint32_t subvolume, uint32_t samples,
+                                 float* d_virtual, float* d_traversal);
+/* BackProjectionOperator::setInput(residual, traversal, blockSize) + execute(subVolume)
+ * (LR/algorithm/projections/back/BackProjectionOperator.cpp:43-98): voxel-driven
+ * update of sub-volume `subvolume` with lambda / block_size (BackProjectionKernel.cpp:94).
+ * samples: parallel = per-voxel detector-plane samples (perfect square);
+ *          perspective = samples per dimension (0: derived from resolutions).
+ * subvolume == ETCU_ALL_SUBVOLUMES runs every slab. */
+#define ETCU_ALL_SUBVOLUMES 0xffffffffu
+ETCU_API etcu_status etcu_back_project(etcu_volume* vol, const etcu_view* view, uint32_t subvolume, uint32_t samples,
+                              float lambda, uint32_t block_size, const float* d_residual,
+                              const float* d_traversal, etcu_sampling sampling);
+/* Perspective back-projection intensity clamps (PerspectiveBeamsBackProjectionKernel.cpp:175-188). */
+ETCU_API etcu_status etcu_volume_set_intensity_clamp(etcu_volume* vol, int use_min, float vmin, int use_max, float vmax);
+/* CompareKernel: residual = real - virtual (ocl_src/Compare.cl:1-9), device images of n floats. */
+ETCU_API etcu_status etcu_compare(etcu_context* ctx, const float* d_real, const float* d_virtual, float* d_residual,
+                         size_t n);
+/* VirtualProjectionKernel (ocl_src/VirtualProjection.cl:3-10): long-object compensation in place. */
+ETCU_API etcu_status etcu_long_object_compensation(etcu_context* ctx, float* d_virtual, float* d_traversal,
+                                          float constant_length, size_t n);
+/* ComputeRayLengthKernel (ocl_src/ComputeRayLength.cl:21-34): parallel-ray chord through the complete volume. */
+ETCU_API etcu_status etcu_compute_ray_length(etcu_volume* vol, const etcu_view* view, float* d_out);
+
+/* ---------------------------------------------------------------- reconstruction */
+/* BlockIterativeReconstructionOperator (LR/algorithm/reconstruction/blockiterative/
+ * BlockIterativeReconstructionOperator.cpp:56-185) with AlgorithmParameterSet /
+ * OptimizationParameterSet semantics (LR/setup/parameterset/AlgorithmParameterSet.cpp:8-53).
+ * block_size: 1 = SART, ETCU_BLOCK_ALL = SIRT, else algorithm.blockSize. */
+#define ETCU_BLOCK_ALL 0xffffffffu
+typedef struct {
+    float lambda;                 /* algorithm.lambda */
+    uint32_t block_size;          /* algorithm.blockSize (1 SART, ETCU_BLOCK_ALL SIRT) */
+    uint32_t fp_samples;          /* forwardProjection.samples (0 -> 1) */
+    uint32_t bp_samples;          /* backProjection.samples */
+    int32_t use_long_object_compensation; /* algorithm.useLongObjectCompensation */
+    etcu_order order;             /* optimization.projectionIteration */
+    etcu_sampling sampling;       /* residual sampling of the back projector */
+    const uint32_t* skip;         /* input.skipProjections (may be NULL) */
+    uint32_t skip_count;
+    int32_t use_graph;            /* capture each iteration in a CUDA graph */
+} etcu_recon_params;
+
+/* Uploads the tilt series (n_views x height x width floats, host memory) once
+ * and prepares per-view geometry, textures and the per-iteration graph. */
+ETCU_API etcu_status etcu_recon_create(etcu_volume* vol, const etcu_view* views, uint32_t n_views,
+                              const float* host_projections, const etcu_recon_params* params, etcu_recon** out);
+/* Same, with the tilt series already in device memory (n_views x height x width floats). */
+ETCU_API etcu_status etcu_recon_create_device(etcu_volume* vol, const etcu_view* views, uint32_t n_views,
+                                     const float* d_projections, const etcu_recon_params* params,
+                                     etcu_recon** out);
+ETCU_API etcu_status etcu_recon_destroy(etcu_recon* rec);
+/* runNiterations (BlockIterativeReconstructionOperator.cpp:66-80). */
+ETCU_API etcu_status etcu_recon_run(etcu_recon* rec, uint32_t iterations);
+/* Sum over the last iteration's views of ||b - Ax||^2 as each view saw it before its
+ * update (FP64 accumulation). */
+ETCU_API etcu_status etcu_recon_last_residual_sq(etcu_recon* rec, double* out);
+/* ||b - Ax||^2 over all views for the current volume (forward projection only, FP64). */
+ETCU_API etcu_status etcu_recon_data_residual_sq(etcu_recon* rec, double* out);
+/* Permutation of view indices the reconstruction iterates in. */
+ETCU_API etcu_status etcu_recon_view_order(const etcu_recon* rec, uint32_t* out, uint32_t capacity, uint32_t* count);
+/* Runs one real iteration launch by launch, with CUDA events around every forward
+ * and back projection; returns their summed device times (ms) and launch counts.
+ * (Per-kernel timing of the hot path; the reference's PerformanceReport of
+ * LR/gpu/opencl/CLAbstractionLayer.cpp:295-324.) */
+ETCU_API etcu_status etcu_recon_profile_iteration(etcu_recon* rec, float* fp_ms, float* bp_ms, uint32_t* fp_launches,
+                                                  uint32_t* bp_launches);
+/* Kernel launches one iteration issues (graph nodes when captured). */
+ETCU_API uint32_t etcu_recon_launches_per_iteration(const etcu_recon* rec);
+
+/* One-call host-buffer reconstruction: upload projections and initial volume,
+ * run `iterations`, download the result (the path a frontend's "ettention --config" run takes). */
+ETCU_API etcu_status etcu_reconstruct(etcu_context* ctx, const etcu_volume_desc* desc, etcu_voxel_type type,
+                             const etcu_view* views, uint32_t n_views, const float* host_projections,
+                             const etcu_recon_params* params, uint32_t iterations, float* host_volume_inout);
+
+/* Projection orderings on their own (LR/model/projectionset/ProjectionSet*.cpp), for callers
+ * that keep their own driver loop. */
+ETCU_API etcu_status etcu_projection_order(etcu_order order, uint32_t n, const uint32_t* skip, uint32_t skip_count,
+                                  uint32_t* out, uint32_t* count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ETTENTION_B200_H */
