@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(HERE, "libettention_b200.so")
 OK = 0
 ERR_INVALID_ARGUMENT, ERR_CUDA, ERR_OUT_OF_MEMORY, ERR_STATE, ERR_UNSUPPORTED, ERR_NO_DEVICE = 1, 2, 3, 4, 5, 6
 VOXEL_FLOAT32, VOXEL_HALF16, VOXEL_F16_MASTER, VOXEL_BF16_MASTER = 0, 1, 2, 3
-SAMPLING_TEXTURE, SAMPLING_EXACT = 0, 1
+SAMPLING_Q8, SAMPLING_EXACT, SAMPLING_HW_TEXTURE = 0, 1, 2
 ORDER_IDENTITY, ORDER_RANDOM, ORDER_MAXANGLE, ORDER_BUCKETS = 0, 1, 2, 3
 ALL_SUBVOLUMES = 0xFFFFFFFF
 BLOCK_ALL = 0xFFFFFFFF

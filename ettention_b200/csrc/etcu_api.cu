@@ -201,7 +201,10 @@ ViewConst make_view_const(const etcu_view& v, const SlabConst& slab, float loc_l
         return a * sg;
     };
     float sdx = sdf(slab.vs.x, inv[0], r.x), sdy = sdf(slab.vs.y, inv[1], r.y), sdz = sdf(slab.vs.z, inv[2], r.z);
-    c.fast2d = (!v.perspective && r.y == 0.f && std::isfinite(sdx) && std::isfinite(sdy) && std::isfinite(sdz)) ? 1 : 0;
+    const bool small = (unsigned long long)slab.rx * (unsigned long long)slab.ry * (unsigned long long)slab.rz <
+                       (1ull << 32);
+    c.fast2d = (!v.perspective && r.y == 0.f && small && std::isfinite(sdx) && std::isfinite(sdy) &&
+                std::isfinite(sdz)) ? 1 : 0;
     return c;
 }
 
@@ -249,38 +252,66 @@ void launch_fp(const etcu_volume* vol, const FpArgs& a, bool persp, uint32_t nvi
     }
 }
 
-template <bool kPersp, bool kMask, int kStore, bool kExact>
-void launch_bp_t(const BpArgs& a, cudaStream_t st) {
-    dim3 block(64, 4, 1);
-    dim3 grid((a.slab.rx + 63) / 64, (a.slab.ry + 3) / 4, a.slab.rz);
-    back_project_kernel<kPersp, kMask, kStore, kExact><<<grid, block, 0, st>>>(a);
+constexpr size_t kBpSmemBudget = 160 * 1024;
+
+template <bool kPersp, bool kMask, int kStore, int kSampling>
+void launch_bp_t(const BpArgs& a, int device, cudaStream_t st) {
+    // Opt in to the large dynamic shared-memory carve-out once per device and instantiation.
+    static unsigned long long opted = 0;
+    auto kern = kPersp ? bp_perspective_kernel<kMask, kStore, kSampling> : bp_parallel_kernel<kMask, kStore, kSampling>;
+    if (device < 64 && !(opted & (1ull << device))) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBpSmemBudget);
+        opted |= 1ull << device;
+    }
+    const size_t smem = bp_smem_bytes(a.nviews, kPersp ? 0 : a.nsamples);
+    const int zc = kPersp ? kBpZPersp : kBpZ;
+    dim3 block(32, 8, 1);
+    dim3 grid((a.slab.rx + 31) / 32, (a.slab.ry + 7) / 8, (a.slab.rz + zc - 1) / zc);
+    kern<<<grid, block, smem, st>>>(a);
 }
 
 template <bool kPersp, bool kMask, int kStore>
-void launch_bp_s(const BpArgs& a, bool exact, cudaStream_t st) {
-    if (exact) launch_bp_t<kPersp, kMask, kStore, true>(a, st);
-    else launch_bp_t<kPersp, kMask, kStore, false>(a, st);
+void launch_bp_s(const BpArgs& a, etcu_sampling sm, int dev, cudaStream_t st) {
+    if (sm == ETCU_SAMPLING_EXACT) launch_bp_t<kPersp, kMask, kStore, kSampleExact>(a, dev, st);
+    else if (sm == ETCU_SAMPLING_HW_TEXTURE) launch_bp_t<kPersp, kMask, kStore, kSampleTexture>(a, dev, st);
+    else launch_bp_t<kPersp, kMask, kStore, kSampleQ8>(a, dev, st);
 }
 
 template <bool kPersp, bool kMask>
-void launch_bp_m(const BpArgs& a, etcu_voxel_type t, bool exact, cudaStream_t st) {
+void launch_bp_m(const BpArgs& a, etcu_voxel_type t, etcu_sampling sm, int dev, cudaStream_t st) {
     switch (t) {
-    case ETCU_VOXEL_FLOAT32: launch_bp_s<kPersp, kMask, 0>(a, exact, st); break;
-    case ETCU_VOXEL_HALF16: launch_bp_s<kPersp, kMask, 1>(a, exact, st); break;
-    case ETCU_VOXEL_F16_MASTER: launch_bp_s<kPersp, kMask, 2>(a, exact, st); break;
-    case ETCU_VOXEL_BF16_MASTER: launch_bp_s<kPersp, kMask, 3>(a, exact, st); break;
+    case ETCU_VOXEL_FLOAT32: launch_bp_s<kPersp, kMask, 0>(a, sm, dev, st); break;
+    case ETCU_VOXEL_HALF16: launch_bp_s<kPersp, kMask, 1>(a, sm, dev, st); break;
+    case ETCU_VOXEL_F16_MASTER: launch_bp_s<kPersp, kMask, 2>(a, sm, dev, st); break;
+    case ETCU_VOXEL_BF16_MASTER: launch_bp_s<kPersp, kMask, 3>(a, sm, dev, st); break;
     }
 }
 
-void launch_bp(const etcu_volume* vol, const BpArgs& a, bool persp, bool exact, cudaStream_t st) {
-    bool mask = a.mask != nullptr;
-    if (persp) {
-        if (mask) launch_bp_m<true, true>(a, vol->type, exact, st);
-        else launch_bp_m<true, false>(a, vol->type, exact, st);
-    } else {
-        if (mask) launch_bp_m<false, true>(a, vol->type, exact, st);
-        else launch_bp_m<false, false>(a, vol->type, exact, st);
+// Back projection of a.nviews views; when their staged constants exceed the
+// shared-memory budget the views are split over consecutive launches, which
+// applies them in the same order.  Returns the number of launches.
+uint32_t launch_bp(const etcu_volume* vol, const BpArgs& a0, bool persp, etcu_sampling sm, cudaStream_t st) {
+    const int dev = vol->ctx->device;
+    const size_t per_view = bp_smem_bytes(1, persp ? 0 : a0.nsamples);
+    const int max_views = (int)std::max<size_t>(1, (kBpSmemBudget - 16) / per_view);
+    uint32_t launches = 0;
+    for (int c0 = 0; c0 < a0.nviews; c0 += max_views) {
+        BpArgs a = a0;
+        a.first = a0.first + (uint32_t)c0;
+        a.nviews = std::min(max_views, a0.nviews - c0);
+        a.rl = a0.rl + (size_t)c0 * a0.rl_slot;
+        if (a0.texs) a.texs = a0.texs + c0;
+        const bool mask = a.mask != nullptr;
+        if (persp) {
+            if (mask) launch_bp_m<true, true>(a, vol->type, sm, dev, st);
+            else launch_bp_m<true, false>(a, vol->type, sm, dev, st);
+        } else {
+            if (mask) launch_bp_m<false, true>(a, vol->type, sm, dev, st);
+            else launch_bp_m<false, false>(a, vol->type, sm, dev, st);
+        }
+        ++launches;
     }
+    return launches;
 }
 
 void fill_bp_volume_ptrs(const etcu_volume* vol, const SlabConst& s, BpArgs& a) {
@@ -678,7 +709,7 @@ etcu_status bp_one_slab(etcu_volume* vol, const etcu_view* view, const SlabConst
     a.use_max = vol->use_max;
     a.vmin = vol->vmin;
     a.vmax = vol->vmax;
-    launch_bp(vol, a, view->perspective != 0, sampling == ETCU_SAMPLING_EXACT, ctx->stream);
+    launch_bp(vol, a, view->perspective != 0, sampling, ctx->stream);
     CKL(ctx);
     return ETCU_OK;
 }
@@ -818,6 +849,7 @@ uint32_t issue_forward(etcu_recon* r, uint32_t first, uint32_t count, cudaStream
 uint32_t issue_backward(etcu_recon* r, uint32_t first, uint32_t count, cudaStream_t st) {
     etcu_volume* vol = r->vol;
     const uint32_t S = (uint32_t)vol->slabs.size();
+    uint32_t n = 0;
     for (int s = (int)S - 1; s >= 0; --s) {
         const SlabConst& slab = vol->slabs[s];
         BpArgs a{};
@@ -842,9 +874,9 @@ uint32_t issue_backward(etcu_recon* r, uint32_t first, uint32_t count, cudaStrea
         a.use_max = vol->use_max;
         a.vmin = vol->vmin;
         a.vmax = vol->vmax;
-        launch_bp(vol, a, r->persp, r->params.sampling == ETCU_SAMPLING_EXACT, st);
+        n += launch_bp(vol, a, r->persp, r->params.sampling, st);
     }
-    return S;
+    return n;
 }
 
 // One iteration (BlockIterativeReconstructionOperator.cpp:92-103).

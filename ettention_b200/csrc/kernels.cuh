@@ -176,28 +176,106 @@ __device__ __forceinline__ void dda_walk3(const DdaStart& st, const SlabConst& g
 // component stays FLT_MAX and never wins; the walk stays in one xz plane of
 // the volume.  Valid (and bit-identical to dda_walk3) when the x and z step
 // differences are finite.
-template <typename VoxT, bool kMask>
+//
+// The loop is restructured for memory-level parallelism without changing
+// the arithmetic: instead of re-testing the voxel index against the slab
+// bounds, each axis carries the number of steps it may still take before it
+// leaves the slab (the same exit condition), and the walk advances
+// kUnroll steps at a time, issuing the kUnroll voxel loads before the
+// kUnroll accumulations (which stay in walk order).  Dead steps after the
+// exit load nothing and add exactly zero.
+template <typename VoxT, bool kMask, int kUnroll = 4>
 __device__ __forceinline__ void dda_walk_xz(const DdaStart& st, const SlabConst& g, const VoxT* __restrict__ vol,
                                            const uint8_t* __restrict__ mask, float& acc, float& accl) {
-    int ix = st.ix, iz = st.iz;
-    float rx = st.res.x, rz = st.res.z;
-    const int plane = g.rx * g.ry;
+    const unsigned plane = (unsigned)g.rx * (unsigned)g.ry;
     const VoxT* row = vol + (size_t)st.iy * (size_t)g.rx;
     const uint8_t* mrow = kMask ? mask + (size_t)st.iy * (size_t)g.rx : nullptr;
     const float sdx = st.sd.x, sdz = st.sd.z;
-    const int six = st.sx, siz = st.sz;
-    for (int it = 0; it < kMaxDdaIterations; ++it) {
-        if ((unsigned)ix >= (unsigned)g.rx || (unsigned)iz >= (unsigned)g.rz) break;
-        float dt = fminf(rx, rz);
-        size_t off = (size_t)iz * (size_t)plane + (size_t)ix;
-        acc = fmaf(dt, load_voxel(row + off), acc);
-        if (kMask) accl = fmaf(dt, mask_weight(mrow + off), accl);
-        else accl += dt;
-        bool bx = rx <= rz;
-        rx = bx ? sdx : fsub(rx, dt);
-        rz = bx ? fsub(rz, dt) : sdz;
-        ix += bx ? six : 0;
-        iz += bx ? 0 : siz;
+    const unsigned dx = (unsigned)st.sx, dz = (unsigned)st.sz * plane;  // two's-complement deltas
+    int nx = st.sx > 0 ? g.rx - st.ix : (st.sx < 0 ? st.ix + 1 : 0x7fffffff);
+    int nz = st.sz > 0 ? g.rz - st.iz : (st.sz < 0 ? st.iz + 1 : 0x7fffffff);
+    int left = kMaxDdaIterations;
+    unsigned off = (unsigned)st.iz * plane + (unsigned)st.ix;
+    float rx = st.res.x, rz = st.res.z;
+    for (;;) {
+        float dts[kUnroll], vals[kUnroll], mws[kUnroll];
+#pragma unroll
+        for (int j = 0; j < kUnroll; ++j) {
+            const bool live = (nx > 0) & (nz > 0) & (left > 0);
+            const float dt = fminf(rx, rz);
+            const bool bx = rx <= rz;
+            dts[j] = live ? dt : 0.f;
+            vals[j] = 0.f;
+            mws[j] = 0.f;
+            if (live) {
+                vals[j] = load_voxel(row + off);
+                if (kMask) mws[j] = mask_weight(mrow + off);
+            }
+            rx = bx ? sdx : fsub(rx, dt);
+            rz = bx ? fsub(rz, dt) : sdz;
+            off += bx ? dx : dz;
+            nx -= bx ? 1 : 0;
+            nz -= bx ? 0 : 1;
+            left -= 1;
+        }
+#pragma unroll
+        for (int j = 0; j < kUnroll; ++j) {
+            acc = fmaf(dts[j], vals[j], acc);
+            if (kMask) accl = fmaf(dts[j], mws[j], accl);
+            else accl += dts[j];
+        }
+        if (!((nx > 0) & (nz > 0) & (left > 0))) break;
+    }
+}
+
+// General 3-D walk with finite step differences, restructured like
+// dda_walk_xz (per-axis step budgets, kUnroll loads in flight, accumulation
+// in walk order).  Idx is the offset type (32-bit when the sub-volume has
+// fewer than 2^32 voxels).
+template <typename VoxT, bool kMask, typename Idx, int kUnroll = 4>
+__device__ __forceinline__ void dda_walk3_fast(const DdaStart& st, const SlabConst& g, const VoxT* __restrict__ vol,
+                                              const uint8_t* __restrict__ mask, float& acc, float& accl) {
+    const Idx rowlen = (Idx)g.rx, plane = (Idx)g.rx * (Idx)g.ry;
+    const Idx dx = (Idx)st.sx, dy = (Idx)st.sy * rowlen, dz = (Idx)st.sz * plane;
+    int nx = st.sx > 0 ? g.rx - st.ix : (st.sx < 0 ? st.ix + 1 : 0x7fffffff);
+    int ny = st.sy > 0 ? g.ry - st.iy : (st.sy < 0 ? st.iy + 1 : 0x7fffffff);
+    int nz = st.sz > 0 ? g.rz - st.iz : (st.sz < 0 ? st.iz + 1 : 0x7fffffff);
+    int left = kMaxDdaIterations;
+    Idx off = (Idx)st.iz * plane + (Idx)st.iy * rowlen + (Idx)st.ix;
+    float rx = st.res.x, ry = st.res.y, rz = st.res.z;
+    const float sdx = st.sd.x, sdy = st.sd.y, sdz = st.sd.z;
+    for (;;) {
+        float dts[kUnroll], vals[kUnroll], mws[kUnroll];
+#pragma unroll
+        for (int j = 0; j < kUnroll; ++j) {
+            const bool live = (nx > 0) & (ny > 0) & (nz > 0) & (left > 0);
+            const float dt = fminf(fminf(rx, ry), rz);
+            const bool bx = rx <= ry && rx <= rz;
+            const bool by = ry < rx && ry <= rz;
+            const bool bz = !bx && !by;  // rz < rx && rz < ry for finite values
+            dts[j] = live ? dt : 0.f;
+            vals[j] = 0.f;
+            mws[j] = 0.f;
+            if (live) {
+                vals[j] = load_voxel(vol + off);
+                if (kMask) mws[j] = mask_weight(mask + off);
+            }
+            rx = bx ? sdx : fsub(rx, dt);
+            ry = by ? sdy : fsub(ry, dt);
+            rz = bz ? sdz : fsub(rz, dt);
+            off += bx ? dx : (by ? dy : dz);
+            nx -= bx ? 1 : 0;
+            ny -= by ? 1 : 0;
+            nz -= bz ? 1 : 0;
+            left -= 1;
+        }
+#pragma unroll
+        for (int j = 0; j < kUnroll; ++j) {
+            acc = fmaf(dts[j], vals[j], acc);
+            if (kMask) accl = fmaf(dts[j], mws[j], accl);
+            else accl += dts[j];
+        }
+        if (!((nx > 0) & (ny > 0) & (nz > 0) & (left > 0))) break;
     }
 }
 
@@ -208,10 +286,12 @@ __device__ __forceinline__ void trace_ray(float3 src, float3 ray, float3 inv, bo
     l = 0.f;
     DdaStart st;
     if (!dda_setup(src, ray, inv, g, st)) return;
+    const bool small = (unsigned long long)g.rx * (unsigned long long)g.ry * (unsigned long long)g.rz < (1ull << 32);
     if (fast2d) {
         dda_walk_xz<VoxT, kMask>(st, g, vol, mask, v, l);
     } else if (isfinite(st.sd.x) && isfinite(st.sd.y) && isfinite(st.sd.z)) {
-        dda_walk3<VoxT, kMask, false>(st, g, vol, mask, v, l);
+        if (small) dda_walk3_fast<VoxT, kMask, unsigned>(st, g, vol, mask, v, l);
+        else dda_walk3_fast<VoxT, kMask, unsigned long long>(st, g, vol, mask, v, l);
     } else {
         dda_walk3<VoxT, kMask, true>(st, g, vol, mask, v, l);
     }
@@ -328,35 +408,37 @@ __global__ void __launch_bounds__(128) forward_project_kernel(const __grid_const
         }
     }
     if (a.mode == kFpPairResidual && a.resid_sq) {
-        // FP64 block reduction of the squared residuals, one atomic per block.
+        // FP64 warp reduction of the squared residuals, one atomic per warp (no block barrier,
+        // so warps whose rays finish early do not wait for the others).
         for (int o = 16; o > 0; o >>= 1) r2 += __shfl_down_sync(0xffffffffu, r2, o);
-        __shared__ double part[4];
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-        if (lane == 0) part[warp] = r2;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double s = 0.0;
-            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += part[w];
-            atomicAdd(a.resid_sq, s);
-        }
+        if ((threadIdx.x & 31) == 0 && r2 != 0.0) atomicAdd(a.resid_sq, r2);
     }
 }
 
 // ---------------------------------------------------------------- back projection
+// Residual / ray-length sampling of the back projector.
+//   kSampleQ8:      bilinear with weights rounded (half up) to 1/256 and FP32 arithmetic --
+//                   the GPU image path of the reference (BackProjectionKernel.cpp:146-163,
+//                   CL_FILTER_LINEAR), which its golden volumes pin
+//   kSampleExact:   FP32 weights, the reference's buffer path (ImageHandler.hl:20-40)
+//   kSampleTexture: this GPU's texture unit (fast, but its FP32 filtering deviates from the
+//                   reference's by ~1e-3 relative, so it is opt-in)
+enum Sampling : int { kSampleQ8 = 0, kSampleExact = 1, kSampleTexture = 2 };
+
 struct BpArgs {
     void* vol;                     // FP32 master / FP32 volume / half volume (sub-volume base)
     void* shadow;                  // 16-bit shadow written after the block (or nullptr)
     const uint8_t* mask;
     SlabConst slab;
-    const ViewConst* views;
+    const ViewConst* views;        // view table by view id (nullptr: inline_view)
     ViewConst inline_view;
     const uint32_t* order;
     uint32_t first;
     int nviews;                    // views of the block, applied in order
-    const cudaTextureObject_t* texs;  // per slot, float2 (residual, length), linear filter, border 0
+    const float2* rl;              // slot p: interleaved (residual, length) at rl + p * rl_slot
+    size_t rl_pitch, rl_slot;      // float2 units
+    const cudaTextureObject_t* texs;  // per slot (kSampleTexture)
     cudaTextureObject_t inline_tex;
-    const float2* rl;              // exact sampling source
-    size_t rl_pitch, rl_slot;
     int W, H;
     float lambda;                  // lambda / blockSize (BackProjectionKernel.cpp:94)
     const float4* samples;         // parallel: per view id, nsamples (x, y, z, chord); nullptr -> inline
@@ -367,123 +449,260 @@ struct BpArgs {
     float vmin, vmax;
 };
 
-__device__ __forceinline__ float2 sample_exact(const float2* __restrict__ img, size_t pitch, int W, int H, float u,
-                                               float v) {
-    // ImageHandler.hl:20-40 (buffer path): fract(c - 0.5), zero outside, mix in x then y.
-    float xb = floorf(fsub(u, 0.5f)), yb = floorf(fsub(v, 0.5f));
-    float ax = fminf(fsub(fsub(u, 0.5f), xb), 0x1.fffffep-1f), ay = fminf(fsub(fsub(v, 0.5f), yb), 0x1.fffffep-1f);
-    int x0 = (int)xb, y0 = (int)yb;
-    float2 r0 = make_float2(0.f, 0.f), r1 = make_float2(0.f, 0.f);
-    auto texel = [&](int x, int y) -> float2 {
-        return (x >= 0 && x < W) ? __ldg(img + (size_t)y * pitch + (size_t)x) : make_float2(0.f, 0.f);
-    };
-    if (y0 >= 0 && y0 < H) {
-        float2 p = texel(x0, y0), q = texel(x0 + 1, y0);
-        r0 = make_float2(fadd(p.x, fmul(fsub(q.x, p.x), ax)), fadd(p.y, fmul(fsub(q.y, p.y), ax)));
-    }
-    if (y0 + 1 >= 0 && y0 + 1 < H) {
-        float2 p = texel(x0, y0 + 1), q = texel(x0 + 1, y0 + 1);
-        r1 = make_float2(fadd(p.x, fmul(fsub(q.x, p.x), ax)), fadd(p.y, fmul(fsub(q.y, p.y), ax)));
-    }
-    return make_float2(fadd(r0.x, fmul(fsub(r1.x, r0.x), ay)), fadd(r0.y, fmul(fsub(r1.y, r0.y), ay)));
+// Per-view constants staged in shared memory by every back-projection block.
+struct BpView {
+    float mu[4], mv[4], mw[4];     // matrix rows: (m0, m4, m8, m12), (m1, m5, m9, m13), (m3, m7, m11, m15)
+    float src[3];
+    int affine;                    // mw == (0, 0, 0, 1): the divide by w is the identity
+    cudaTextureObject_t tex;
+};
+
+__host__ __device__ constexpr size_t bp_smem_bytes(int nviews, int nsamples) {
+    return ((size_t)nviews * sizeof(BpView) + 15) / 16 * 16 + (size_t)nviews * (size_t)nsamples * sizeof(float4);
 }
 
-__device__ __forceinline__ void project_point(const float* m, float px, float py, float pz, float& u, float& v) {
-    // Matrix4x4.hl:38-58 MultiplyG + TransformCoordG
-    float x = fadd(fadd(fadd(fmul(m[0], px), fmul(m[4], py)), fmul(m[8], pz)), m[12]);
-    float y = fadd(fadd(fadd(fmul(m[1], px), fmul(m[5], py)), fmul(m[9], pz)), m[13]);
-    float w = fadd(fadd(fadd(fmul(m[3], px), fmul(m[7], py)), fmul(m[11], pz)), m[15]);
-    u = fdiv(x, w);
-    v = fdiv(y, w);
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// a / b to within one ulp: reciprocal estimate, one Newton correction of the quotient.
+__device__ __forceinline__ float div_fast(float a, float b) {
+    const float r = rcp_approx(b);
+    const float q = a * r;
+    const float e = fmaf(-b, q, a);
+    return fmaf(e, r, q);
+}
+
+template <int kSampling>
+__device__ __forceinline__ float2 sample_pair(const float2* __restrict__ img, size_t pitch, int W, int H,
+                                              cudaTextureObject_t tex, float u, float v) {
+    if (kSampling == kSampleTexture) return tex2D<float2>(tex, u, v);
+    const float xs = fsub(u, 0.5f), ys = fsub(v, 0.5f);
+    const float xb = floorf(xs), yb = floorf(ys);
+    float a = fminf(fsub(xs, xb), 0x1.fffffep-1f), b = fminf(fsub(ys, yb), 0x1.fffffep-1f);
+    const int x0 = (int)xb, y0 = (int)yb;
+    const bool in_x0 = (unsigned)x0 < (unsigned)W, in_x1 = (unsigned)(x0 + 1) < (unsigned)W;
+    const bool in_y0 = (unsigned)y0 < (unsigned)H, in_y1 = (unsigned)(y0 + 1) < (unsigned)H;
+    const float2 zero = make_float2(0.f, 0.f);
+    const float2* r0 = img + (size_t)y0 * pitch + x0;
+    const float2* r1 = r0 + pitch;
+    const float2 t00 = (in_y0 && in_x0) ? __ldg(r0) : zero;
+    const float2 t10 = (in_y0 && in_x1) ? __ldg(r0 + 1) : zero;
+    const float2 t01 = (in_y1 && in_x0) ? __ldg(r1) : zero;
+    const float2 t11 = (in_y1 && in_x1) ? __ldg(r1 + 1) : zero;
+    if (kSampling == kSampleQ8) {
+        a = fmul(floorf(fadd(fmul(a, 256.f), 0.5f)), 1.f / 256.f);
+        b = fmul(floorf(fadd(fmul(b, 256.f), 0.5f)), 1.f / 256.f);
+        const float w00 = fmul(fsub(1.f, a), fsub(1.f, b)), w10 = fmul(a, fsub(1.f, b));
+        const float w01 = fmul(fsub(1.f, a), b), w11 = fmul(a, b);
+        return make_float2(
+            fadd(fadd(fadd(fmul(w00, t00.x), fmul(w10, t10.x)), fmul(w01, t01.x)), fmul(w11, t11.x)),
+            fadd(fadd(fadd(fmul(w00, t00.y), fmul(w10, t10.y)), fmul(w01, t01.y)), fmul(w11, t11.y)));
+    }
+    // ImageHandler.hl:20-40: mix along x inside each row, then along y; absent rows are 0
+    float2 p0 = zero, p1 = zero;
+    if (in_y0) p0 = make_float2(fadd(t00.x, fmul(fsub(t10.x, t00.x), a)), fadd(t00.y, fmul(fsub(t10.y, t00.y), a)));
+    if (in_y1) p1 = make_float2(fadd(t01.x, fmul(fsub(t11.x, t01.x), a)), fadd(t01.y, fmul(fsub(t11.y, t01.y), a)));
+    return make_float2(fadd(p0.x, fmul(fsub(p1.x, p0.x), b)), fadd(p0.y, fmul(fsub(p1.y, p0.y), b)));
+}
+
+// Stages the block's view constants (and parallel sample patterns) in shared memory.
+__device__ __forceinline__ void bp_stage(const BpArgs& a, BpView* sv, float4* ss, bool parallel) {
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x, nt = blockDim.x * blockDim.y;
+    for (int p = tid; p < a.nviews; p += nt) {
+        const uint32_t vid = a.order ? a.order[a.first + p] : (a.first + p);
+        const ViewConst& vc = a.views ? a.views[vid] : a.inline_view;
+        BpView v;
+        v.mu[0] = vc.mat[0]; v.mu[1] = vc.mat[4]; v.mu[2] = vc.mat[8]; v.mu[3] = vc.mat[12];
+        v.mv[0] = vc.mat[1]; v.mv[1] = vc.mat[5]; v.mv[2] = vc.mat[9]; v.mv[3] = vc.mat[13];
+        v.mw[0] = vc.mat[3]; v.mw[1] = vc.mat[7]; v.mw[2] = vc.mat[11]; v.mw[3] = vc.mat[15];
+        v.src[0] = vc.source.x; v.src[1] = vc.source.y; v.src[2] = vc.source.z;
+        v.affine = (v.mw[0] == 0.f && v.mw[1] == 0.f && v.mw[2] == 0.f && v.mw[3] == 1.f) ? 1 : 0;
+        v.tex = a.texs ? a.texs[p] : a.inline_tex;
+        sv[p] = v;
+    }
+    if (parallel) {
+        const int ns = a.nsamples;
+        for (int i = tid; i < a.nviews * ns; i += nt) {
+            const int p = i / ns, k = i - p * ns;
+            const uint32_t vid = a.order ? a.order[a.first + p] : (a.first + p);
+            ss[i] = a.samples ? a.samples[(size_t)vid * ns + k] : a.inline_samples[k];
+        }
+    }
+    __syncthreads();
+}
+
+template <int kStore>
+__device__ __forceinline__ float bp_load(const BpArgs& a, size_t idx) {
+    if (kStore == 1) return __half2float(((const __half*)a.vol)[idx]);
+    return ((const float*)a.vol)[idx];
+}
+
+template <int kStore>
+__device__ __forceinline__ void bp_store(const BpArgs& a, size_t idx, float val) {
+    if (kStore == 1) ((__half*)a.vol)[idx] = __float2half_rn(val);
+    else ((float*)a.vol)[idx] = val;
+    if (kStore == 2) ((__half*)a.shadow)[idx] = __float2half_rn(val);
+    if (kStore == 3) ((__nv_bfloat16*)a.shadow)[idx] = __float2bfloat16_rn(val);
+}
+
+constexpr int kBpZ = 8;  // voxels per thread along z (parallel)
+constexpr int kBpZPersp = 4;
+
+// ParallelBeamsBackProjection.cl:9-52.  Each thread owns kBpZ voxels of one (x, y)
+// column and applies the block's views to them in order (no atomics); the view
+// constants come from shared memory, the projected coordinates are evaluated in
+// the reference's operation order with the z-independent part hoisted.
+// Storage kStore: 0 FP32 volume, 1 half volume re-rounded after every view
+// (reference half mode), 2 FP32 master + half shadow, 3 FP32 master + bf16 shadow.
+template <bool kMask, int kStore, int kSampling>
+__global__ void __launch_bounds__(256) bp_parallel_kernel(const __grid_constant__ BpArgs a) {
+    extern __shared__ __align__(16) unsigned char bp_smem[];
+    BpView* sv = (BpView*)bp_smem;
+    float4* ss = (float4*)(bp_smem + ((size_t)a.nviews * sizeof(BpView) + 15) / 16 * 16);
+    bp_stage(a, sv, ss, true);
+    const SlabConst& g = a.slab;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int z0 = blockIdx.z * kBpZ;
+    if (x >= g.rx || y >= g.ry) return;
+    const int nzc = min(kBpZ, g.rz - z0);
+    const size_t plane = (size_t)g.rx * (size_t)g.ry;
+    const size_t base = (size_t)z0 * plane + (size_t)y * (size_t)g.rx + (size_t)x;
+    float val[kBpZ], mwt[kBpZ], cz[kBpZ];
+#pragma unroll
+    for (int j = 0; j < kBpZ; ++j) {
+        val[j] = 0.f;
+        mwt[j] = 1.f;
+        cz[j] = fadd(g.bmin.z, fmul(fadd((float)(z0 + j), 0.5f), g.vs.z));  // VolumeGeometry.hl:17-20
+        if (j < nzc) {
+            val[j] = bp_load<kStore>(a, base + (size_t)j * plane);
+            if (kMask) mwt[j] = mask_weight(a.mask + base + (size_t)j * plane);
+        }
+    }
+    const float cx = fadd(g.bmin.x, fmul(fadd((float)x, 0.5f), g.vs.x));
+    const float cy = fadd(g.bmin.y, fmul(fadd((float)y, 0.5f), g.vs.y));
+    const int ns = a.nsamples;
+    for (int p = 0; p < a.nviews; ++p) {
+        const BpView& V = sv[p];
+        const float2* img = a.rl + (size_t)p * a.rl_slot;
+        float pv[kBpZ];
+        unsigned used[kBpZ];
+#pragma unroll
+        for (int j = 0; j < kBpZ; ++j) {
+            pv[j] = 0.f;
+            used[j] = 0;
+        }
+        for (int k = 0; k < ns; ++k) {
+            const float4 s = ss[p * ns + k];
+            const float px = fadd(cx, s.x), py = fadd(cy, s.y);
+            const float au = fadd(fmul(V.mu[0], px), fmul(V.mu[1], py));
+            const float av = fadd(fmul(V.mv[0], px), fmul(V.mv[1], py));
+            const float aw = fadd(fmul(V.mw[0], px), fmul(V.mw[1], py));
+#pragma unroll
+            for (int j = 0; j < kBpZ; ++j) {
+                if (j < nzc) {
+                    const float pz = fadd(cz[j], s.z);
+                    float u = fadd(fadd(au, fmul(V.mu[2], pz)), V.mu[3]);
+                    float v = fadd(fadd(av, fmul(V.mv[2], pz)), V.mv[3]);
+                    if (!V.affine) {  // Matrix4x4.hl:54-58 divide by w
+                        const float w = fadd(fadd(aw, fmul(V.mw[2], pz)), V.mw[3]);
+                        u = fdiv(u, w);
+                        v = fdiv(v, w);
+                    }
+                    const float2 rl = sample_pair<kSampling>(img, a.rl_pitch, a.W, a.H, V.tex, u, v);
+                    const float contrib = fmul(fmul(rl.x, a.lambda), div_fast(s.w, rl.y));
+                    if (rl.y > kEps) {
+                        pv[j] = fadd(pv[j], contrib);
+                        used[j] += 1;
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kBpZ; ++j) {
+            if (used[j] != 0) {
+                const float num = fmul(mwt[j], pv[j]);
+                val[j] = fadd(val[j], used[j] == 1 ? num : div_fast(num, (float)used[j]));
+            }
+            if (kStore == 1) val[j] = __half2float(__float2half_rn(val[j]));  // vstore_half after every view
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < kBpZ; ++j)
+        if (j < nzc) bp_store<kStore>(a, base + (size_t)j * plane, val[j]);
 }
 
 // PerspectiveBeamsBackProjection.cl:10-17 getRayLengthInVoxel
 __device__ __forceinline__ float chord_in_voxel(float3 o, float3 dir, float3 c, float3 vs) {
     float3 bmin = make_float3(fsub(c.x, fmul(0.5f, vs.x)), fsub(c.y, fmul(0.5f, vs.y)), fsub(c.z, fmul(0.5f, vs.z)));
     float3 bmax = make_float3(fadd(c.x, fmul(0.5f, vs.x)), fadd(c.y, fmul(0.5f, vs.y)), fadd(c.z, fmul(0.5f, vs.z)));
-    float n = __fsqrt_rn(fadd(fadd(fmul(dir.x, dir.x), fmul(dir.y, dir.y)), fmul(dir.z, dir.z)));
-    float3 inv = make_float3(fdiv(1.f, fdiv(dir.x, n)), fdiv(1.f, fdiv(dir.y, n)), fdiv(1.f, fdiv(dir.z, n)));
+    const float n = __fsqrt_rn(fadd(fadd(fmul(dir.x, dir.x), fmul(dir.y, dir.y)), fmul(dir.z, dir.z)));
+    // 1 / normalize(dir) = |dir| / dir
+    float3 inv = make_float3(div_fast(n, dir.x), div_fast(n, dir.y), div_fast(n, dir.z));
     float tin, tout;
     slab_test(bmin, bmax, o, inv, tin, tout);
     return fmaxf(0.f, fsub(tout, tin));
 }
 
-// Storage of the updated volume: kStore = 0 FP32 volume, 1 half volume
-// re-rounded after every view (reference half mode), 2 FP32 master + half
-// shadow, 3 FP32 master + bf16 shadow.
-template <bool kPerspective, bool kMask, int kStore, bool kExact>
-__global__ void __launch_bounds__(256) back_project_kernel(const __grid_constant__ BpArgs a) {
+// PerspectiveBeamsBackProjection.cl:28-71: n^3 sub-voxel samples, each weighted by
+// its own chord through the voxel; optional intensity clamps.
+template <bool kMask, int kStore, int kSampling>
+__global__ void __launch_bounds__(256) bp_perspective_kernel(const __grid_constant__ BpArgs a) {
+    extern __shared__ __align__(16) unsigned char bp_smem[];
+    BpView* sv = (BpView*)bp_smem;
+    bp_stage(a, sv, nullptr, false);
+    const SlabConst& g = a.slab;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int z = blockIdx.z;
-    const SlabConst& g = a.slab;
-    if (x >= g.rx || y >= g.ry || z >= g.rz) return;
-    const size_t idx = ((size_t)z * (size_t)g.ry + (size_t)y) * (size_t)g.rx + (size_t)x;
-    // VolumeGeometry.hl:17-20 GetVoxelCenter
+    const int z0 = blockIdx.z * kBpZPersp;
+    if (x >= g.rx || y >= g.ry) return;
+    const int nzc = min(kBpZPersp, g.rz - z0);
+    const size_t plane = (size_t)g.rx * (size_t)g.ry;
+    const size_t base = (size_t)z0 * plane + (size_t)y * (size_t)g.rx + (size_t)x;
+    const int n = a.persp_n;
+    const unsigned count = (unsigned)(n * n * n);
+    const float3 vs = make_float3(g.vs.x, g.vs.y, g.vs.z);
     const float cx = fadd(g.bmin.x, fmul(fadd((float)x, 0.5f), g.vs.x));
     const float cy = fadd(g.bmin.y, fmul(fadd((float)y, 0.5f), g.vs.y));
-    const float cz = fadd(g.bmin.z, fmul(fadd((float)z, 0.5f), g.vs.z));
-    float val;
-    if (kStore == 1) val = __half2float(((const __half*)a.vol)[idx]);
-    else val = ((const float*)a.vol)[idx];
-    const float mw = kMask ? mask_weight(a.mask + idx) : 1.f;
-
-    for (int p = 0; p < a.nviews; ++p) {
-        const uint32_t vid = a.order ? a.order[a.first + p] : (a.first + p);
-        const ViewConst& vc = a.views ? a.views[vid] : a.inline_view;
-        const cudaTextureObject_t tex = a.texs ? a.texs[p] : a.inline_tex;
-        const float2* img = a.rl + (size_t)p * a.rl_slot;
-        if (!kPerspective) {
-            // ParallelBeamsBackProjection.cl:26-51
-            const float4* smp = a.samples ? a.samples + (size_t)vid * (size_t)a.nsamples : a.inline_samples;
-            float pv = 0.f;
-            unsigned used = 0;
-            for (int k = 0; k < a.nsamples; ++k) {
-                const float4 s = smp[k];
-                float u, v;
-                project_point(vc.mat, fadd(cx, s.x), fadd(cy, s.y), fadd(cz, s.z), u, v);
-                float2 rl = kExact ? sample_exact(img, a.rl_pitch, a.W, a.H, u, v) : tex2D<float2>(tex, u, v);
-                float w = fdiv(s.w, rl.y);
-                float contrib = fmul(fmul(rl.x, a.lambda), w);
-                if (rl.y > kEps) {
-                    pv = fadd(pv, contrib);
-                    used += 1;
-                }
-            }
-            if (used != 0) val = fadd(val, fdiv(fmul(mw, pv), (float)used));
-        } else {
-            // PerspectiveBeamsBackProjection.cl:42-69
-            const int n = a.persp_n;
-            const unsigned count = (unsigned)(n * n * n);
+    for (int j = 0; j < nzc; ++j) {
+        const size_t idx = base + (size_t)j * plane;
+        const float cz = fadd(g.bmin.z, fmul(fadd((float)(z0 + j), 0.5f), g.vs.z));
+        const float3 c = make_float3(cx, cy, cz);
+        const float bxv = fsub(cx, fmul(0.5f, g.vs.x)), byv = fsub(cy, fmul(0.5f, g.vs.y)),
+                    bzv = fsub(cz, fmul(0.5f, g.vs.z));
+        float val = bp_load<kStore>(a, idx);
+        const float mw = kMask ? mask_weight(a.mask + idx) : 1.f;
+        for (int p = 0; p < a.nviews; ++p) {
+            const BpView& V = sv[p];
+            const float2* img = a.rl + (size_t)p * a.rl_slot;
             float value = 0.f;
-            const float3 c = make_float3(cx, cy, cz);
-            const float3 vs = make_float3(g.vs.x, g.vs.y, g.vs.z);
-            const float bxv = fsub(cx, fmul(0.5f, g.vs.x)), byv = fsub(cy, fmul(0.5f, g.vs.y)),
-                        bzv = fsub(cz, fmul(0.5f, g.vs.z));
             for (unsigned k = 0; k < count; ++k) {
-                unsigned dx = k % (unsigned)n, dy = (k / (unsigned)n) % (unsigned)n, dz = k / (unsigned)(n * n);
-                float px = fadd(bxv, fdiv(fmul(g.vs.x, fadd((float)dx, 0.5f)), (float)n));
-                float py = fadd(byv, fdiv(fmul(g.vs.y, fadd((float)dy, 0.5f)), (float)n));
-                float pz = fadd(bzv, fdiv(fmul(g.vs.z, fadd((float)dz, 0.5f)), (float)n));
-                float u, v;
-                project_point(vc.mat, px, py, pz, u, v);
-                float2 rl = kExact ? sample_exact(img, a.rl_pitch, a.W, a.H, u, v) : tex2D<float2>(tex, u, v);
+                const unsigned dx = k % (unsigned)n, dy = (k / (unsigned)n) % (unsigned)n, dz = k / (unsigned)(n * n);
+                const float px = fadd(bxv, fdiv(fmul(g.vs.x, fadd((float)dx, 0.5f)), (float)n));
+                const float py = fadd(byv, fdiv(fmul(g.vs.y, fadd((float)dy, 0.5f)), (float)n));
+                const float pz = fadd(bzv, fdiv(fmul(g.vs.z, fadd((float)dz, 0.5f)), (float)n));
+                float u = fadd(fadd(fadd(fmul(V.mu[0], px), fmul(V.mu[1], py)), fmul(V.mu[2], pz)), V.mu[3]);
+                float v = fadd(fadd(fadd(fmul(V.mv[0], px), fmul(V.mv[1], py)), fmul(V.mv[2], pz)), V.mv[3]);
+                const float w = fadd(fadd(fadd(fmul(V.mw[0], px), fmul(V.mw[1], py)), fmul(V.mw[2], pz)), V.mw[3]);
+                u = div_fast(u, w);
+                v = div_fast(v, w);
+                const float2 rl = sample_pair<kSampling>(img, a.rl_pitch, a.W, a.H, V.tex, u, v);
                 if (rl.y >= kEps) {
-                    float3 dir = make_float3(fsub(px, vc.source.x), fsub(py, vc.source.y), fsub(pz, vc.source.z));
-                    float l = chord_in_voxel(make_float3(px, py, pz), dir, c, vs);
-                    value = fadd(value, fdiv(fmul(rl.x, l), rl.y));
+                    const float3 dir = make_float3(fsub(px, V.src[0]), fsub(py, V.src[1]), fsub(pz, V.src[2]));
+                    const float l = chord_in_voxel(make_float3(px, py, pz), dir, c, vs);
+                    value = fadd(value, div_fast(fmul(rl.x, l), rl.y));
                 }
             }
-            val = fadd(val, fdiv(fmul(fmul(a.lambda, value), mw), (float)count));
+            val = fadd(val, div_fast(fmul(fmul(a.lambda, value), mw), (float)count));
             if (a.use_min) val = fmaxf(a.vmin, val);
             if (a.use_max) val = fminf(a.vmax, val);
+            if (kStore == 1) val = __half2float(__float2half_rn(val));
         }
-        if (kStore == 1) val = __half2float(__float2half_rn(val));  // vstore_half after every view
+        bp_store<kStore>(a, idx, val);
     }
-    if (kStore == 1) ((__half*)a.vol)[idx] = __float2half_rn(val);
-    else ((float*)a.vol)[idx] = val;
-    if (kStore == 2) ((__half*)a.shadow)[idx] = __float2half_rn(val);
-    if (kStore == 3) ((__nv_bfloat16*)a.shadow)[idx] = __float2bfloat16_rn(val);
 }
 
 // ---------------------------------------------------------------- small kernels

@@ -291,7 +291,7 @@ class BackProjectionOperator:
     ALL_SUB_VOLUMES = _abi.ALL_SUBVOLUMES
 
     def __init__(self, volume: GPUMappedVolume, lam: float, samples: int = 1,
-                 sampling: int = _abi.SAMPLING_TEXTURE):
+                 sampling: int = _abi.SAMPLING_Q8):
         self.volume = volume
         self.lam = float(lam)
         self.samples = int(samples)
@@ -368,7 +368,7 @@ class AlgebraicParameterSet:
     xaxis_tilt: float = 0.0
     vmin: Optional[float] = None
     vmax: Optional[float] = None
-    sampling: int = _abi.SAMPLING_TEXTURE
+    sampling: int = _abi.SAMPLING_Q8
 
     @classmethod
     def from_config(cls, cfg: Dict[str, str]) -> "AlgebraicParameterSet":

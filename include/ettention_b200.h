@@ -60,11 +60,15 @@ typedef enum {
 } etcu_voxel_type;
 
 /* Bilinear sampling of residual / ray-length images in back projection.
- * TEXTURE: GPU texture filtering (1/256 weights), the reference's image path
- *          (LR/algorithm/projections/back/BackProjectionKernel.cpp:146-163).
- * EXACT:   FP32 weights, the reference's buffer path
- *          (ettention/libReconstruction/ocl_src/ImageHandler.hl:20-40). */
-typedef enum { ETCU_SAMPLING_TEXTURE = 0, ETCU_SAMPLING_EXACT = 1 } etcu_sampling;
+ * Q8:         software bilinear with weights rounded (half up) to 1/256 and FP32
+ *             arithmetic: the GPU image path of the reference
+ *             (LR/algorithm/projections/back/BackProjectionKernel.cpp:146-163,
+ *             CL_FILTER_LINEAR), which its golden volumes pin.  Default.
+ * EXACT:      FP32 weights, the reference's buffer path
+ *             (ettention/libReconstruction/ocl_src/ImageHandler.hl:20-40).
+ * HW_TEXTURE: this GPU's texture unit; its FP32 filtering deviates from the
+ *             reference's by ~1e-3 relative, so it is opt-in. */
+typedef enum { ETCU_SAMPLING_Q8 = 0, ETCU_SAMPLING_EXACT = 1, ETCU_SAMPLING_HW_TEXTURE = 2 } etcu_sampling;
 
 /* Projection iteration order, optimization.projectionIteration
  * (LR/model/projectionset/factory/ProjectionIteratorFactory.cpp:11-22). */

@@ -214,7 +214,7 @@ def test_bp_parallel_vs_oracle(torch, ctx, angle, samples, sampling):
     from oracle import oracle as O
     from ettention_b200.operators import mrc_base_geometry
     from tests.helpers import oracle_geometry
-    rng = np.random.Generator(np.random.PCG64(int(angle * 10) + samples))
+    rng = np.random.Generator(np.random.PCG64(abs(int(angle * 10)) + samples))
     g = mrc_base_geometry(96, 80).rotated(angle)
     og = oracle_geometry(g)
     vg = O.VolumeGeometry.centered((96, 80, 40))
@@ -365,7 +365,9 @@ def test_recon_graph_equals_stream_and_residual_decreases(ctx, c1):
     p = AlgebraicParameterSet(algorithm="sart", block_size=1, iterations=3, lam=0.3, order=_abi.ORDER_IDENTITY)
     a, la, da, _ = run_cuda_recon(ctx, geoms, projs, (128, 128, 64), p, 3, use_graph=True)
     b, lb, db, _ = run_cuda_recon(ctx, geoms, projs, (128, 128, 64), p, 3, use_graph=False)
-    assert np.array_equal(a, b) and la == lb and da == db
+    assert np.array_equal(a, b)
+    # FP64 sums reduced with atomics: equal up to summation order
+    assert abs(la - lb) <= 1e-12 * la and abs(da - db) <= 1e-12 * da
     _, _, d1, _ = run_cuda_recon(ctx, geoms, projs, (128, 128, 64), p, 1)
     assert da < d1
     b2 = float(np.sum(projs.astype(np.float64) ** 2))
