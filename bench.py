@@ -56,6 +56,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-reps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ncu-case", action="store_true",
+                    help="small profiling case for ncu: 512x512x256 volume, 8 views, one SART iteration "
+                         "launched kernel by kernel (8 forward + 8 back projections), then per-kernel times")
     return ap.parse_args()
 
 
@@ -387,8 +390,33 @@ def run_ours(args, rank, world, local):
     ctx.close()
 
 
+def run_ncu_case():
+    """A case small enough for an ncu capture (256 MB volume, larger than L2)."""
+    from ettention_b200 import _abi
+    from ettention_b200.operators import (AlgebraicParameterSet, BlockIterativeReconstructionOperator, Context,
+                                          GPUMappedVolume, mrc_base_geometry)
+    X, Y, Z = 512, 512, 256
+    ctx = Context(0)
+    rng = np.random.Generator(np.random.PCG64(0))
+    vol = GPUMappedVolume(ctx, (X, Y, Z))
+    vol.upload(rng.uniform(0, 0.01, (Z, Y, X)).astype(np.float32))
+    geoms = [mrc_base_geometry(X, Y).rotated(float(a)) for a in np.linspace(-60, 60, 8)]
+    projs = rng.uniform(0, 3, (8, Y, X)).astype(np.float32)
+    p = AlgebraicParameterSet(algorithm="sart", block_size=1, iterations=1, lam=LAMBDA, order=_abi.ORDER_IDENTITY)
+    rec = BlockIterativeReconstructionOperator(vol, geoms, projs, p, use_graph=False)
+    rec.runNiterations(1)
+    f, b, nf, nb = rec.profile_iteration()
+    print(json.dumps({"ncu_case": "512x512x256 f32, 8 views, SART", "forward_ms": f / nf, "back_ms": b / nb}))
+    rec.close()
+    vol.close()
+    ctx.close()
+
+
 def main():
     args = parse()
+    if args.ncu_case:
+        run_ncu_case()
+        return
     rank, world, local = dist_init()
     try:
         if args.impl == "reference":
