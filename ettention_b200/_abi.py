@@ -18,6 +18,7 @@ VOXEL_FLOAT32, VOXEL_HALF16, VOXEL_F16_MASTER, VOXEL_BF16_MASTER = 0, 1, 2, 3
 SAMPLING_Q8, SAMPLING_EXACT, SAMPLING_HW_TEXTURE = 0, 1, 2
 ORDER_IDENTITY, ORDER_RANDOM, ORDER_MAXANGLE, ORDER_BUCKETS = 0, 1, 2, 3
 ALL_SUBVOLUMES = 0xFFFFFFFF
+NOALLOC_MAX_PIXELS = 1024 * 1024
 BLOCK_ALL = 0xFFFFFFFF
 
 
@@ -94,6 +95,8 @@ _SIG = {
     "etcu_reconstruct": (_S, [_P, ctypes.POINTER(VolumeDesc), _I, ctypes.POINTER(View), _U, _P,
                               ctypes.POINTER(ReconParams), _U, _P]),
     "etcu_projection_order": (_S, [_I, _U, _P, _U, _P, ctypes.POINTER(_U)]),
+    "etcu_sart_view_update_noalloc": (_S, [ctypes.POINTER(VolumeDesc), _P, _P, ctypes.POINTER(View), _U, _U, _F, _P,
+                                           ctypes.POINTER(ctypes.c_double)]),
 }
 
 

@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1140,4 +1141,170 @@ extern "C" etcu_status etcu_reconstruct(etcu_context* ctx, const etcu_volume_des
     etcu_recon_destroy(rec);
     etcu_volume_destroy(vol);
     return s;
+}
+
+// =============================================================== allocation-free view update
+// Scratch of etcu_sart_view_update_noalloc: one interleaved (residual, length)
+// image and the FP64 residual accumulator, in static device memory.
+static __device__ __align__(256) float2 g_noalloc_pairs[ETCU_NOALLOC_MAX_PIXELS];
+static __device__ __align__(256) double g_noalloc_resid[1];
+
+namespace {
+struct NoAllocScratch {
+    float2* pairs = nullptr;
+    double* resid = nullptr;
+    bool ready = false;
+};
+NoAllocScratch g_noalloc[64];
+std::mutex g_noalloc_mutex;
+thread_local std::string g_noalloc_error;
+
+etcu_status noalloc_fail(etcu_status st, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_noalloc_error = buf;
+    g_create_error = buf;  // readable through etcu_last_error(NULL)
+    return st;
+}
+
+// Device addresses of the static scratch for the current device (looked up once).
+etcu_status noalloc_scratch(int dev, NoAllocScratch& out) {
+    if (dev < 0 || dev >= 64) return noalloc_fail(ETCU_ERR_UNSUPPORTED, "device %d out of range", dev);
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    NoAllocScratch& s = g_noalloc[dev];
+    if (!s.ready) {
+        cudaError_t e = cudaGetSymbolAddress((void**)&s.pairs, g_noalloc_pairs);
+        if (e != cudaSuccess)
+            return noalloc_fail(ETCU_ERR_CUDA, "cudaGetSymbolAddress(scratch image) failed: %s", cudaGetErrorString(e));
+        e = cudaGetSymbolAddress((void**)&s.resid, g_noalloc_resid);
+        if (e != cudaSuccess)
+            return noalloc_fail(ETCU_ERR_CUDA, "cudaGetSymbolAddress(residual) failed: %s", cudaGetErrorString(e));
+        s.ready = true;
+    }
+    out = s;
+    return ETCU_OK;
+}
+}  // namespace
+
+extern "C" etcu_status etcu_sart_view_update_noalloc(const etcu_volume_desc* desc, float* d_volume,
+                                                     const float* d_projection, const etcu_view* view,
+                                                     uint32_t fp_samples, uint32_t bp_samples, float lambda,
+                                                     void* cuda_stream, double* residual_sq) {
+    if (!desc || !d_volume || !d_projection || !view)
+        return noalloc_fail(ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (desc->subvolume_count > 1)
+        return noalloc_fail(ETCU_ERR_UNSUPPORTED, "the allocation-free update takes a single sub-volume");
+    if (view->width == 0 || view->height == 0)
+        return noalloc_fail(ETCU_ERR_INVALID_ARGUMENT, "projection resolution must be non-zero");
+    if ((uint64_t)view->width * view->height > ETCU_NOALLOC_MAX_PIXELS)
+        return noalloc_fail(ETCU_ERR_INVALID_ARGUMENT,
+                            "detector of %u x %u pixels exceeds the %u-pixel scratch of the allocation-free update",
+                            view->width, view->height, (unsigned)ETCU_NOALLOC_MAX_PIXELS);
+    float mat[16];
+    if (!projection_matrix(*view, mat)) return noalloc_fail(ETCU_ERR_INVALID_ARGUMENT, "matrix not invertible");
+    if (desc->resolution[0] == 0 || desc->resolution[1] == 0 || desc->resolution[2] == 0)
+        return noalloc_fail(ETCU_ERR_INVALID_ARGUMENT, "volume resolution must be non-zero");
+    // the single sub-volume of VolumeProperties::setSubVolumeCount(1)
+    SlabConst slab{};
+    {
+        float vs[3], ivs[3];
+        for (int i = 0; i < 3; ++i) {
+            vs[i] = (desc->bbox_max[i] - desc->bbox_min[i]) / (float)desc->resolution[i];
+            ivs[i] = 1.0f / vs[i];
+        }
+        float smax[3] = {desc->bbox_min[0] + (float)desc->resolution[0] * vs[0],
+                         desc->bbox_min[1] + (float)desc->resolution[1] * vs[1],
+                         desc->bbox_min[2] + (float)desc->resolution[2] * vs[2]};
+        slab.rx = (int)desc->resolution[0];
+        slab.ry = (int)desc->resolution[1];
+        slab.rz = (int)desc->resolution[2];
+        slab.z0 = 0;
+        slab.bmin = f4(desc->bbox_min);
+        slab.bmax = f4(smax);
+        slab.cmin = f4(desc->bbox_min);
+        slab.cmax = f4(desc->bbox_max);
+        slab.vs = f4(vs);
+        slab.ivs = f4(ivs);
+    }
+    std::string err;
+    float4 pattern[kMaxInlineSamples];
+    if (!view->perspective) {
+        if (bp_samples > (uint32_t)kMaxInlineSamples)
+            return noalloc_fail(ETCU_ERR_UNSUPPORTED, "at most %d back-projection samples per voxel", kMaxInlineSamples);
+        float vs[3] = {slab.vs.x, slab.vs.y, slab.vs.z};
+        if (!sample_pattern(*view, vs, bp_samples, (float*)pattern, &err))
+            return noalloc_fail(ETCU_ERR_INVALID_ARGUMENT, "%s", err.c_str());
+    }
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return noalloc_fail(ETCU_ERR_NO_DEVICE, "cudaGetDevice failed: %s", cudaGetErrorString(e));
+    NoAllocScratch sc;
+    etcu_status st = noalloc_scratch(dev, sc);
+    if (st != ETCU_OK) return st;
+    cudaStream_t stream = (cudaStream_t)cuda_stream;
+    const int W = (int)view->width, H = (int)view->height;
+    e = cudaMemsetAsync(sc.resid, 0, sizeof(double), stream);
+    if (e != cudaSuccess) return noalloc_fail(ETCU_ERR_CUDA, "cudaMemsetAsync failed: %s", cudaGetErrorString(e));
+    // forward projection; the single slab overwrites every pixel of the scratch image
+    FpArgs fa{};
+    fa.vol = d_volume;
+    fa.mask = nullptr;
+    fa.slab = slab;
+    fa.views = nullptr;
+    fa.inline_view = make_view_const(*view, slab, 0.f);
+    fa.order = nullptr;
+    fa.first = 0;
+    fa.W = W;
+    fa.H = H;
+    fa.samples = fp_samples == 0 ? 1 : (int)fp_samples;
+    fa.mode = kFpPairResidual;
+    fa.overwrite = 1;
+    fa.loc = 0;
+    fa.rl = sc.pairs;
+    fa.rl_pitch = (size_t)W;
+    fa.rl_slot = (size_t)W * H;
+    fa.real = d_projection;
+    fa.resid_sq = sc.resid;
+    if (view->perspective) launch_fp_t<float, false, true>(fa, 1, stream);
+    else launch_fp_t<float, false, false>(fa, 1, stream);
+    // back projection of the view with lambda / 1
+    BpArgs ba{};
+    ba.vol = d_volume;
+    ba.shadow = nullptr;
+    ba.mask = nullptr;
+    ba.slab = slab;
+    ba.views = nullptr;
+    ba.inline_view = fa.inline_view;
+    ba.order = nullptr;
+    ba.first = 0;
+    ba.nviews = 1;
+    ba.rl = sc.pairs;
+    ba.rl_pitch = (size_t)W;
+    ba.rl_slot = (size_t)W * H;
+    ba.texs = nullptr;
+    ba.inline_tex = 0;
+    ba.W = W;
+    ba.H = H;
+    ba.lambda = lambda;
+    ba.samples = nullptr;
+    if (!view->perspective) {
+        ba.nsamples = (int)bp_samples;
+        for (uint32_t k = 0; k < bp_samples; ++k) ba.inline_samples[k] = pattern[k];
+    } else {
+        uint32_t res[3] = {(uint32_t)slab.rx, (uint32_t)slab.ry, (uint32_t)slab.rz};
+        ba.persp_n = (int)perspective_sampling_factor(view->width, view->height, res, bp_samples);
+    }
+    if (view->perspective) launch_bp_t<true, false, 0, kSampleQ8>(ba, dev, stream);
+    else launch_bp_t<false, false, 0, kSampleQ8>(ba, dev, stream);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return noalloc_fail(ETCU_ERR_CUDA, "launch failed: %s", cudaGetErrorString(e));
+    if (residual_sq) {
+        e = cudaMemcpyAsync(residual_sq, sc.resid, sizeof(double), cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return noalloc_fail(ETCU_ERR_CUDA, "residual read-back failed: %s", cudaGetErrorString(e));
+    }
+    return ETCU_OK;
 }

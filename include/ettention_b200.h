@@ -234,6 +234,29 @@ ETCU_API etcu_status etcu_reconstruct(etcu_context* ctx, const etcu_volume_desc*
                              const etcu_view* views, uint32_t n_views, const float* host_projections,
                              const etcu_recon_params* params, uint32_t iterations, float* host_volume_inout);
 
+/* One SART update of one view (forward projection, residual b - Ax, back projection
+ * with block size 1) that allocates no device memory, for callers that cannot
+ * allocate: hosts whose device memory is reserved up front by their own pool
+ * allocator, or processing loops in which allocation after start-up is not
+ * allowed.  The caller passes the FP32 volume (device pointer, layout as
+ * etcu_volume, one sub-volume), the measured projection of this view (device
+ * pointer, height x width floats) and the stream to run on (NULL: the legacy
+ * default stream).  The (residual, ray length) image lives in a static device
+ * array of ETCU_NOALLOC_MAX_PIXELS float2 (8 MiB) that every GPU loading the
+ * library holds until the process exits; larger detectors are rejected.  The
+ * first call on a device looks up that array's device address, so make the
+ * first call before any stream capture.  All calls share the array and keep
+ * the last call's contents: calls that overlap on the GPU (other streams or
+ * threads on the same device) race and must be serialised by the caller.
+ * residual_sq (optional, host) receives sum (b - Ax)^2 over the view, which
+ * synchronises the stream.  Sampling is ETCU_SAMPLING_Q8.
+ * No counterpart in the reference. */
+#define ETCU_NOALLOC_MAX_PIXELS (1024u * 1024u)
+ETCU_API etcu_status etcu_sart_view_update_noalloc(const etcu_volume_desc* desc, float* d_volume,
+                                                   const float* d_projection, const etcu_view* view,
+                                                   uint32_t fp_samples, uint32_t bp_samples, float lambda,
+                                                   void* cuda_stream, double* residual_sq);
+
 /* Projection orderings on their own (LR/model/projectionset/ProjectionSet*.cpp), for callers
  * that keep their own driver loop. */
 ETCU_API etcu_status etcu_projection_order(etcu_order order, uint32_t n, const uint32_t* skip, uint32_t skip_count,
