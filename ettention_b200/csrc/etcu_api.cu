@@ -31,7 +31,8 @@ struct etcu_context {
     size_t bytes = 0;
     size_t tex_align = 512, tex_pitch_align = 32;
     // scratch of the single-view back projector: interleaved (residual, length) image
-    float2* pair = nullptr;
+    float2* pair = nullptr;  // texel (0, 0) of the padded image
+    float2* pair_base = nullptr;
     void* pair_raw = nullptr;
     size_t pair_pitch = 0;  // float2 units
     uint32_t pair_w = 0, pair_h = 0;
@@ -63,7 +64,8 @@ struct etcu_recon {
     uint32_t* d_order = nullptr;
     float4* d_samples = nullptr;
     uint32_t nsamples = 1;
-    float2* rl = nullptr;
+    float2* rl = nullptr;       // texel (0, 0) of slot 0 (images are padded by kPad zero texels)
+    float2* rl_base = nullptr;  // first byte of slot 0
     void* rl_raw = nullptr;
     size_t rl_pitch = 0, rl_slot = 0;  // float2 units
     uint32_t slots = 0;
@@ -74,6 +76,7 @@ struct etcu_recon {
     cudaGraphExec_t exec = nullptr;
     uint32_t launches = 0;
     bool persp = false;
+    std::vector<int> fp_paths;  // per slab
 };
 
 namespace {
@@ -223,33 +226,45 @@ size_t slab_offset_elems(const etcu_volume* vol, const SlabConst& s) {
 }
 
 // ------------------------------------------------------------- launches
-template <typename VoxT, bool kMask, bool kPersp>
+template <typename VoxT, bool kMask, int kPath>
 void launch_fp_t(const FpArgs& a, uint32_t nviews, cudaStream_t st) {
     dim3 block(128);
     dim3 grid;
-    if (kPersp) grid = dim3((a.W + 15) / 16, (a.H + 7) / 8, nviews);
+    if (kPath == kFpPathPerspective) grid = dim3((a.W + 15) / 16, (a.H + 7) / 8, nviews);
     else grid = dim3((a.W + 127) / 128, a.H, nviews);
-    forward_project_kernel<VoxT, kMask, kPersp><<<grid, block, 0, st>>>(a);
+    forward_project_kernel<VoxT, kMask, kPath><<<grid, block, 0, st>>>(a);
 }
 
-template <typename VoxT>
-void launch_fp_v(const FpArgs& a, bool mask, bool persp, uint32_t nviews, cudaStream_t st) {
-    if (persp) {
-        if (mask) launch_fp_t<VoxT, true, true>(a, nviews, st);
-        else launch_fp_t<VoxT, false, true>(a, nviews, st);
-    } else {
-        if (mask) launch_fp_t<VoxT, true, false>(a, nviews, st);
-        else launch_fp_t<VoxT, false, false>(a, nviews, st);
+template <typename VoxT, bool kMask>
+void launch_fp_m(const FpArgs& a, int path, uint32_t nviews, cudaStream_t st) {
+    switch (path) {
+    case kFpPathXz: launch_fp_t<VoxT, kMask, kFpPathXz>(a, nviews, st); break;
+    case kFpPathXzNoCap: launch_fp_t<VoxT, kMask, kFpPathXzNoCap>(a, nviews, st); break;
+    case kFpPathPerspective: launch_fp_t<VoxT, kMask, kFpPathPerspective>(a, nviews, st); break;
+    default: launch_fp_t<VoxT, kMask, kFpPathGeneral>(a, nviews, st); break;
     }
 }
 
-void launch_fp(const etcu_volume* vol, const FpArgs& a, bool persp, uint32_t nviews, cudaStream_t st) {
+template <typename VoxT>
+void launch_fp_v(const FpArgs& a, bool mask, int path, uint32_t nviews, cudaStream_t st) {
+    if (mask) launch_fp_m<VoxT, true>(a, path, nviews, st);
+    else launch_fp_m<VoxT, false>(a, path, nviews, st);
+}
+
+// Walk specialisation shared by every view of a launch.
+int fp_path(bool persp, bool all_fast2d, const SlabConst& slab) {
+    if (persp) return kFpPathPerspective;
+    if (!all_fast2d) return kFpPathGeneral;
+    return (slab.rx + slab.rz - 1 <= kMaxDdaIterations) ? kFpPathXzNoCap : kFpPathXz;
+}
+
+void launch_fp(const etcu_volume* vol, const FpArgs& a, int path, uint32_t nviews, cudaStream_t st) {
     bool mask = a.mask != nullptr;
     switch (vol->type) {
-    case ETCU_VOXEL_FLOAT32: launch_fp_v<float>(a, mask, persp, nviews, st); break;
+    case ETCU_VOXEL_FLOAT32: launch_fp_v<float>(a, mask, path, nviews, st); break;
     case ETCU_VOXEL_HALF16:
-    case ETCU_VOXEL_F16_MASTER: launch_fp_v<__half>(a, mask, persp, nviews, st); break;
-    case ETCU_VOXEL_BF16_MASTER: launch_fp_v<__nv_bfloat16>(a, mask, persp, nviews, st); break;
+    case ETCU_VOXEL_F16_MASTER: launch_fp_v<__half>(a, mask, path, nviews, st); break;
+    case ETCU_VOXEL_BF16_MASTER: launch_fp_v<__nv_bfloat16>(a, mask, path, nviews, st); break;
     }
 }
 
@@ -266,8 +281,10 @@ void launch_bp_t(const BpArgs& a, int device, cudaStream_t st) {
     }
     const size_t smem = bp_smem_bytes(a.nviews, kPersp ? 0 : a.nsamples);
     const int zc = kPersp ? kBpZPersp : kBpZ;
+    const int zchunks = (a.slab.rz + zc - 1) / zc;
     dim3 block(32, 8, 1);
-    dim3 grid((a.slab.rx + 31) / 32, (a.slab.ry + 7) / 8, (a.slab.rz + zc - 1) / zc);
+    // parallel: each block walks up to 4 z-chunks (grid-stride) to amortise its staging
+    dim3 grid((a.slab.rx + 31) / 32, (a.slab.ry + 7) / 8, kPersp ? zchunks : (zchunks + 3) / 4);
     kern<<<grid, block, smem, st>>>(a);
 }
 
@@ -355,20 +372,25 @@ etcu_status make_pair_texture(etcu_context* ctx, float2* base, size_t pitch_elem
 
 size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
+// Padded (residual, length) image of the single-view back projector: kPad zero
+// texels around the W x H image, texel (0, 0) at `pair`.
 etcu_status ensure_pair_scratch(etcu_context* ctx, uint32_t W, uint32_t H) {
     if (ctx->pair && ctx->pair_w == W && ctx->pair_h == H) return ETCU_OK;
     if (ctx->pair_tex) cudaDestroyTextureObject(ctx->pair_tex);
     ctx->pair_tex = 0;
-    dfree(ctx, ctx->pair_raw, ctx->pair_pitch * sizeof(float2) * ctx->pair_h + ctx->tex_align);
+    dfree(ctx, ctx->pair_raw, ctx->pair_pitch * sizeof(float2) * (ctx->pair_h + 2 * kPad) + ctx->tex_align);
     ctx->pair = nullptr;
     ctx->pair_raw = nullptr;
-    size_t pitch_bytes = round_up((size_t)W * sizeof(float2), ctx->tex_pitch_align);
-    etcu_status s = dalloc_aligned(ctx, &ctx->pair_raw, (void**)&ctx->pair, pitch_bytes * H, ctx->tex_align);
+    const size_t pw = (size_t)W + 2 * kPad, ph = (size_t)H + 2 * kPad;
+    size_t pitch_bytes = round_up(pw * sizeof(float2), ctx->tex_pitch_align);
+    etcu_status s = dalloc_aligned(ctx, &ctx->pair_raw, (void**)&ctx->pair_base, pitch_bytes * ph, ctx->tex_align);
     if (s != ETCU_OK) return s;
+    CK(ctx, cudaMemsetAsync(ctx->pair_base, 0, pitch_bytes * ph, ctx->stream));
     ctx->pair_pitch = pitch_bytes / sizeof(float2);
+    ctx->pair = ctx->pair_base + kPad * ctx->pair_pitch + kPad;
     ctx->pair_w = W;
     ctx->pair_h = H;
-    return make_pair_texture(ctx, ctx->pair, ctx->pair_pitch, W, H, &ctx->pair_tex);
+    return make_pair_texture(ctx, ctx->pair_base, ctx->pair_pitch, (uint32_t)pw, (uint32_t)ph, &ctx->pair_tex);
 }
 
 etcu_status upload_host_float(etcu_context* ctx, float* dst, const float* host, size_t n) {
@@ -672,7 +694,7 @@ extern "C" etcu_status etcu_forward_project(etcu_volume* vol, const etcu_view* v
     a.mode = kFpSeparateAccumulate;
     a.out_v = d_virtual;
     a.out_l = d_traversal;
-    launch_fp(vol, a, view->perspective != 0, 1, ctx->stream);
+    launch_fp(vol, a, fp_path(view->perspective != 0, a.inline_view.fast2d != 0, slab), 1, ctx->stream);
     CKL(ctx);
     return ETCU_OK;
 }
@@ -840,7 +862,7 @@ uint32_t issue_forward(etcu_recon* r, uint32_t first, uint32_t count, cudaStream
         a.rl_slot = r->rl_slot;
         a.real = r->d_proj;
         a.resid_sq = r->d_resid;
-        launch_fp(vol, a, r->persp, count, st);
+        launch_fp(vol, a, r->fp_paths[s], count, st);
     }
     return S;
 }
@@ -958,6 +980,12 @@ etcu_status recon_build(etcu_volume* vol, const etcu_view* views, uint32_t n_vie
                 loc = traversal_length(views[i], vol->desc.bbox_min, vol->desc.bbox_max);
             vc[sl * n_views + i] = make_view_const(views[i], vol->slabs[sl], loc);
         }
+    r->fp_paths.resize(S);
+    for (size_t sl = 0; sl < S; ++sl) {
+        bool all = true;
+        for (uint32_t i = 0; i < n_views; ++i) all &= vc[sl * n_views + i].fast2d != 0;
+        r->fp_paths[sl] = fp_path(persp, all, vol->slabs[sl]);
+    }
     if ((s = dalloc(ctx, (void**)&r->d_views, vc.size() * sizeof(ViewConst))) != ETCU_OK) return s;
     CK(ctx, cudaMemcpyAsync(r->d_views, vc.data(), vc.size() * sizeof(ViewConst), cudaMemcpyHostToDevice, ctx->stream));
     if ((s = dalloc(ctx, (void**)&r->d_order, M * sizeof(uint32_t))) != ETCU_OK) return s;
@@ -978,17 +1006,22 @@ etcu_status recon_build(etcu_volume* vol, const etcu_view* views, uint32_t n_vie
     } else {
         r->nsamples = 0;
     }
-    // per-slot interleaved (residual, length) images and their textures
-    size_t pitch_bytes = round_up((size_t)W * sizeof(float2), ctx->tex_pitch_align);
-    size_t slot_bytes = round_up(pitch_bytes * H, std::max<size_t>(ctx->tex_align, 256));
+    // per-slot interleaved (residual, length) images, padded by kPad zero texels, and
+    // their textures (texture-unit sampling mode)
+    const size_t pw = (size_t)W + 2 * kPad, ph = (size_t)H + 2 * kPad;
+    size_t pitch_bytes = round_up(pw * sizeof(float2), ctx->tex_pitch_align);
+    size_t slot_bytes = round_up(pitch_bytes * ph, std::max<size_t>(ctx->tex_align, 256));
     r->rl_pitch = pitch_bytes / sizeof(float2);
     r->rl_slot = slot_bytes / sizeof(float2);
-    if ((s = dalloc_aligned(ctx, &r->rl_raw, (void**)&r->rl, slot_bytes * r->slots, ctx->tex_align)) != ETCU_OK)
+    if ((s = dalloc_aligned(ctx, &r->rl_raw, (void**)&r->rl_base, slot_bytes * r->slots, ctx->tex_align)) != ETCU_OK)
         return s;
-    CK(ctx, cudaMemsetAsync(r->rl, 0, slot_bytes * r->slots, ctx->stream));
+    CK(ctx, cudaMemsetAsync(r->rl_base, 0, slot_bytes * r->slots, ctx->stream));
+    r->rl = r->rl_base + kPad * r->rl_pitch + kPad;
     r->texs.resize(r->slots);
     for (uint32_t p = 0; p < r->slots; ++p)
-        if ((s = make_pair_texture(ctx, r->rl + p * r->rl_slot, r->rl_pitch, W, H, &r->texs[p])) != ETCU_OK) return s;
+        if ((s = make_pair_texture(ctx, r->rl_base + p * r->rl_slot, r->rl_pitch, (uint32_t)pw, (uint32_t)ph,
+                                   &r->texs[p])) != ETCU_OK)
+            return s;
     if ((s = dalloc(ctx, (void**)&r->d_texs, r->slots * sizeof(cudaTextureObject_t))) != ETCU_OK) return s;
     CK(ctx, cudaMemcpyAsync(r->d_texs, r->texs.data(), r->slots * sizeof(cudaTextureObject_t), cudaMemcpyHostToDevice,
                             ctx->stream));
@@ -1146,7 +1179,10 @@ extern "C" etcu_status etcu_reconstruct(etcu_context* ctx, const etcu_volume_des
 // =============================================================== allocation-free view update
 // Scratch of etcu_sart_view_update_noalloc: one interleaved (residual, length)
 // image and the FP64 residual accumulator, in static device memory.
-static __device__ __align__(256) float2 g_noalloc_pairs[ETCU_NOALLOC_MAX_PIXELS];
+// (width + 2 kPad) x (height + 2 kPad) texels covers every detector of at most
+// 1024 x 1024 pixels.
+constexpr size_t kNoAllocScratchTexels = (size_t)ETCU_NOALLOC_MAX_PIXELS + 8 * 1024 + 16;
+static __device__ __align__(256) float2 g_noalloc_pairs[kNoAllocScratchTexels];
 static __device__ __align__(256) double g_noalloc_resid[1];
 
 namespace {
@@ -1199,7 +1235,8 @@ extern "C" etcu_status etcu_sart_view_update_noalloc(const etcu_volume_desc* des
         return noalloc_fail(ETCU_ERR_UNSUPPORTED, "the allocation-free update takes a single sub-volume");
     if (view->width == 0 || view->height == 0)
         return noalloc_fail(ETCU_ERR_INVALID_ARGUMENT, "projection resolution must be non-zero");
-    if ((uint64_t)view->width * view->height > ETCU_NOALLOC_MAX_PIXELS)
+    if ((uint64_t)view->width * view->height > ETCU_NOALLOC_MAX_PIXELS ||
+        ((uint64_t)view->width + 2 * kPad) * ((uint64_t)view->height + 2 * kPad) > kNoAllocScratchTexels)
         return noalloc_fail(ETCU_ERR_INVALID_ARGUMENT,
                             "detector of %u x %u pixels exceeds the %u-pixel scratch of the allocation-free update",
                             view->width, view->height, (unsigned)ETCU_NOALLOC_MAX_PIXELS);
@@ -1246,7 +1283,11 @@ extern "C" etcu_status etcu_sart_view_update_noalloc(const etcu_volume_desc* des
     if (st != ETCU_OK) return st;
     cudaStream_t stream = (cudaStream_t)cuda_stream;
     const int W = (int)view->width, H = (int)view->height;
-    e = cudaMemsetAsync(sc.resid, 0, sizeof(double), stream);
+    // the padded image of this call (its zero border included) starts from zero
+    const size_t pitch = (size_t)W + 2 * kPad, rows = (size_t)H + 2 * kPad;
+    float2* origin = sc.pairs + kPad * pitch + kPad;
+    e = cudaMemsetAsync(sc.pairs, 0, pitch * rows * sizeof(float2), stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(sc.resid, 0, sizeof(double), stream);
     if (e != cudaSuccess) return noalloc_fail(ETCU_ERR_CUDA, "cudaMemsetAsync failed: %s", cudaGetErrorString(e));
     // forward projection; the single slab overwrites every pixel of the scratch image
     FpArgs fa{};
@@ -1263,13 +1304,12 @@ extern "C" etcu_status etcu_sart_view_update_noalloc(const etcu_volume_desc* des
     fa.mode = kFpPairResidual;
     fa.overwrite = 1;
     fa.loc = 0;
-    fa.rl = sc.pairs;
-    fa.rl_pitch = (size_t)W;
-    fa.rl_slot = (size_t)W * H;
+    fa.rl = origin;
+    fa.rl_pitch = pitch;
+    fa.rl_slot = pitch * rows;
     fa.real = d_projection;
     fa.resid_sq = sc.resid;
-    if (view->perspective) launch_fp_t<float, false, true>(fa, 1, stream);
-    else launch_fp_t<float, false, false>(fa, 1, stream);
+    launch_fp_m<float, false>(fa, fp_path(view->perspective != 0, fa.inline_view.fast2d != 0, slab), 1, stream);
     // back projection of the view with lambda / 1
     BpArgs ba{};
     ba.vol = d_volume;
@@ -1281,9 +1321,9 @@ extern "C" etcu_status etcu_sart_view_update_noalloc(const etcu_volume_desc* des
     ba.order = nullptr;
     ba.first = 0;
     ba.nviews = 1;
-    ba.rl = sc.pairs;
-    ba.rl_pitch = (size_t)W;
-    ba.rl_slot = (size_t)W * H;
+    ba.rl = origin;
+    ba.rl_pitch = pitch;
+    ba.rl_slot = pitch * rows;
     ba.texs = nullptr;
     ba.inline_tex = 0;
     ba.W = W;

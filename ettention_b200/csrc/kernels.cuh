@@ -26,6 +26,11 @@ namespace etcu {
 constexpr float kEps = 1e-4f;           // ocl_src/Math.hl:4
 constexpr int kMaxDdaIterations = 2048; // DDARaytracer.hl:85-107: counter < 4096, bumped twice per step
 constexpr int kMaxInlineSamples = 64;
+// Zero border (texels) around every (residual, length) image: bilinear taps of
+// any coordinate, clamped into [-kPad, W] x [-kPad, H], stay inside the
+// allocation and read zeros outside the image, as the reference's
+// clamp-to-border sampler does.
+constexpr int kPad = 2;
 
 struct ViewConst {
     float4 ray;       // normalised ray direction (parallel) / central direction (perspective)
@@ -184,7 +189,7 @@ __device__ __forceinline__ void dda_walk3(const DdaStart& st, const SlabConst& g
 // kUnroll steps at a time, issuing the kUnroll voxel loads before the
 // kUnroll accumulations (which stay in walk order).  Dead steps after the
 // exit load nothing and add exactly zero.
-template <typename VoxT, bool kMask, int kUnroll = 4>
+template <typename VoxT, bool kMask, bool kCapped = true, int kUnroll = 4>
 __device__ __forceinline__ void dda_walk_xz(const DdaStart& st, const SlabConst& g, const VoxT* __restrict__ vol,
                                            const uint8_t* __restrict__ mask, float& acc, float& accl) {
     const unsigned plane = (unsigned)g.rx * (unsigned)g.ry;
@@ -201,7 +206,7 @@ __device__ __forceinline__ void dda_walk_xz(const DdaStart& st, const SlabConst&
         float dts[kUnroll], vals[kUnroll], mws[kUnroll];
 #pragma unroll
         for (int j = 0; j < kUnroll; ++j) {
-            const bool live = (nx > 0) & (nz > 0) & (left > 0);
+            const bool live = (nx > 0) & (nz > 0) & (!kCapped || left > 0);
             const float dt = fminf(rx, rz);
             const bool bx = rx <= rz;
             dts[j] = live ? dt : 0.f;
@@ -224,7 +229,7 @@ __device__ __forceinline__ void dda_walk_xz(const DdaStart& st, const SlabConst&
             if (kMask) accl = fmaf(dts[j], mws[j], accl);
             else accl += dts[j];
         }
-        if (!((nx > 0) & (nz > 0) & (left > 0))) break;
+        if (!((nx > 0) & (nz > 0) & (!kCapped || left > 0))) break;
     }
 }
 
@@ -322,8 +327,15 @@ struct FpArgs {
     double* resid_sq;           // mode 2: optional sum of residual^2 (FP64)
 };
 
-template <typename VoxT, bool kMask, bool kPerspective>
-__global__ void __launch_bounds__(128) forward_project_kernel(const __grid_constant__ FpArgs a) {
+// kPath: kFpPathGeneral parallel rays (walk chosen per ray), kFpPathXz / kFpPathXzNoCap
+// parallel views tilted about y (xz walk; the loop cap is dropped when the sub-volume
+// cannot reach it, rx + rz - 1 <= 2048 steps), kFpPathPerspective.
+enum FpPath : int { kFpPathGeneral = 0, kFpPathXz = 1, kFpPathXzNoCap = 2, kFpPathPerspective = 3 };
+
+template <typename VoxT, bool kMask, int kPath>
+__global__ void __launch_bounds__(128, (kPath == kFpPathXz || kPath == kFpPathXzNoCap) ? 10 : 4)
+    forward_project_kernel(const __grid_constant__ FpArgs a) {
+    constexpr bool kPerspective = kPath == kFpPathPerspective;
     int gx, gy;
     if (kPerspective) {
         gx = blockIdx.x * 16 + (threadIdx.x & 15);
@@ -353,8 +365,14 @@ __global__ void __launch_bounds__(128) forward_project_kernel(const __grid_const
                     float3 s = make_float3(fadd(fadd(vc.source.x, fmul(vc.hpitch.x, fx)), fmul(vc.vpitch.x, fy)),
                                            fadd(fadd(vc.source.y, fmul(vc.hpitch.y, fx)), fmul(vc.vpitch.y, fy)),
                                            fadd(fadd(vc.source.z, fmul(vc.hpitch.z, fx)), fmul(vc.vpitch.z, fy)));
-                    float v, l;
-                    trace_ray<VoxT, kMask>(s, ray, inv, vc.fast2d != 0, a.slab, vol, a.mask, v, l);
+                    float v = 0.f, l = 0.f;
+                    if (kPath == kFpPathGeneral) {
+                        trace_ray<VoxT, kMask>(s, ray, inv, vc.fast2d != 0, a.slab, vol, a.mask, v, l);
+                    } else {
+                        DdaStart st;
+                        if (dda_setup(s, ray, inv, a.slab, st))
+                            dda_walk_xz<VoxT, kMask, kPath == kFpPathXz>(st, a.slab, vol, a.mask, v, l);
+                    }
                     accv += v;
                     accl += l;
                 }
@@ -475,37 +493,56 @@ __device__ __forceinline__ float div_fast(float a, float b) {
     return fmaf(e, r, q);
 }
 
+// Bilinear taps of the four texels around (x0, y0) from a padded image.
+__device__ __forceinline__ void taps(const float2* __restrict__ row0, size_t pitch, int x0, float2& t00, float2& t10,
+                                     float2& t01, float2& t11) {
+    const float2* r1 = row0 + pitch;
+    t00 = __ldg(row0 + x0);
+    t10 = __ldg(row0 + x0 + 1);
+    t01 = __ldg(r1 + x0);
+    t11 = __ldg(r1 + x0 + 1);
+}
+
+// 1/256 weight of the texture filter: the fraction rounded half up to 8 bits.
+__device__ __forceinline__ float q8_weight(float a) { return fmul(floorf(fadd(fmul(a, 256.f), 0.5f)), 1.f / 256.f); }
+
 template <int kSampling>
-__device__ __forceinline__ float2 sample_pair(const float2* __restrict__ img, size_t pitch, int W, int H,
-                                              cudaTextureObject_t tex, float u, float v) {
-    if (kSampling == kSampleTexture) return tex2D<float2>(tex, u, v);
-    const float xs = fsub(u, 0.5f), ys = fsub(v, 0.5f);
-    const float xb = floorf(xs), yb = floorf(ys);
-    float a = fminf(fsub(xs, xb), 0x1.fffffep-1f), b = fminf(fsub(ys, yb), 0x1.fffffep-1f);
-    const int x0 = (int)xb, y0 = (int)yb;
-    const bool in_x0 = (unsigned)x0 < (unsigned)W, in_x1 = (unsigned)(x0 + 1) < (unsigned)W;
-    const bool in_y0 = (unsigned)y0 < (unsigned)H, in_y1 = (unsigned)(y0 + 1) < (unsigned)H;
-    const float2 zero = make_float2(0.f, 0.f);
-    const float2* r0 = img + (size_t)y0 * pitch + x0;
-    const float2* r1 = r0 + pitch;
-    const float2 t00 = (in_y0 && in_x0) ? __ldg(r0) : zero;
-    const float2 t10 = (in_y0 && in_x1) ? __ldg(r0 + 1) : zero;
-    const float2 t01 = (in_y1 && in_x0) ? __ldg(r1) : zero;
-    const float2 t11 = (in_y1 && in_x1) ? __ldg(r1 + 1) : zero;
+__device__ __forceinline__ float2 blend(float a, float b, float2 t00, float2 t10, float2 t01, float2 t11) {
     if (kSampling == kSampleQ8) {
-        a = fmul(floorf(fadd(fmul(a, 256.f), 0.5f)), 1.f / 256.f);
-        b = fmul(floorf(fadd(fmul(b, 256.f), 0.5f)), 1.f / 256.f);
         const float w00 = fmul(fsub(1.f, a), fsub(1.f, b)), w10 = fmul(a, fsub(1.f, b));
         const float w01 = fmul(fsub(1.f, a), b), w11 = fmul(a, b);
         return make_float2(
             fadd(fadd(fadd(fmul(w00, t00.x), fmul(w10, t10.x)), fmul(w01, t01.x)), fmul(w11, t11.x)),
             fadd(fadd(fadd(fmul(w00, t00.y), fmul(w10, t10.y)), fmul(w01, t01.y)), fmul(w11, t11.y)));
     }
-    // ImageHandler.hl:20-40: mix along x inside each row, then along y; absent rows are 0
-    float2 p0 = zero, p1 = zero;
-    if (in_y0) p0 = make_float2(fadd(t00.x, fmul(fsub(t10.x, t00.x), a)), fadd(t00.y, fmul(fsub(t10.y, t00.y), a)));
-    if (in_y1) p1 = make_float2(fadd(t01.x, fmul(fsub(t11.x, t01.x), a)), fadd(t01.y, fmul(fsub(t11.y, t01.y), a)));
+    // ImageHandler.hl:20-40: mix along x inside each row, then along y (zero rows mix to zero)
+    const float2 p0 = make_float2(fadd(t00.x, fmul(fsub(t10.x, t00.x), a)), fadd(t00.y, fmul(fsub(t10.y, t00.y), a)));
+    const float2 p1 = make_float2(fadd(t01.x, fmul(fsub(t11.x, t01.x), a)), fadd(t01.y, fmul(fsub(t11.y, t01.y), a)));
     return make_float2(fadd(p0.x, fmul(fsub(p1.x, p0.x), b)), fadd(p0.y, fmul(fsub(p1.y, p0.y), b)));
+}
+
+// Texel-space fraction and clamped base index of one coordinate.
+template <int kSampling>
+__device__ __forceinline__ void split_coord(float c, int n, int& i0, float& frac) {
+    const float cs = fsub(c, 0.5f);
+    const float cb = floorf(cs);
+    frac = fminf(fsub(cs, cb), 0x1.fffffep-1f);  // OpenCL fract() clamp
+    if (kSampling == kSampleQ8) frac = q8_weight(frac);
+    i0 = min(max((int)cb, -kPad), n);
+}
+
+// img points at texel (0, 0) of a padded image with row pitch `pitch` (float2 units).
+template <int kSampling>
+__device__ __forceinline__ float2 sample_pair(const float2* __restrict__ img, size_t pitch, int W, int H,
+                                              cudaTextureObject_t tex, float u, float v) {
+    if (kSampling == kSampleTexture) return tex2D<float2>(tex, u + (float)kPad, v + (float)kPad);
+    int x0, y0;
+    float a, b;
+    split_coord<kSampling>(u, W, x0, a);
+    split_coord<kSampling>(v, H, y0, b);
+    float2 t00, t10, t01, t11;
+    taps(img + (ptrdiff_t)y0 * (ptrdiff_t)pitch, pitch, x0, t00, t10, t01, t11);
+    return blend<kSampling>(a, b, t00, t10, t01, t11);
 }
 
 // Stages the block's view constants (and parallel sample patterns) in shared memory.
@@ -551,12 +588,122 @@ __device__ __forceinline__ void bp_store(const BpArgs& a, size_t idx, float val)
 constexpr int kBpZ = 8;  // voxels per thread along z (parallel)
 constexpr int kBpZPersp = 4;
 
+// One view's update of kBpZ voxels of a column (ParallelBeamsBackProjection.cl:26-51).
+// kRowConst: the detector row coordinate does not depend on x or z (affine matrix with
+// m1 == m9 == 0, every view tilted about y), so the row taps are fixed per sample and
+// only the column coordinate is evaluated per voxel -- in the same operations as the
+// general form (the skipped terms are exact zeros).
+template <bool kMask, int kSampling, bool kRowConst>
+__device__ __forceinline__ void bp_parallel_view(const BpArgs& a, const BpView& V, const float4* __restrict__ smp,
+                                                 const float2* __restrict__ img, float cx, float cy,
+                                                 const float* cz, int nzc, const float* mwt, float* val) {
+    const int ns = a.nsamples;
+    if (ns == 1) {
+        // one sample: used is 0 or 1, the average is the sample itself
+        const float4 s = smp[0];
+        const float px = fadd(cx, s.x), py = fadd(cy, s.y);
+        const float au = fadd(fmul(V.mu[0], px), fmul(V.mu[1], py));
+        const float av = fadd(fmul(V.mv[0], px), fmul(V.mv[1], py));
+        const float aw = fadd(fmul(V.mw[0], px), fmul(V.mw[1], py));
+        int y0 = 0;
+        float b = 0.f;
+        const float2* row0 = img;
+        if (kRowConst) {
+            split_coord<kSampling>(fadd(av, V.mv[3]), a.H, y0, b);
+            row0 = img + (ptrdiff_t)y0 * (ptrdiff_t)a.rl_pitch;
+        }
+#pragma unroll
+        for (int j = 0; j < kBpZ; ++j) {
+            if (j < nzc) {
+                const float pz = fadd(cz[j], s.z);
+                float u = fadd(fadd(au, fmul(V.mu[2], pz)), V.mu[3]);
+                float2 rl;
+                if (kRowConst && kSampling != kSampleTexture) {
+                    int x0;
+                    float ax;
+                    split_coord<kSampling>(u, a.W, x0, ax);
+                    float2 t00, t10, t01, t11;
+                    taps(row0, a.rl_pitch, x0, t00, t10, t01, t11);
+                    rl = blend<kSampling>(ax, b, t00, t10, t01, t11);
+                } else {
+                    float v = fadd(fadd(av, fmul(V.mv[2], pz)), V.mv[3]);
+                    if (!V.affine) {  // Matrix4x4.hl:54-58 divide by w
+                        const float w = fadd(fadd(aw, fmul(V.mw[2], pz)), V.mw[3]);
+                        u = fdiv(u, w);
+                        v = fdiv(v, w);
+                    }
+                    rl = sample_pair<kSampling>(img, a.rl_pitch, a.W, a.H, V.tex, u, v);
+                }
+                const float contrib = fmul(fmul(rl.x, a.lambda), div_fast(s.w, rl.y));
+                if (rl.y > kEps) val[j] = fadd(val[j], kMask ? fmul(mwt[j], contrib) : contrib);
+            }
+        }
+        return;
+    }
+    float pv[kBpZ];
+    unsigned used[kBpZ];
+#pragma unroll
+    for (int j = 0; j < kBpZ; ++j) {
+        pv[j] = 0.f;
+        used[j] = 0;
+    }
+    for (int k = 0; k < ns; ++k) {
+        const float4 s = smp[k];
+        const float px = fadd(cx, s.x), py = fadd(cy, s.y);
+        const float au = fadd(fmul(V.mu[0], px), fmul(V.mu[1], py));
+        const float av = fadd(fmul(V.mv[0], px), fmul(V.mv[1], py));
+        const float aw = fadd(fmul(V.mw[0], px), fmul(V.mw[1], py));
+        int y0 = 0;
+        float b = 0.f;
+        const float2* row0 = img;
+        if (kRowConst) {
+            split_coord<kSampling>(fadd(av, V.mv[3]), a.H, y0, b);
+            row0 = img + (ptrdiff_t)y0 * (ptrdiff_t)a.rl_pitch;
+        }
+#pragma unroll
+        for (int j = 0; j < kBpZ; ++j) {
+            if (j < nzc) {
+                const float pz = fadd(cz[j], s.z);
+                float u = fadd(fadd(au, fmul(V.mu[2], pz)), V.mu[3]);
+                float2 rl;
+                if (kRowConst && kSampling != kSampleTexture) {
+                    int x0;
+                    float ax;
+                    split_coord<kSampling>(u, a.W, x0, ax);
+                    float2 t00, t10, t01, t11;
+                    taps(row0, a.rl_pitch, x0, t00, t10, t01, t11);
+                    rl = blend<kSampling>(ax, b, t00, t10, t01, t11);
+                } else {
+                    float v = fadd(fadd(av, fmul(V.mv[2], pz)), V.mv[3]);
+                    if (!V.affine) {  // Matrix4x4.hl:54-58 divide by w
+                        const float w = fadd(fadd(aw, fmul(V.mw[2], pz)), V.mw[3]);
+                        u = fdiv(u, w);
+                        v = fdiv(v, w);
+                    }
+                    rl = sample_pair<kSampling>(img, a.rl_pitch, a.W, a.H, V.tex, u, v);
+                }
+                const float contrib = fmul(fmul(rl.x, a.lambda), div_fast(s.w, rl.y));
+                if (rl.y > kEps) {
+                    pv[j] = fadd(pv[j], contrib);
+                    used[j] += 1;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < kBpZ; ++j) {
+        if (used[j] != 0) {
+            const float num = kMask ? fmul(mwt[j], pv[j]) : pv[j];
+            val[j] = fadd(val[j], used[j] == 1 ? num : div_fast(num, (float)used[j]));
+        }
+    }
+}
+
 // ParallelBeamsBackProjection.cl:9-52.  Each thread owns kBpZ voxels of one (x, y)
-// column and applies the block's views to them in order (no atomics); the view
-// constants come from shared memory, the projected coordinates are evaluated in
-// the reference's operation order with the z-independent part hoisted.
-// Storage kStore: 0 FP32 volume, 1 half volume re-rounded after every view
-// (reference half mode), 2 FP32 master + half shadow, 3 FP32 master + bf16 shadow.
+// column at a time and applies the block's views to them in order (no atomics); blocks
+// walk z-chunks in a grid-stride loop so the view constants staged in shared memory
+// serve many voxels.  Storage kStore: 0 FP32 volume, 1 half volume re-rounded after
+// every view (reference half mode), 2 FP32 master + half shadow, 3 FP32 master + bf16 shadow.
 template <bool kMask, int kStore, int kSampling>
 __global__ void __launch_bounds__(256) bp_parallel_kernel(const __grid_constant__ BpArgs a) {
     extern __shared__ __align__(16) unsigned char bp_smem[];
@@ -566,73 +713,41 @@ __global__ void __launch_bounds__(256) bp_parallel_kernel(const __grid_constant_
     const SlabConst& g = a.slab;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int z0 = blockIdx.z * kBpZ;
     if (x >= g.rx || y >= g.ry) return;
-    const int nzc = min(kBpZ, g.rz - z0);
+    bool row_const = true;
+    for (int p = 0; p < a.nviews; ++p)
+        row_const &= sv[p].affine && sv[p].mv[0] == 0.f && sv[p].mv[2] == 0.f;
     const size_t plane = (size_t)g.rx * (size_t)g.ry;
-    const size_t base = (size_t)z0 * plane + (size_t)y * (size_t)g.rx + (size_t)x;
-    float val[kBpZ], mwt[kBpZ], cz[kBpZ];
-#pragma unroll
-    for (int j = 0; j < kBpZ; ++j) {
-        val[j] = 0.f;
-        mwt[j] = 1.f;
-        cz[j] = fadd(g.bmin.z, fmul(fadd((float)(z0 + j), 0.5f), g.vs.z));  // VolumeGeometry.hl:17-20
-        if (j < nzc) {
-            val[j] = bp_load<kStore>(a, base + (size_t)j * plane);
-            if (kMask) mwt[j] = mask_weight(a.mask + base + (size_t)j * plane);
-        }
-    }
     const float cx = fadd(g.bmin.x, fmul(fadd((float)x, 0.5f), g.vs.x));
     const float cy = fadd(g.bmin.y, fmul(fadd((float)y, 0.5f), g.vs.y));
-    const int ns = a.nsamples;
-    for (int p = 0; p < a.nviews; ++p) {
-        const BpView& V = sv[p];
-        const float2* img = a.rl + (size_t)p * a.rl_slot;
-        float pv[kBpZ];
-        unsigned used[kBpZ];
+    for (int z0 = blockIdx.z * kBpZ; z0 < g.rz; z0 += gridDim.z * kBpZ) {
+        const int nzc = min(kBpZ, g.rz - z0);
+        const size_t base = (size_t)z0 * plane + (size_t)y * (size_t)g.rx + (size_t)x;
+        float val[kBpZ], mwt[kBpZ], cz[kBpZ];
 #pragma unroll
         for (int j = 0; j < kBpZ; ++j) {
-            pv[j] = 0.f;
-            used[j] = 0;
+            val[j] = 0.f;
+            mwt[j] = 1.f;
+            cz[j] = fadd(g.bmin.z, fmul(fadd((float)(z0 + j), 0.5f), g.vs.z));  // VolumeGeometry.hl:17-20
+            if (j < nzc) {
+                val[j] = bp_load<kStore>(a, base + (size_t)j * plane);
+                if (kMask) mwt[j] = mask_weight(a.mask + base + (size_t)j * plane);
+            }
         }
-        for (int k = 0; k < ns; ++k) {
-            const float4 s = ss[p * ns + k];
-            const float px = fadd(cx, s.x), py = fadd(cy, s.y);
-            const float au = fadd(fmul(V.mu[0], px), fmul(V.mu[1], py));
-            const float av = fadd(fmul(V.mv[0], px), fmul(V.mv[1], py));
-            const float aw = fadd(fmul(V.mw[0], px), fmul(V.mw[1], py));
+        for (int p = 0; p < a.nviews; ++p) {
+            const float2* img = a.rl + (size_t)p * a.rl_slot;
+            const float4* smp = ss + p * a.nsamples;
+            if (row_const) bp_parallel_view<kMask, kSampling, true>(a, sv[p], smp, img, cx, cy, cz, nzc, mwt, val);
+            else bp_parallel_view<kMask, kSampling, false>(a, sv[p], smp, img, cx, cy, cz, nzc, mwt, val);
+            if (kStore == 1) {
 #pragma unroll
-            for (int j = 0; j < kBpZ; ++j) {
-                if (j < nzc) {
-                    const float pz = fadd(cz[j], s.z);
-                    float u = fadd(fadd(au, fmul(V.mu[2], pz)), V.mu[3]);
-                    float v = fadd(fadd(av, fmul(V.mv[2], pz)), V.mv[3]);
-                    if (!V.affine) {  // Matrix4x4.hl:54-58 divide by w
-                        const float w = fadd(fadd(aw, fmul(V.mw[2], pz)), V.mw[3]);
-                        u = fdiv(u, w);
-                        v = fdiv(v, w);
-                    }
-                    const float2 rl = sample_pair<kSampling>(img, a.rl_pitch, a.W, a.H, V.tex, u, v);
-                    const float contrib = fmul(fmul(rl.x, a.lambda), div_fast(s.w, rl.y));
-                    if (rl.y > kEps) {
-                        pv[j] = fadd(pv[j], contrib);
-                        used[j] += 1;
-                    }
-                }
+                for (int j = 0; j < kBpZ; ++j) val[j] = __half2float(__float2half_rn(val[j]));  // vstore_half per view
             }
         }
 #pragma unroll
-        for (int j = 0; j < kBpZ; ++j) {
-            if (used[j] != 0) {
-                const float num = fmul(mwt[j], pv[j]);
-                val[j] = fadd(val[j], used[j] == 1 ? num : div_fast(num, (float)used[j]));
-            }
-            if (kStore == 1) val[j] = __half2float(__float2half_rn(val[j]));  // vstore_half after every view
-        }
+        for (int j = 0; j < kBpZ; ++j)
+            if (j < nzc) bp_store<kStore>(a, base + (size_t)j * plane, val[j]);
     }
-#pragma unroll
-    for (int j = 0; j < kBpZ; ++j)
-        if (j < nzc) bp_store<kStore>(a, base + (size_t)j * plane, val[j]);
 }
 
 // PerspectiveBeamsBackProjection.cl:10-17 getRayLengthInVoxel

@@ -242,8 +242,9 @@ ETCU_API etcu_status etcu_reconstruct(etcu_context* ctx, const etcu_volume_desc*
  * etcu_volume, one sub-volume), the measured projection of this view (device
  * pointer, height x width floats) and the stream to run on (NULL: the legacy
  * default stream).  The (residual, ray length) image lives in a static device
- * array of ETCU_NOALLOC_MAX_PIXELS float2 (8 MiB) that every GPU loading the
- * library holds until the process exits; larger detectors are rejected.  The
+ * array of about ETCU_NOALLOC_MAX_PIXELS float2 (8 MiB) that every GPU loading
+ * the library holds until the process exits; detectors of up to 1024 x 1024
+ * pixels fit, larger ones are rejected.  The
  * first call on a device looks up that array's device address, so make the
  * first call before any stream capture.  All calls share the array and keep
  * the last call's contents: calls that overlap on the GPU (other streams or
