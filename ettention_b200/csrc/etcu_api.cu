@@ -76,7 +76,8 @@ struct etcu_recon {
     cudaGraphExec_t exec = nullptr;
     uint32_t launches = 0;
     bool persp = false;
-    std::vector<int> fp_paths;  // per slab
+    std::vector<int> fp_paths;      // per slab
+    std::vector<uint8_t> row_const; // per view id
 };
 
 namespace {
@@ -212,6 +213,12 @@ ViewConst make_view_const(const etcu_view& v, const SlabConst& slab, float loc_l
     return c;
 }
 
+// Affine projection whose detector row depends only on y (parallel views tilted about y).
+bool row_constant(const ViewConst& c) {
+    return c.mat[1] == 0.f && c.mat[9] == 0.f && c.mat[3] == 0.f && c.mat[7] == 0.f && c.mat[11] == 0.f &&
+           c.mat[15] == 1.f;
+}
+
 etcu_status check_view(etcu_context* ctx, const etcu_view* v) {
     if (!v) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "view is NULL");
     if (v->width == 0 || v->height == 0)
@@ -305,11 +312,38 @@ void launch_bp_m(const BpArgs& a, etcu_voxel_type t, etcu_sampling sm, int dev, 
     }
 }
 
+template <bool kMask, int kStore>
+void launch_bp_sart(const BpArgs& a, etcu_sampling sm, cudaStream_t st) {
+    const int bx = (a.slab.rx + 31) / 32, by = (a.slab.ry + 7) / 8;
+    // enough blocks for a few waves; each thread then walks its column's z range
+    const int want = 148 * 16;
+    int zs = std::max(1, std::min((a.slab.rz + 15) / 16, (want + bx * by - 1) / (bx * by)));
+    dim3 block(32, 8, 1), grid(bx, by, zs);
+    if (sm == ETCU_SAMPLING_EXACT) bp_sart_row_kernel<kMask, kStore, kSampleExact><<<grid, block, 0, st>>>(a);
+    else bp_sart_row_kernel<kMask, kStore, kSampleQ8><<<grid, block, 0, st>>>(a);
+}
+
+template <bool kMask>
+void launch_bp_sart_m(const BpArgs& a, etcu_voxel_type t, etcu_sampling sm, cudaStream_t st) {
+    switch (t) {
+    case ETCU_VOXEL_FLOAT32: launch_bp_sart<kMask, 0>(a, sm, st); break;
+    case ETCU_VOXEL_HALF16: launch_bp_sart<kMask, 1>(a, sm, st); break;
+    case ETCU_VOXEL_F16_MASTER: launch_bp_sart<kMask, 2>(a, sm, st); break;
+    case ETCU_VOXEL_BF16_MASTER: launch_bp_sart<kMask, 3>(a, sm, st); break;
+    }
+}
+
 // Back projection of a.nviews views; when their staged constants exceed the
 // shared-memory budget the views are split over consecutive launches, which
 // applies them in the same order.  Returns the number of launches.
-uint32_t launch_bp(const etcu_volume* vol, const BpArgs& a0, bool persp, etcu_sampling sm, cudaStream_t st) {
+uint32_t launch_bp(const etcu_volume* vol, const BpArgs& a0, bool persp, etcu_sampling sm, cudaStream_t st,
+                   bool row_const = false) {
     const int dev = vol->ctx->device;
+    if (!persp && row_const && a0.nviews == 1 && a0.nsamples == 1 && sm != ETCU_SAMPLING_HW_TEXTURE) {
+        if (a0.mask) launch_bp_sart_m<true>(a0, vol->type, sm, st);
+        else launch_bp_sart_m<false>(a0, vol->type, sm, st);
+        return 1;
+    }
     const size_t per_view = bp_smem_bytes(1, persp ? 0 : a0.nsamples);
     const int max_views = (int)std::max<size_t>(1, (kBpSmemBudget - 16) / per_view);
     uint32_t launches = 0;
@@ -732,7 +766,7 @@ etcu_status bp_one_slab(etcu_volume* vol, const etcu_view* view, const SlabConst
     a.use_max = vol->use_max;
     a.vmin = vol->vmin;
     a.vmax = vol->vmax;
-    launch_bp(vol, a, view->perspective != 0, sampling, ctx->stream);
+    launch_bp(vol, a, view->perspective != 0, sampling, ctx->stream, row_constant(a.inline_view));
     CKL(ctx);
     return ETCU_OK;
 }
@@ -897,7 +931,7 @@ uint32_t issue_backward(etcu_recon* r, uint32_t first, uint32_t count, cudaStrea
         a.use_max = vol->use_max;
         a.vmin = vol->vmin;
         a.vmax = vol->vmax;
-        n += launch_bp(vol, a, r->persp, r->params.sampling, st);
+        n += launch_bp(vol, a, r->persp, r->params.sampling, st, count == 1 && r->row_const[r->order[first]]);
     }
     return n;
 }
@@ -980,6 +1014,8 @@ etcu_status recon_build(etcu_volume* vol, const etcu_view* views, uint32_t n_vie
                 loc = traversal_length(views[i], vol->desc.bbox_min, vol->desc.bbox_max);
             vc[sl * n_views + i] = make_view_const(views[i], vol->slabs[sl], loc);
         }
+    r->row_const.resize(n_views);
+    for (uint32_t i = 0; i < n_views; ++i) r->row_const[i] = row_constant(vc[i]) ? 1 : 0;
     r->fp_paths.resize(S);
     for (size_t sl = 0; sl < S; ++sl) {
         bool all = true;
@@ -1338,6 +1374,7 @@ extern "C" etcu_status etcu_sart_view_update_noalloc(const etcu_volume_desc* des
         ba.persp_n = (int)perspective_sampling_factor(view->width, view->height, res, bp_samples);
     }
     if (view->perspective) launch_bp_t<true, false, 0, kSampleQ8>(ba, dev, stream);
+    else if (bp_samples == 1 && row_constant(ba.inline_view)) launch_bp_sart<false, 0>(ba, ETCU_SAMPLING_Q8, stream);
     else launch_bp_t<false, false, 0, kSampleQ8>(ba, dev, stream);
     e = cudaGetLastError();
     if (e != cudaSuccess) return noalloc_fail(ETCU_ERR_CUDA, "launch failed: %s", cudaGetErrorString(e));

@@ -202,34 +202,48 @@ __device__ __forceinline__ void dda_walk_xz(const DdaStart& st, const SlabConst&
     int left = kMaxDdaIterations;
     unsigned off = (unsigned)st.iz * plane + (unsigned)st.ix;
     float rx = st.res.x, rz = st.res.z;
+    // One DDA step (DDARaytracer.hl:89-105): returns the segment length and the voxel it crossed.
+    auto step = [&](float& dt, unsigned& at) {
+        dt = fminf(rx, rz);
+        const bool bx = rx <= rz;
+        at = off;
+        rx = bx ? sdx : fsub(rx, dt);
+        rz = bx ? fsub(rz, dt) : sdz;
+        off += bx ? dx : dz;
+        nx -= bx ? 1 : 0;
+        nz -= bx ? 0 : 1;
+    };
     for (;;) {
-        float dts[kUnroll], vals[kUnroll], mws[kUnroll];
+        // Neither axis can leave the slab (nor the loop cap run out) within the next
+        // min(nx, nz[, left]) steps, so they run without exit tests.
+        int m = min(nx, nz);
+        if (kCapped) m = min(m, left);
+        if (m <= 0) break;
+        if (kCapped) left -= m;
+        for (; m >= kUnroll; m -= kUnroll) {
+            float dts[kUnroll], vals[kUnroll], mws[kUnroll];
 #pragma unroll
-        for (int j = 0; j < kUnroll; ++j) {
-            const bool live = (nx > 0) & (nz > 0) & (!kCapped || left > 0);
-            const float dt = fminf(rx, rz);
-            const bool bx = rx <= rz;
-            dts[j] = live ? dt : 0.f;
-            vals[j] = 0.f;
-            mws[j] = 0.f;
-            if (live) {
-                vals[j] = load_voxel(row + off);
-                if (kMask) mws[j] = mask_weight(mrow + off);
+            for (int j = 0; j < kUnroll; ++j) {
+                unsigned at;
+                step(dts[j], at);
+                vals[j] = load_voxel(row + at);
+                if (kMask) mws[j] = mask_weight(mrow + at);
             }
-            rx = bx ? sdx : fsub(rx, dt);
-            rz = bx ? fsub(rz, dt) : sdz;
-            off += bx ? dx : dz;
-            nx -= bx ? 1 : 0;
-            nz -= bx ? 0 : 1;
-            left -= 1;
-        }
 #pragma unroll
-        for (int j = 0; j < kUnroll; ++j) {
-            acc = fmaf(dts[j], vals[j], acc);
-            if (kMask) accl = fmaf(dts[j], mws[j], accl);
-            else accl += dts[j];
+            for (int j = 0; j < kUnroll; ++j) {
+                acc = fmaf(dts[j], vals[j], acc);
+                if (kMask) accl = fmaf(dts[j], mws[j], accl);
+                else accl += dts[j];
+            }
         }
-        if (!((nx > 0) & (nz > 0) & (!kCapped || left > 0))) break;
+        for (; m > 0; --m) {
+            float dt;
+            unsigned at;
+            step(dt, at);
+            acc = fmaf(dt, load_voxel(row + at), acc);
+            if (kMask) accl = fmaf(dt, mask_weight(mrow + at), accl);
+            else accl += dt;
+        }
     }
 }
 
@@ -588,6 +602,43 @@ __device__ __forceinline__ void bp_store(const BpArgs& a, size_t idx, float val)
 constexpr int kBpZ = 8;  // voxels per thread along z (parallel)
 constexpr int kBpZPersp = 4;
 
+// Row-constant view, one sample, 1/256 weights: the per-voxel sequence reduced to the
+// column coordinate.  q = floor((u - 0.5) * 256 + 0.5) is the 1/256-rounded texel
+// coordinate (u * 256 - 127.5 is exact for |u| < 2^15); x0 = floor(q / 256) and
+// a = q / 256 - x0 give the same taps and weights as split_coord (a weight that rounds
+// up to 1 becomes weight 0 on the next texel, which blends to the same value).
+template <bool kMask>
+__device__ __forceinline__ void bp_rowconst_q8_single(const BpArgs& a, const BpView& V, float4 s,
+                                                      const float2* __restrict__ img, float cx, float cy,
+                                                      const float* cz, int nzc, const float* mwt, float* val) {
+    const float px = fadd(cx, s.x), py = fadd(cy, s.y);
+    const float au = fadd(fmul(V.mu[0], px), fmul(V.mu[1], py));
+    const float av = fadd(fmul(V.mv[0], px), fmul(V.mv[1], py));
+    int y0;
+    float b;
+    split_coord<kSampleQ8>(fadd(av, V.mv[3]), a.H, y0, b);
+    const float2* row0 = img + (ptrdiff_t)y0 * (ptrdiff_t)a.rl_pitch;
+    const float2* row1 = row0 + a.rl_pitch;
+    const float mu2 = V.mu[2], mu3 = V.mu[3], lam = a.lambda, d = s.w;
+    const int W = a.W;
+#pragma unroll
+    for (int j = 0; j < kBpZ; ++j) {
+        if (j < nzc) {
+            const float pz = fadd(cz[j], s.z);
+            const float u = fadd(fadd(au, fmul(mu2, pz)), mu3);
+            const float qf = floorf(fmaf(u, 256.f, -127.5f));
+            const float x0f = floorf(qf * (1.f / 256.f));
+            const float ax = fmaf(qf, 1.f / 256.f, -x0f);
+            const int x0 = min(max((int)x0f, -kPad), W);
+            const float2 t00 = __ldg(row0 + x0), t10 = __ldg(row0 + x0 + 1);
+            const float2 t01 = __ldg(row1 + x0), t11 = __ldg(row1 + x0 + 1);
+            const float2 rl = blend<kSampleQ8>(ax, b, t00, t10, t01, t11);
+            const float contrib = fmul(fmul(rl.x, lam), div_fast(d, rl.y));
+            if (rl.y > kEps) val[j] = fadd(val[j], kMask ? fmul(mwt[j], contrib) : contrib);
+        }
+    }
+}
+
 // One view's update of kBpZ voxels of a column (ParallelBeamsBackProjection.cl:26-51).
 // kRowConst: the detector row coordinate does not depend on x or z (affine matrix with
 // m1 == m9 == 0, every view tilted about y), so the row taps are fixed per sample and
@@ -598,6 +649,10 @@ __device__ __forceinline__ void bp_parallel_view(const BpArgs& a, const BpView& 
                                                  const float2* __restrict__ img, float cx, float cy,
                                                  const float* cz, int nzc, const float* mwt, float* val) {
     const int ns = a.nsamples;
+    if (kRowConst && kSampling == kSampleQ8 && ns == 1) {
+        bp_rowconst_q8_single<kMask>(a, V, smp[0], img, cx, cy, cz, nzc, mwt, val);
+        return;
+    }
     if (ns == 1) {
         // one sample: used is 0 or 1, the average is the sample itself
         const float4 s = smp[0];
@@ -705,7 +760,7 @@ __device__ __forceinline__ void bp_parallel_view(const BpArgs& a, const BpView& 
 // serve many voxels.  Storage kStore: 0 FP32 volume, 1 half volume re-rounded after
 // every view (reference half mode), 2 FP32 master + half shadow, 3 FP32 master + bf16 shadow.
 template <bool kMask, int kStore, int kSampling>
-__global__ void __launch_bounds__(256) bp_parallel_kernel(const __grid_constant__ BpArgs a) {
+__global__ void __launch_bounds__(256, 4) bp_parallel_kernel(const __grid_constant__ BpArgs a) {
     extern __shared__ __align__(16) unsigned char bp_smem[];
     BpView* sv = (BpView*)bp_smem;
     float4* ss = (float4*)(bp_smem + ((size_t)a.nviews * sizeof(BpView) + 15) / 16 * 16);
@@ -747,6 +802,120 @@ __global__ void __launch_bounds__(256) bp_parallel_kernel(const __grid_constant_
 #pragma unroll
         for (int j = 0; j < kBpZ; ++j)
             if (j < nzc) bp_store<kStore>(a, base + (size_t)j * plane, val[j]);
+    }
+}
+
+// ---- single-view, single-sample parallel back projection (SART's hot case) ----
+// Paired FP32 arithmetic (two voxels per instruction); every lane rounds to nearest
+// exactly as the scalar operations do, so results are bit-identical to
+// bp_parallel_kernel.
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 splat(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+// One voxel pair's sample: the 1/256-rounded (or exact) blend of the (residual, length)
+// image at column coordinates u2, row taps fixed by (row0, row1, b).
+template <int kSampling>
+__device__ __forceinline__ void row_blend_pair(float2 u2, const float2* __restrict__ row0,
+                                               const float2* __restrict__ row1, float b, float omb, int W,
+                                               float2& rl_a, float2& rl_b) {
+    float2 ax2;
+    int x0a, x0b;
+    if (kSampling == kSampleQ8) {
+        // q = floor((u - 0.5) * 256 + 0.5); u * 256 - 127.5 is exact for |u| < 2^15
+        const float2 t = fma2(u2, splat(256.f), splat(-127.5f));
+        const float2 q = f2(floorf(t.x), floorf(t.y));
+        const float2 qs = mul2(q, splat(1.f / 256.f));
+        const float2 xf = f2(floorf(qs.x), floorf(qs.y));
+        ax2 = fma2(q, splat(1.f / 256.f), f2(-xf.x, -xf.y));
+        x0a = (int)xf.x;
+        x0b = (int)xf.y;
+    } else {
+        const float2 cs = add2(u2, splat(-0.5f));
+        const float2 cb = f2(floorf(cs.x), floorf(cs.y));
+        const float2 fr = add2(cs, f2(-cb.x, -cb.y));
+        ax2 = f2(fminf(fr.x, 0x1.fffffep-1f), fminf(fr.y, 0x1.fffffep-1f));
+        x0a = (int)cb.x;
+        x0b = (int)cb.y;
+    }
+    x0a = min(max(x0a, -kPad), W);
+    x0b = min(max(x0b, -kPad), W);
+    const float2 a00 = __ldg(row0 + x0a), a10 = __ldg(row0 + x0a + 1), a01 = __ldg(row1 + x0a), a11 = __ldg(row1 + x0a + 1);
+    const float2 b00 = __ldg(row0 + x0b), b10 = __ldg(row0 + x0b + 1), b01 = __ldg(row1 + x0b), b11 = __ldg(row1 + x0b + 1);
+    if (kSampling == kSampleQ8) {
+        const float2 oma = add2(splat(1.f), f2(-ax2.x, -ax2.y));
+        const float2 w00 = mul2(oma, splat(omb)), w10 = mul2(ax2, splat(omb));
+        const float2 w01 = mul2(oma, splat(b)), w11 = mul2(ax2, splat(b));
+        rl_a = add2(add2(add2(mul2(splat(w00.x), a00), mul2(splat(w10.x), a10)), mul2(splat(w01.x), a01)),
+                    mul2(splat(w11.x), a11));
+        rl_b = add2(add2(add2(mul2(splat(w00.y), b00), mul2(splat(w10.y), b10)), mul2(splat(w01.y), b01)),
+                    mul2(splat(w11.y), b11));
+    } else {
+        auto mix = [](float2 p, float2 q, float t) { return add2(p, mul2(add2(q, f2(-p.x, -p.y)), splat(t))); };
+        rl_a = mix(mix(a00, a10, ax2.x), mix(a01, a11, ax2.x), b);
+        rl_b = mix(mix(b00, b10, ax2.y), mix(b01, b11, ax2.y), b);
+    }
+}
+
+// ParallelBeamsBackProjection.cl:9-52 for one view with one sample per voxel and a
+// detector row that depends only on y (every view tilted about y): each thread owns
+// an (x, y) column over a z range, computes the view's row taps once and updates
+// voxel pairs with paired FP32 instructions.
+template <bool kMask, int kStore, int kSampling>
+__global__ void __launch_bounds__(256) bp_sart_row_kernel(const __grid_constant__ BpArgs a) {
+    const SlabConst& g = a.slab;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= g.rx || y >= g.ry) return;
+    const int zper = (g.rz + gridDim.z - 1) / gridDim.z;
+    const int zb = blockIdx.z * zper, ze = min(g.rz, zb + zper);
+    if (zb >= ze) return;
+    const uint32_t vid = a.order ? a.order[a.first] : a.first;
+    const ViewConst& vc = a.views ? a.views[vid] : a.inline_view;
+    const float4 s = a.samples ? a.samples[vid] : a.inline_samples[0];
+    const float cx = fadd(g.bmin.x, fmul(fadd((float)x, 0.5f), g.vs.x));
+    const float cy = fadd(g.bmin.y, fmul(fadd((float)y, 0.5f), g.vs.y));
+    const float px = fadd(cx, s.x), py = fadd(cy, s.y);
+    const float au = fadd(fmul(vc.mat[0], px), fmul(vc.mat[4], py));
+    const float av = fadd(fmul(vc.mat[1], px), fmul(vc.mat[5], py));
+    int y0;
+    float b;
+    split_coord<kSampling>(fadd(av, vc.mat[13]), a.H, y0, b);
+    const float2* row0 = a.rl + (ptrdiff_t)y0 * (ptrdiff_t)a.rl_pitch;
+    const float2* row1 = row0 + a.rl_pitch;
+    const float omb = fsub(1.f, b);
+    const float2 mu2 = splat(vc.mat[8]), mu3 = splat(vc.mat[12]), sz = splat(s.z), lam = splat(a.lambda);
+    const float2 d = splat(s.w), bz = splat(g.bmin.z), vz = splat(g.vs.z);
+    const size_t plane = (size_t)g.rx * (size_t)g.ry;
+    size_t idx = (size_t)zb * plane + (size_t)y * (size_t)g.rx + (size_t)x;
+    for (int z = zb; z < ze; z += 2) {
+        const bool two = z + 1 < ze;
+        const float2 zf = f2((float)z, (float)(z + 1));
+        const float2 cz = add2(bz, mul2(add2(zf, splat(0.5f)), vz));  // VolumeGeometry.hl:17-20
+        const float2 pz = add2(cz, sz);
+        const float2 u2 = add2(add2(splat(au), mul2(mu2, pz)), mu3);
+        float2 ra, rb;
+        row_blend_pair<kSampling>(u2, row0, row1, b, omb, a.W, ra, rb);
+        // contribution r * lambda * (d / L), division refined from the reciprocal estimate
+        const float2 L = f2(ra.y, rb.y), R = f2(ra.x, rb.x);
+        const float2 rc = f2(rcp_approx(L.x), rcp_approx(L.y));
+        float2 q = mul2(d, rc);
+        const float2 e = fma2(f2(-L.x, -L.y), q, d);
+        q = fma2(e, rc, q);
+        float2 c = mul2(mul2(R, lam), q);
+        float va = bp_load<kStore>(a, idx);
+        float vb = two ? bp_load<kStore>(a, idx + plane) : 0.f;
+        if (kMask) {
+            c = mul2(f2(mask_weight(a.mask + idx), two ? mask_weight(a.mask + idx + plane) : 0.f), c);
+        }
+        const float2 nv = add2(f2(va, vb), c);
+        va = L.x > kEps ? nv.x : va;
+        vb = L.y > kEps ? nv.y : vb;
+        bp_store<kStore>(a, idx, va);
+        if (two) bp_store<kStore>(a, idx + plane, vb);
+        idx += 2 * plane;
     }
 }
 
