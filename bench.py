@@ -271,6 +271,44 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_e2e(args, ctx, geoms, b, params, world, lib_stream):
+    """30 iterations through etcu_reconstruct with pinned host buffers (in and out)."""
+    import torch
+    from ettention_b200 import _abi
+    from ettention_b200._abi import View, VolumeDesc, lib
+    host_proj = torch.empty(b.shape, dtype=torch.float32, pin_memory=True)
+    host_proj.copy_(b.cpu())
+    X, Y, Z = RES
+    host_vol = torch.zeros((Z, Y, X), dtype=torch.float32, pin_memory=True)
+    views = (View * N_VIEWS)(*[g.to_view() for g in geoms])
+    desc = VolumeDesc()
+    for i in range(3):
+        desc.resolution[i] = RES[i]
+        desc.bbox_min[i] = -0.5 * RES[i]
+        desc.bbox_max[i] = 0.5 * RES[i]
+    desc.subvolume_count = 1
+    rp = params.recon_params(True)
+    torch.cuda.empty_cache()
+    e2e_times = []
+    for rep in range(1 + args.e2e_reps):
+        host_vol.zero_()
+        barrier(world)
+        ctx.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(lib_stream)
+        ctx.check(lib().etcu_reconstruct(ctx.handle, ctypes.byref(desc), _abi.VOXEL_FLOAT32, views, N_VIEWS,
+                                         host_proj.data_ptr(), ctypes.byref(rp), TARGET_ITERS, host_vol.data_ptr()))
+        e1.record(lib_stream)
+        torch.cuda.synchronize()
+        if rep > 0:
+            e2e_times.append(e0.elapsed_time(e1))
+    e2e_ms = max_over_ranks(statistics.mean(e2e_times), world)
+    h2d = host_proj.numel() * 4 + host_vol.numel() * 4
+    d2h = host_vol.numel() * 4
+    return {"value": e2e_ms * 1e-3, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+
+
 # ------------------------------------------------------------------ ours
 def run_ours(args, rank, world, local):
     import torch
@@ -333,37 +371,10 @@ def run_ours(args, rank, world, local):
     rec.close()
     vol.close()
     # ---- e2e: one-call host-buffer reconstruction through the C ABI ----
-    host_proj = torch.empty(b.shape, dtype=torch.float32, pin_memory=True)
-    host_proj.copy_(b.cpu())
-    X, Y, Z = RES
-    host_vol = torch.zeros((Z, Y, X), dtype=torch.float32, pin_memory=True)
-    views = (View * N_VIEWS)(*[g.to_view() for g in geoms])
-    desc = VolumeDesc()
-    for i in range(3):
-        desc.resolution[i] = RES[i]
-        desc.bbox_min[i] = -0.5 * RES[i]
-        desc.bbox_max[i] = 0.5 * RES[i]
-    desc.subvolume_count = 1
-    rp = params.recon_params(True)
+    e2e = None
+    if args.e2e_reps > 0:
+        e2e = run_e2e(args, ctx, geoms, b, params, world, lib_stream)
     del b
-    torch.cuda.empty_cache()
-    e2e_times = []
-    for rep in range(1 + args.e2e_reps):
-        host_vol.zero_()
-        barrier(world)
-        ctx.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(lib_stream)
-        ctx.check(lib().etcu_reconstruct(ctx.handle, ctypes.byref(desc), _abi.VOXEL_FLOAT32, views, N_VIEWS,
-                                         host_proj.data_ptr(), ctypes.byref(rp), TARGET_ITERS, host_vol.data_ptr()))
-        e1.record(lib_stream)
-        torch.cuda.synchronize()
-        if rep > 0:
-            e2e_times.append(e0.elapsed_time(e1))
-    e2e_ms = max_over_ranks(statistics.mean(e2e_times), world)
-    h2d = host_proj.numel() * 4 + host_vol.numel() * 4
-    d2h = host_vol.numel() * 4
     # ---- CPU baseline (rank 0, N = 1 only) ----
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -381,7 +392,7 @@ def run_ours(args, rank, world, local):
                            "volume": list(RES), "views": N_VIEWS, "detector": list(DET), "lambda": LAMBDA,
                            "storage": "f32", "l2": "inputs larger than L2 (1 GiB volume)",
                            "parallelism": f"independent series per GPU x{world}"},
-                "e2e": {"value": e2e_ms * 1e-3, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                "e2e": e2e,
                 "gpu_launches": launches_per_iter * args.steps,
                 "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks.summary(),
                 "residual_sq": {"before": d0, "after_warmup_and_timed": d1},

@@ -189,7 +189,7 @@ __device__ __forceinline__ void dda_walk3(const DdaStart& st, const SlabConst& g
 // kUnroll steps at a time, issuing the kUnroll voxel loads before the
 // kUnroll accumulations (which stay in walk order).  Dead steps after the
 // exit load nothing and add exactly zero.
-template <typename VoxT, bool kMask, bool kCapped = true, int kUnroll = 4>
+template <typename VoxT, bool kMask, bool kCapped = true, int kUnroll = 8>
 __device__ __forceinline__ void dda_walk_xz(const DdaStart& st, const SlabConst& g, const VoxT* __restrict__ vol,
                                            const uint8_t* __restrict__ mask, float& acc, float& accl) {
     const unsigned plane = (unsigned)g.rx * (unsigned)g.ry;
@@ -347,7 +347,7 @@ struct FpArgs {
 enum FpPath : int { kFpPathGeneral = 0, kFpPathXz = 1, kFpPathXzNoCap = 2, kFpPathPerspective = 3 };
 
 template <typename VoxT, bool kMask, int kPath>
-__global__ void __launch_bounds__(128, (kPath == kFpPathXz || kPath == kFpPathXzNoCap) ? 10 : 4)
+__global__ void __launch_bounds__(128, (kPath == kFpPathXz || kPath == kFpPathXzNoCap) ? 9 : 4)
     forward_project_kernel(const __grid_constant__ FpArgs a) {
     constexpr bool kPerspective = kPath == kFpPathPerspective;
     int gx, gy;
@@ -864,7 +864,7 @@ __device__ __forceinline__ void row_blend_pair(float2 u2, const float2* __restri
 // an (x, y) column over a z range, computes the view's row taps once and updates
 // voxel pairs with paired FP32 instructions.
 template <bool kMask, int kStore, int kSampling>
-__global__ void __launch_bounds__(256) bp_sart_row_kernel(const __grid_constant__ BpArgs a) {
+__global__ void __launch_bounds__(256, 8) bp_sart_row_kernel(const __grid_constant__ BpArgs a) {
     const SlabConst& g = a.slab;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
