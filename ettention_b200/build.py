@@ -19,8 +19,12 @@ LIB = os.path.join(HERE, "libettention_b200.so")
 SOURCES = ["etcu_api.cu"]
 HEADERS = ["geometry.hpp", "kernels.cuh"]
 
+# -fmad=false: no multiply-add is formed implicitly.  The kernels follow the
+# reference's operation order step by step and write every intended fused
+# multiply-add explicitly (fmaf, __ffma2_rn); the paired FP32 operations
+# (__fmul2_rn, __fadd2_rn) are otherwise contracted by the compiler.
 NVCC_FLAGS = [
-    "-O3", "-std=c++17", "-lineinfo",
+    "-O3", "-std=c++17", "-lineinfo", "-fmad=false",
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
     "-shared", "--expt-relaxed-constexpr", "-cudart", "static",

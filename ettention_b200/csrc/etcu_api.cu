@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -37,6 +38,7 @@ struct etcu_context {
     size_t pair_pitch = 0;  // float2 units
     uint32_t pair_w = 0, pair_h = 0;
     cudaTextureObject_t pair_tex = 0;
+    bool bp_column = true;  // column-pipelined single-view back projection (ETCU_BP_COLUMN=0 disables)
 };
 
 struct etcu_volume {
@@ -78,6 +80,8 @@ struct etcu_recon {
     bool persp = false;
     std::vector<int> fp_paths;      // per slab
     std::vector<uint8_t> row_const; // per view id
+    std::vector<ViewConst> hvc;     // host copy of the view constants, [slab][view id]
+    std::vector<float4> hsamples;   // host copy of the sample patterns, [view id][sample]
 };
 
 namespace {
@@ -333,13 +337,161 @@ void launch_bp_sart_m(const BpArgs& a, etcu_voxel_type t, etcu_sampling sm, cuda
     }
 }
 
+struct BpColPlan {
+    int cols = 0;  // x columns per thread (1, 2, 4 or 8)
+    bool full = false;  // rx == cols * kBpColThreads
+    int x0lo = 0, ntaps = 0;
+    int zper = 0, zchunks = 0, grid = 0;
+    size_t smem = 0;
+};
+
+template <int kCols, bool kFull>
+void bp_col_limits(int dev, size_t smem, int& per_sm) {
+    static std::mutex mu;
+    static std::vector<char> opted;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if ((int)opted.size() <= dev) opted.resize(dev + 1, 0);
+        if (!opted[dev]) {
+            cudaDeviceProp prop;
+            if (cudaGetDeviceProperties(&prop, dev) == cudaSuccess)
+                cudaFuncSetAttribute(bp_sart_column_kernel<kCols, kFull>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)prop.sharedMemPerBlockOptin);
+            cudaGetLastError();
+            opted[dev] = 1;
+        }
+    }
+    per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_sart_column_kernel<kCols, kFull>, kBpColThreads, smem) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        per_sm = 0;
+    }
+}
+
+int device_sms(int dev) {
+    static std::mutex mu;
+    static std::vector<int> sms;
+    std::lock_guard<std::mutex> lock(mu);
+    if ((int)sms.size() <= dev) sms.resize(dev + 1, 0);
+    if (sms[dev] == 0) {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) cudaGetLastError();
+        sms[dev] = n;
+    }
+    return sms[dev];
+}
+
+// Whether the column-pipelined back projector applies to this view and
+// sub-volume, and its tap window, item and grid sizes.  It needs an FP32 volume
+// without mask and rows of at most 2048 voxels.  The tap window spans the
+// columns floor(u - 0.5) of every voxel centre with two columns of margin on each
+// side (the kernel's float coordinate is within a few ulps of the double
+// evaluated here at the sub-volume's corners; u is affine in the voxel indices).
+bool plan_bp_col(const etcu_volume* vol, const SlabConst& g, const ViewConst& vc, const float4& smp, BpColPlan& p) {
+    etcu_context* ctx = vol->ctx;
+    if (!ctx->bp_column || vol->type != ETCU_VOXEL_FLOAT32 || vol->mask) return false;
+    if (g.rx <= 0 || g.ry <= 0 || g.rz <= 0 || g.rx > 8 * kBpColThreads) return false;
+    double umin = 1e300, umax = -1e300;
+    for (int c = 0; c < 8; ++c) {
+        const double x = (c & 1) ? g.rx - 1 : 0, y = (c & 2) ? g.ry - 1 : 0, z = (c & 4) ? g.rz - 1 : 0;
+        const double px = (double)g.bmin.x + (x + 0.5) * g.vs.x + smp.x;
+        const double py = (double)g.bmin.y + (y + 0.5) * g.vs.y + smp.y;
+        const double pz = (double)g.bmin.z + (z + 0.5) * g.vs.z + smp.z;
+        const double u = (double)vc.mat[0] * px + (double)vc.mat[4] * py + (double)vc.mat[8] * pz + vc.mat[12];
+        umin = std::min(umin, u);
+        umax = std::max(umax, u);
+    }
+    if (!(umin > -16000.0 && umax < 16000.0)) return false;  // |256 u| < 2^22 for the tap split
+    p.x0lo = (int)std::floor(umin - 0.5) - 2;
+    p.ntaps = (int)std::floor(umax - 0.5) + 2 - p.x0lo + 1;
+    p.smem = bp_col_smem_bytes(g.rz, p.ntaps);
+    if (p.smem > 96 * 1024) return false;
+    const int need = (g.rx + kBpColThreads - 1) / kBpColThreads;
+    p.cols = need <= 1 ? 1 : need <= 2 ? 2 : need <= 4 ? 4 : 8;
+    p.full = g.rx == p.cols * kBpColThreads;
+    const int dev = ctx->device;
+    int per_sm = 0;
+    switch (p.cols * 2 + (p.full ? 1 : 0)) {
+    case 2: bp_col_limits<1, false>(dev, p.smem, per_sm); break;
+    case 3: bp_col_limits<1, true>(dev, p.smem, per_sm); break;
+    case 4: bp_col_limits<2, false>(dev, p.smem, per_sm); break;
+    case 5: bp_col_limits<2, true>(dev, p.smem, per_sm); break;
+    case 8: bp_col_limits<4, false>(dev, p.smem, per_sm); break;
+    case 9: bp_col_limits<4, true>(dev, p.smem, per_sm); break;
+    case 16: bp_col_limits<8, false>(dev, p.smem, per_sm); break;
+    default: bp_col_limits<8, true>(dev, p.smem, per_sm); break;
+    }
+    const int sms = device_sms(dev);
+    if (per_sm < 1 || sms < 1) return false;
+    const long long cap = (long long)sms * per_sm;
+    // z chunking: balance items over the resident blocks, counting about eight
+    // z rows of staging and pipeline start per item
+    long long best = -1;
+    for (int zc = 1; zc <= g.rz; ++zc) {
+        const int zper = (g.rz + zc - 1) / zc;
+        const int zcn = (g.rz + zper - 1) / zper;
+        const long long items = (long long)g.ry * zcn;
+        if (items > (1ll << 30)) break;
+        const long long grid = std::min(items, cap);
+        const long long cost = (items + grid - 1) / grid * (zper + 8);
+        if (best < 0 || cost < best) {
+            best = cost;
+            p.zper = zper;
+            p.zchunks = zcn;
+            p.grid = (int)grid;
+        }
+        if (items >= 64 * cap) break;
+    }
+    return best > 0;
+}
+
+void launch_bp_col(const BpArgs& a0, const BpColPlan& p, cudaStream_t st) {
+    BpColArgs a{};
+    a.vol = (float*)a0.vol;
+    a.slab = a0.slab;
+    a.views = a0.views;
+    a.order = a0.order;
+    a.first = a0.first;
+    a.inline_view = a0.inline_view;
+    a.samples = a0.samples;
+    a.inline_sample = a0.inline_samples[0];
+    a.rl = a0.rl;
+    a.rl_pitch = a0.rl_pitch;
+    a.W = a0.W;
+    a.H = a0.H;
+    a.lambda = a0.lambda;
+    a.x0lo = p.x0lo;
+    a.ntaps = p.ntaps;
+    a.zper = p.zper;
+    a.zchunks = p.zchunks;
+    const dim3 grid(p.grid), block(kBpColThreads);
+    switch (p.cols * 2 + (p.full ? 1 : 0)) {
+    case 2: bp_sart_column_kernel<1, false><<<grid, block, p.smem, st>>>(a); break;
+    case 3: bp_sart_column_kernel<1, true><<<grid, block, p.smem, st>>>(a); break;
+    case 4: bp_sart_column_kernel<2, false><<<grid, block, p.smem, st>>>(a); break;
+    case 5: bp_sart_column_kernel<2, true><<<grid, block, p.smem, st>>>(a); break;
+    case 8: bp_sart_column_kernel<4, false><<<grid, block, p.smem, st>>>(a); break;
+    case 9: bp_sart_column_kernel<4, true><<<grid, block, p.smem, st>>>(a); break;
+    case 16: bp_sart_column_kernel<8, false><<<grid, block, p.smem, st>>>(a); break;
+    default: bp_sart_column_kernel<8, true><<<grid, block, p.smem, st>>>(a); break;
+    }
+}
+
 // Back projection of a.nviews views; when their staged constants exceed the
 // shared-memory budget the views are split over consecutive launches, which
-// applies them in the same order.  Returns the number of launches.
+// applies them in the same order.  `hvc` / `hsmp` are host copies of the single
+// view's constants and sample (they select the column-pipelined kernel).  Returns the
+// number of launches.
 uint32_t launch_bp(const etcu_volume* vol, const BpArgs& a0, bool persp, etcu_sampling sm, cudaStream_t st,
-                   bool row_const = false) {
+                   bool row_const = false, const ViewConst* hvc = nullptr, const float4* hsmp = nullptr) {
     const int dev = vol->ctx->device;
     if (!persp && row_const && a0.nviews == 1 && a0.nsamples == 1 && sm != ETCU_SAMPLING_HW_TEXTURE) {
+        BpColPlan plan;
+        if (sm == ETCU_SAMPLING_Q8 && hvc && hsmp && plan_bp_col(vol, a0.slab, *hvc, *hsmp, plan)) {
+            launch_bp_col(a0, plan, st);
+            return 1;
+        }
         if (a0.mask) launch_bp_sart_m<true>(a0, vol->type, sm, st);
         else launch_bp_sart_m<false>(a0, vol->type, sm, st);
         return 1;
@@ -480,6 +632,7 @@ extern "C" etcu_status etcu_context_create(int device, etcu_context** out) {
     if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamDefault) != cudaSuccess)
         return fail(nullptr, ETCU_ERR_CUDA, "cudaStreamCreate failed");
     c->stream = c->own_stream;
+    if (const char* env = getenv("ETCU_BP_COLUMN")) c->bp_column = atoi(env) != 0;
     *out = c.release();
     return ETCU_OK;
 }
@@ -766,7 +919,8 @@ etcu_status bp_one_slab(etcu_volume* vol, const etcu_view* view, const SlabConst
     a.use_max = vol->use_max;
     a.vmin = vol->vmin;
     a.vmax = vol->vmax;
-    launch_bp(vol, a, view->perspective != 0, sampling, ctx->stream, row_constant(a.inline_view));
+    launch_bp(vol, a, view->perspective != 0, sampling, ctx->stream, row_constant(a.inline_view), &a.inline_view,
+              &a.inline_samples[0]);
     CKL(ctx);
     return ETCU_OK;
 }
@@ -931,7 +1085,10 @@ uint32_t issue_backward(etcu_recon* r, uint32_t first, uint32_t count, cudaStrea
         a.use_max = vol->use_max;
         a.vmin = vol->vmin;
         a.vmax = vol->vmax;
-        n += launch_bp(vol, a, r->persp, r->params.sampling, st, count == 1 && r->row_const[r->order[first]]);
+        const uint32_t vid = r->order[first];
+        n += launch_bp(vol, a, r->persp, r->params.sampling, st, count == 1 && r->row_const[vid],
+                       &r->hvc[(size_t)s * r->n_input + vid],
+                       r->hsamples.empty() ? nullptr : &r->hsamples[(size_t)vid * r->nsamples]);
     }
     return n;
 }
@@ -1014,6 +1171,7 @@ etcu_status recon_build(etcu_volume* vol, const etcu_view* views, uint32_t n_vie
                 loc = traversal_length(views[i], vol->desc.bbox_min, vol->desc.bbox_max);
             vc[sl * n_views + i] = make_view_const(views[i], vol->slabs[sl], loc);
         }
+    r->hvc = vc;
     r->row_const.resize(n_views);
     for (uint32_t i = 0; i < n_views; ++i) r->row_const[i] = row_constant(vc[i]) ? 1 : 0;
     r->fp_paths.resize(S);
@@ -1035,6 +1193,10 @@ etcu_status recon_build(etcu_volume* vol, const etcu_view* views, uint32_t n_vie
             std::string err;
             if (!sample_pattern(views[i], vs, params->bp_samples, pat.data() + 4 * (size_t)params->bp_samples * i, &err))
                 return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "%s", err.c_str());
+        }
+        if (params->bp_samples > 0) {
+            r->hsamples.resize(pat.size() / 4);
+            std::memcpy(r->hsamples.data(), pat.data(), pat.size() * sizeof(float));
         }
         if ((s = dalloc(ctx, (void**)&r->d_samples, pat.size() * sizeof(float))) != ETCU_OK) return s;
         CK(ctx, cudaMemcpyAsync(r->d_samples, pat.data(), pat.size() * sizeof(float), cudaMemcpyHostToDevice,

@@ -806,63 +806,44 @@ __global__ void __launch_bounds__(256, 4) bp_parallel_kernel(const __grid_consta
 }
 
 // ---- single-view, single-sample parallel back projection (SART's hot case) ----
-// Paired FP32 arithmetic (two voxels per instruction); every lane rounds to nearest
-// exactly as the scalar operations do, so results are bit-identical to
-// bp_parallel_kernel.
+// Paired FP32 helpers.  The compiler fuses a paired multiply into a following
+// paired add (even with -fmad=false), so they are used only where no product
+// feeds a sum; every product that feeds a sum is a scalar __fmul_rn.
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 __device__ __forceinline__ float2 splat(float a) { return make_float2(a, a); }
 __device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 
-// One voxel pair's sample: the 1/256-rounded (or exact) blend of the (residual, length)
-// image at column coordinates u2, row taps fixed by (row0, row1, b).
+// One voxel's sample from a detector row pair fixed by (row0, row0 + pitch, b):
+// column split and blend exactly as sample_pair.
 template <int kSampling>
-__device__ __forceinline__ void row_blend_pair(float2 u2, const float2* __restrict__ row0,
-                                               const float2* __restrict__ row1, float b, float omb, int W,
-                                               float2& rl_a, float2& rl_b) {
-    float2 ax2;
-    int x0a, x0b;
-    if (kSampling == kSampleQ8) {
-        // q = floor((u - 0.5) * 256 + 0.5); u * 256 - 127.5 is exact for |u| < 2^15
-        const float2 t = fma2(u2, splat(256.f), splat(-127.5f));
-        const float2 q = f2(floorf(t.x), floorf(t.y));
-        const float2 qs = mul2(q, splat(1.f / 256.f));
-        const float2 xf = f2(floorf(qs.x), floorf(qs.y));
-        ax2 = fma2(q, splat(1.f / 256.f), f2(-xf.x, -xf.y));
-        x0a = (int)xf.x;
-        x0b = (int)xf.y;
-    } else {
-        const float2 cs = add2(u2, splat(-0.5f));
-        const float2 cb = f2(floorf(cs.x), floorf(cs.y));
-        const float2 fr = add2(cs, f2(-cb.x, -cb.y));
-        ax2 = f2(fminf(fr.x, 0x1.fffffep-1f), fminf(fr.y, 0x1.fffffep-1f));
-        x0a = (int)cb.x;
-        x0b = (int)cb.y;
-    }
-    x0a = min(max(x0a, -kPad), W);
-    x0b = min(max(x0b, -kPad), W);
-    const float2 a00 = __ldg(row0 + x0a), a10 = __ldg(row0 + x0a + 1), a01 = __ldg(row1 + x0a), a11 = __ldg(row1 + x0a + 1);
-    const float2 b00 = __ldg(row0 + x0b), b10 = __ldg(row0 + x0b + 1), b01 = __ldg(row1 + x0b), b11 = __ldg(row1 + x0b + 1);
-    if (kSampling == kSampleQ8) {
-        const float2 oma = add2(splat(1.f), f2(-ax2.x, -ax2.y));
-        const float2 w00 = mul2(oma, splat(omb)), w10 = mul2(ax2, splat(omb));
-        const float2 w01 = mul2(oma, splat(b)), w11 = mul2(ax2, splat(b));
-        rl_a = add2(add2(add2(mul2(splat(w00.x), a00), mul2(splat(w10.x), a10)), mul2(splat(w01.x), a01)),
-                    mul2(splat(w11.x), a11));
-        rl_b = add2(add2(add2(mul2(splat(w00.y), b00), mul2(splat(w10.y), b10)), mul2(splat(w01.y), b01)),
-                    mul2(splat(w11.y), b11));
-    } else {
-        auto mix = [](float2 p, float2 q, float t) { return add2(p, mul2(add2(q, f2(-p.x, -p.y)), splat(t))); };
-        rl_a = mix(mix(a00, a10, ax2.x), mix(a01, a11, ax2.x), b);
-        rl_b = mix(mix(b00, b10, ax2.y), mix(b01, b11, ax2.y), b);
-    }
+__device__ __forceinline__ float2 row_sample(float u, const float2* __restrict__ row0, size_t pitch, float b, int W) {
+    int x0;
+    float ax;
+    split_coord<kSampling>(u, W, x0, ax);
+    float2 t00, t10, t01, t11;
+    taps(row0, pitch, x0, t00, t10, t01, t11);
+    return blend<kSampling>(ax, b, t00, t10, t01, t11);
+}
+
+// voxel + mask * r * lambda * (d / L) when L > eps (ParallelBeamsBackProjection.cl:40-50),
+// the division refined from the reciprocal estimate.
+__device__ __forceinline__ float sart_update(float v, float2 rl, float lam, float d, float mw, bool masked) {
+    const float L = rl.y;
+    const float rc = rcp_approx(L);
+    float q = fmul(d, rc);
+    const float e = fmaf(-L, q, d);
+    q = fmaf(e, rc, q);
+    float c = fmul(fmul(rl.x, lam), q);
+    if (masked) c = fmul(mw, c);
+    return L > kEps ? fadd(v, c) : v;
 }
 
 // ParallelBeamsBackProjection.cl:9-52 for one view with one sample per voxel and a
 // detector row that depends only on y (every view tilted about y): each thread owns
 // an (x, y) column over a z range, computes the view's row taps once and updates
-// voxel pairs with paired FP32 instructions.
+// two voxels per iteration.  Same operations as bp_parallel_kernel.
 template <bool kMask, int kStore, int kSampling>
 __global__ void __launch_bounds__(256, 8) bp_sart_row_kernel(const __grid_constant__ BpArgs a) {
     const SlabConst& g = a.slab;
@@ -884,38 +865,166 @@ __global__ void __launch_bounds__(256, 8) bp_sart_row_kernel(const __grid_consta
     float b;
     split_coord<kSampling>(fadd(av, vc.mat[13]), a.H, y0, b);
     const float2* row0 = a.rl + (ptrdiff_t)y0 * (ptrdiff_t)a.rl_pitch;
-    const float2* row1 = row0 + a.rl_pitch;
-    const float omb = fsub(1.f, b);
-    const float2 mu2 = splat(vc.mat[8]), mu3 = splat(vc.mat[12]), sz = splat(s.z), lam = splat(a.lambda);
-    const float2 d = splat(s.w), bz = splat(g.bmin.z), vz = splat(g.vs.z);
+    const float m8 = vc.mat[8], m12 = vc.mat[12], lam = a.lambda, d = s.w;
     const size_t plane = (size_t)g.rx * (size_t)g.ry;
     size_t idx = (size_t)zb * plane + (size_t)y * (size_t)g.rx + (size_t)x;
     for (int z = zb; z < ze; z += 2) {
         const bool two = z + 1 < ze;
-        const float2 zf = f2((float)z, (float)(z + 1));
-        const float2 cz = add2(bz, mul2(add2(zf, splat(0.5f)), vz));  // VolumeGeometry.hl:17-20
-        const float2 pz = add2(cz, sz);
-        const float2 u2 = add2(add2(splat(au), mul2(mu2, pz)), mu3);
-        float2 ra, rb;
-        row_blend_pair<kSampling>(u2, row0, row1, b, omb, a.W, ra, rb);
-        // contribution r * lambda * (d / L), division refined from the reciprocal estimate
-        const float2 L = f2(ra.y, rb.y), R = f2(ra.x, rb.x);
-        const float2 rc = f2(rcp_approx(L.x), rcp_approx(L.y));
-        float2 q = mul2(d, rc);
-        const float2 e = fma2(f2(-L.x, -L.y), q, d);
-        q = fma2(e, rc, q);
-        float2 c = mul2(mul2(R, lam), q);
+        // VolumeGeometry.hl:17-20 voxel centres of z and z + 1
+        const float pza = fadd(fadd(g.bmin.z, fmul(fadd((float)z, 0.5f), g.vs.z)), s.z);
+        const float pzb = fadd(fadd(g.bmin.z, fmul(fadd((float)(z + 1), 0.5f), g.vs.z)), s.z);
+        const float2 ra = row_sample<kSampling>(fadd(fadd(au, fmul(m8, pza)), m12), row0, a.rl_pitch, b, a.W);
+        const float2 rb = row_sample<kSampling>(fadd(fadd(au, fmul(m8, pzb)), m12), row0, a.rl_pitch, b, a.W);
         float va = bp_load<kStore>(a, idx);
         float vb = two ? bp_load<kStore>(a, idx + plane) : 0.f;
-        if (kMask) {
-            c = mul2(f2(mask_weight(a.mask + idx), two ? mask_weight(a.mask + idx + plane) : 0.f), c);
-        }
-        const float2 nv = add2(f2(va, vb), c);
-        va = L.x > kEps ? nv.x : va;
-        vb = L.y > kEps ? nv.y : vb;
+        const float mwa = kMask ? mask_weight(a.mask + idx) : 1.f;
+        const float mwb = kMask && two ? mask_weight(a.mask + idx + plane) : 1.f;
+        va = sart_update(va, ra, lam, d, mwa, kMask);
+        vb = sart_update(vb, rb, lam, d, mwb, kMask);
         bp_store<kStore>(a, idx, va);
         if (two) bp_store<kStore>(a, idx + plane, vb);
         idx += 2 * plane;
+    }
+}
+
+// ---- column-pipelined single-view back projection (SART's hot case, FP32 volume) ----
+// A block owns items (y, z range) of the sub-volume; each thread owns kCols x
+// columns of the item and walks them down z with the volume loads of the next two
+// z rows in flight (2 * kCols coalesced loads per thread), so the block needs no
+// barrier inside an item.
+// Sampling: the view's detector row coordinate is fixed for the item, so its row
+// weight b is too, and the two detector rows are blended once per item,
+// P[x] = (1 - b) * t0[x] + b * t1[x], into a staged window of tap pairs
+// (P[x0], P[x0 + 1]) over the columns [x0lo, x0lo + ntaps) that the host bounds
+// from the view and sub-volume corners.  Each voxel then takes one 16-byte shared
+// load and blends along x with the 1/256 weight a: (1 - a) * P[x0] + a * P[x0 + 1].
+// This is the same bilinear weighting as blend<kSampleQ8> with the row pass
+// first; only the rounding order differs (by an ulp of the sample; identical when
+// b == 0).  The window holds zeros outside the padded image, where the direct
+// kernels clamp onto zero border texels, so no clamp is needed per voxel.  The
+// 1/256 split of the column coordinate is integer work on the bits of
+// fl_down(t + 1.5 * 2^23), which is 1.5 * 2^23 + floor(t) for |t| < 2^22.
+struct BpColArgs {
+    float* vol;                 // sub-volume base, x-fastest [z][y][x]
+    SlabConst slab;
+    const ViewConst* views;     // view table by view id (nullptr: inline_view)
+    const uint32_t* order;
+    uint32_t first;
+    ViewConst inline_view;
+    const float4* samples;      // one (x, y, z, chord) per view id; nullptr -> inline_sample
+    float4 inline_sample;
+    const float2* rl;           // texel (0, 0) of the padded (residual, length) image
+    size_t rl_pitch;            // float2 units
+    int W, H;
+    float lambda;
+    int x0lo, ntaps;            // staged tap pairs: columns x0lo .. x0lo + ntaps - 1
+    int zper;                   // z rows per item
+    int zchunks;                // items per y
+};
+
+constexpr int kBpColThreads = 256;
+
+__host__ __device__ constexpr size_t bp_col_smem_bytes(int rz, int ntaps) {
+    return (size_t)ntaps * 16 + (size_t)rz * 4;  // row-blended tap pairs, per-z term
+}
+
+// Column tap of one voxel from f = fl_down(t + 1.5 * 2^23) = 1.5 * 2^23 + floor(t),
+// t = u * 256 - 127.5 (exact): tap-pair index x0 - x0lo and 1 + a, where
+// a = (floor(t) mod 256) / 256 is the 1/256 weight (exact).
+__device__ __forceinline__ void q8_tap_bits(float f, int x0lo, int& e, float& a1) {
+    const int bits = __float_as_int(f);
+    e = (bits >> 8) - ((0x4B400000 >> 8) + x0lo);
+    a1 = __int_as_float(((bits << 15) & 0x007F8000) | 0x3F800000);
+}
+
+// kFull: every thread owns all kCols columns (rx == kCols * kBpColThreads).
+template <int kCols, bool kFull>
+__global__ void __launch_bounds__(kBpColThreads, 4) bp_sart_column_kernel(const __grid_constant__ BpColArgs a) {
+    extern __shared__ __align__(16) unsigned char bp_col_smem[];
+    const SlabConst& g = a.slab;
+    const int rx = g.rx, ry = g.ry, rz = g.rz, tid = threadIdx.x;
+    const int ntaps = a.ntaps, x0lo = a.x0lo;
+    float4* taps = (float4*)bp_col_smem;
+    float* K = (float*)(taps + ntaps);
+
+    const uint32_t vid = a.order ? a.order[a.first] : a.first;
+    const ViewConst& vc = a.views ? a.views[vid] : a.inline_view;
+    const float4 s = a.samples ? a.samples[vid] : a.inline_sample;
+
+    // ParallelBeamsBackProjection.cl coordinate terms, in the kernel's operation order
+    for (int z = tid; z < rz; z += kBpColThreads)
+        K[z] = fmul(vc.mat[8], fadd(fadd(g.bmin.z, fmul(fadd((float)z, 0.5f), g.vs.z)), s.z));
+    float A[kCols];
+#pragma unroll
+    for (int k = 0; k < kCols; ++k)
+        A[k] = fmul(vc.mat[0], fadd(fadd(g.bmin.x, fmul(fadd((float)(tid + k * kBpColThreads), 0.5f), g.vs.x)), s.x));
+    const int ncols = kFull ? kCols : min(kCols, max(0, (rx - tid + kBpColThreads - 1) / kBpColThreads));
+    const float lam = a.lambda, d = s.w, m12 = vc.mat[12];
+    const float px0 = fadd(fadd(g.bmin.x, fmul(0.5f, g.vs.x)), s.x);
+    const size_t plane = (size_t)rx * (size_t)ry;
+    const float2 zero = make_float2(0.f, 0.f);
+    const int items = ry * a.zchunks;
+
+    for (int it = blockIdx.x; it < items; it += gridDim.x) {
+        const int y = it / a.zchunks;
+        const int z0 = (it - y * a.zchunks) * a.zper, z1 = min(rz, z0 + a.zper);
+        // the item's detector row (uniform over the block)
+        const float py = fadd(fadd(g.bmin.y, fmul(fadd((float)y, 0.5f), g.vs.y)), s.y);
+        const float av = fadd(fmul(vc.mat[1], px0), fmul(vc.mat[5], py));
+        int y0;
+        float b;
+        split_coord<kSampleQ8>(fadd(av, vc.mat[13]), a.H, y0, b);
+        const float omb = fsub(1.f, b);
+        const float cy4 = fmul(vc.mat[4], py);
+        const float2* r0 = a.rl + (ptrdiff_t)y0 * (ptrdiff_t)a.rl_pitch;
+        const float2* r1 = r0 + a.rl_pitch;
+        __syncthreads();  // the previous item's taps are no longer read (K is ready the first time)
+        for (int e = tid; e < ntaps; e += kBpColThreads) {
+            // columns outside the padded image read zero, as the clamped taps of the
+            // direct kernels read the zero border
+            const int x0 = x0lo + e;
+            const bool in0 = x0 >= -kPad && x0 < a.W + kPad, in1 = x0 + 1 >= -kPad && x0 + 1 < a.W + kPad;
+            const float2 p0 = in0 ? __ldg(r0 + x0) : zero, q0 = in1 ? __ldg(r0 + x0 + 1) : zero;
+            const float2 p1 = in0 ? __ldg(r1 + x0) : zero, q1 = in1 ? __ldg(r1 + x0 + 1) : zero;
+            taps[e] = make_float4(fadd(fmul(omb, p0.x), fmul(b, p1.x)), fadd(fmul(omb, p0.y), fmul(b, p1.y)),
+                                  fadd(fmul(omb, q0.x), fmul(b, q1.x)), fadd(fmul(omb, q0.y), fmul(b, q1.y)));
+        }
+        __syncthreads();
+        if (z0 >= z1 || ncols == 0) continue;
+        float au[kCols];
+#pragma unroll
+        for (int k = 0; k < kCols; ++k) au[k] = fadd(A[k], cy4);
+        float* p = a.vol + ((size_t)z0 * ry + y) * rx + tid;
+        float cur[kCols], nxt[kCols];
+#pragma unroll
+        for (int k = 0; k < kCols; ++k) {
+            cur[k] = k < ncols ? __ldg(p + k * kBpColThreads) : 0.f;
+            nxt[k] = (k < ncols && z0 + 1 < z1) ? __ldg(p + plane + k * kBpColThreads) : 0.f;
+        }
+        for (int z = z0; z < z1; ++z) {
+            float nn[kCols];
+            const bool more = z + 2 < z1;
+            const float* pn = p + 2 * plane;
+#pragma unroll
+            for (int k = 0; k < kCols; ++k) nn[k] = (more && k < ncols) ? __ldg(pn + k * kBpColThreads) : 0.f;
+            const float kz = K[z];
+#pragma unroll
+            for (int k = 0; k < kCols; ++k) {
+                if (k < ncols) {
+                    const float u = fadd(fadd(au[k], kz), m12);
+                    int e;
+                    float a1;
+                    q8_tap_bits(__fadd_rd(fmaf(u, 256.f, -127.5f), 12582912.0f), x0lo, e, a1);
+                    const float4 t = taps[e];
+                    const float ax = fsub(a1, 1.f), oma = fsub(1.f, ax);
+                    const float2 rl = make_float2(fadd(fmul(oma, t.x), fmul(ax, t.z)), fadd(fmul(oma, t.y), fmul(ax, t.w)));
+                    p[k * kBpColThreads] = sart_update(cur[k], rl, lam, d, 1.f, false);
+                }
+                cur[k] = nxt[k];
+                nxt[k] = nn[k];
+            }
+            p += plane;
+        }
     }
 }
 

@@ -1,0 +1,179 @@
+"""Column-pipelined single-view back projection (SART's hot case on an FP32
+volume): detector taps staged in shared memory per (y, z range) item, each thread
+walking its x columns down z with the next rows' volume loads in flight.
+
+It blends the two detector rows once per item and then along x (the direct
+kernels blend all four taps per voxel), so it matches the direct single-view
+kernel (a context created with ETCU_BP_COLUMN=0 never uses it) to rounding:
+relative L2 of the volume updates <= 1e-6 (measured ~1e-7), and the oracle
+within the back-projection tolerance, for row weights b == 0.5 (the MRC tilt
+geometry), b != 0.5 (shifted or finer detector rows), ragged sizes (x rows that do
+not fill a block, odd z counts), voxels that project beyond the detector edge
+and several sub-volumes.  Half-precision volumes, masked volumes and exact
+(unquantised) sampling fall back to the direct kernel.
+"""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+BP_TOL = 1e-4
+SAME_TOL = 1e-6  # column vs direct kernel: bilinear sums in another order
+
+
+@pytest.fixture(scope="module")
+def ctxs():
+    import torch
+    from ettention_b200.operators import Context
+    assert torch.cuda.is_available()
+    old = os.environ.get("ETCU_BP_COLUMN")
+    os.environ["ETCU_BP_COLUMN"] = "0"
+    try:
+        direct = Context(0)
+    finally:
+        if old is None:
+            del os.environ["ETCU_BP_COLUMN"]
+        else:
+            os.environ["ETCU_BP_COLUMN"] = old
+    column = Context(0)
+    yield direct, column
+    column.close()
+    direct.close()
+
+
+def kernel_names(fn):
+    """CUDA kernels launched by fn (CUPTI activity records through torch.profiler)."""
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        fn()
+        torch.cuda.synchronize()
+    return {e.name for e in prof.events()}
+
+
+def geometry(X, Y, angle, dy=0.0, vpitch=1.0, width=None):
+    from ettention_b200.operators import ScannerGeometry
+    W = X if width is None else width
+    H = int(round(Y / vpitch))
+    base = ScannerGeometry([-0.5 * W, -0.5 * H * vpitch + dy, float(X)], [-0.5 * W, -0.5 * H * vpitch + dy, -float(X)],
+                           [1.0, 0.0, 0.0], [0.0, vpitch, 0.0], W, H, False)
+    return base.rotated(angle)
+
+
+def back_project(ctx, shape_xyz, g, res, L, lam, init, subvolumes=1, sampling=0, mask=None, voxel_type=0):
+    import torch
+    from ettention_b200.operators import BackProjectionOperator, GPUMappedVolume
+    vol = GPUMappedVolume(ctx, shape_xyz, subvolume_count=subvolumes, voxel_type=voxel_type)
+    vol.upload(init)
+    if mask is not None:
+        vol.set_mask(mask)
+    bp = BackProjectionOperator(vol, lam, 1, sampling)
+    bp.setScannerGeometry(g)
+    bp.setInput(torch.as_tensor(res).cuda(), torch.as_tensor(L).cuda(), 1)
+    bp.execute()
+    ctx.synchronize()
+    out = vol.download()
+    vol.close()
+    return out
+
+
+def oracle_bp(shape_xyz, g, res, L, lam, init, subvolumes=1, sampling=0, mask=None, half=False):
+    from oracle import oracle as O
+    from tests.helpers import oracle_geometry
+    vg = O.VolumeGeometry.centered(shape_xyz, subvolumes=subvolumes)
+    v = O.to_half(init) if half else init.copy()
+    O.back_project(v, vg, oracle_geometry(g), res, L, lam, 1, 32, O.WEIGHTS_EXACT if sampling else O.WEIGHTS_Q8,
+                   mask=mask)
+    return v.astype(np.float32)
+
+
+CASES = [
+    # (X, Y, Z), angle, detector y shift, vertical pitch, detector width, sub-volumes
+    ((96, 80, 40), -60.0, 0.0, 1.0, None, 1),
+    ((96, 80, 40), 33.0, 0.0, 1.0, None, 1),    # corner voxels project beyond the detector edge
+    ((96, 80, 40), 0.0, 0.37, 1.0, None, 1),    # rows between detector pixels: b != 0
+    ((68, 24, 37), 17.5, 0.0, 1.0, None, 1),    # 68-voxel rows, odd z count
+    ((68, 24, 37), -41.0, 0.0, 0.75, None, 1),  # b varies with y
+    ((528, 6, 21), 9.0, 0.25, 1.0, None, 1),    # rows longer than a block, short z
+    ((64, 40, 48), 52.0, 0.0, 1.0, None, 3),    # three sub-volumes
+    ((96, 40, 24), 20.0, 0.0, 1.0, 48, 1),      # detector narrower than the volume's shadow
+]
+
+
+@pytest.mark.parametrize("shape,angle,dy,vpitch,width,subs", CASES)
+def test_column_bp_bit_identical_to_direct_and_matches_oracle(ctxs, shape, angle, dy, vpitch, width, subs):
+    from oracle import oracle as O
+    direct, column = ctxs
+    X, Y, Z = shape
+    rng = np.random.Generator(np.random.PCG64(X * 1000 + Z + int(abs(angle) * 10)))
+    g = geometry(X, Y, angle, dy, vpitch, width)
+    res = rng.normal(size=(g.height, g.width)).astype(np.float32)
+    L = rng.uniform(0.5, 2.0 * Z, size=(g.height, g.width)).astype(np.float32)
+    L[rng.uniform(size=L.shape) < 0.05] = 0.0  # pixels no ray crossed
+    init = rng.uniform(0, 1, size=(Z, Y, X)).astype(np.float32)
+
+    def run():
+        run.out = back_project(column, shape, g, res, L, 0.3, init, subs)
+    names = kernel_names(run)
+    v_col = run.out
+    assert any("bp_sart_column_kernel" in n for n in names), sorted(names)
+    v_direct = back_project(direct, shape, g, res, L, 0.3, init, subs)
+    assert O.rel_l2(v_col - init, v_direct - init) <= SAME_TOL
+    vo = oracle_bp(shape, g, res, L, 0.3, init, subs)
+    assert O.rel_l2(v_col - init, vo - init) <= BP_TOL
+
+
+@pytest.mark.parametrize("shape,sampling,masked,half", [((66, 20, 16), 0, False, True),  # half volume
+                                                        ((64, 20, 16), 1, False, False),  # exact sampling
+                                                        ((64, 20, 16), 0, True, False)])  # masked volume
+def test_ineligible_cases_fall_back(ctxs, shape, sampling, masked, half):
+    from oracle import oracle as O
+    _, column = ctxs
+    X, Y, Z = shape
+    rng = np.random.Generator(np.random.PCG64(X + 10 * sampling + int(masked)))
+    g = geometry(X, Y, 20.0)
+    res = rng.normal(size=(g.height, g.width)).astype(np.float32)
+    L = rng.uniform(0.5, 40.0, size=(g.height, g.width)).astype(np.float32)
+    init = rng.uniform(0, 1, size=(Z, Y, X)).astype(np.float32)
+    mask = rng.integers(0, 256, size=(Z, Y, X), dtype=np.uint8) if masked else None
+
+
+    def run():
+        run.out = back_project(column, shape, g, res, L, 0.3, init, sampling=sampling, mask=mask,
+                               voxel_type=1 if half else 0)
+    names = kernel_names(run)
+    assert not any("bp_sart_column_kernel" in n for n in names)
+    assert any("bp_sart_row_kernel" in n for n in names)
+    vo = oracle_bp(shape, g, res, L, 0.3, init, sampling=sampling, mask=mask, half=half)
+    if half:  # half storage: volumes within half rounding, as the direct kernel's own parity test
+        assert O.rel_l2(run.out, vo) <= 1e-3
+    else:
+        assert O.rel_l2(run.out - init, vo - init) <= BP_TOL
+
+
+def test_sart_reconstruction_column_matches_direct(ctxs):
+    from oracle import oracle as O
+    from ettention_b200 import _abi
+    from ettention_b200.operators import (AlgebraicParameterSet, BlockIterativeReconstructionOperator,
+                                          GPUMappedVolume, mrc_base_geometry)
+    from tests.helpers import ellipsoid_phantom
+    direct, column = ctxs
+    X, Y, Z = 112, 64, 44
+    rng = np.random.Generator(np.random.PCG64(7))
+    geoms = [mrc_base_geometry(X, Y).rotated(float(a)) for a in np.linspace(-60, 60, 13)]
+    projs = rng.uniform(0, 4, size=(13, Y, X)).astype(np.float32)
+    init = ellipsoid_phantom((X, Y, Z), 6, seed=7)
+    p = AlgebraicParameterSet(algorithm="sart", block_size=1, iterations=2, lam=0.3, order=_abi.ORDER_RANDOM)
+    outs = []
+    for ctx in (direct, column):
+        vol = GPUMappedVolume(ctx, (X, Y, Z), subvolume_count=2)
+        vol.upload(init)
+        rec = BlockIterativeReconstructionOperator(vol, geoms, projs, p, use_graph=True)
+        rec.runNiterations(2)
+        outs.append(rec.getReconstructedVolume())
+        rec.close()
+        vol.close()
+    assert np.abs(outs[1] - init).max() > 0
+    assert O.rel_l2(outs[1] - init, outs[0] - init) <= 1e-5
