@@ -210,9 +210,12 @@ ViewConst make_view_const(const etcu_view& v, const SlabConst& slab, float loc_l
         return a * sg;
     };
     float sdx = sdf(slab.vs.x, inv[0], r.x), sdy = sdf(slab.vs.y, inv[1], r.y), sdz = sdf(slab.vs.z, inv[2], r.z);
-    const bool small = (unsigned long long)slab.rx * (unsigned long long)slab.ry * (unsigned long long)slab.rz <
-                       (1ull << 32);
-    c.fast2d = (!v.perspective && r.y == 0.f && small && std::isfinite(sdx) && std::isfinite(sdy) &&
+    // The xz walk decodes (iz, ix) from its 32-bit offset iz * rx * ry + ix: a step off
+    // the x range must not alias a voxel of another z row (ry >= 2), and one below
+    // z = 0 must wrap past the last row ((rz + 1) * rx * ry <= 2^32).
+    const bool decodable = slab.ry >= 2 && (unsigned long long)slab.rx * (unsigned long long)slab.ry *
+                                                   (unsigned long long)(slab.rz + 1) <= (1ull << 32);
+    c.fast2d = (!v.perspective && r.y == 0.f && decodable && std::isfinite(sdx) && std::isfinite(sdy) &&
                 std::isfinite(sdz)) ? 1 : 0;
     return c;
 }

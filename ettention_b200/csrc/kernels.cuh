@@ -42,7 +42,7 @@ struct ViewConst {
     float mat[16];    // column-major projection matrix
     float loc_length; // long-object constant length
     int perspective;
-    int fast2d;       // parallel view with ray.y == 0 and finite step differences
+    int fast2d;       // parallel view with ray.y == 0, finite step differences, a decodable sub-volume
     int pad;
 };
 
@@ -184,12 +184,13 @@ __device__ __forceinline__ void dda_walk3(const DdaStart& st, const SlabConst& g
 //
 // The loop is restructured for memory-level parallelism without changing
 // the arithmetic: instead of re-testing the voxel index against the slab
-// bounds, each axis carries the number of steps it may still take before it
-// leaves the slab (the same exit condition), and the walk advances
-// kUnroll steps at a time, issuing the kUnroll voxel loads before the
-// kUnroll accumulations (which stay in walk order).  Dead steps after the
-// exit load nothing and add exactly zero.
-template <typename VoxT, bool kMask, bool kCapped = true, int kUnroll = 8>
+// bounds every step, the walk decodes the current voxel from its offset,
+// takes the number of steps each axis may still make before it leaves the
+// slab (the same exit condition) and runs the smaller count unchecked,
+// kUnroll steps at a time, issuing the kUnroll voxel loads before the kUnroll
+// accumulations (which stay in walk order).  The decode needs ry >= 2 and
+// (rz + 1) * rx * ry <= 2^32 (ViewConst::fast2d).
+template <typename VoxT, bool kMask, bool kCapped = true, int kUnroll = 16>
 __device__ __forceinline__ void dda_walk_xz(const DdaStart& st, const SlabConst& g, const VoxT* __restrict__ vol,
                                            const uint8_t* __restrict__ mask, float& acc, float& accl) {
     const unsigned plane = (unsigned)g.rx * (unsigned)g.ry;
@@ -197,10 +198,8 @@ __device__ __forceinline__ void dda_walk_xz(const DdaStart& st, const SlabConst&
     const uint8_t* mrow = kMask ? mask + (size_t)st.iy * (size_t)g.rx : nullptr;
     const float sdx = st.sd.x, sdz = st.sd.z;
     const unsigned dx = (unsigned)st.sx, dz = (unsigned)st.sz * plane;  // two's-complement deltas
-    int nx = st.sx > 0 ? g.rx - st.ix : (st.sx < 0 ? st.ix + 1 : 0x7fffffff);
-    int nz = st.sz > 0 ? g.rz - st.iz : (st.sz < 0 ? st.iz + 1 : 0x7fffffff);
     int left = kMaxDdaIterations;
-    unsigned off = (unsigned)st.iz * plane + (unsigned)st.ix;
+    unsigned off = (unsigned)st.iz * plane + (unsigned)st.ix;  // iz * plane + ix (row carries iy)
     float rx = st.res.x, rz = st.res.z;
     // One DDA step (DDARaytracer.hl:89-105): returns the segment length and the voxel it crossed.
     auto step = [&](float& dt, unsigned& at) {
@@ -210,12 +209,15 @@ __device__ __forceinline__ void dda_walk_xz(const DdaStart& st, const SlabConst&
         rx = bx ? sdx : fsub(rx, dt);
         rz = bx ? fsub(rz, dt) : sdz;
         off += bx ? dx : dz;
-        nx -= bx ? 1 : 0;
-        nz -= bx ? 0 : 1;
     };
     for (;;) {
-        // Neither axis can leave the slab (nor the loop cap run out) within the next
+        // Steps each axis may still take before it leaves the slab, from the current
+        // voxel; neither axis (nor the loop cap) can run out within the next
         // min(nx, nz[, left]) steps, so they run without exit tests.
+        const unsigned iz = off / plane, ix = off - iz * plane;
+        const int nx = st.sx > 0 ? g.rx - (int)ix : (st.sx < 0 ? (int)ix + 1 : 0x7fffffff);
+        const int nz = st.sz > 0 ? g.rz - (int)iz : (st.sz < 0 ? (int)iz + 1 : 0x7fffffff);
+        if (nx <= 0 || nz <= 0 || ix >= (unsigned)g.rx || iz >= (unsigned)g.rz) break;
         int m = min(nx, nz);
         if (kCapped) m = min(m, left);
         if (m <= 0) break;
@@ -346,8 +348,45 @@ struct FpArgs {
 // cannot reach it, rx + rz - 1 <= 2048 steps), kFpPathPerspective.
 enum FpPath : int { kFpPathGeneral = 0, kFpPathXz = 1, kFpPathXzNoCap = 2, kFpPathPerspective = 3 };
 
+// Projection epilogue of one detector pixel (ForwardProjectionKernel /
+// VirtualProjection.cl:8-9 / Compare.cl:8): normalise by the sub-ray count and
+// write by mode.  Returns residual^2 (mode 2) or 0.
+__device__ __forceinline__ double fp_store(const FpArgs& a, const ViewConst& vc, uint32_t vid, int p, int gx, int gy,
+                                           float accv, float accl, float total) {
+    float pv = fdiv(accv, total), pl = fdiv(accl, total);
+    const size_t i = (size_t)gy * (size_t)a.W + (size_t)gx;
+    if (a.mode == kFpSeparateAccumulate) {
+        a.out_v[i] = fadd(a.out_v[i], pv);
+        a.out_l[i] = fadd(a.out_l[i], pl);
+        return 0.0;
+    }
+    float2* slot = a.rl + (size_t)p * a.rl_slot + (size_t)gy * a.rl_pitch + (size_t)gx;
+    float2 prev = a.overwrite ? make_float2(0.f, 0.f) : *slot;
+    float vv = fadd(prev.x, pv), ll = fadd(prev.y, pl);
+    if (a.mode == kFpPairAccumulate) {
+        *slot = make_float2(vv, ll);
+        return 0.0;
+    }
+    if (a.loc) {  // VirtualProjection.cl:8-9
+        vv = ll > kEps ? fdiv(fmul(vv, vc.loc_length), ll) : 0.f;
+        ll = vc.loc_length;
+    }
+    float r = fsub(a.real[(size_t)vid * (size_t)a.W * (size_t)a.H + i], vv);  // Compare.cl:8
+    *slot = make_float2(r, ll);
+    return (double)r * (double)r;
+}
+
+// FP64 warp reduction of the squared residuals, one atomic per warp (no block
+// barrier, so warps whose rays finish early do not wait for the others).
+__device__ __forceinline__ void fp_reduce_resid(const FpArgs& a, double r2) {
+    if (a.mode == kFpPairResidual && a.resid_sq) {
+        for (int o = 16; o > 0; o >>= 1) r2 += __shfl_down_sync(0xffffffffu, r2, o);
+        if ((threadIdx.x & 31) == 0 && r2 != 0.0) atomicAdd(a.resid_sq, r2);
+    }
+}
+
 template <typename VoxT, bool kMask, int kPath>
-__global__ void __launch_bounds__(128, (kPath == kFpPathXz || kPath == kFpPathXzNoCap) ? 9 : 4)
+__global__ void __launch_bounds__(128, (kPath == kFpPathXz || kPath == kFpPathXzNoCap) ? 7 : 4)
     forward_project_kernel(const __grid_constant__ FpArgs a) {
     constexpr bool kPerspective = kPath == kFpPathPerspective;
     int gx, gy;
@@ -416,35 +455,8 @@ __global__ void __launch_bounds__(128, (kPath == kFpPathXz || kPath == kFpPathXz
         }
     }
     double r2 = 0.0;
-    if (active) {
-        float pv = fdiv(accv, total), pl = fdiv(accl, total);
-        const size_t i = (size_t)gy * (size_t)a.W + (size_t)gx;
-        if (a.mode == kFpSeparateAccumulate) {
-            a.out_v[i] = fadd(a.out_v[i], pv);
-            a.out_l[i] = fadd(a.out_l[i], pl);
-        } else {
-            float2* slot = a.rl + (size_t)p * a.rl_slot + (size_t)gy * a.rl_pitch + (size_t)gx;
-            float2 prev = a.overwrite ? make_float2(0.f, 0.f) : *slot;
-            float vv = fadd(prev.x, pv), ll = fadd(prev.y, pl);
-            if (a.mode == kFpPairAccumulate) {
-                *slot = make_float2(vv, ll);
-            } else {
-                if (a.loc) {  // VirtualProjection.cl:8-9
-                    vv = ll > kEps ? fdiv(fmul(vv, vc.loc_length), ll) : 0.f;
-                    ll = vc.loc_length;
-                }
-                float r = fsub(a.real[(size_t)vid * (size_t)a.W * (size_t)a.H + i], vv);  // Compare.cl:8
-                *slot = make_float2(r, ll);
-                r2 = (double)r * (double)r;
-            }
-        }
-    }
-    if (a.mode == kFpPairResidual && a.resid_sq) {
-        // FP64 warp reduction of the squared residuals, one atomic per warp (no block barrier,
-        // so warps whose rays finish early do not wait for the others).
-        for (int o = 16; o > 0; o >>= 1) r2 += __shfl_down_sync(0xffffffffu, r2, o);
-        if ((threadIdx.x & 31) == 0 && r2 != 0.0) atomicAdd(a.resid_sq, r2);
-    }
+    if (active) r2 = fp_store(a, vc, vid, p, gx, gy, accv, accl, total);
+    fp_reduce_resid(a, r2);
 }
 
 // ---------------------------------------------------------------- back projection
@@ -895,15 +907,17 @@ __global__ void __launch_bounds__(256, 8) bp_sart_row_kernel(const __grid_consta
 // Sampling: the view's detector row coordinate is fixed for the item, so its row
 // weight b is too, and the two detector rows are blended once per item,
 // P[x] = (1 - b) * t0[x] + b * t1[x], into a staged window of tap pairs
-// (P[x0], P[x0 + 1]) over the columns [x0lo, x0lo + ntaps) that the host bounds
-// from the view and sub-volume corners.  Each voxel then takes one 16-byte shared
-// load and blends along x with the 1/256 weight a: (1 - a) * P[x0] + a * P[x0 + 1].
-// This is the same bilinear weighting as blend<kSampleQ8> with the row pass
-// first; only the rounding order differs (by an ulp of the sample; identical when
-// b == 0).  The window holds zeros outside the padded image, where the direct
-// kernels clamp onto zero border texels, so no clamp is needed per voxel.  The
-// 1/256 split of the column coordinate is integer work on the bits of
-// fl_down(t + 1.5 * 2^23), which is 1.5 * 2^23 + floor(t) for |t| < 2^22.
+// (P[x0], P[x0 + 1] - P[x0]) over the columns [x0lo, x0lo + ntaps) that the host
+// bounds from the view and sub-volume corners.  Each voxel then takes one 16-byte
+// shared load and one multiply-add per channel with the 1/256 weight a:
+// P[x0] + a * (P[x0 + 1] - P[x0]).  This is the bilinear weighting of
+// blend<kSampleQ8> (same coordinates, same 1/256 weights) evaluated in another
+// order, and the update r * lambda * d / L takes the reciprocal estimate of L
+// (within an ulp): each update is within a few ulps of the direct kernels'.  The
+// window holds zeros outside the padded image, where the direct kernels clamp
+// onto zero border texels, so no clamp is needed per voxel.  The 1/256 split of
+// the column coordinate is integer work on the bits of fl_down(t + 1.5 * 2^23),
+// which is 1.5 * 2^23 + floor(t) for |t| < 2^22.
 struct BpColArgs {
     float* vol;                 // sub-volume base, x-fastest [z][y][x]
     SlabConst slab;
@@ -959,7 +973,7 @@ __global__ void __launch_bounds__(kBpColThreads, 4) bp_sart_column_kernel(const 
     for (int k = 0; k < kCols; ++k)
         A[k] = fmul(vc.mat[0], fadd(fadd(g.bmin.x, fmul(fadd((float)(tid + k * kBpColThreads), 0.5f), g.vs.x)), s.x));
     const int ncols = kFull ? kCols : min(kCols, max(0, (rx - tid + kBpColThreads - 1) / kBpColThreads));
-    const float lam = a.lambda, d = s.w, m12 = vc.mat[12];
+    const float lamd = fmul(a.lambda, s.w), m12 = vc.mat[12];
     const float px0 = fadd(fadd(g.bmin.x, fmul(0.5f, g.vs.x)), s.x);
     const size_t plane = (size_t)rx * (size_t)ry;
     const float2 zero = make_float2(0.f, 0.f);
@@ -986,8 +1000,9 @@ __global__ void __launch_bounds__(kBpColThreads, 4) bp_sart_column_kernel(const 
             const bool in0 = x0 >= -kPad && x0 < a.W + kPad, in1 = x0 + 1 >= -kPad && x0 + 1 < a.W + kPad;
             const float2 p0 = in0 ? __ldg(r0 + x0) : zero, q0 = in1 ? __ldg(r0 + x0 + 1) : zero;
             const float2 p1 = in0 ? __ldg(r1 + x0) : zero, q1 = in1 ? __ldg(r1 + x0 + 1) : zero;
-            taps[e] = make_float4(fadd(fmul(omb, p0.x), fmul(b, p1.x)), fadd(fmul(omb, p0.y), fmul(b, p1.y)),
-                                  fadd(fmul(omb, q0.x), fmul(b, q1.x)), fadd(fmul(omb, q0.y), fmul(b, q1.y)));
+            const float2 P0 = make_float2(fadd(fmul(omb, p0.x), fmul(b, p1.x)), fadd(fmul(omb, p0.y), fmul(b, p1.y)));
+            const float2 P1 = make_float2(fadd(fmul(omb, q0.x), fmul(b, q1.x)), fadd(fmul(omb, q0.y), fmul(b, q1.y)));
+            taps[e] = make_float4(P0.x, P0.y, fsub(P1.x, P0.x), fsub(P1.y, P0.y));
         }
         __syncthreads();
         if (z0 >= z1 || ncols == 0) continue;
@@ -1016,9 +1031,11 @@ __global__ void __launch_bounds__(kBpColThreads, 4) bp_sart_column_kernel(const 
                     float a1;
                     q8_tap_bits(__fadd_rd(fmaf(u, 256.f, -127.5f), 12582912.0f), x0lo, e, a1);
                     const float4 t = taps[e];
-                    const float ax = fsub(a1, 1.f), oma = fsub(1.f, ax);
-                    const float2 rl = make_float2(fadd(fmul(oma, t.x), fmul(ax, t.z)), fadd(fmul(oma, t.y), fmul(ax, t.w)));
-                    p[k * kBpColThreads] = sart_update(cur[k], rl, lam, d, 1.f, false);
+                    const float ax = fsub(a1, 1.f);
+                    const float R = fmaf(ax, t.z, t.x), L = fmaf(ax, t.w, t.y);
+                    // ParallelBeamsBackProjection.cl:40-50: v + r * lambda * d / L where L > eps
+                    const float c = fmul(fmul(R, rcp_approx(L)), lamd);
+                    p[k * kBpColThreads] = L > kEps ? fadd(cur[k], c) : cur[k];
                 }
                 cur[k] = nxt[k];
                 nxt[k] = nn[k];
