@@ -341,14 +341,13 @@ void launch_bp_sart_m(const BpArgs& a, etcu_voxel_type t, etcu_sampling sm, cuda
 }
 
 struct BpColPlan {
-    int cols = 0;  // x columns per thread (1, 2, 4 or 8)
-    bool full = false;  // rx == cols * kBpColThreads
+    int groups = 0;  // 4-voxel x groups per thread (1 or 2)
     int x0lo = 0, ntaps = 0;
     int zper = 0, zchunks = 0, grid = 0;
     size_t smem = 0;
 };
 
-template <int kCols, bool kFull>
+template <int kGroups>
 void bp_col_limits(int dev, size_t smem, int& per_sm) {
     static std::mutex mu;
     static std::vector<char> opted;
@@ -358,14 +357,14 @@ void bp_col_limits(int dev, size_t smem, int& per_sm) {
         if (!opted[dev]) {
             cudaDeviceProp prop;
             if (cudaGetDeviceProperties(&prop, dev) == cudaSuccess)
-                cudaFuncSetAttribute(bp_sart_column_kernel<kCols, kFull>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                cudaFuncSetAttribute(bp_sart_column_kernel<kGroups>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)prop.sharedMemPerBlockOptin);
             cudaGetLastError();
             opted[dev] = 1;
         }
     }
     per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_sart_column_kernel<kCols, kFull>, kBpColThreads, smem) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_sart_column_kernel<kGroups>, kBpColThreads, smem) !=
         cudaSuccess) {
         cudaGetLastError();
         per_sm = 0;
@@ -387,14 +386,14 @@ int device_sms(int dev) {
 
 // Whether the column-pipelined back projector applies to this view and
 // sub-volume, and its tap window, item and grid sizes.  It needs an FP32 volume
-// without mask and rows of at most 2048 voxels.  The tap window spans the
+// without mask and x rows of a multiple of 4 and at most 2048 voxels.  The tap window spans the
 // columns floor(u - 0.5) of every voxel centre with two columns of margin on each
 // side (the kernel's float coordinate is within a few ulps of the double
 // evaluated here at the sub-volume's corners; u is affine in the voxel indices).
 bool plan_bp_col(const etcu_volume* vol, const SlabConst& g, const ViewConst& vc, const float4& smp, BpColPlan& p) {
     etcu_context* ctx = vol->ctx;
     if (!ctx->bp_column || vol->type != ETCU_VOXEL_FLOAT32 || vol->mask) return false;
-    if (g.rx <= 0 || g.ry <= 0 || g.rz <= 0 || g.rx > 8 * kBpColThreads) return false;
+    if (g.rx <= 0 || g.ry <= 0 || g.rz <= 0 || g.rx % 4 != 0 || g.rx > 8 * kBpColThreads) return false;
     double umin = 1e300, umax = -1e300;
     for (int c = 0; c < 8; ++c) {
         const double x = (c & 1) ? g.rx - 1 : 0, y = (c & 2) ? g.ry - 1 : 0, z = (c & 4) ? g.rz - 1 : 0;
@@ -408,23 +407,13 @@ bool plan_bp_col(const etcu_volume* vol, const SlabConst& g, const ViewConst& vc
     if (!(umin > -16000.0 && umax < 16000.0)) return false;  // |256 u| < 2^22 for the tap split
     p.x0lo = (int)std::floor(umin - 0.5) - 2;
     p.ntaps = (int)std::floor(umax - 0.5) + 2 - p.x0lo + 1;
-    p.smem = bp_col_smem_bytes(g.rz, p.ntaps);
-    if (p.smem > 96 * 1024) return false;
-    const int need = (g.rx + kBpColThreads - 1) / kBpColThreads;
-    p.cols = need <= 1 ? 1 : need <= 2 ? 2 : need <= 4 ? 4 : 8;
-    p.full = g.rx == p.cols * kBpColThreads;
+    p.groups = g.rx <= 4 * kBpColThreads ? 1 : 2;
+    p.smem = bp_col_smem_bytes(g.rz, p.ntaps, p.groups);
+    if (p.smem > 112 * 1024) return false;
     const int dev = ctx->device;
     int per_sm = 0;
-    switch (p.cols * 2 + (p.full ? 1 : 0)) {
-    case 2: bp_col_limits<1, false>(dev, p.smem, per_sm); break;
-    case 3: bp_col_limits<1, true>(dev, p.smem, per_sm); break;
-    case 4: bp_col_limits<2, false>(dev, p.smem, per_sm); break;
-    case 5: bp_col_limits<2, true>(dev, p.smem, per_sm); break;
-    case 8: bp_col_limits<4, false>(dev, p.smem, per_sm); break;
-    case 9: bp_col_limits<4, true>(dev, p.smem, per_sm); break;
-    case 16: bp_col_limits<8, false>(dev, p.smem, per_sm); break;
-    default: bp_col_limits<8, true>(dev, p.smem, per_sm); break;
-    }
+    if (p.groups == 1) bp_col_limits<1>(dev, p.smem, per_sm);
+    else bp_col_limits<2>(dev, p.smem, per_sm);
     const int sms = device_sms(dev);
     if (per_sm < 1 || sms < 1) return false;
     const long long cap = (long long)sms * per_sm;
@@ -469,16 +458,8 @@ void launch_bp_col(const BpArgs& a0, const BpColPlan& p, cudaStream_t st) {
     a.zper = p.zper;
     a.zchunks = p.zchunks;
     const dim3 grid(p.grid), block(kBpColThreads);
-    switch (p.cols * 2 + (p.full ? 1 : 0)) {
-    case 2: bp_sart_column_kernel<1, false><<<grid, block, p.smem, st>>>(a); break;
-    case 3: bp_sart_column_kernel<1, true><<<grid, block, p.smem, st>>>(a); break;
-    case 4: bp_sart_column_kernel<2, false><<<grid, block, p.smem, st>>>(a); break;
-    case 5: bp_sart_column_kernel<2, true><<<grid, block, p.smem, st>>>(a); break;
-    case 8: bp_sart_column_kernel<4, false><<<grid, block, p.smem, st>>>(a); break;
-    case 9: bp_sart_column_kernel<4, true><<<grid, block, p.smem, st>>>(a); break;
-    case 16: bp_sart_column_kernel<8, false><<<grid, block, p.smem, st>>>(a); break;
-    default: bp_sart_column_kernel<8, true><<<grid, block, p.smem, st>>>(a); break;
-    }
+    if (p.groups == 1) bp_sart_column_kernel<1><<<grid, block, p.smem, st>>>(a);
+    else bp_sart_column_kernel<2><<<grid, block, p.smem, st>>>(a);
 }
 
 // Back projection of a.nviews views; when their staged constants exceed the

@@ -900,10 +900,13 @@ __global__ void __launch_bounds__(256, 8) bp_sart_row_kernel(const __grid_consta
 }
 
 // ---- column-pipelined single-view back projection (SART's hot case, FP32 volume) ----
-// A block owns items (y, z range) of the sub-volume; each thread owns kCols x
-// columns of the item and walks them down z with the volume loads of the next two
-// z rows in flight (2 * kCols coalesced loads per thread), so the block needs no
-// barrier inside an item.
+// A block owns items (y, z range) of the sub-volume; each thread owns groups of
+// four consecutive x voxels of the item and walks them down z.  The volume rows
+// come in through a per-thread ring of kBpColDepth 16-byte shared-memory slots
+// filled by cp.async kBpColDepth - 1 rows ahead: a thread only ever reads the
+// slots its own copies filled (cp.async.wait_group), so the walk needs no
+// barrier and holds no prefetched values in registers; the four updated voxels
+// leave as one 16-byte store.
 // Sampling: the view's detector row coordinate is fixed for the item, so its row
 // weight b is too, and the two detector rows are blended once per item,
 // P[x] = (1 - b) * t0[x] + b * t1[x], into a staged window of tap pairs
@@ -937,9 +940,23 @@ struct BpColArgs {
 };
 
 constexpr int kBpColThreads = 256;
+constexpr int kBpColDepth = 8;  // ring slots per thread: rows in flight + the one being updated
 
-__host__ __device__ constexpr size_t bp_col_smem_bytes(int rz, int ntaps) {
-    return (size_t)ntaps * 16 + (size_t)rz * 4;  // row-blended tap pairs, per-z term
+// row-blended tap pairs, per-z term, per-thread rings of kGroups 16-byte slots
+__host__ __device__ constexpr size_t bp_col_smem_bytes(int rz, int ntaps, int groups) {
+    return (size_t)ntaps * 16 + ((size_t)rz * 4 + 15) / 16 * 16 +
+           (size_t)kBpColDepth * (size_t)groups * kBpColThreads * 16;
+}
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 // Column tap of one voxel from f = fl_down(t + 1.5 * 2^23) = 1.5 * 2^23 + floor(t),
@@ -952,7 +969,8 @@ __device__ __forceinline__ void q8_tap_bits(float f, int x0lo, int& e, float& a1
 }
 
 // kFull: every thread owns all kCols columns (rx == kCols * kBpColThreads).
-template <int kCols, bool kFull>
+// kGroups: 4-voxel x groups per thread (rx <= 4 * kGroups * kBpColThreads, rx % 4 == 0).
+template <int kGroups>
 __global__ void __launch_bounds__(kBpColThreads, 4) bp_sart_column_kernel(const __grid_constant__ BpColArgs a) {
     extern __shared__ __align__(16) unsigned char bp_col_smem[];
     const SlabConst& g = a.slab;
@@ -960,6 +978,11 @@ __global__ void __launch_bounds__(kBpColThreads, 4) bp_sart_column_kernel(const 
     const int ntaps = a.ntaps, x0lo = a.x0lo;
     float4* taps = (float4*)bp_col_smem;
     float* K = (float*)(taps + ntaps);
+    // slot (ring row r, group k) of this thread: ring[(r * kGroups + k) * kBpColThreads + tid]
+    float4* ring = (float4*)(bp_col_smem + (size_t)ntaps * 16 + ((size_t)rz * 4 + 15) / 16 * 16);
+    const float4* my = ring + tid;
+    const uint32_t my_s = smem_addr(my);
+    constexpr uint32_t kSlotBytes = kGroups * kBpColThreads * 16, kGroupBytes = kBpColThreads * 16;
 
     const uint32_t vid = a.order ? a.order[a.first] : a.first;
     const ViewConst& vc = a.views ? a.views[vid] : a.inline_view;
@@ -968,17 +991,52 @@ __global__ void __launch_bounds__(kBpColThreads, 4) bp_sart_column_kernel(const 
     // ParallelBeamsBackProjection.cl coordinate terms, in the kernel's operation order
     for (int z = tid; z < rz; z += kBpColThreads)
         K[z] = fmul(vc.mat[8], fadd(fadd(g.bmin.z, fmul(fadd((float)z, 0.5f), g.vs.z)), s.z));
-    float A[kCols];
+    float A[kGroups][4];
+    bool on[kGroups];
 #pragma unroll
-    for (int k = 0; k < kCols; ++k)
-        A[k] = fmul(vc.mat[0], fadd(fadd(g.bmin.x, fmul(fadd((float)(tid + k * kBpColThreads), 0.5f), g.vs.x)), s.x));
-    const int ncols = kFull ? kCols : min(kCols, max(0, (rx - tid + kBpColThreads - 1) / kBpColThreads));
-    const float lamd = fmul(a.lambda, s.w), m12 = vc.mat[12];
+    for (int k = 0; k < kGroups; ++k) {
+        const int x4 = 4 * (tid + k * kBpColThreads);
+        on[k] = x4 < rx;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            A[k][j] = fmul(vc.mat[0], fadd(fadd(g.bmin.x, fmul(fadd((float)(x4 + j), 0.5f), g.vs.x)), s.x));
+    }
+    const float lamd = fmul(a.lambda, s.w);
+    const float2 m12 = splat(vc.mat[12]);
     const float px0 = fadd(fadd(g.bmin.x, fmul(0.5f, g.vs.x)), s.x);
     const size_t plane = (size_t)rx * (size_t)ry;
     const float2 zero = make_float2(0.f, 0.f);
     const int items = ry * a.zchunks;
 
+    // Fetch cursor: walks the rows of this block's items in the order they are
+    // updated, one row (or, past the last row, nothing) per commit group, so the
+    // j-th row updated is in the j-th group; kBpColDepth - 1 groups run ahead.
+    int fit = blockIdx.x, fz = 0, fz1 = 0, ws = 0;
+    const float* src = nullptr;
+    auto start_item = [&](int i) {
+        const int iy = i / a.zchunks;
+        fz = (i - iy * a.zchunks) * a.zper;
+        fz1 = min(rz, fz + a.zper);
+        src = a.vol + ((size_t)fz * ry + iy) * rx + 4 * tid;
+    };
+    if (fit < items) start_item(fit);
+    auto fetch = [&]() {
+        if (fit < items) {
+#pragma unroll
+            for (int k = 0; k < kGroups; ++k)
+                if (on[k]) cp_async16(my_s + (uint32_t)ws * kSlotBytes + k * kGroupBytes, src + 4 * k * kBpColThreads);
+            ws = (ws + 1) & (kBpColDepth - 1);
+            src += plane;
+            if (++fz == fz1) {
+                fit += gridDim.x;
+                if (fit < items) start_item(fit);
+            }
+        }
+        cp_async_commit();
+    };
+    for (int i = 0; i < kBpColDepth - 1; ++i) fetch();
+
+    int rs = 0;  // read slot
     for (int it = blockIdx.x; it < items; it += gridDim.x) {
         const int y = it / a.zchunks;
         const int z0 = (it - y * a.zchunks) * a.zper, z1 = min(rz, z0 + a.zper);
@@ -995,54 +1053,62 @@ __global__ void __launch_bounds__(kBpColThreads, 4) bp_sart_column_kernel(const 
         __syncthreads();  // the previous item's taps are no longer read (K is ready the first time)
         for (int e = tid; e < ntaps; e += kBpColThreads) {
             // columns outside the padded image read zero, as the clamped taps of the
-            // direct kernels read the zero border
+            // direct kernels read the zero border; the residual taps carry lambda * d
             const int x0 = x0lo + e;
             const bool in0 = x0 >= -kPad && x0 < a.W + kPad, in1 = x0 + 1 >= -kPad && x0 + 1 < a.W + kPad;
             const float2 p0 = in0 ? __ldg(r0 + x0) : zero, q0 = in1 ? __ldg(r0 + x0 + 1) : zero;
             const float2 p1 = in0 ? __ldg(r1 + x0) : zero, q1 = in1 ? __ldg(r1 + x0 + 1) : zero;
             const float2 P0 = make_float2(fadd(fmul(omb, p0.x), fmul(b, p1.x)), fadd(fmul(omb, p0.y), fmul(b, p1.y)));
             const float2 P1 = make_float2(fadd(fmul(omb, q0.x), fmul(b, q1.x)), fadd(fmul(omb, q0.y), fmul(b, q1.y)));
-            taps[e] = make_float4(P0.x, P0.y, fsub(P1.x, P0.x), fsub(P1.y, P0.y));
+            taps[e] = make_float4(fmul(P0.x, lamd), P0.y, fmul(fsub(P1.x, P0.x), lamd), fsub(P1.y, P0.y));
         }
         __syncthreads();
-        if (z0 >= z1 || ncols == 0) continue;
-        float au[kCols];
+        float2 au[kGroups][2];
 #pragma unroll
-        for (int k = 0; k < kCols; ++k) au[k] = fadd(A[k], cy4);
-        float* p = a.vol + ((size_t)z0 * ry + y) * rx + tid;
-        float cur[kCols], nxt[kCols];
-#pragma unroll
-        for (int k = 0; k < kCols; ++k) {
-            cur[k] = k < ncols ? __ldg(p + k * kBpColThreads) : 0.f;
-            nxt[k] = (k < ncols && z0 + 1 < z1) ? __ldg(p + plane + k * kBpColThreads) : 0.f;
+        for (int k = 0; k < kGroups; ++k) {
+            au[k][0] = f2(fadd(A[k][0], cy4), fadd(A[k][1], cy4));
+            au[k][1] = f2(fadd(A[k][2], cy4), fadd(A[k][3], cy4));
         }
-        for (int z = z0; z < z1; ++z) {
-            float nn[kCols];
-            const bool more = z + 2 < z1;
-            const float* pn = p + 2 * plane;
+        float* dst = a.vol + ((size_t)z0 * ry + y) * rx + 4 * tid;
+        const int nrows = z1 - z0;
+        for (int r = 0; r < nrows; ++r) {
+            fetch();
+            cp_async_wait<kBpColDepth - 1>();  // the row in read slot rs has landed
+            const float2 kz = splat(K[z0 + r]);
 #pragma unroll
-            for (int k = 0; k < kCols; ++k) nn[k] = (more && k < ncols) ? __ldg(pn + k * kBpColThreads) : 0.f;
-            const float kz = K[z];
+            for (int k = 0; k < kGroups; ++k) {
+                if (!on[k]) continue;
+                const float4 v = my[(rs * kGroups + k) * kBpColThreads];
+                const float vin[4] = {v.x, v.y, v.z, v.w};
+                float vout[4];
 #pragma unroll
-            for (int k = 0; k < kCols; ++k) {
-                if (k < ncols) {
-                    const float u = fadd(fadd(au[k], kz), m12);
-                    int e;
-                    float a1;
-                    q8_tap_bits(__fadd_rd(fmaf(u, 256.f, -127.5f), 12582912.0f), x0lo, e, a1);
-                    const float4 t = taps[e];
-                    const float ax = fsub(a1, 1.f);
-                    const float R = fmaf(ax, t.z, t.x), L = fmaf(ax, t.w, t.y);
-                    // ParallelBeamsBackProjection.cl:40-50: v + r * lambda * d / L where L > eps
-                    const float c = fmul(fmul(R, rcp_approx(L)), lamd);
-                    p[k * kBpColThreads] = L > kEps ? fadd(cur[k], c) : cur[k];
+                for (int h = 0; h < 2; ++h) {
+                    // u = (au + m8 * pz) + m12 and the column split, two voxels per instruction
+                    const float2 u = add2(add2(au[k][h], kz), m12);
+                    const float2 f = __fadd2_rd(fma2(u, splat(256.f), splat(-127.5f)), splat(12582912.0f));
+                    int e0, e1;
+                    float a0, a1;
+                    q8_tap_bits(f.x, x0lo, e0, a0);
+                    q8_tap_bits(f.y, x0lo, e1, a1);
+                    const float2 ax = add2(f2(a0, a1), splat(-1.f));
+#pragma unroll
+                    for (int q = 0; q < 2; ++q) {
+                        const float4 t = taps[q ? e1 : e0];
+                        const float w = q ? ax.y : ax.x;
+                        const float R = fmaf(w, t.z, t.x), L = fmaf(w, t.w, t.y);
+                        // ParallelBeamsBackProjection.cl:40-50: v + r * lambda * d / L where L > eps
+                        const float c = fmul(R, rcp_approx(L));
+                        const float vi = vin[2 * h + q];
+                        vout[2 * h + q] = L > kEps ? fadd(vi, c) : vi;
+                    }
                 }
-                cur[k] = nxt[k];
-                nxt[k] = nn[k];
+                *reinterpret_cast<float4*>(dst + 4 * k * kBpColThreads) = make_float4(vout[0], vout[1], vout[2], vout[3]);
             }
-            p += plane;
+            rs = (rs + 1) & (kBpColDepth - 1);
+            dst += plane;
         }
     }
+    cp_async_wait<0>();
 }
 
 // PerspectiveBeamsBackProjection.cl:10-17 getRayLengthInVoxel

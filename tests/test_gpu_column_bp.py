@@ -1,6 +1,7 @@
 """Column-pipelined single-view back projection (SART's hot case on an FP32
 volume): detector taps staged in shared memory per (y, z range) item, each thread
-walking its x columns down z with the next rows' volume loads in flight.
+walking groups of four x voxels down z with the next rows in flight through its
+own cp.async ring in shared memory.
 
 It blends the two detector rows once per item and then along x (the direct
 kernels blend all four taps per voxel), so it matches the direct single-view
@@ -9,8 +10,9 @@ relative L2 of the volume updates <= 1e-6 (measured ~1e-7), and the oracle
 within the back-projection tolerance, for row weights b == 0.5 (the MRC tilt
 geometry), b != 0.5 (shifted or finer detector rows), ragged sizes (x rows that do
 not fill a block, odd z counts), voxels that project beyond the detector edge
-and several sub-volumes.  Half-precision volumes, masked volumes and exact
-(unquantised) sampling fall back to the direct kernel.
+and several sub-volumes.  Half-precision volumes, x sizes that are not a multiple
+of 4, masked volumes and exact (unquantised) sampling fall back to the direct
+kernel.
 """
 import os
 
@@ -96,7 +98,8 @@ CASES = [
     ((96, 80, 40), 0.0, 0.37, 1.0, None, 1),    # rows between detector pixels: b != 0
     ((68, 24, 37), 17.5, 0.0, 1.0, None, 1),    # 68-voxel rows, odd z count
     ((68, 24, 37), -41.0, 0.0, 0.75, None, 1),  # b varies with y
-    ((528, 6, 21), 9.0, 0.25, 1.0, None, 1),    # rows longer than a block, short z
+    ((528, 6, 21), 9.0, 0.25, 1.0, None, 1),    # short z
+    ((1100, 4, 9), 11.0, 0.0, 1.0, None, 1),    # two 4-voxel groups per thread
     ((64, 40, 48), 52.0, 0.0, 1.0, None, 3),    # three sub-volumes
     ((96, 40, 24), 20.0, 0.0, 1.0, 48, 1),      # detector narrower than the volume's shadow
 ]
@@ -126,6 +129,7 @@ def test_column_bp_bit_identical_to_direct_and_matches_oracle(ctxs, shape, angle
 
 
 @pytest.mark.parametrize("shape,sampling,masked,half", [((66, 20, 16), 0, False, True),  # half volume
+                                                        ((66, 20, 16), 0, False, False),  # x not a multiple of 4
                                                         ((64, 20, 16), 1, False, False),  # exact sampling
                                                         ((64, 20, 16), 0, True, False)])  # masked volume
 def test_ineligible_cases_fall_back(ctxs, shape, sampling, masked, half):
