@@ -942,9 +942,14 @@ struct BpColArgs {
 constexpr int kBpColThreads = 256;
 constexpr int kBpColDepth = 8;  // ring slots per thread: rows in flight + the one being updated
 
+// Tap pair e sits at index e + e / 8 (one 16-byte pad per 8 entries): the lanes of a
+// warp read entries about 4 cos(theta) apart (four x voxels per thread), which the
+// pad spreads over distinct shared-memory banks.
+__host__ __device__ constexpr int bp_col_tap_slots(int ntaps) { return ntaps + ntaps / 8 + 1; }
+
 // row-blended tap pairs, per-z term, per-thread rings of kGroups 16-byte slots
 __host__ __device__ constexpr size_t bp_col_smem_bytes(int rz, int ntaps, int groups) {
-    return (size_t)ntaps * 16 + ((size_t)rz * 4 + 15) / 16 * 16 +
+    return (size_t)bp_col_tap_slots(ntaps) * 16 + ((size_t)rz * 4 + 15) / 16 * 16 +
            (size_t)kBpColDepth * (size_t)groups * kBpColThreads * 16;
 }
 
@@ -977,9 +982,9 @@ __global__ void __launch_bounds__(kBpColThreads, 4) bp_sart_column_kernel(const 
     const int rx = g.rx, ry = g.ry, rz = g.rz, tid = threadIdx.x;
     const int ntaps = a.ntaps, x0lo = a.x0lo;
     float4* taps = (float4*)bp_col_smem;
-    float* K = (float*)(taps + ntaps);
+    float* K = (float*)(taps + bp_col_tap_slots(ntaps));
     // slot (ring row r, group k) of this thread: ring[(r * kGroups + k) * kBpColThreads + tid]
-    float4* ring = (float4*)(bp_col_smem + (size_t)ntaps * 16 + ((size_t)rz * 4 + 15) / 16 * 16);
+    float4* ring = (float4*)(bp_col_smem + (size_t)bp_col_tap_slots(ntaps) * 16 + ((size_t)rz * 4 + 15) / 16 * 16);
     const float4* my = ring + tid;
     const uint32_t my_s = smem_addr(my);
     constexpr uint32_t kSlotBytes = kGroups * kBpColThreads * 16, kGroupBytes = kBpColThreads * 16;
@@ -1060,7 +1065,7 @@ __global__ void __launch_bounds__(kBpColThreads, 4) bp_sart_column_kernel(const 
             const float2 p1 = in0 ? __ldg(r1 + x0) : zero, q1 = in1 ? __ldg(r1 + x0 + 1) : zero;
             const float2 P0 = make_float2(fadd(fmul(omb, p0.x), fmul(b, p1.x)), fadd(fmul(omb, p0.y), fmul(b, p1.y)));
             const float2 P1 = make_float2(fadd(fmul(omb, q0.x), fmul(b, q1.x)), fadd(fmul(omb, q0.y), fmul(b, q1.y)));
-            taps[e] = make_float4(fmul(P0.x, lamd), P0.y, fmul(fsub(P1.x, P0.x), lamd), fsub(P1.y, P0.y));
+            taps[e + (e >> 3)] = make_float4(fmul(P0.x, lamd), P0.y, fmul(fsub(P1.x, P0.x), lamd), fsub(P1.y, P0.y));
         }
         __syncthreads();
         float2 au[kGroups][2];
@@ -1093,7 +1098,8 @@ __global__ void __launch_bounds__(kBpColThreads, 4) bp_sart_column_kernel(const 
                     const float2 ax = add2(f2(a0, a1), splat(-1.f));
 #pragma unroll
                     for (int q = 0; q < 2; ++q) {
-                        const float4 t = taps[q ? e1 : e0];
+                        const int eq = q ? e1 : e0;
+                        const float4 t = taps[eq + (eq >> 3)];
                         const float w = q ? ax.y : ax.x;
                         const float R = fmaf(w, t.z, t.x), L = fmaf(w, t.w, t.y);
                         // ParallelBeamsBackProjection.cl:40-50: v + r * lambda * d / L where L > eps
