@@ -63,7 +63,13 @@ def parse():
 
 
 # ------------------------------------------------------------------ distributed plumbing
-def dist_init():
+_DIST_DEVICE = "cpu"
+
+
+def dist_init(timeout_s: int = 300):
+    """One process per GPU (torchrun env).  NCCL when CUDA is present, else gloo on CPU
+    (the multi-process logic is tested that way).  Returns (rank, world, local rank)."""
+    global _DIST_DEVICE
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -71,9 +77,14 @@ def dist_init():
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=timeout_s),
+                                    device_id=torch.device("cuda", local))
+            _DIST_DEVICE = "cuda"
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=timeout_s))
+            _DIST_DEVICE = "cpu"
     return rank, world, local
 
 
@@ -88,9 +99,14 @@ def max_over_ranks(x: float, world: int) -> float:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_DIST_DEVICE)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def series_seed(rank: int) -> int:
+    """Each rank reconstructs its own tilt series (weak scaling, no data-path collective)."""
+    return 2000 + rank
 
 
 # ------------------------------------------------------------------ clocks
@@ -225,6 +241,22 @@ def algorithmic_bytes():
     return fp, bp
 
 
+# DRAM bytes per voxel of one launch, dram__bytes_read.sum + dram__bytes_write.sum from an
+# ncu capture of the 512x512x256 case (python bench.py --ncu-case, 67,108,864 voxels,
+# 512^2 detector): forward_project_kernel 269,974,272 + 5,381,120 B, bp_sart_column_kernel
+# 270,639,104 + 205,491,712 B.  Both grow with the voxel count; the back projector's
+# figure undercounts its writes by the dirty lines still in L2 when the launch ends
+# (at most the L2 size, about 63 MB in that capture).
+FP_DRAM_BYTES_PER_VOXEL = (269974272 + 5381120) / 67108864
+BP_DRAM_BYTES_PER_VOXEL = (270639104 + 205491712) / 67108864
+
+
+def dram_traffic():
+    """Measured DRAM bytes per launch scaled to the bench volume (forward, back)."""
+    V = RES[0] * RES[1] * RES[2]
+    return FP_DRAM_BYTES_PER_VOXEL * V, BP_DRAM_BYTES_PER_VOXEL * V
+
+
 # ------------------------------------------------------------------ CPU baseline (oracle)
 def cpu_sample_seconds(threads: int, views: int = 1):
     """Times the FP32 CPU restatement of the reference kernels (oracle/) on `views` views
@@ -318,7 +350,7 @@ def run_ours(args, rank, world, local):
                                           GPUMappedVolume)
     torch.cuda.set_device(local)
     ctx = Context(local)
-    geoms, b = make_problem(ctx, 2000 + rank)
+    geoms, b = make_problem(ctx, series_seed(rank))
     params = AlgebraicParameterSet(algorithm="sart", block_size=1, iterations=TARGET_ITERS, lam=LAMBDA,
                                    order=_abi.ORDER_IDENTITY)
     vol = GPUMappedVolume(ctx, RES)
@@ -362,12 +394,15 @@ def run_ours(args, rank, world, local):
     bp_gbs = bp_bytes / (bp_avg * 1e-3) / 1e9
     dominant = "back_project" if bp_ms >= fp_ms else "forward_project"
     ach = bp_gbs if dominant == "back_project" else fp_gbs
+    fp_traffic, bp_traffic = dram_traffic()
     roofline = {"bound": "hbm", "kernel": dominant, "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
-                "frac": ach / hbm_peak, "peak_source": peak_src, "traffic": None,
+                "frac": ach / hbm_peak, "peak_source": peak_src,
+                "traffic": bp_traffic if dominant == "back_project" else fp_traffic,
+                "traffic_source": "ncu dram bytes of the 512x512x256 case, scaled by voxel count",
                 "per_kernel": {"forward_project": {"avg_ms": fp_avg, "launches": nf, "algorithmic_bytes": fp_bytes,
-                                                   "gbs": fp_gbs, "frac": fp_gbs / hbm_peak},
+                                                   "gbs": fp_gbs, "frac": fp_gbs / hbm_peak, "traffic": fp_traffic},
                                "back_project": {"avg_ms": bp_avg, "launches": nb, "algorithmic_bytes": bp_bytes,
-                                                "gbs": bp_gbs, "frac": bp_gbs / hbm_peak}}}
+                                                "gbs": bp_gbs, "frac": bp_gbs / hbm_peak, "traffic": bp_traffic}}}
     rec.close()
     vol.close()
     # ---- e2e: one-call host-buffer reconstruction through the C ABI ----

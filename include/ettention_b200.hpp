@@ -1,0 +1,404 @@
+/*
+ * C++ operator surface of the B200 block-iterative reconstruction path, over the
+ * C ABI of ettention_b200.h (header-only; link libettention_b200.so).
+ *
+ * It keeps the class and method names of the reference's libReconstruction
+ * operators (paths relative to ettention/libReconstruction/src):
+ *   Framework                              LR/framework/Framework.cpp (owns the GPU context)
+ *   ScannerGeometry                        LR/model/geometry/ScannerGeometry.cpp:39-46,
+ *                                          ParallelScannerGeometry.cpp:44-69,
+ *                                          SingleAxisTiltRotator.cpp:42-78, MRCStack.cpp:250-261
+ *   GPUMappedVolume                        LR/model/volume/GPUMappedVolume.cpp:9-41,
+ *                                          VolumeProperties.cpp:21-98 (z-slab sub-volumes)
+ *   ForwardProjectionOperator              LR/algorithm/projections/forward/ForwardProjectionOperator.cpp:11-55
+ *   BackProjectionOperator                 LR/algorithm/projections/back/BackProjectionOperator.cpp:13-98
+ *   AlgebraicParameterSet::fromConfig      LR/setup/parameterset/AlgorithmParameterSet.cpp:8-53,
+ *                                          OptimizationParameterSet, VolumeParameterSet, HardwareParameterSet
+ *   BlockIterativeReconstructionOperator   LR/algorithm/reconstruction/blockiterative/
+ *                                          BlockIterativeReconstructionOperator.cpp:56-185
+ * Errors: every non-OK status of the ABI is rethrown as ettention::b200::Exception
+ * (validation) or GPUException (device errors), with the library's message, as
+ * the reference throws ettention::Exception / GPUException.
+ *
+ * Device images (SetOutput / setInput) are device pointers of width * height
+ * floats; the operators are stream-ordered on the Framework's stream and
+ * synchronise after each call, as the reference waits after every launch.
+ */
+#pragma once
+
+#include <array>
+#include <cstdint>
+#include <map>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "ettention_b200.h"
+
+namespace ettention {
+namespace b200 {
+
+class Exception : public std::runtime_error {
+public:
+    Exception(etcu_status status, const std::string& what) : std::runtime_error(what), status_(status) {}
+    etcu_status status() const { return status_; }
+
+private:
+    etcu_status status_;
+};
+
+class GPUException : public Exception {
+public:
+    using Exception::Exception;
+};
+
+inline void check(etcu_status status, const etcu_context* ctx) {
+    if (status == ETCU_OK) return;
+    const char* msg = etcu_last_error(ctx);
+    std::string text = msg && *msg ? msg : "ettention_b200 status " + std::to_string((int)status);
+    if (status == ETCU_ERR_CUDA || status == ETCU_ERR_NO_DEVICE || status == ETCU_ERR_OUT_OF_MEMORY)
+        throw GPUException(status, text);
+    throw Exception(status, text);
+}
+
+// The reference's Framework owns the OpenCL abstraction layer; here it owns the
+// CUDA context and stream of one device.
+class Framework {
+public:
+    explicit Framework(int device = 0) { check(etcu_context_create(device, &ctx_), nullptr); }
+    ~Framework() { etcu_context_destroy(ctx_); }
+    Framework(const Framework&) = delete;
+    Framework& operator=(const Framework&) = delete;
+    etcu_context* handle() const { return ctx_; }
+    void synchronize() { check(etcu_synchronize(ctx_), ctx_); }
+    // Work is ordered on this CUDA stream (nullptr: the context's own stream).
+    void setStream(void* cuda_stream) { check(etcu_set_stream(ctx_, cuda_stream), ctx_); }
+
+private:
+    etcu_context* ctx_ = nullptr;
+};
+
+class ScannerGeometry {
+public:
+    ScannerGeometry() = default;
+    explicit ScannerGeometry(const etcu_view& v) : view_(v) {}
+
+    // MRCStack.cpp:250-261: parallel base geometry of an nx x ny tilt series.
+    static ScannerGeometry mrcBase(uint32_t nx, uint32_t ny) {
+        etcu_view v{};
+        const float fx = (float)nx, fy = (float)ny;
+        const float src[3] = {-0.5f * fx, -0.5f * fy, fx}, det[3] = {-0.5f * fx, -0.5f * fy, -fx};
+        for (int i = 0; i < 3; ++i) {
+            v.source[i] = src[i];
+            v.detector[i] = det[i];
+            v.hpitch[i] = i == 0 ? 1.f : 0.f;
+            v.vpitch[i] = i == 1 ? 1.f : 0.f;
+        }
+        v.width = nx;
+        v.height = ny;
+        v.perspective = 0;
+        return ScannerGeometry(v);
+    }
+
+    // SingleAxisTiltRotator::createRotatedScannerGeometry.
+    ScannerGeometry rotated(float tilt_deg, float xaxis_tilt_deg = 0.f) const {
+        etcu_view out{};
+        check(etcu_view_rotate(&view_, tilt_deg, xaxis_tilt_deg, &out), nullptr);
+        return ScannerGeometry(out);
+    }
+
+    std::array<float, 16> getProjectionMatrix() const {
+        std::array<float, 16> m{};
+        check(etcu_view_projection_matrix(&view_, m.data()), nullptr);
+        return m;
+    }
+
+    float getTraversalLengthThroughBoundingBox(const float bbox_min[3], const float bbox_max[3]) const {
+        float r = 0.f;
+        check(etcu_view_traversal_length(&view_, bbox_min, bbox_max, &r), nullptr);
+        return r;
+    }
+
+    const etcu_view& view() const { return view_; }
+    uint32_t width() const { return view_.width; }
+    uint32_t height() const { return view_.height; }
+
+private:
+    etcu_view view_{};
+};
+
+class GPUMappedVolume {
+public:
+    // resolution (x, y, z); bounding box centred on origin with extent dimension
+    // (VolumeParameterSet.cpp:68-71); subVolumeCount z slabs.
+    GPUMappedVolume(Framework& fw, const std::array<uint32_t, 3>& resolution, const std::array<float, 3>& bbox_min,
+                    const std::array<float, 3>& bbox_max, etcu_voxel_type type = ETCU_VOXEL_FLOAT32,
+                    uint32_t subvolume_count = 1, float init_value = 0.f)
+        : fw_(&fw), res_(resolution) {
+        desc_ = etcu_volume_desc{};
+        for (int i = 0; i < 3; ++i) {
+            desc_.resolution[i] = resolution[i];
+            desc_.bbox_min[i] = bbox_min[i];
+            desc_.bbox_max[i] = bbox_max[i];
+        }
+        desc_.subvolume_count = subvolume_count;
+        check(etcu_volume_create(fw.handle(), &desc_, type, init_value, &vol_), fw.handle());
+    }
+
+    // Centred volume with unit voxels.
+    GPUMappedVolume(Framework& fw, const std::array<uint32_t, 3>& resolution, etcu_voxel_type type = ETCU_VOXEL_FLOAT32,
+                    uint32_t subvolume_count = 1)
+        : GPUMappedVolume(fw, resolution,
+                          {-0.5f * resolution[0], -0.5f * resolution[1], -0.5f * resolution[2]},
+                          {0.5f * resolution[0], 0.5f * resolution[1], 0.5f * resolution[2]}, type,
+                          subvolume_count) {}
+
+    ~GPUMappedVolume() { etcu_volume_destroy(vol_); }
+    GPUMappedVolume(const GPUMappedVolume&) = delete;
+    GPUMappedVolume& operator=(const GPUMappedVolume&) = delete;
+
+    size_t voxelCount() const { return (size_t)res_[0] * res_[1] * res_[2]; }
+    const std::array<uint32_t, 3>& resolution() const { return res_; }
+    const etcu_volume_desc& description() const { return desc_; }
+    uint32_t getSubVolumeCount() const { return desc_.subvolume_count ? desc_.subvolume_count : 1; }
+    etcu_volume* handle() const { return vol_; }
+    Framework& framework() const { return *fw_; }
+
+    // Host float32 volume, x fastest.
+    void upload(const float* host) { check(etcu_volume_upload(vol_, host), fw_->handle()); }
+    void download(float* host) const { check(etcu_volume_download(vol_, host), fw_->handle()); }
+    std::vector<float> download() const {
+        std::vector<float> out(voxelCount());
+        download(out.data());
+        return out;
+    }
+    // Prior-knowledge mask (value / 255); nullptr removes it.
+    void setMask(const uint8_t* host_mask) { check(etcu_volume_set_mask(vol_, host_mask), fw_->handle()); }
+
+private:
+    Framework* fw_;
+    std::array<uint32_t, 3> res_;
+    etcu_volume_desc desc_{};
+    etcu_volume* vol_ = nullptr;
+};
+
+class ForwardProjectionOperator {
+public:
+    ForwardProjectionOperator(GPUMappedVolume& vol, uint32_t samples = 1) : vol_(&vol), samples_(samples) {}
+    void setScannerGeometry(const ScannerGeometry& g) { geo_ = g; }
+    void SetOutput(float* d_virtual, float* d_traversal) {
+        virt_ = d_virtual;
+        trav_ = d_traversal;
+    }
+    // Adds the sub-volume's line integrals into the outputs (the caller clears them).
+    void Execute(uint32_t subvolume) {
+        etcu_context* ctx = vol_->framework().handle();
+        check(etcu_forward_project(vol_->handle(), &geo_.view(), subvolume, samples_, virt_, trav_), ctx);
+        vol_->framework().synchronize();
+    }
+
+private:
+    GPUMappedVolume* vol_;
+    uint32_t samples_;
+    ScannerGeometry geo_;
+    float* virt_ = nullptr;
+    float* trav_ = nullptr;
+};
+
+class BackProjectionOperator {
+public:
+    static constexpr uint32_t ALL_SUB_VOLUMES = ETCU_ALL_SUBVOLUMES;
+
+    BackProjectionOperator(GPUMappedVolume& vol, float lambda, uint32_t samples = 1,
+                           etcu_sampling sampling = ETCU_SAMPLING_Q8)
+        : vol_(&vol), lambda_(lambda), samples_(samples), sampling_(sampling) {}
+    void setScannerGeometry(const ScannerGeometry& g) { geo_ = g; }
+    void setInput(const float* d_residual, const float* d_traversal, uint32_t block_size) {
+        res_ = d_residual;
+        trav_ = d_traversal;
+        block_ = block_size;
+    }
+    // Updates with lambda / blockSize (BackProjectionKernel.cpp:94).
+    void execute(uint32_t subvolume = ALL_SUB_VOLUMES) {
+        etcu_context* ctx = vol_->framework().handle();
+        check(etcu_back_project(vol_->handle(), &geo_.view(), subvolume, samples_, lambda_, block_, res_, trav_,
+                                sampling_),
+              ctx);
+        vol_->framework().synchronize();
+    }
+
+private:
+    GPUMappedVolume* vol_;
+    float lambda_;
+    uint32_t samples_;
+    etcu_sampling sampling_;
+    ScannerGeometry geo_;
+    const float* res_ = nullptr;
+    const float* trav_ = nullptr;
+    uint32_t block_ = 1;
+};
+
+// The reference's configuration keys of the block-iterative reconstruction.
+struct AlgebraicParameterSet {
+    std::string algorithm = "sart";
+    uint32_t blockSize = 1;
+    uint32_t iterations = 1;
+    float lambda = 0.3f;
+    bool useLongObjectCompensation = false;
+    uint32_t fpSamples = 1, bpSamples = 1;
+    etcu_voxel_type voxelType = ETCU_VOXEL_FLOAT32;
+    etcu_order order = ETCU_ORDER_RANDOM;  // optimization.projectionIteration default
+    etcu_sampling sampling = ETCU_SAMPLING_Q8;
+    uint32_t subVolumeCount = 1;
+    std::array<uint32_t, 3> resolution{{0, 0, 0}};
+    std::array<float, 3> dimension{{0.f, 0.f, 0.f}};
+    std::array<float, 3> origin{{0.f, 0.f, 0.f}};
+    bool hasDimension = false;
+    float initValue = 0.f;
+    std::vector<uint32_t> skip;
+    float xAxisTilt = 0.f;
+
+    static std::vector<float> vec(const std::string& s) {
+        std::string t = s;
+        for (char& c : t)
+            if (c == ',') c = ' ';
+        std::istringstream in(t);
+        std::vector<float> out;
+        float f;
+        while (in >> f) out.push_back(f);
+        return out;
+    }
+
+    // AlgorithmParameterSet.cpp:10-23 and the optimization / volume / hardware /
+    // input parameter sets; the messages are the reference's.
+    static AlgebraicParameterSet fromConfig(const std::map<std::string, std::string>& cfg) {
+        auto get = [&](const std::string& k, const std::string& dflt) {
+            auto it = cfg.find(k);
+            return it == cfg.end() ? dflt : it->second;
+        };
+        AlgebraicParameterSet p;
+        auto alg = cfg.find("algorithm");
+        if (alg == cfg.end()) throw Exception(ETCU_ERR_INVALID_ARGUMENT, "missing parameter algorithm");
+        p.algorithm = alg->second;
+        if (p.algorithm == "sart") p.blockSize = 1;
+        else if (p.algorithm == "sirt") p.blockSize = ETCU_BLOCK_ALL;
+        else p.blockSize = (uint32_t)std::stoul(get("algorithm.blockSize", std::to_string(ETCU_BLOCK_ALL)));
+        p.iterations = (uint32_t)std::stoul(get("algorithm.numberOfIterations", "1"));
+        p.lambda = std::stof(get("algorithm.lambda", "0.3"));
+        const std::string loc = get("algorithm.useLongObjectCompensation", "false");
+        p.useLongObjectCompensation = loc == "true" || loc == "1" || loc == "yes";
+        const std::string basis = get("algorithm.basisFunctions", "voxels");
+        if (basis == "blobs")
+            throw Exception(ETCU_ERR_UNSUPPORTED, "blob basis functions are not part of the voxel hot path");
+        if (basis != "voxels")
+            throw Exception(ETCU_ERR_INVALID_ARGUMENT,
+                            "Illegal value for parameter \"algorithm.basisFunctions\": " + basis + "!");
+        p.fpSamples = (uint32_t)std::stoul(get("forwardProjection.samples", "1"));
+        p.bpSamples = (uint32_t)std::stoul(get("backProjection.samples", "1"));
+        const std::string vt = get("optimization.internalVoxelRepresentationType", "float");
+        if (vt == "float" || vt == "float32") p.voxelType = ETCU_VOXEL_FLOAT32;
+        else if (vt == "half") p.voxelType = ETCU_VOXEL_HALF16;
+        else if (vt == "half_master") p.voxelType = ETCU_VOXEL_F16_MASTER;
+        else if (vt == "bf16_master") p.voxelType = ETCU_VOXEL_BF16_MASTER;
+        else throw Exception(ETCU_ERR_INVALID_ARGUMENT, "UChar is not supported as a valid internal voxel storage data type.");
+        const std::string ord = get("optimization.projectionIteration", "random");
+        if (ord == "identity") p.order = ETCU_ORDER_IDENTITY;
+        else if (ord == "random") p.order = ETCU_ORDER_RANDOM;
+        else if (ord == "maxangle") p.order = ETCU_ORDER_MAXANGLE;
+        else if (ord == "buckets") p.order = ETCU_ORDER_BUCKETS;
+        else throw Exception(ETCU_ERR_INVALID_ARGUMENT, "Illegal ProjectionSetType!");
+        p.subVolumeCount = (uint32_t)std::stoul(get("hardware.subVolumeCount", "1"));
+        if (cfg.count("volume.dimension")) {
+            const auto d = vec(cfg.at("volume.dimension"));
+            for (int i = 0; i < 3 && i < (int)d.size(); ++i) {
+                p.dimension[i] = d[i];
+                p.resolution[i] = (uint32_t)d[i];
+            }
+            p.hasDimension = true;
+        }
+        if (cfg.count("volume.resolution")) {
+            const auto r = vec(cfg.at("volume.resolution"));
+            for (int i = 0; i < 3 && i < (int)r.size(); ++i) p.resolution[i] = (uint32_t)r[i];
+        }
+        if (cfg.count("volume.origin")) {
+            const auto o = vec(cfg.at("volume.origin"));
+            for (int i = 0; i < 3 && i < (int)o.size(); ++i) p.origin[i] = o[i];
+        }
+        p.initValue = std::stof(get("volume.initValue", "0"));
+        if (cfg.count("input.skipProjections"))
+            for (float f : vec(cfg.at("input.skipProjections"))) p.skip.push_back((uint32_t)f);
+        p.xAxisTilt = std::stof(get("input.xAxisTilt", "0"));
+        if (p.blockSize == 0) throw Exception(ETCU_ERR_INVALID_ARGUMENT, "Illegal ProjectionBlockSize!");
+        return p;
+    }
+
+    etcu_recon_params reconParams(bool use_graph = true) const {
+        etcu_recon_params r{};
+        r.lambda = lambda;
+        r.block_size = blockSize;
+        r.fp_samples = fpSamples;
+        r.bp_samples = bpSamples;
+        r.use_long_object_compensation = useLongObjectCompensation ? 1 : 0;
+        r.order = order;
+        r.sampling = sampling;
+        r.skip = skip.empty() ? nullptr : skip.data();
+        r.skip_count = (uint32_t)skip.size();
+        r.use_graph = use_graph ? 1 : 0;
+        return r;
+    }
+};
+
+class BlockIterativeReconstructionOperator {
+public:
+    // The tilt series (views.size() x height x width floats, host) is uploaded once.
+    BlockIterativeReconstructionOperator(GPUMappedVolume& vol, const std::vector<ScannerGeometry>& views,
+                                         const float* host_projections, const AlgebraicParameterSet& p,
+                                         bool use_graph = true)
+        : vol_(&vol), params_(p) {
+        std::vector<etcu_view> v;
+        v.reserve(views.size());
+        for (const auto& g : views) v.push_back(g.view());
+        const etcu_recon_params rp = p.reconParams(use_graph);
+        check(etcu_recon_create(vol.handle(), v.data(), (uint32_t)v.size(), host_projections, &rp, &rec_),
+              vol.framework().handle());
+    }
+    ~BlockIterativeReconstructionOperator() { etcu_recon_destroy(rec_); }
+    BlockIterativeReconstructionOperator(const BlockIterativeReconstructionOperator&) = delete;
+    BlockIterativeReconstructionOperator& operator=(const BlockIterativeReconstructionOperator&) = delete;
+
+    void run() { runNiterations(params_.iterations); }
+    void runSingleIteration() { runNiterations(1); }
+    void runNiterations(uint32_t n) {
+        check(etcu_recon_run(rec_, n), vol_->framework().handle());
+        vol_->framework().synchronize();
+    }
+    void getReconstructedVolume(float* host) const { vol_->download(host); }
+    std::vector<float> getReconstructedVolume() const { return vol_->download(); }
+    double lastResidualSq() const {
+        double r = 0.0;
+        check(etcu_recon_last_residual_sq(rec_, &r), vol_->framework().handle());
+        return r;
+    }
+    double dataResidualSq() const {
+        double r = 0.0;
+        check(etcu_recon_data_residual_sq(rec_, &r), vol_->framework().handle());
+        return r;
+    }
+    std::vector<uint32_t> viewOrder() const {
+        std::vector<uint32_t> out(1u << 16);
+        uint32_t n = 0;
+        check(etcu_recon_view_order(rec_, out.data(), (uint32_t)out.size(), &n), vol_->framework().handle());
+        out.resize(n);
+        return out;
+    }
+
+private:
+    GPUMappedVolume* vol_;
+    AlgebraicParameterSet params_;
+    etcu_recon* rec_ = nullptr;
+};
+
+}  // namespace b200
+}  // namespace ettention

@@ -1,0 +1,48 @@
+// Host-only checks of include/ettention_b200.hpp: geometry, configuration keys and
+// error mapping.  Prints one "key value..." line per result for tests/test_cpp_shim.py.
+#include <cstdio>
+#include <map>
+#include <string>
+
+#include "ettention_b200.hpp"
+
+using namespace ettention::b200;
+
+static void config_case(const char* name, const std::map<std::string, std::string>& cfg) {
+    try {
+        AlgebraicParameterSet p = AlgebraicParameterSet::fromConfig(cfg);
+        std::printf("config %s ok %u %u %g %d %u\n", name, p.blockSize, p.iterations, p.lambda, (int)p.order,
+                    p.subVolumeCount);
+    } catch (const Exception& e) {
+        std::printf("config %s error %d %s\n", name, (int)e.status(), e.what());
+    }
+}
+
+int main() {
+    const ScannerGeometry g = ScannerGeometry::mrcBase(96, 80).rotated(30.f);
+    const auto m = g.getProjectionMatrix();
+    std::printf("matrix");
+    for (float v : m) std::printf(" %.9g", v);
+    std::printf("\n");
+    const float lo[3] = {-48.f, -40.f, -20.f}, hi[3] = {48.f, 40.f, 20.f};
+    std::printf("traversal %.9g\n", g.getTraversalLengthThroughBoundingBox(lo, hi));
+    config_case("sart", {{"algorithm", "sart"}, {"algorithm.numberOfIterations", "5"}, {"algorithm.lambda", "0.3"},
+                         {"optimization.projectionIteration", "identity"}});
+    config_case("sirt", {{"algorithm", "sirt"}, {"algorithm.numberOfIterations", "3"}, {"algorithm.lambda", "0.5"}});
+    config_case("block", {{"algorithm", "blockIterative"}, {"algorithm.blockSize", "8"},
+                          {"algorithm.numberOfIterations", "2"}, {"algorithm.lambda", "0.2"},
+                          {"optimization.projectionIteration", "maxangle"}, {"hardware.subVolumeCount", "3"}});
+    config_case("zero_block", {{"algorithm", "blockIterative"}, {"algorithm.blockSize", "0"},
+                               {"algorithm.numberOfIterations", "1"}, {"algorithm.lambda", "0.2"}});
+    config_case("bad_order", {{"algorithm", "sart"}, {"optimization.projectionIteration", "zigzag"}});
+    config_case("missing", {{"algorithm.lambda", "0.2"}});
+    try {
+        Framework fw(0);
+        std::printf("framework ok\n");
+    } catch (const GPUException& e) {
+        std::printf("framework gpu_error %d %s\n", (int)e.status(), e.what());
+    } catch (const Exception& e) {
+        std::printf("framework error %d %s\n", (int)e.status(), e.what());
+    }
+    return 0;
+}
