@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-reps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c4"],
+                    help="c2: the headline SART workload (default); c4: 64 batched series of uneven sizes")
     ap.add_argument("--ncu-case", action="store_true",
                     help="small profiling case for ncu: 512x512x256 volume, 8 views, one SART iteration "
                          "launched kernel by kernel (8 forward + 8 back projections), then per-kernel times")
@@ -167,16 +169,16 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ workload
-def make_phantom_torch(seed: int, device):
-    """200 ellipsoids (centres uniform, semi-axes U(8,128), uniform rotation,
+def make_phantom_torch(seed: int, device, res=None, count: int = 200, axes=(8.0, 128.0)):
+    """`count` ellipsoids (centres uniform, semi-axes U(axes), uniform rotation,
     density U(0.05,1.0), additive), scaled by MU_SCALE; built on the GPU."""
     import torch
     rng = np.random.Generator(np.random.PCG64(seed))
-    X, Y, Z = RES
+    X, Y, Z = RES if res is None else res
     vol = torch.zeros((Z, Y, X), dtype=torch.float32, device=device)
-    for _ in range(200):
+    for _ in range(count):
         c = rng.uniform([0, 0, 0], [X, Y, Z])
-        a = rng.uniform(8.0, 128.0, 3)
+        a = rng.uniform(axes[0], axes[1], 3)
         q = rng.normal(size=4)
         q /= np.linalg.norm(q)
         w, x, y, z = q
@@ -458,10 +460,118 @@ def run_ncu_case():
     ctx.close()
 
 
+# ------------------------------------------------------------------ C4: many uneven series
+C4_SERIES = 64
+
+
+def c4_shapes(seed: int = 4000):
+    """64 seeded tilt series between 96^3 and 256x256x128 voxels, 41 to 81 views over
+    +-50 to +-70 degrees (detector = volume x by y, pitch 1)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for _ in range(C4_SERIES):
+        X = int(rng.integers(6, 17)) * 16
+        Y = int(rng.integers(6, 17)) * 16
+        Z = int(rng.integers(6, 9)) * 16
+        nv = int(rng.integers(20, 41)) * 2 + 1
+        tmax = float(rng.uniform(50.0, 70.0))
+        out.append(((X, Y, Z), nv, tmax))
+    return out
+
+
+def run_c4(args):
+    """Batched SART of the 64 C4 series (one forward and one back-projection launch per
+    step over all series, one graph per iteration) against the same series one after
+    another (one graph per series)."""
+    import torch
+    from ettention_b200 import _abi
+    from ettention_b200.operators import (AlgebraicParameterSet, BatchReconstructionOperator,
+                                          BlockIterativeReconstructionOperator, Context,
+                                          ForwardProjectionOperator, GPUMappedVolume, mrc_base_geometry)
+    ctx = Context(0)
+    dev = torch.device("cuda", 0)
+    problems = []
+    for i, ((X, Y, Z), nv, tmax) in enumerate(c4_shapes()):
+        ph = make_phantom_torch(4100 + i, dev, (X, Y, Z), count=40, axes=(4.0, 48.0))
+        geoms = [mrc_base_geometry(X, Y).rotated(float(a)) for a in np.linspace(-tmax, tmax, nv)]
+        vol = GPUMappedVolume(ctx, (X, Y, Z))
+        vol.upload(ph.cpu().numpy())
+        fp = ForwardProjectionOperator(vol, 1)
+        projs = torch.zeros((nv, Y, X), dtype=torch.float32, device=dev)
+        scratch = torch.zeros((Y, X), dtype=torch.float32, device=dev)
+        for k, g in enumerate(geoms):
+            fp.setScannerGeometry(g)
+            fp.SetOutput(projs[k], scratch)
+            fp.Execute(0)
+        vol.close()
+        problems.append(((X, Y, Z), geoms, projs.cpu().numpy()))
+    p = AlgebraicParameterSet(algorithm="sart", block_size=1, iterations=1, lam=LAMBDA, order=_abi.ORDER_IDENTITY)
+    stream = torch.cuda.ExternalStream(ctx.stream_handle)
+
+    def timed(run, reps):
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ctx.synchronize()
+        ev0.record(stream)
+        for _ in range(reps):
+            run()
+        ev1.record(stream)
+        ev1.synchronize()
+        return ev0.elapsed_time(ev1) / reps
+
+    vols = [GPUMappedVolume(ctx, shape) for shape, _, _ in problems]
+    batch = BatchReconstructionOperator([(v, g, pr) for v, (_, g, pr) in zip(vols, problems)], p)
+    for _ in range(args.warmup):
+        batch.runNiterations(1)
+    batch_ms = timed(lambda: batch.runNiterations(1), args.steps)
+    launches = batch.launches_per_iteration
+    batch.close()
+    for v in vols:
+        v.close()
+    seq = []
+    for shape, geoms, projs in problems:
+        vol = GPUMappedVolume(ctx, shape)
+        rec = BlockIterativeReconstructionOperator(vol, geoms, projs, p)
+        seq.append((vol, rec))
+    def run_seq():
+        for _, rec in seq:
+            rec.runNiterations(1)
+    for _ in range(args.warmup):
+        run_seq()
+    seq_ms = timed(run_seq, args.steps)
+    seq_launches = sum(r.launches_per_iteration for _, r in seq)
+    for vol, rec in seq:
+        rec.close()
+        vol.close()
+    updates = sum(s[0] * s[1] * s[2] * len(g) for s, g, _ in problems)
+    byts = sum(len(g) * (3 * s[0] * s[1] * s[2] * 4 + 20 * s[0] * s[1]) for s, g, _ in problems)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    print(json.dumps({
+        "metric": "C4 batched SART ms per iteration (64 series)", "value": batch_ms, "unit": "ms",
+        "higher_is_better": False, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "dtype": "f32",
+        "data": "synthetic (seeded 40-ellipsoid phantoms per series, CUDA-forward-projected, noise-free)",
+        "config": {"workload": "C4: 64 SART series, 96^3 to 256x256x128, 41 to 81 views over +-50..70 deg",
+                   "series": C4_SERIES, "voxel_view_updates_per_iteration": updates},
+        "sequential_ms": seq_ms, "speedup_vs_sequential": seq_ms / batch_ms,
+        "launches_per_iteration": {"batched": launches, "sequential": seq_launches},
+        "voxel_updates_per_s": updates / (batch_ms * 1e-3),
+        "roofline": {"bound": "hbm", "achieved": byts / (batch_ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
+                     "frac": byts / (batch_ms * 1e-3) / 1e9 / hbm,
+                     "bytes": "per view: 4V forward read + 8V back read+write + 20P"}}))
+    ctx.close()
+
+
 def main():
     args = parse()
     if args.ncu_case:
         run_ncu_case()
+        return
+    if args.workload == "c4":
+        run_c4(args)
         return
     rank, world, local = dist_init()
     try:

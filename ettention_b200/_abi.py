@@ -48,6 +48,11 @@ class ReconParams(ctypes.Structure):
                 ("skip_count", ctypes.c_uint32), ("use_graph", ctypes.c_int32)]
 
 
+class BatchSeries(ctypes.Structure):
+    _fields_ = [("volume", ctypes.c_void_p), ("views", ctypes.POINTER(View)), ("n_views", ctypes.c_uint32),
+                ("host_projections", ctypes.c_void_p)]
+
+
 _lib = None
 
 # name -> (restype, argtypes)
@@ -95,6 +100,11 @@ _SIG = {
     "etcu_reconstruct": (_S, [_P, ctypes.POINTER(VolumeDesc), _I, ctypes.POINTER(View), _U, _P,
                               ctypes.POINTER(ReconParams), _U, _P]),
     "etcu_projection_order": (_S, [_I, _U, _P, _U, _P, ctypes.POINTER(_U)]),
+    "etcu_batch_create": (_S, [_P, ctypes.POINTER(BatchSeries), _U, ctypes.POINTER(ReconParams), ctypes.POINTER(_P)]),
+    "etcu_batch_destroy": (_S, [_P]),
+    "etcu_batch_run": (_S, [_P, _U]),
+    "etcu_batch_last_residual_sq": (_S, [_P, _P]),
+    "etcu_batch_launches_per_iteration": (_U, [_P]),
     "etcu_sart_view_update_noalloc": (_S, [ctypes.POINTER(VolumeDesc), _P, _P, ctypes.POINTER(View), _U, _U, _F, _P,
                                            ctypes.POINTER(ctypes.c_double)]),
 }

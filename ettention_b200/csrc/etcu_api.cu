@@ -1339,6 +1339,266 @@ extern "C" etcu_status etcu_recon_profile_iteration(etcu_recon* r, float* fp_ms,
     return ETCU_OK;
 }
 
+// ================================================================ batched series
+struct etcu_batch {
+    etcu_context* ctx = nullptr;
+    uint32_t n = 0;
+    std::vector<etcu_volume*> vols;
+    std::vector<int> steps;                // views per series
+    std::vector<std::pair<void*, size_t>> allocs;  // device allocations (pointer, bytes)
+    FpArgs* d_fp = nullptr;                // per-series forward-projection arguments
+    BpArgs* d_bp = nullptr;                // per-series back-projection arguments
+    int* d_steps = nullptr;
+    double* d_resid = nullptr;             // per series
+    int fp_path = kFpPathGeneral;
+    int max_steps = 0, max_w = 0, max_h = 0, max_rx = 0, max_ry = 0;
+    etcu_sampling sampling = ETCU_SAMPLING_Q8;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint32_t launches = 0;
+};
+
+namespace {
+
+void batch_free(etcu_batch* b) {
+    etcu_context* ctx = b->ctx;
+    cudaStreamSynchronize(ctx->stream);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    for (auto& a : b->allocs) dfree(ctx, a.first, a.second);
+    b->allocs.clear();
+}
+
+etcu_status batch_alloc(etcu_batch* b, void** p, size_t bytes) {
+    etcu_status s = dalloc(b->ctx, p, bytes);
+    if (s == ETCU_OK && *p) b->allocs.emplace_back(*p, bytes);
+    return s;
+}
+
+template <int kPath>
+void launch_fp_batch_t(const etcu_batch* b, int step, cudaStream_t st) {
+    dim3 grid((b->max_w + 127) / 128, b->max_h, b->n);
+    forward_project_batch_kernel<float, false, kPath><<<grid, 128, 0, st>>>(b->d_fp, b->d_steps, step);
+}
+
+// One SART step of every series: forward projection of the view at order position
+// `step` with the residual epilogue, then its back projection.
+void issue_batch_step(const etcu_batch* b, int step, cudaStream_t st) {
+    switch (b->fp_path) {
+    case kFpPathXzNoCap: launch_fp_batch_t<kFpPathXzNoCap>(b, step, st); break;
+    case kFpPathXz: launch_fp_batch_t<kFpPathXz>(b, step, st); break;
+    default: launch_fp_batch_t<kFpPathGeneral>(b, step, st); break;
+    }
+    dim3 grid((b->max_rx + 31) / 32, (b->max_ry + 7) / 8, b->n), block(32, 8, 1);
+    if (b->sampling == ETCU_SAMPLING_EXACT)
+        bp_sart_row_batch_kernel<kSampleExact><<<grid, block, 0, st>>>(b->d_bp, b->d_steps, step);
+    else
+        bp_sart_row_batch_kernel<kSampleQ8><<<grid, block, 0, st>>>(b->d_bp, b->d_steps, step);
+}
+
+etcu_status issue_batch_iteration(etcu_batch* b, cudaStream_t st) {
+    etcu_context* ctx = b->ctx;
+    CK(ctx, cudaMemsetAsync(b->d_resid, 0, sizeof(double) * b->n, st));
+    for (int k = 0; k < b->max_steps; ++k) issue_batch_step(b, k, st);
+    CKL(ctx);
+    return ETCU_OK;
+}
+
+etcu_status batch_build(etcu_context* ctx, const etcu_batch_series* series, uint32_t n,
+                        const etcu_recon_params* params, etcu_batch* b) {
+    if (params->block_size != 1)
+        return fail(ctx, ETCU_ERR_UNSUPPORTED, "batched series run SART (block size 1)");
+    if (params->bp_samples > 1)
+        return fail(ctx, ETCU_ERR_UNSUPPORTED, "batched series use one back-projection sample");
+    if (params->sampling != ETCU_SAMPLING_Q8 && params->sampling != ETCU_SAMPLING_EXACT)
+        return fail(ctx, ETCU_ERR_UNSUPPORTED, "batched series sample with ETCU_SAMPLING_Q8 or _EXACT");
+    if ((int)params->order < 0 || (int)params->order > 3)
+        return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "Illegal ProjectionSetType!");
+    b->sampling = params->sampling;
+    std::vector<FpArgs> fp(n);
+    std::vector<BpArgs> bp(n);
+    bool all_fast2d = true, all_nocap = true;
+    etcu_status s;
+    for (uint32_t i = 0; i < n; ++i) {
+        const etcu_batch_series& sr = series[i];
+        etcu_volume* vol = sr.volume;
+        if (!vol || !sr.views || !sr.host_projections || sr.n_views == 0)
+            return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "series %u: NULL volume, views or projections", i);
+        if (vol->ctx != ctx) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "series %u: volume of another context", i);
+        if (vol->type != ETCU_VOXEL_FLOAT32 || vol->mask || vol->slabs.size() != 1)
+            return fail(ctx, ETCU_ERR_UNSUPPORTED, "series %u: batched series need an FP32 volume, one sub-volume, no mask",
+                        i);
+        const SlabConst& slab = vol->slabs[0];
+        const uint32_t W = sr.views[0].width, H = sr.views[0].height;
+        for (uint32_t v = 0; v < sr.n_views; ++v) {
+            if ((s = check_view(ctx, &sr.views[v])) != ETCU_OK) return s;
+            if (sr.views[v].perspective || sr.views[v].width != W || sr.views[v].height != H)
+                return fail(ctx, ETCU_ERR_UNSUPPORTED, "series %u: batched series need parallel views of one size", i);
+        }
+        const std::vector<uint32_t> order =
+            projection_order(params->order, sr.n_views, params->skip, params->skip ? params->skip_count : 0);
+        if (order.empty()) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "series %u: no projections left", i);
+        std::vector<ViewConst> vc(sr.n_views);
+        std::vector<float> pat(4 * (size_t)sr.n_views);
+        float vs[3] = {slab.vs.x, slab.vs.y, slab.vs.z};
+        for (uint32_t v = 0; v < sr.n_views; ++v) {
+            float loc = 0.f;
+            if (params->use_long_object_compensation)
+                loc = traversal_length(sr.views[v], vol->desc.bbox_min, vol->desc.bbox_max);
+            vc[v] = make_view_const(sr.views[v], slab, loc);
+            if (!row_constant(vc[v]))
+                return fail(ctx, ETCU_ERR_UNSUPPORTED, "series %u: batched series need views tilted about y", i);
+            all_fast2d &= vc[v].fast2d != 0;
+            std::string err;
+            if (!sample_pattern(sr.views[v], vs, 1, pat.data() + 4 * (size_t)v, &err))
+                return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "%s", err.c_str());
+        }
+        all_nocap &= slab.rx + slab.rz - 1 <= kMaxDdaIterations;
+        // device copies: projections, view table, order, samples, padded (residual, length) image
+        float* d_proj;
+        ViewConst* d_views;
+        uint32_t* d_order;
+        float4* d_samples;
+        const size_t P = (size_t)W * H;
+        if ((s = batch_alloc(b, (void**)&d_proj, P * sr.n_views * sizeof(float))) != ETCU_OK) return s;
+        if ((s = batch_alloc(b, (void**)&d_views, vc.size() * sizeof(ViewConst))) != ETCU_OK) return s;
+        if ((s = batch_alloc(b, (void**)&d_order, order.size() * sizeof(uint32_t))) != ETCU_OK) return s;
+        if ((s = batch_alloc(b, (void**)&d_samples, pat.size() * sizeof(float))) != ETCU_OK) return s;
+        CK(ctx, cudaMemcpyAsync(d_proj, sr.host_projections, P * sr.n_views * sizeof(float), cudaMemcpyHostToDevice,
+                                ctx->stream));
+        CK(ctx, cudaMemcpyAsync(d_views, vc.data(), vc.size() * sizeof(ViewConst), cudaMemcpyHostToDevice, ctx->stream));
+        CK(ctx, cudaMemcpyAsync(d_order, order.data(), order.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                                ctx->stream));
+        CK(ctx, cudaMemcpyAsync(d_samples, pat.data(), pat.size() * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+        const size_t pw = (size_t)W + 2 * kPad, ph = (size_t)H + 2 * kPad;
+        const size_t pitch = pw, slot = pw * ph;
+        float2* rl_base;
+        if ((s = batch_alloc(b, (void**)&rl_base, slot * sizeof(float2))) != ETCU_OK) return s;
+        CK(ctx, cudaMemsetAsync(rl_base, 0, slot * sizeof(float2), ctx->stream));
+        float2* rl = rl_base + kPad * pitch + kPad;
+        FpArgs& f = fp[i];
+        f = FpArgs{};
+        fill_fp_volume_ptrs(vol, slab, f);
+        f.slab = slab;
+        f.views = d_views;
+        f.order = d_order;
+        f.first = 0;
+        f.W = (int)W;
+        f.H = (int)H;
+        f.samples = params->fp_samples == 0 ? 1 : (int)params->fp_samples;
+        f.mode = kFpPairResidual;
+        f.overwrite = 1;
+        f.loc = params->use_long_object_compensation ? 1 : 0;
+        f.rl = rl;
+        f.rl_pitch = pitch;
+        f.rl_slot = slot;
+        f.real = d_proj;
+        f.resid_sq = nullptr;  // set below (per-series element of d_resid)
+        BpArgs& g = bp[i];
+        g = BpArgs{};
+        fill_bp_volume_ptrs(vol, slab, g);
+        g.slab = slab;
+        g.views = d_views;
+        g.order = d_order;
+        g.first = 0;
+        g.nviews = 1;
+        g.rl = rl;
+        g.rl_pitch = pitch;
+        g.rl_slot = slot;
+        g.W = (int)W;
+        g.H = (int)H;
+        g.lambda = params->lambda;  // block size 1 (BackProjectionKernel.cpp:94)
+        g.samples = d_samples;
+        g.nsamples = 1;
+        b->vols.push_back(vol);
+        b->steps.push_back((int)order.size());
+        b->max_steps = std::max(b->max_steps, (int)order.size());
+        b->max_w = std::max(b->max_w, (int)W);
+        b->max_h = std::max(b->max_h, (int)H);
+        b->max_rx = std::max(b->max_rx, slab.rx);
+        b->max_ry = std::max(b->max_ry, slab.ry);
+    }
+    b->fp_path = !all_fast2d ? kFpPathGeneral : (all_nocap ? kFpPathXzNoCap : kFpPathXz);
+    if ((s = batch_alloc(b, (void**)&b->d_resid, sizeof(double) * n)) != ETCU_OK) return s;
+    for (uint32_t i = 0; i < n; ++i) fp[i].resid_sq = b->d_resid + i;
+    if ((s = batch_alloc(b, (void**)&b->d_fp, sizeof(FpArgs) * n)) != ETCU_OK) return s;
+    if ((s = batch_alloc(b, (void**)&b->d_bp, sizeof(BpArgs) * n)) != ETCU_OK) return s;
+    if ((s = batch_alloc(b, (void**)&b->d_steps, sizeof(int) * n)) != ETCU_OK) return s;
+    CK(ctx, cudaMemcpyAsync(b->d_fp, fp.data(), sizeof(FpArgs) * n, cudaMemcpyHostToDevice, ctx->stream));
+    CK(ctx, cudaMemcpyAsync(b->d_bp, bp.data(), sizeof(BpArgs) * n, cudaMemcpyHostToDevice, ctx->stream));
+    CK(ctx, cudaMemcpyAsync(b->d_steps, b->steps.data(), sizeof(int) * n, cudaMemcpyHostToDevice, ctx->stream));
+    CK(ctx, cudaMemsetAsync(b->d_resid, 0, sizeof(double) * n, ctx->stream));
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    b->launches = 2u * (uint32_t)b->max_steps;
+    if (params->use_graph) {
+        cudaStream_t cs = ctx->stream;
+        CK(ctx, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        etcu_status is = issue_batch_iteration(b, cs);
+        cudaGraph_t gr = nullptr;
+        cudaError_t e = cudaStreamEndCapture(cs, &gr);
+        if (is != ETCU_OK) {
+            if (gr) cudaGraphDestroy(gr);
+            return is;
+        }
+        CK(ctx, e);
+        b->graph = gr;
+        CK(ctx, cudaGraphInstantiate(&b->exec, gr, 0));
+    }
+    return ETCU_OK;
+}
+
+}  // namespace
+
+extern "C" etcu_status etcu_batch_create(etcu_context* ctx, const etcu_batch_series* series, uint32_t n_series,
+                                         const etcu_recon_params* params, etcu_batch** out) {
+    if (!ctx || !series || !params || !out) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    if (n_series == 0) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "no series");
+    if (n_series > 65535) return fail(ctx, ETCU_ERR_UNSUPPORTED, "at most 65535 series per batch");
+    std::unique_ptr<etcu_batch, void (*)(etcu_batch*)> b(new etcu_batch(), [](etcu_batch* p) {
+        batch_free(p);
+        delete p;
+    });
+    b->ctx = ctx;
+    b->n = n_series;
+    etcu_status s = batch_build(ctx, series, n_series, params, b.get());
+    if (s != ETCU_OK) return s;
+    *out = b.release();
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_batch_destroy(etcu_batch* b) {
+    if (!b) return ETCU_OK;
+    batch_free(b);
+    delete b;
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_batch_run(etcu_batch* b, uint32_t iterations) {
+    if (!b) return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL batch");
+    etcu_context* ctx = b->ctx;
+    for (uint32_t it = 0; it < iterations; ++it) {
+        if (b->exec) {
+            CK(ctx, cudaGraphLaunch(b->exec, ctx->stream));
+        } else {
+            etcu_status s = issue_batch_iteration(b, ctx->stream);
+            if (s != ETCU_OK) return s;
+        }
+    }
+    CKL(ctx);
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_batch_last_residual_sq(etcu_batch* b, double* out) {
+    if (!b || !out) return fail(b ? b->ctx : nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    etcu_context* ctx = b->ctx;
+    CK(ctx, cudaMemcpyAsync(out, b->d_resid, sizeof(double) * b->n, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    return ETCU_OK;
+}
+
+extern "C" uint32_t etcu_batch_launches_per_iteration(const etcu_batch* b) { return b ? b->launches : 0; }
+
 extern "C" etcu_status etcu_reconstruct(etcu_context* ctx, const etcu_volume_desc* desc, etcu_voxel_type type,
                                         const etcu_view* views, uint32_t n_views, const float* host_projections,
                                         const etcu_recon_params* params, uint32_t iterations,

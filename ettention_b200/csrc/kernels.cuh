@@ -385,9 +385,9 @@ __device__ __forceinline__ void fp_reduce_resid(const FpArgs& a, double r2) {
     }
 }
 
+// One detector pixel (gx, gy) of view slot p (order position first + p).
 template <typename VoxT, bool kMask, int kPath>
-__global__ void __launch_bounds__(128, (kPath == kFpPathXz || kPath == kFpPathXzNoCap) ? 7 : 4)
-    forward_project_kernel(const __grid_constant__ FpArgs a) {
+__device__ __forceinline__ void fp_pixel(const FpArgs& a, uint32_t first, int p) {
     constexpr bool kPerspective = kPath == kFpPathPerspective;
     int gx, gy;
     if (kPerspective) {
@@ -397,8 +397,7 @@ __global__ void __launch_bounds__(128, (kPath == kFpPathXz || kPath == kFpPathXz
         gx = blockIdx.x * blockDim.x + threadIdx.x;
         gy = blockIdx.y;
     }
-    const int p = blockIdx.z;
-    const uint32_t vid = a.order ? a.order[a.first + p] : (a.first + p);
+    const uint32_t vid = a.order ? a.order[first + p] : (first + p);
     const ViewConst& vc = a.views ? a.views[vid] : a.inline_view;
     const bool active = gx < a.W && gy < a.H;
     const VoxT* vol = (const VoxT*)a.vol;
@@ -457,6 +456,25 @@ __global__ void __launch_bounds__(128, (kPath == kFpPathXz || kPath == kFpPathXz
     double r2 = 0.0;
     if (active) r2 = fp_store(a, vc, vid, p, gx, gy, accv, accl, total);
     fp_reduce_resid(a, r2);
+}
+
+template <typename VoxT, bool kMask, int kPath>
+__global__ void __launch_bounds__(128, (kPath == kFpPathXz || kPath == kFpPathXzNoCap) ? 7 : 4)
+    forward_project_kernel(const __grid_constant__ FpArgs a) {
+    fp_pixel<VoxT, kMask, kPath>(a, a.first, blockIdx.z);
+}
+
+// Batched tilt series: series s = blockIdx.z reads its arguments from table[s]
+// and projects the view at order position `step` when it has one (steps[s] views);
+// the grid covers the largest detector of the batch.
+template <typename VoxT, bool kMask, int kPath>
+__global__ void __launch_bounds__(128, (kPath == kFpPathXz || kPath == kFpPathXzNoCap) ? 7 : 4)
+    forward_project_batch_kernel(const FpArgs* __restrict__ table, const int* __restrict__ steps, int step) {
+    const int s = blockIdx.z;
+    if (step >= steps[s]) return;
+    const FpArgs& a = table[s];
+    if ((int)(blockIdx.x * blockDim.x) >= a.W || (int)blockIdx.y >= a.H) return;
+    fp_pixel<VoxT, kMask, kPath>(a, (uint32_t)step, 0);
 }
 
 // ---------------------------------------------------------------- back projection
@@ -857,15 +875,9 @@ __device__ __forceinline__ float sart_update(float v, float2 rl, float lam, floa
 // an (x, y) column over a z range, computes the view's row taps once and updates
 // two voxels per iteration.  Same operations as bp_parallel_kernel.
 template <bool kMask, int kStore, int kSampling>
-__global__ void __launch_bounds__(256, 8) bp_sart_row_kernel(const __grid_constant__ BpArgs a) {
+__device__ __forceinline__ void bp_sart_row_column(const BpArgs& a, uint32_t first, int x, int y, int zb, int ze) {
     const SlabConst& g = a.slab;
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    if (x >= g.rx || y >= g.ry) return;
-    const int zper = (g.rz + gridDim.z - 1) / gridDim.z;
-    const int zb = blockIdx.z * zper, ze = min(g.rz, zb + zper);
-    if (zb >= ze) return;
-    const uint32_t vid = a.order ? a.order[a.first] : a.first;
+    const uint32_t vid = a.order ? a.order[first] : first;
     const ViewConst& vc = a.views ? a.views[vid] : a.inline_view;
     const float4 s = a.samples ? a.samples[vid] : a.inline_samples[0];
     const float cx = fadd(g.bmin.x, fmul(fadd((float)x, 0.5f), g.vs.x));
@@ -897,6 +909,32 @@ __global__ void __launch_bounds__(256, 8) bp_sart_row_kernel(const __grid_consta
         if (two) bp_store<kStore>(a, idx + plane, vb);
         idx += 2 * plane;
     }
+}
+
+template <bool kMask, int kStore, int kSampling>
+__global__ void __launch_bounds__(256, 8) bp_sart_row_kernel(const __grid_constant__ BpArgs a) {
+    const SlabConst& g = a.slab;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= g.rx || y >= g.ry) return;
+    const int zper = (g.rz + gridDim.z - 1) / gridDim.z;
+    const int zb = blockIdx.z * zper, ze = min(g.rz, zb + zper);
+    if (zb >= ze) return;
+    bp_sart_row_column<kMask, kStore, kSampling>(a, a.first, x, y, zb, ze);
+}
+
+// Batched tilt series (FP32 volumes, no mask): series s = blockIdx.z back projects the
+// view at order position `step` when it has one; each thread owns a whole (x, y) column.
+template <int kSampling>
+__global__ void __launch_bounds__(256, 8)
+    bp_sart_row_batch_kernel(const BpArgs* __restrict__ table, const int* __restrict__ steps, int step) {
+    const int s = blockIdx.z;
+    if (step >= steps[s]) return;
+    const BpArgs& a = table[s];
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= a.slab.rx || y >= a.slab.ry) return;
+    bp_sart_row_column<false, 0, kSampling>(a, (uint32_t)step, x, y, 0, a.slab.rz);
 }
 
 // ---- column-pipelined single-view back projection (SART's hot case, FP32 volume) ----

@@ -529,3 +529,67 @@ class BlockIterativeReconstructionOperator:
         self.volume.ctx.check(lib().etcu_recon_profile_iteration(self.handle, ctypes.byref(f), ctypes.byref(b),
                                                                  ctypes.byref(nf), ctypes.byref(nb)))
         return float(f.value), float(b.value), int(nf.value), int(nb.value)
+
+
+class BatchReconstructionOperator:
+    """Many independent tilt series of uneven sizes reconstructed together with SART:
+    every step runs one forward-projection and one back-projection launch over all
+    series, each iteration one CUDA graph (etcu_batch_*).  No counterpart in the
+    reference, which reconstructs one series per run.
+
+    ``series`` is a list of (GPUMappedVolume, [ScannerGeometry], projections (N, H, W)
+    float32 array); the volumes share one Context."""
+
+    def __init__(self, series, params: AlgebraicParameterSet, use_graph: bool = True):
+        if not series:
+            raise EttentionError(_abi.ERR_INVALID_ARGUMENT, "no series")
+        self.volumes = [v for v, _, _ in series]
+        self.params = params
+        ctx = self.volumes[0].ctx
+        self._views = [(View * len(g))(*[x.to_view() for x in g]) for _, g, _ in series]
+        self._projs = [np.ascontiguousarray(p, np.float32) for _, _, p in series]
+        arr = (_abi.BatchSeries * len(series))()
+        for i, (vol, geoms, _) in enumerate(series):
+            arr[i].volume = vol.handle
+            arr[i].views = ctypes.cast(self._views[i], ctypes.POINTER(View))
+            arr[i].n_views = len(geoms)
+            arr[i].host_projections = self._projs[i].ctypes.data
+        rp = params.recon_params(use_graph)
+        self._skip = (ctypes.c_uint32 * max(1, len(params.skip)))(*[int(s) for s in params.skip])
+        if len(params.skip):
+            rp.skip = ctypes.cast(self._skip, ctypes.POINTER(ctypes.c_uint32))
+            rp.skip_count = len(params.skip)
+        h = ctypes.c_void_p()
+        ctx.check(lib().etcu_batch_create(ctx.handle, arr, len(series), ctypes.byref(rp), ctypes.byref(h)))
+        self.handle = h
+        self.ctx = ctx
+        ctx._adopt(self)
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib().etcu_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def runNiterations(self, n: int = 1) -> None:
+        self.ctx.check(lib().etcu_batch_run(self.handle, int(n)))
+
+    def run(self) -> None:
+        self.runNiterations(self.params.iterations)
+
+    def getReconstructedVolumes(self) -> List[np.ndarray]:
+        return [v.download() for v in self.volumes]
+
+    def last_residual_sq(self) -> List[float]:
+        out = np.zeros(len(self.volumes), np.float64)
+        self.ctx.check(lib().etcu_batch_last_residual_sq(self.handle, out.ctypes.data))
+        return [float(x) for x in out]
+
+    @property
+    def launches_per_iteration(self) -> int:
+        return int(lib().etcu_batch_launches_per_iteration(self.handle))

@@ -234,6 +234,35 @@ ETCU_API etcu_status etcu_reconstruct(etcu_context* ctx, const etcu_volume_desc*
                              const etcu_view* views, uint32_t n_views, const float* host_projections,
                              const etcu_recon_params* params, uint32_t iterations, float* host_volume_inout);
 
+/* ---------------------------------------------------------------- batched series */
+/* Many independent tilt series of uneven sizes reconstructed together: every SART
+ * step runs one forward-projection launch and one back-projection launch over all
+ * series (series without a view at that step sit it out), and each iteration is one
+ * CUDA graph.  Per series the result is the block-iterative reconstruction of
+ * etcu_recon_* with block size 1 (BlockIterativeReconstructionOperator.cpp:92-142).
+ * No counterpart in the reference, which reconstructs one series per run.
+ * Supported: SART (block_size 1), one back-projection sample, parallel views whose
+ * detector row depends on y only (single-axis tilt about y), FP32 volumes with one
+ * sub-volume and no mask, ETCU_SAMPLING_Q8 or _EXACT; anything else returns
+ * ETCU_ERR_UNSUPPORTED.  All volumes belong to ctx. */
+typedef struct {
+    etcu_volume* volume;
+    const etcu_view* views;
+    uint32_t n_views;
+    const float* host_projections; /* n_views x height x width floats */
+} etcu_batch_series;
+typedef struct etcu_batch etcu_batch;
+
+ETCU_API etcu_status etcu_batch_create(etcu_context* ctx, const etcu_batch_series* series, uint32_t n_series,
+                                       const etcu_recon_params* params, etcu_batch** out);
+ETCU_API etcu_status etcu_batch_destroy(etcu_batch* batch);
+ETCU_API etcu_status etcu_batch_run(etcu_batch* batch, uint32_t iterations);
+/* Per series (n_series doubles): sum over the last iteration's views of ||b - Ax||^2
+ * as each view saw it before its update (FP64). */
+ETCU_API etcu_status etcu_batch_last_residual_sq(etcu_batch* batch, double* out);
+/* Kernel launches one iteration issues. */
+ETCU_API uint32_t etcu_batch_launches_per_iteration(const etcu_batch* batch);
+
 /* One SART update of one view (forward projection, residual b - Ax, back projection
  * with block size 1) that allocates no device memory, for callers that cannot
  * allocate: hosts whose device memory is reserved up front by their own pool
