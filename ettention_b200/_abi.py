@@ -48,6 +48,15 @@ class ReconParams(ctypes.Structure):
                 ("skip_count", ctypes.c_uint32), ("use_graph", ctypes.c_int32)]
 
 
+class MrcInfo(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_uint32), ("ny", ctypes.c_uint32), ("nz", ctypes.c_uint32), ("mode", ctypes.c_int32),
+                ("dmin", ctypes.c_float), ("dmax", ctypes.c_float), ("dmean", ctypes.c_float),
+                ("extended_bytes", ctypes.c_uint32)]
+
+
+AXES_XYZ, AXES_XZY = 0, 1
+
+
 class BatchSeries(ctypes.Structure):
     _fields_ = [("volume", ctypes.c_void_p), ("views", ctypes.POINTER(View)), ("n_views", ctypes.c_uint32),
                 ("host_projections", ctypes.c_void_p)]
@@ -100,6 +109,10 @@ _SIG = {
     "etcu_reconstruct": (_S, [_P, ctypes.POINTER(VolumeDesc), _I, ctypes.POINTER(View), _U, _P,
                               ctypes.POINTER(ReconParams), _U, _P]),
     "etcu_projection_order": (_S, [_I, _U, _P, _U, _P, ctypes.POINTER(_U)]),
+    "etcu_mrc_read_info": (_S, [ctypes.c_char_p, ctypes.POINTER(MrcInfo)]),
+    "etcu_mrc_read_stack": (_S, [ctypes.c_char_p, _I, _P, ctypes.c_size_t]),
+    "etcu_read_tilt_angles": (_S, [ctypes.c_char_p, _P, _U, ctypes.POINTER(_U)]),
+    "etcu_mrc_write_volume": (_S, [ctypes.c_char_p, _P, _P, _I]),
     "etcu_batch_create": (_S, [_P, ctypes.POINTER(BatchSeries), _U, ctypes.POINTER(ReconParams), ctypes.POINTER(_P)]),
     "etcu_batch_destroy": (_S, [_P]),
     "etcu_batch_run": (_S, [_P, _U]),

@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libettention_b200.so")
-SOURCES = ["etcu_api.cu"]
+SOURCES = ["etcu_api.cu", "etcu_io.cpp"]
 HEADERS = ["geometry.hpp", "kernels.cuh"]
 
 # -fmad=false: no multiply-add is formed implicitly.  The kernels follow the

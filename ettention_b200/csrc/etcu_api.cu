@@ -632,6 +632,8 @@ extern "C" etcu_status etcu_context_destroy(etcu_context* ctx) {
     return ETCU_OK;
 }
 
+void etcu_set_context_free_error(const char* message) { g_create_error = message ? message : ""; }
+
 extern "C" const char* etcu_last_error(const etcu_context* ctx) {
     return ctx ? ctx->err.c_str() : g_create_error.c_str();
 }

@@ -106,6 +106,69 @@ def projection_order(order: int, n: int, skip: Sequence[int] = ()) -> List[int]:
     return [int(i) for i in out[: cnt.value]]
 
 
+class MRCStack:
+    """LR/io/datasource/MRCStack.cpp: a tilt series in an MRC file (modes 0/1/2/6) with an
+    optional tilt-angle file; projections as float32 (log-transformed when
+    ``logarithmize``, the reference's input.logarithmize), the MRC base geometry and
+    SingleAxisTiltRotator views."""
+
+    def __init__(self, path: str, tilt_path: Optional[str] = None, logarithmize: bool = False):
+        self.path = str(path)
+        info = _abi.MrcInfo()
+        _check_free(lib().etcu_mrc_read_info(self.path.encode(), ctypes.byref(info)))
+        self.info = info
+        self.logarithmize = bool(logarithmize)
+        if tilt_path is None:
+            self.tilt_angles = [0.0] * info.nz  # MRCStack::setEmptyTiltAngles
+        else:
+            self.tilt_angles = read_tilt_angles(tilt_path)
+            if len(self.tilt_angles) != info.nz:  # ImageStackDatasource.cpp:75-78
+                raise EttentionError(_abi.ERR_INVALID_ARGUMENT,
+                                     f"Number of projections DIFFERS from number of Tilt Angles given in {tilt_path}")
+
+    def getNumberOfProjections(self) -> int:
+        return int(self.info.nz)
+
+    def getResolution(self):
+        return int(self.info.nx), int(self.info.ny)
+
+    def load_projections(self) -> np.ndarray:
+        """All projections, (nz, ny, nx) float32."""
+        out = np.empty((self.info.nz, self.info.ny, self.info.nx), np.float32)
+        _check_free(lib().etcu_mrc_read_stack(self.path.encode(), int(self.logarithmize), out.ctypes.data, out.size))
+        return out
+
+    def createScannerGeometry(self, index: int, xaxis_tilt_deg: float = 0.0) -> "ScannerGeometry":
+        return mrc_base_geometry(*self.getResolution()).rotated(float(self.tilt_angles[index]), xaxis_tilt_deg)
+
+    def geometries(self, xaxis_tilt_deg: float = 0.0) -> List["ScannerGeometry"]:
+        return [self.createScannerGeometry(i, xaxis_tilt_deg) for i in range(self.getNumberOfProjections())]
+
+
+def _check_free(status: int) -> None:
+    if status != _abi.OK:
+        msg = lib().etcu_last_error(None)
+        raise EttentionError(status, (msg or b"").decode() or f"etcu status {status}")
+
+
+def read_tilt_angles(path: str) -> List[float]:
+    """ImageStackDatasource::readTiltAngles: every whitespace-separated float of the file."""
+    n = ctypes.c_uint32()
+    _check_free(lib().etcu_read_tilt_angles(str(path).encode(), None, 0, ctypes.byref(n)))
+    out = np.zeros(max(1, n.value), np.float32)
+    _check_free(lib().etcu_read_tilt_angles(str(path).encode(), out.ctypes.data, n.value, ctypes.byref(n)))
+    return [float(a) for a in out[: n.value]]
+
+
+def write_mrc_volume(path: str, volume: np.ndarray, orientation: str = "xzy") -> None:
+    """VolumeFileFormatWriter + MRCWriter, float32: ``volume`` is (z, y, x); orientation
+    'xzy' (the reference's default output.options.orientation) or 'xyz'."""
+    v = np.ascontiguousarray(volume, np.float32)
+    res = np.array([v.shape[2], v.shape[1], v.shape[0]], np.uint32)
+    axes = {"xyz": _abi.AXES_XYZ, "xzy": _abi.AXES_XZY}[orientation.lower()]
+    _check_free(lib().etcu_mrc_write_volume(str(path).encode(), v.ctypes.data, res.ctypes.data, axes))
+
+
 ORDERS = {"identity": _abi.ORDER_IDENTITY, "random": _abi.ORDER_RANDOM, "maxangle": _abi.ORDER_MAXANGLE,
           "buckets": _abi.ORDER_BUCKETS}
 VOXEL_TYPES = {"float": _abi.VOXEL_FLOAT32, "float32": _abi.VOXEL_FLOAT32, "half": _abi.VOXEL_HALF16,

@@ -234,6 +234,34 @@ ETCU_API etcu_status etcu_reconstruct(etcu_context* ctx, const etcu_volume_desc*
                              const etcu_view* views, uint32_t n_views, const float* host_projections,
                              const etcu_recon_params* params, uint32_t iterations, float* host_volume_inout);
 
+/* ---------------------------------------------------------------- files */
+/* Host-side formats of the reference's front door; context-free (errors via
+ * etcu_last_error(NULL)).  MRC stacks: LR/io/datasource/MRCStack.cpp:136-250 (modes
+ * 0 = uint8, 1 = int16, 2 = float32, 6 = uint16; the extended header is skipped). */
+typedef struct {
+    uint32_t nx, ny, nz;     /* columns, rows, sections (projections of a stack) */
+    int32_t mode;
+    float dmin, dmax, dmean; /* as stored in the header */
+    uint32_t extended_bytes;
+} etcu_mrc_info;
+ETCU_API etcu_status etcu_mrc_read_info(const char* path, etcu_mrc_info* out);
+/* Every section as float32 (nx * ny * nz values, x fastest).  logarithmize != 0 applies
+ * MRCStack's transform log(M / (raw - m)) over the stack's data range: M = max - min + 1,
+ * m = min - 1 for modes 1 and 2; M = max + 1, m = -1 for modes 0 and 6
+ * (MRCStack.cpp:161-172, 226-236; input.logarithmize). */
+ETCU_API etcu_status etcu_mrc_read_stack(const char* path, int logarithmize, float* out, size_t capacity);
+/* Tilt-angle file (ImageStackDatasource.cpp:49-79): every whitespace-separated float;
+ * *count = the number in the file, at most capacity of them stored in out. */
+ETCU_API etcu_status etcu_read_tilt_angles(const char* path, float* out, uint32_t capacity, uint32_t* count);
+/* Coordinate order of a written volume (output.options.orientation,
+ * LR/setup/parameterset/IOEnumerations.cpp:79-126): XZY (the reference's default)
+ * stores y as the file's sections and z as its rows. */
+typedef enum { ETCU_AXES_XYZ = 0, ETCU_AXES_XZY = 1 } etcu_orientation;
+/* VolumeFileFormatWriter / MRCWriter with output.options.voxelType float32: mode-2 MRC
+ * with min / max / mean in the header; volume is x fastest, then y, then z. */
+ETCU_API etcu_status etcu_mrc_write_volume(const char* path, const float* volume, const uint32_t resolution[3],
+                                           etcu_orientation orientation);
+
 /* ---------------------------------------------------------------- batched series */
 /* Many independent tilt series of uneven sizes reconstructed together: every SART
  * step runs one forward-projection launch and one back-projection launch over all
