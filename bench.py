@@ -56,8 +56,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-reps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c4"],
-                    help="c2: the headline SART workload (default); c4: 64 batched series of uneven sizes")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4"],
+                    help="c2: the headline SART workload (default); c3: 2048^2 x 512 perspective, block 8, "
+                         "bf16 shadow; c4: 64 batched series of uneven sizes")
     ap.add_argument("--ncu-case", action="store_true",
                     help="small profiling case for ncu: 512x512x256 volume, 8 views, one SART iteration "
                          "launched kernel by kernel (8 forward + 8 back projections), then per-kernel times")
@@ -196,10 +197,12 @@ def make_phantom_torch(seed: int, device, res=None, count: int = 200, axes=(8.0,
         yy = torch.arange(y0, y1, device=device, dtype=torch.float32) + 0.5 - float(c[1])
         xx = torch.arange(x0, x1, device=device, dtype=torch.float32) + 0.5 - float(c[0])
         Rt = torch.tensor(R, dtype=torch.float32, device=device)
-        p = (xx[None, None, :, None] * Rt[0] + yy[None, :, None, None] * Rt[1] + zz[:, None, None, None] * Rt[2])
         at = torch.tensor(a, dtype=torch.float32, device=device)
-        inside = ((p / at) ** 2).sum(-1) <= 1.0
-        vol[z0:z1, y0:y1, x0:x1] += float(d * MU_SCALE) * inside.float()
+        for zc in range(0, z1 - z0, 64):  # z chunks bound the temporary (chunk, y, x, 3) tensor
+            zs = zz[zc:zc + 64]
+            p = (xx[None, None, :, None] * Rt[0] + yy[None, :, None, None] * Rt[1] + zs[:, None, None, None] * Rt[2])
+            inside = ((p / at) ** 2).sum(-1) <= 1.0
+            vol[z0 + zc:z0 + zc + zs.numel(), y0:y1, x0:x1] += float(d * MU_SCALE) * inside.float()
     return vol
 
 
@@ -565,6 +568,96 @@ def run_c4(args):
     ctx.close()
 
 
+# ------------------------------------------------------------------ C3: perspective, BF16 shadow, block 8
+C3_RES = (2048, 2048, 512)
+C3_VIEWS = 121
+
+
+def c3_geometry(tilt: float):
+    """Perspective view of a 2048^2 detector: source 10 x volume width above the volume
+    centre, detector plane one unit from the source with a pitch that spans the volume
+    at its centre (the reference's perspective convention, ProjectionTestBase.cpp:137-145),
+    rotated by -tilt about y."""
+    from ettention_b200.operators import ScannerGeometry
+    D = 10.0 * C3_RES[0]
+    pitch = 1.0 / D
+    W, H = C3_RES[0], C3_RES[1]
+    base = ScannerGeometry([0.0, 0.0, D], [-0.5 * W * pitch, -0.5 * H * pitch, D - 1.0], [pitch, 0.0, 0.0],
+                           [0.0, pitch, 0.0], W, H, True)
+    return base.rotated(tilt)
+
+
+def run_c3(args):
+    """C3: 2048^2 x 512 volume, 121 perspective views (-60..60 step 1), block size 8,
+    FP32 master + BF16 shadow, random order, Poisson I0 = 200; one block-iterative
+    iteration per step."""
+    import torch
+    from ettention_b200 import _abi
+    from ettention_b200.operators import (AlgebraicParameterSet, BlockIterativeReconstructionOperator, Context,
+                                          ForwardProjectionOperator, GPUMappedVolume)
+    ctx = Context(0)
+    dev = torch.device("cuda", 0)
+    X, Y, Z = C3_RES
+    phantom = make_phantom_torch(3000, dev, C3_RES, count=500, axes=(8.0, 256.0))
+    geoms = [c3_geometry(float(a)) for a in np.linspace(-60.0, 60.0, C3_VIEWS)]
+    vol = GPUMappedVolume(ctx, C3_RES)
+    vol.upload(phantom.cpu().numpy())
+    del phantom
+    fp = ForwardProjectionOperator(vol, 1)
+    projs = torch.zeros((C3_VIEWS, Y, X), dtype=torch.float32, device=dev)
+    scratch = torch.zeros((Y, X), dtype=torch.float32, device=dev)
+    for i, g in enumerate(geoms):
+        fp.setScannerGeometry(g)
+        fp.SetOutput(projs[i], scratch)
+        fp.Execute(0)
+    vol.close()
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(3000)
+    counts = torch.poisson(200.0 * torch.exp(-projs), generator=gen)
+    b = (-torch.log(torch.clamp(counts, min=1.0) / 200.0)).contiguous()
+    del counts, projs, scratch
+    torch.cuda.synchronize()
+    p = AlgebraicParameterSet(algorithm="blockIterative", block_size=8, iterations=1, lam=0.2,
+                              order=_abi.ORDER_RANDOM)
+    vol = GPUMappedVolume(ctx, C3_RES, voxel_type=_abi.VOXEL_BF16_MASTER)
+    rec = BlockIterativeReconstructionOperator(vol, geoms, b, p)
+    stream = torch.cuda.ExternalStream(ctx.stream_handle)
+    for _ in range(args.warmup):
+        rec.runNiterations(1)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ctx.synchronize()
+    ev0.record(stream)
+    rec.runNiterations(args.steps)
+    ev1.record(stream)
+    ev1.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    fp_ms, bp_ms, nf, nb = rec.profile_iteration()
+    rec.close()
+    vol.close()
+    ctx.close()
+    V, P, N, B = X * Y * Z, X * Y, C3_VIEWS, 8
+    nblocks = (N + B - 1) // B
+    # byte model: FP reads the BF16 shadow, b, writes (r, L); BP read-modify-writes the
+    # FP32 master once per block and rewrites the shadow; it reads (r, L) per view
+    byts = N * (V * 2 + P * 4 + P * 8) + nblocks * (2 * V * 4 + V * 2) + N * P * 8
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    print(json.dumps({
+        "metric": "C3 block-iterative s per iteration", "value": ms / 1e3, "unit": "s", "higher_is_better": False,
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "dtype": "f32 math, bf16 shadow, f32 master",
+        "data": "synthetic (seeded 500-ellipsoid phantom, CUDA-forward-projected, Poisson I0=200)",
+        "config": {"workload": "C3: 2048x2048x512, 121 perspective views -60..60 step 1, 2048^2 detector, "
+                               "block 8, lambda 0.2, random order", "voxel_type": "bf16_master"},
+        "per_kernel_ms": {"forward_project_total": fp_ms, "back_project_total": bp_ms,
+                          "forward_launches": nf, "back_launches": nb},
+        "roofline": {"bound": "hbm", "bytes_per_iteration": byts, "achieved": byts / (ms * 1e-3) / 1e9,
+                     "peak": hbm, "unit": "GB/s", "frac": byts / (ms * 1e-3) / 1e9 / hbm}}))
+
+
 def main():
     args = parse()
     if args.ncu_case:
@@ -572,6 +665,9 @@ def main():
         return
     if args.workload == "c4":
         run_c4(args)
+        return
+    if args.workload == "c3":
+        run_c3(args)
         return
     rank, world, local = dist_init()
     try:
