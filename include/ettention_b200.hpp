@@ -16,6 +16,8 @@
  *                                          OptimizationParameterSet, VolumeParameterSet, HardwareParameterSet
  *   BlockIterativeReconstructionOperator   LR/algorithm/reconstruction/blockiterative/
  *                                          BlockIterativeReconstructionOperator.cpp:56-185
+ *   MRCStack, writeMrcVolume               LR/io/datasource/MRCStack.cpp, LR/io/serializer/MRCWriter.cpp
+ *   BatchReconstructionOperator            many series per launch (no counterpart in the reference)
  * Errors: every non-OK status of the ABI is rethrown as ettention::b200::Exception
  * (validation) or GPUException (device errors), with the library's message, as
  * the reference throws ettention::Exception / GPUException.
@@ -398,6 +400,99 @@ private:
     GPUMappedVolume* vol_;
     AlgebraicParameterSet params_;
     etcu_recon* rec_ = nullptr;
+};
+
+// LR/io/datasource/MRCStack.cpp: a tilt series in an MRC file (modes 0/1/2/6) with an
+// optional tilt-angle file (ImageStackDatasource::readTiltAngles); projections as
+// float32, log-transformed when logarithmize (input.logarithmize).
+class MRCStack {
+public:
+    explicit MRCStack(const std::string& path, const std::string& tilt_path = std::string(), bool logarithmize = false)
+        : path_(path), log_(logarithmize) {
+        check(etcu_mrc_read_info(path.c_str(), &info_), nullptr);
+        if (tilt_path.empty()) {
+            angles_.assign(info_.nz, 0.f);  // MRCStack::setEmptyTiltAngles
+        } else {
+            uint32_t n = 0;
+            check(etcu_read_tilt_angles(tilt_path.c_str(), nullptr, 0, &n), nullptr);
+            angles_.resize(n);
+            check(etcu_read_tilt_angles(tilt_path.c_str(), angles_.data(), n, &n), nullptr);
+            if (n != info_.nz)
+                throw Exception(ETCU_ERR_INVALID_ARGUMENT,
+                                "Number of projections DIFFERS from number of Tilt Angles given in " + tilt_path);
+        }
+    }
+    uint32_t getNumberOfProjections() const { return info_.nz; }
+    std::array<uint32_t, 2> getResolution() const { return {{info_.nx, info_.ny}}; }
+    const etcu_mrc_info& info() const { return info_; }
+    const std::vector<float>& tiltAngles() const { return angles_; }
+    // All projections, nz x ny x nx floats.
+    std::vector<float> loadProjections() const {
+        std::vector<float> out((size_t)info_.nx * info_.ny * info_.nz);
+        check(etcu_mrc_read_stack(path_.c_str(), log_ ? 1 : 0, out.data(), out.size()), nullptr);
+        return out;
+    }
+    ScannerGeometry createScannerGeometry(uint32_t index, float xaxis_tilt_deg = 0.f) const {
+        return ScannerGeometry::mrcBase(info_.nx, info_.ny).rotated(angles_.at(index), xaxis_tilt_deg);
+    }
+
+private:
+    std::string path_;
+    bool log_;
+    etcu_mrc_info info_{};
+    std::vector<float> angles_;
+};
+
+// VolumeFileFormatWriter + MRCWriter, float32 (x fastest, then y, then z); XZY is the
+// reference's default output.options.orientation.
+inline void writeMrcVolume(const std::string& path, const float* volume, const std::array<uint32_t, 3>& resolution,
+                           etcu_orientation orientation = ETCU_AXES_XZY) {
+    check(etcu_mrc_write_volume(path.c_str(), volume, resolution.data(), orientation), nullptr);
+}
+
+// Many independent tilt series reconstructed together with SART (etcu_batch_*): one
+// forward and one back-projection launch per step over all series.
+class BatchReconstructionOperator {
+public:
+    struct Series {
+        GPUMappedVolume* volume;
+        std::vector<ScannerGeometry> views;
+        const float* host_projections;  // views.size() x height x width floats
+    };
+    BatchReconstructionOperator(Framework& fw, const std::vector<Series>& series, const AlgebraicParameterSet& p,
+                                bool use_graph = true)
+        : fw_(&fw) {
+        std::vector<std::vector<etcu_view>> views(series.size());
+        std::vector<etcu_batch_series> arr(series.size());
+        for (size_t i = 0; i < series.size(); ++i) {
+            for (const auto& g : series[i].views) views[i].push_back(g.view());
+            arr[i].volume = series[i].volume->handle();
+            arr[i].views = views[i].data();
+            arr[i].n_views = (uint32_t)views[i].size();
+            arr[i].host_projections = series[i].host_projections;
+        }
+        const etcu_recon_params rp = p.reconParams(use_graph);
+        check(etcu_batch_create(fw.handle(), arr.data(), (uint32_t)arr.size(), &rp, &batch_), fw.handle());
+        n_ = series.size();
+    }
+    ~BatchReconstructionOperator() { etcu_batch_destroy(batch_); }
+    BatchReconstructionOperator(const BatchReconstructionOperator&) = delete;
+    BatchReconstructionOperator& operator=(const BatchReconstructionOperator&) = delete;
+    void runNiterations(uint32_t n) {
+        check(etcu_batch_run(batch_, n), fw_->handle());
+        fw_->synchronize();
+    }
+    std::vector<double> lastResidualSq() const {
+        std::vector<double> r(n_);
+        check(etcu_batch_last_residual_sq(batch_, r.data()), fw_->handle());
+        return r;
+    }
+    uint32_t launchesPerIteration() const { return etcu_batch_launches_per_iteration(batch_); }
+
+private:
+    Framework* fw_;
+    etcu_batch* batch_ = nullptr;
+    size_t n_ = 0;
 };
 
 }  // namespace b200

@@ -18,7 +18,7 @@ static void config_case(const char* name, const std::map<std::string, std::strin
     }
 }
 
-int main() {
+int main(int argc, char** argv) {
     const ScannerGeometry g = ScannerGeometry::mrcBase(96, 80).rotated(30.f);
     const auto m = g.getProjectionMatrix();
     std::printf("matrix");
@@ -36,6 +36,24 @@ int main() {
                                {"algorithm.numberOfIterations", "1"}, {"algorithm.lambda", "0.2"}});
     config_case("bad_order", {{"algorithm", "sart"}, {"optimization.projectionIteration", "zigzag"}});
     config_case("missing", {{"algorithm.lambda", "0.2"}});
+    {  // files: a 4 x 3 x 2 volume written in XZY order reads back as sections y, rows z
+        std::vector<float> vol(24);
+        for (int i = 0; i < 24; ++i) vol[i] = (float)i;
+        const char* path = argc > 1 ? argv[1] : "shim_cpu_volume.mrc";
+        writeMrcVolume(path, vol.data(), {{4, 3, 2}});
+        MRCStack st(path);
+        const std::vector<float> back = st.loadProjections();
+        bool ok = st.getNumberOfProjections() == 3 && st.getResolution()[0] == 4 && st.getResolution()[1] == 2;
+        for (int y = 0; y < 3; ++y)
+            for (int z = 0; z < 2; ++z)
+                for (int x = 0; x < 4; ++x) ok &= back[(y * 2 + z) * 4 + x] == vol[(z * 3 + y) * 4 + x];
+        std::printf("mrc %s %g %g\n", ok ? "ok" : "mismatch", st.info().dmin, st.info().dmax);
+        try {
+            MRCStack missing(std::string(path) + ".absent");
+        } catch (const Exception& e) {
+            std::printf("mrc_missing error %d\n", (int)e.status());
+        }
+    }
     try {
         Framework fw(0);
         std::printf("framework ok\n");

@@ -30,7 +30,8 @@ def build_and_run(tmp_path, src, extra=()):
 def test_cpp_shim_host_side(tmp_path):
     from ettention_b200.operators import mrc_base_geometry
     exe = build_and_run(tmp_path, "shim_cpu.cpp")
-    out = subprocess.run([exe], capture_output=True, text=True, timeout=120, check=True).stdout
+    out = subprocess.run([exe, str(tmp_path / "v.mrc")], capture_output=True, text=True, timeout=120,
+                         check=True).stdout
     lines = {l.split()[0] + (" " + l.split()[1] if l.startswith("config") else ""): l.split()
              for l in out.splitlines()}
     g = mrc_base_geometry(96, 80).rotated(30.0)
@@ -44,6 +45,8 @@ def test_cpp_shim_host_side(tmp_path):
     assert " ".join(lines["config zero_block"][2:]) == "error 1 Illegal ProjectionBlockSize!"
     assert " ".join(lines["config bad_order"][2:]) == "error 1 Illegal ProjectionSetType!"
     assert lines["config missing"][2:4] == ["error", "1"]
+    assert lines["mrc"][1:] == ["ok", "0", "23"]
+    assert lines["mrc_missing"][1:] == ["error", "1"]
     import torch
     if torch.cuda.is_available():
         assert lines["framework"][1] == "ok"
