@@ -57,6 +57,17 @@ class MrcInfo(ctypes.Structure):
 AXES_XYZ, AXES_XZY = 0, 1
 
 
+class ImageInfo(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("pages", ctypes.c_uint32),
+                ("bits_per_sample", ctypes.c_uint32), ("sample_format", ctypes.c_uint32),
+                ("compression", ctypes.c_uint32)]
+
+
+class ImageStackInfo(ctypes.Structure):
+    _fields_ = [("count", ctypes.c_uint32), ("width", ctypes.c_uint32), ("height", ctypes.c_uint32),
+                ("base", View)]
+
+
 class BatchSeries(ctypes.Structure):
     _fields_ = [("volume", ctypes.c_void_p), ("views", ctypes.POINTER(View)), ("n_views", ctypes.c_uint32),
                 ("host_projections", ctypes.c_void_p)]
@@ -113,6 +124,17 @@ _SIG = {
     "etcu_mrc_read_stack": (_S, [ctypes.c_char_p, _I, _P, ctypes.c_size_t]),
     "etcu_read_tilt_angles": (_S, [ctypes.c_char_p, _P, _U, ctypes.POINTER(_U)]),
     "etcu_mrc_write_volume": (_S, [ctypes.c_char_p, _P, _P, _I]),
+    "etcu_tiff_read_info": (_S, [ctypes.c_char_p, _U, ctypes.POINTER(ImageInfo)]),
+    "etcu_tiff_read": (_S, [ctypes.c_char_p, _U, _P, ctypes.c_size_t]),
+    "etcu_tiff_write": (_S, [ctypes.c_char_p, _P, _U, _U]),
+    "etcu_image_stack_open": (_S, [ctypes.c_char_p, ctypes.POINTER(_P)]),
+    "etcu_image_stack_destroy": (None, [_P]),
+    "etcu_image_stack_info_get": (_S, [_P, ctypes.POINTER(ImageStackInfo)]),
+    "etcu_image_stack_tilt_angles": (_S, [_P, _P, _U]),
+    "etcu_image_stack_load": (_S, [_P, _U, _U, _P, ctypes.c_size_t]),
+    "etcu_image_stack_write_metadata": (_S, [ctypes.c_char_p, _P, ctypes.POINTER(ctypes.c_char_p), _U,
+                                             ctypes.POINTER(View), _P]),
+    "etcu_xml_config_read": (_S, [ctypes.c_char_p, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
     "etcu_batch_create": (_S, [_P, ctypes.POINTER(BatchSeries), _U, ctypes.POINTER(ReconParams), ctypes.POINTER(_P)]),
     "etcu_batch_destroy": (_S, [_P]),
     "etcu_batch_run": (_S, [_P, _U]),

@@ -16,8 +16,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libettention_b200.so")
-SOURCES = ["etcu_api.cu", "etcu_io.cpp"]
-HEADERS = ["geometry.hpp", "kernels.cuh"]
+SOURCES = ["etcu_api.cu", "etcu_io.cpp", "etcu_tiff.cpp", "etcu_stack.cpp"]
+HEADERS = ["geometry.hpp", "kernels.cuh", "io_util.hpp"]
 
 # -fmad=false: no multiply-add is formed implicitly.  The kernels follow the
 # reference's operation order step by step and write every intended fused
@@ -27,7 +27,7 @@ NVCC_FLAGS = [
     "-O3", "-std=c++17", "-lineinfo", "-fmad=false",
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
-    "-shared", "--expt-relaxed-constexpr", "-cudart", "static",
+    "-shared", "--expt-relaxed-constexpr", "-cudart", "static", "-lz",
 ]
 
 

@@ -20,6 +20,7 @@ memory.
 from __future__ import annotations
 
 import ctypes
+import os
 import weakref
 from dataclasses import dataclass, field
 from typing import Dict, Iterable, List, Optional, Sequence
@@ -167,6 +168,269 @@ def write_mrc_volume(path: str, volume: np.ndarray, orientation: str = "xzy") ->
     res = np.array([v.shape[2], v.shape[1], v.shape[0]], np.uint32)
     axes = {"xyz": _abi.AXES_XYZ, "xzy": _abi.AXES_XZY}[orientation.lower()]
     _check_free(lib().etcu_mrc_write_volume(str(path).encode(), v.ctypes.data, res.ctypes.data, axes))
+
+
+def read_tiff(path: str, page: int = 0) -> np.ndarray:
+    """ImageDeserializer::readImage / readImageFromStack (LR/io/deserializer/
+    ImageDeserializer.cpp:10-62): one page as (height, width) float32, row 0 the file's
+    first row; 8-bit grey / 255, 16-bit grey / 65535, 32-bit float as is."""
+    info = _abi.ImageInfo()
+    _check_free(lib().etcu_tiff_read_info(str(path).encode(), int(page), ctypes.byref(info)))
+    out = np.empty((info.height, info.width), np.float32)
+    _check_free(lib().etcu_tiff_read(str(path).encode(), int(page), out.ctypes.data, out.size))
+    return out
+
+
+def tiff_page_count(path: str) -> int:
+    """ImageDeserializer::getNumberOfImagesInStack."""
+    info = _abi.ImageInfo()
+    _check_free(lib().etcu_tiff_read_info(str(path).encode(), 0, ctypes.byref(info)))
+    return int(info.pages)
+
+
+def write_tiff(path: str, image: np.ndarray) -> None:
+    """ImageSerializer::writeImage(..., TIFF_GRAY_32): (height, width) as 32-bit float grey."""
+    a = np.ascontiguousarray(image, np.float32)
+    if a.ndim != 2:
+        raise EttentionError(_abi.ERR_INVALID_ARGUMENT, "an image is a 2-D array")
+    _check_free(lib().etcu_tiff_write(str(path).encode(), a.ctypes.data, a.shape[1], a.shape[0]))
+
+
+class ImageStackDirectoryDatasource:
+    """LR/io/datasource/ImageStackDirectoryDatasource.cpp: a directory of projection
+    images described by metadata.xml (base parallel geometry, one tilt angle per
+    image, optional <logscale/>, multi-page <projectionstack> entries); the detector
+    size is the first image's; views are SingleAxisTiltRotator rotations of the base
+    geometry."""
+
+    METADATA = "metadata.xml"
+
+    def __init__(self, directory: str):
+        self.directory = str(directory)
+        h = ctypes.c_void_p()
+        _check_free(lib().etcu_image_stack_open(self.directory.encode(), ctypes.byref(h)))
+        self.handle = h
+        info = _abi.ImageStackInfo()
+        _check_free(lib().etcu_image_stack_info_get(h, ctypes.byref(info)))
+        self.count, self.width, self.height = int(info.count), int(info.width), int(info.height)
+        self.base_geometry = ScannerGeometry.from_view(info.base)
+        a = np.zeros(max(1, self.count), np.float32)
+        _check_free(lib().etcu_image_stack_tilt_angles(h, a.ctypes.data, self.count))
+        self.tilt_angles = [float(x) for x in a[: self.count]]
+
+    @staticmethod
+    def canHandleResource(path: str) -> bool:
+        """:74-87: a directory that holds metadata.xml."""
+        return os.path.isdir(path) and os.path.exists(os.path.join(path, ImageStackDirectoryDatasource.METADATA))
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib().etcu_image_stack_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def getNumberOfProjections(self) -> int:
+        return self.count
+
+    def getResolution(self):
+        return self.width, self.height
+
+    def getTiltAngle(self, index: int) -> float:
+        return self.tilt_angles[index]
+
+    def load_projections(self, first: int = 0, count: Optional[int] = None) -> np.ndarray:
+        """Projections first .. first + count - 1 as (count, height, width) float32."""
+        n = self.count - int(first) if count is None else int(count)
+        out = np.empty((n, self.height, self.width), np.float32)
+        _check_free(lib().etcu_image_stack_load(self.handle, int(first), n, out.ctypes.data, out.size))
+        return out
+
+    def getProjectionImage(self, index: int) -> np.ndarray:
+        return self.load_projections(index, 1)[0]
+
+    def createScannerGeometry(self, index: int, xaxis_tilt_deg: float = 0.0) -> ScannerGeometry:
+        return self.base_geometry.rotated(self.tilt_angles[index], xaxis_tilt_deg)
+
+    def geometries(self, xaxis_tilt_deg: float = 0.0) -> List[ScannerGeometry]:
+        return [self.createScannerGeometry(i, xaxis_tilt_deg) for i in range(self.count)]
+
+    @staticmethod
+    def writeMetaDataFile(path: str, tilt_angles: Sequence[float], filenames: Sequence[str],
+                          base: ScannerGeometry, volume_resolution: Sequence[int]) -> None:
+        """:121-175: base geometry, volume dimensions, one <projection> per image."""
+        if len(tilt_angles) != len(filenames):
+            raise EttentionError(_abi.ERR_INVALID_ARGUMENT, "Filename count does not match tilt angle count!")
+        a = np.asarray(tilt_angles, np.float32)
+        names = (ctypes.c_char_p * max(1, len(filenames)))(*[str(f).encode() for f in filenames])
+        res = np.asarray(volume_resolution, np.uint32)
+        _check_free(lib().etcu_image_stack_write_metadata(str(path).encode(), a.ctypes.data, names, len(filenames),
+                                                          ctypes.byref(base.to_view()), res.ctypes.data))
+
+
+def mrc_can_handle(path: str) -> bool:
+    """MRCStack::canHandleResource (MRCStack.cpp:70-83): a file ending in .mrc or .ali."""
+    return os.path.isfile(path) and os.path.splitext(path)[1] in (".mrc", ".ali")
+
+
+def open_image_stack(projections: str, tilt_angles: Optional[str] = None, logarithmize: bool = False):
+    """ImageStackDatasourceFactory::instantiate (LR/io/ImageStackDataSourceFactory.cpp:19-44):
+    the directory datasource is asked first, then the MRC stack."""
+    if ImageStackDirectoryDatasource.canHandleResource(projections):
+        return ImageStackDirectoryDatasource(projections)
+    if mrc_can_handle(projections):
+        return MRCStack(projections, tilt_angles, logarithmize)
+    raise EttentionError(_abi.ERR_INVALID_ARGUMENT,
+                         f"Unable to open image stack {projections}! Incorrect filename or plugin missing?")
+
+
+PATH_PARAMETERS = ("input.projections", "input.tiltAngles", "output.filename", "volume.initFile",
+                   "priorknowledge.maskVolumeFilename", "debug.performanceReportFile", "debug.infoPath",
+                   "debug.meshExportPath")
+
+
+class XMLParameterSource:
+    """LR/setup/parametersource/XMLParameterSource.cpp: the value attribute of every
+    element by its dotted path; path parameters use '/' for '\\' and are relative to
+    the file's directory (:24-35)."""
+
+    def __init__(self, filename: str):
+        self.filename = str(filename)
+        n = ctypes.c_size_t()
+        _check_free(lib().etcu_xml_config_read(self.filename.encode(), None, 0, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(n.value)
+        _check_free(lib().etcu_xml_config_read(self.filename.encode(), buf, n.value, ctypes.byref(n)))
+        self.values: Dict[str, str] = {}
+        for line in buf.value.decode().splitlines():
+            key, _, value = line.partition("\t")
+            self.values[key] = value
+
+    def parameterExists(self, name: str) -> bool:
+        return name in self.values
+
+    def getStringParameter(self, name: str) -> str:
+        if name not in self.values:
+            raise EttentionError(_abi.ERR_INVALID_ARGUMENT, f"xml config file entry does not exist: {name}")
+        return self.values[name]
+
+    def getPathParameter(self, name: str) -> str:
+        p = self.getStringParameter(name).replace("\\", "/")
+        if not os.path.isabs(p):
+            p = os.path.join(os.path.dirname(os.path.abspath(self.filename)), p)
+        return os.path.normpath(p)
+
+    def config(self) -> Dict[str, str]:
+        """Every value, path parameters resolved: the input of AlgebraicParameterSet.from_config."""
+        cfg = dict(self.values)
+        for k in PATH_PARAMETERS:
+            if k in cfg:
+                cfg[k] = self.getPathParameter(k)
+        return cfg
+
+
+def _true(v) -> bool:
+    return str(v).strip().lower() in ("true", "1", "yes")
+
+
+# CoordinateOrder (LR/setup/parameterset/IOEnumerations.cpp:7-35, "xzy_order" ...):
+# working coordinate k = file coordinate perm[k] (BlockIterativeConfiguration.cpp:176-197).
+_ORIENTATIONS = {"xyz": (0, 1, 2), "xzy": (0, 2, 1), "yxz": (1, 0, 2), "yzx": (2, 0, 1), "zxy": (1, 2, 0),
+                 "zyx": (2, 1, 0)}
+
+
+def _coordinate_order(value: str) -> str:
+    v = str(value).strip().lower()
+    v = v[:-len("_order")] if v.endswith("_order") else v
+    if v not in _ORIENTATIONS:
+        raise EttentionError(_abi.ERR_INVALID_ARGUMENT, f"Unknown CoordinateOrder given: {value}")
+    return v
+
+
+def load_init_volume(path: str, orientation: str, resolution: Sequence[int]) -> np.ndarray:
+    """volume.initFile (BlockIterativeConfiguration.cpp:36-40, :155-198): an MRC volume
+    whose file coordinates map to the working volume's by ``orientation``; returns
+    the (z, y, x) float32 working volume."""
+    X, Y, Z = (int(r) for r in resolution)
+    perm = _ORIENTATIONS[_coordinate_order(orientation)]
+    raw = MRCStack(path).load_projections()  # (nz, ny, nx): file coordinates (x, y, z)
+    work_xyz = np.transpose(np.transpose(raw, (2, 1, 0)), perm)
+    if work_xyz.shape != (X, Y, Z):
+        raise EttentionError(_abi.ERR_INVALID_ARGUMENT,
+                             f"Resolution of volume from file {path} does not match resolution given in config file!")
+    return np.ascontiguousarray(np.transpose(work_xyz, (2, 1, 0)), np.float32)
+
+
+def load_mask_volume(path: str, resolution: Sequence[int]) -> np.ndarray:
+    """priorknowledge.maskVolumeFilename (BlockIterativeConfiguration.cpp:46-50,
+    VolumeDeserializer.cpp:15-47): an MRC volume in file order, each value cast to an
+    8-bit voxel (ByteVolume::convertValueFromFloat; clamped to 0..255 here)."""
+    X, Y, Z = (int(r) for r in resolution)
+    m = MRCStack(path).load_projections()
+    if m.shape != (Z, Y, X):
+        raise EttentionError(_abi.ERR_INVALID_ARGUMENT, f"mask volume {path} does not match the volume's resolution")
+    return np.clip(m, 0, 255).astype(np.uint8)
+
+
+def reconstruct_from_config(config, device: int = 0, write_output: bool = True) -> np.ndarray:
+    """A block-iterative run as the reference's frontend performs it from a parameter
+    file: parameters (XMLParameterSource or a dict of keys with resolved paths),
+    the projections through open_image_stack (input.projections, input.tiltAngles,
+    input.logarithmize, input.xAxisTilt), the volume from volume.* and
+    hardware.subVolumeCount, optionally volume.initFile (MRC in
+    volume.initFileOrientation, XZY by default; BlockIterativeConfiguration.cpp:36-40,
+    :155-198) and priorknowledge.maskVolumeFilename (MRC read in file order, values
+    cast to 8 bits; :46-50), the iterations of BlockIterativeReconstructionOperator
+    on the GPU, and Framework::writeFinalVolume to output.filename (float32 MRC,
+    output.options.orientation xyz_order or xzy_order, XZY by default).  Returns the
+    (z, y, x) volume."""
+    cfg = config.config() if isinstance(config, XMLParameterSource) else dict(config)
+    p = AlgebraicParameterSet.from_config(cfg)
+    if p.resolution is None:
+        raise EttentionError(_abi.ERR_INVALID_ARGUMENT, "xml config file entry does not exist: volume.dimension")
+    if "input.projections" not in cfg:
+        raise EttentionError(_abi.ERR_INVALID_ARGUMENT, "xml config file entry does not exist: input.projections")
+    vt = cfg.get("output.options.voxelType", "float32")
+    if write_output and "output.filename" in cfg and vt != "float32":
+        raise EttentionError(_abi.ERR_UNSUPPORTED, f"output.options.voxelType {vt}: only float32 is written")
+    if _true(cfg.get("output.options.invert", "false")):
+        raise EttentionError(_abi.ERR_UNSUPPORTED, "output.options.invert is not supported")
+    out_order = _coordinate_order(cfg.get("output.options.orientation", "xzy_order"))
+    if write_output and "output.filename" in cfg and out_order not in ("xyz", "xzy"):
+        raise EttentionError(_abi.ERR_UNSUPPORTED, f"output orientation {out_order}: XYZ and XZY are written")
+    stack = open_image_stack(cfg["input.projections"], cfg.get("input.tiltAngles"),
+                             _true(cfg.get("input.logarithmize", "false")))
+    views = stack.geometries(p.xaxis_tilt)
+    data = stack.load_projections()
+    X, Y, Z = (int(r) for r in p.resolution)
+    init = None
+    if "volume.initFile" in cfg:
+        init = load_init_volume(cfg["volume.initFile"], cfg.get("volume.initFileOrientation", "xzy_order"), (X, Y, Z))
+    mask = None
+    if "priorknowledge.maskVolumeFilename" in cfg:
+        mask = load_mask_volume(cfg["priorknowledge.maskVolumeFilename"], (X, Y, Z))
+    ctx = Context(device)
+    try:
+        lo, hi = p.bbox()
+        vol = GPUMappedVolume(ctx, (X, Y, Z), lo, hi, voxel_type=p.voxel_type, init_value=p.init_value,
+                              subvolume_count=p.subvolume_count)
+        if init is not None:
+            vol.upload(init)
+        if mask is not None:
+            vol.set_mask(mask)
+        rec = BlockIterativeReconstructionOperator(vol, views, data, p)
+        rec.run()
+        v = rec.getReconstructedVolume()
+    finally:
+        ctx.close()
+        if isinstance(stack, ImageStackDirectoryDatasource):
+            stack.close()
+    if write_output and "output.filename" in cfg:
+        write_mrc_volume(cfg["output.filename"], v, out_order)
+    return v
 
 
 ORDERS = {"identity": _abi.ORDER_IDENTITY, "random": _abi.ORDER_RANDOM, "maxangle": _abi.ORDER_MAXANGLE,

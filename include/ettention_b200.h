@@ -262,6 +262,60 @@ typedef enum { ETCU_AXES_XYZ = 0, ETCU_AXES_XZY = 1 } etcu_orientation;
 ETCU_API etcu_status etcu_mrc_write_volume(const char* path, const float* volume, const uint32_t resolution[3],
                                            etcu_orientation orientation);
 
+/* TIFF images (LR/io/deserializer/ImageDeserializer.cpp:10-62, replacing FreeImage):
+ * grey, one sample per pixel, 8 / 16-bit unsigned or 32-bit float samples, converted
+ * to float as the reference does (8-bit / 255, 16-bit / 65535, float as is); strips
+ * or tiles; no compression, LZW, Deflate or PackBits; predictors 1, 2 and 3.  Image
+ * row y is the y-th row of the file.  Multi-page files are image stacks. */
+typedef struct {
+    uint32_t width, height;
+    uint32_t pages;            /* pages in the file */
+    uint32_t bits_per_sample;  /* of the page asked for */
+    uint32_t sample_format;    /* 1 unsigned, 2 signed, 3 float */
+    uint32_t compression;      /* 1 none, 5 LZW, 8 / 32946 Deflate, 32773 PackBits */
+} etcu_image_info;
+ETCU_API etcu_status etcu_tiff_read_info(const char* path, uint32_t page, etcu_image_info* out);
+/* One page as width * height floats (x fastest). */
+ETCU_API etcu_status etcu_tiff_read(const char* path, uint32_t page, float* out, size_t capacity);
+/* ImageSerializer::writeImage(..., TIFF_GRAY_32): one page of 32-bit float grey. */
+ETCU_API etcu_status etcu_tiff_write(const char* path, const float* image, uint32_t width, uint32_t height);
+
+/* A directory of projection images described by its metadata.xml
+ * (LR/io/datasource/ImageStackDirectoryDatasource.cpp): <geometry> holds the base
+ * parallel geometry (sourcePosition, detectorPosition, horizontalPitch,
+ * verticalPitch); every <projection> an <image filename=.../>, a <tiltAngle
+ * value=.../> and optionally <logscale/> (pixels are then exp()'d); a
+ * <projectionstack> names a multi-page image whose pages share one tilt angle.
+ * Projections are numbered by tilt angle in order of first appearance, repeated
+ * angles after one another (:200-240); the detector size is the first image's. */
+typedef struct etcu_image_stack etcu_image_stack;
+typedef struct {
+    uint32_t count;   /* projections */
+    uint32_t width, height;
+    etcu_view base;   /* untilted geometry; rotate with etcu_view_rotate */
+} etcu_image_stack_info;
+ETCU_API etcu_status etcu_image_stack_open(const char* directory, etcu_image_stack** out);
+ETCU_API void etcu_image_stack_destroy(etcu_image_stack* stack);
+ETCU_API etcu_status etcu_image_stack_info_get(const etcu_image_stack* stack, etcu_image_stack_info* out);
+/* Tilt angle of every projection (degrees), count of them. */
+ETCU_API etcu_status etcu_image_stack_tilt_angles(const etcu_image_stack* stack, float* out, uint32_t capacity);
+/* Projections first .. first + count - 1 as count * height * width floats. */
+ETCU_API etcu_status etcu_image_stack_load(const etcu_image_stack* stack, uint32_t first, uint32_t count, float* out,
+                                           size_t capacity);
+/* ImageStackDirectoryDatasource::writeMetaDataFile (:121-175): the base geometry,
+ * volume dimensions and one <projection> per (file name, tilt angle). */
+ETCU_API etcu_status etcu_image_stack_write_metadata(const char* path, const float* tilt_angles,
+                                                     const char* const* filenames, uint32_t count,
+                                                     const etcu_view* base, const uint32_t volume_resolution[3]);
+
+/* XML parameter files (LR/setup/parametersource/XMLParameterSource.cpp): every element
+ * with a value attribute becomes "path.to.element<TAB>value<NEWLINE>" (the first
+ * element of a path wins, as a property-tree lookup does).  *needed = bytes of the
+ * text including its terminating NUL; out (capacity bytes) receives it when it fits.
+ * Relative paths in values are relative to the file's directory
+ * (XMLParameterSource.cpp:24-35); resolving them is the caller's. */
+ETCU_API etcu_status etcu_xml_config_read(const char* path, char* out, size_t capacity, size_t* needed);
+
 /* ---------------------------------------------------------------- batched series */
 /* Many independent tilt series of uneven sizes reconstructed together: every SART
  * step runs one forward-projection launch and one back-projection launch over all

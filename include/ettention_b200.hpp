@@ -17,6 +17,9 @@
  *   BlockIterativeReconstructionOperator   LR/algorithm/reconstruction/blockiterative/
  *                                          BlockIterativeReconstructionOperator.cpp:56-185
  *   MRCStack, writeMrcVolume               LR/io/datasource/MRCStack.cpp, LR/io/serializer/MRCWriter.cpp
+ *   ImageStackDirectoryDatasource,         LR/io/datasource/ImageStackDirectoryDatasource.cpp,
+ *   readTiff, writeTiff                    LR/io/deserializer/ImageDeserializer.cpp, ImageSerializer.cpp
+ *   XMLParameterSource                     LR/setup/parametersource/XMLParameterSource.cpp
  *   BatchReconstructionOperator            many series per launch (no counterpart in the reference)
  * Errors: every non-OK status of the ABI is rethrown as ettention::b200::Exception
  * (validation) or GPUException (device errors), with the library's message, as
@@ -449,6 +452,107 @@ inline void writeMrcVolume(const std::string& path, const float* volume, const s
                            etcu_orientation orientation = ETCU_AXES_XZY) {
     check(etcu_mrc_write_volume(path.c_str(), volume, resolution.data(), orientation), nullptr);
 }
+
+// ImageDeserializer::readImage / readImageFromStack: one page as height x width floats.
+inline std::vector<float> readTiff(const std::string& path, uint32_t page, uint32_t* width, uint32_t* height) {
+    etcu_image_info info{};
+    check(etcu_tiff_read_info(path.c_str(), page, &info), nullptr);
+    std::vector<float> out((size_t)info.width * info.height);
+    check(etcu_tiff_read(path.c_str(), page, out.data(), out.size()), nullptr);
+    if (width) *width = info.width;
+    if (height) *height = info.height;
+    return out;
+}
+
+// ImageSerializer::writeImage(..., TIFF_GRAY_32).
+inline void writeTiff(const std::string& path, const float* image, uint32_t width, uint32_t height) {
+    check(etcu_tiff_write(path.c_str(), image, width, height), nullptr);
+}
+
+// ImageStackDirectoryDatasource: a directory of images described by metadata.xml.
+class ImageStackDirectoryDatasource {
+public:
+    explicit ImageStackDirectoryDatasource(const std::string& directory) {
+        check(etcu_image_stack_open(directory.c_str(), &stack_), nullptr);
+        check(etcu_image_stack_info_get(stack_, &info_), nullptr);
+        angles_.resize(info_.count);
+        check(etcu_image_stack_tilt_angles(stack_, angles_.data(), info_.count), nullptr);
+    }
+    ~ImageStackDirectoryDatasource() { etcu_image_stack_destroy(stack_); }
+    ImageStackDirectoryDatasource(const ImageStackDirectoryDatasource&) = delete;
+    ImageStackDirectoryDatasource& operator=(const ImageStackDirectoryDatasource&) = delete;
+
+    uint32_t getNumberOfProjections() const { return info_.count; }
+    std::array<uint32_t, 2> getResolution() const { return {{info_.width, info_.height}}; }
+    const std::vector<float>& tiltAngles() const { return angles_; }
+    ScannerGeometry baseGeometry() const { return ScannerGeometry(info_.base); }
+    ScannerGeometry createScannerGeometry(uint32_t index, float xaxis_tilt_deg = 0.f) const {
+        return baseGeometry().rotated(angles_.at(index), xaxis_tilt_deg);
+    }
+    // Projections first .. first + count - 1, count x height x width floats.
+    std::vector<float> loadProjections(uint32_t first = 0, uint32_t count = UINT32_MAX) const {
+        if (count == UINT32_MAX) count = info_.count - first;
+        std::vector<float> out((size_t)info_.width * info_.height * count);
+        check(etcu_image_stack_load(stack_, first, count, out.data(), out.size()), nullptr);
+        return out;
+    }
+    // ImageStackDirectoryDatasource::writeMetaDataFile.
+    static void writeMetaDataFile(const std::string& path, const std::vector<float>& tilt_angles,
+                                  const std::vector<std::string>& filenames, const ScannerGeometry& base,
+                                  const std::array<uint32_t, 3>& volume_resolution) {
+        if (tilt_angles.size() != filenames.size())
+            throw Exception(ETCU_ERR_INVALID_ARGUMENT, "Filename count does not match tilt angle count!");
+        std::vector<const char*> names;
+        for (const auto& f : filenames) names.push_back(f.c_str());
+        check(etcu_image_stack_write_metadata(path.c_str(), tilt_angles.data(), names.data(),
+                                              (uint32_t)names.size(), &base.view(), volume_resolution.data()),
+              nullptr);
+    }
+
+private:
+    etcu_image_stack* stack_ = nullptr;
+    etcu_image_stack_info info_{};
+    std::vector<float> angles_;
+};
+
+// XMLParameterSource: the value attribute of every element by its dotted path, the
+// input of AlgebraicParameterSet::fromConfig.  getPathParameter resolves a value
+// relative to the file's directory, '\' read as '/'.
+class XMLParameterSource {
+public:
+    explicit XMLParameterSource(const std::string& filename) : filename_(filename) {
+        size_t n = 0;
+        check(etcu_xml_config_read(filename.c_str(), nullptr, 0, &n), nullptr);
+        std::string text(n, '\0');
+        check(etcu_xml_config_read(filename.c_str(), &text[0], n, &n), nullptr);
+        std::istringstream in(text.c_str());
+        std::string line;
+        while (std::getline(in, line)) {
+            const size_t tab = line.find('\t');
+            if (tab != std::string::npos) values_.emplace(line.substr(0, tab), line.substr(tab + 1));
+        }
+    }
+    bool parameterExists(const std::string& name) const { return values_.count(name) != 0; }
+    const std::string& getStringParameter(const std::string& name) const {
+        auto it = values_.find(name);
+        if (it == values_.end())
+            throw Exception(ETCU_ERR_INVALID_ARGUMENT, "xml config file entry does not exist: " + name);
+        return it->second;
+    }
+    std::string getPathParameter(const std::string& name) const {
+        std::string v = getStringParameter(name);
+        for (char& c : v)
+            if (c == '\\') c = '/';
+        if (!v.empty() && v[0] == '/') return v;
+        const size_t slash = filename_.rfind('/');
+        return slash == std::string::npos ? v : filename_.substr(0, slash + 1) + v;
+    }
+    const std::map<std::string, std::string>& values() const { return values_; }
+
+private:
+    std::string filename_;
+    std::map<std::string, std::string> values_;
+};
 
 // Many independent tilt series reconstructed together with SART (etcu_batch_*): one
 // forward and one back-projection launch per step over all series.

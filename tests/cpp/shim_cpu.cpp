@@ -53,6 +53,36 @@ int main(int argc, char** argv) {
         } catch (const Exception& e) {
             std::printf("mrc_missing error %d\n", (int)e.status());
         }
+        // a directory stack of two TIFF projections with metadata.xml, and a parameter file
+        const std::string dir = std::string(path) + ".d";
+        std::vector<float> img(6 * 5);
+        for (int i = 0; i < 30; ++i) img[i] = 0.25f * (float)i;
+        writeTiff(dir + "_p0.tif", img.data(), 6, 5);
+        for (float& v : img) v = -v;
+        writeTiff(dir + "_p1.tif", img.data(), 6, 5);
+        const std::string base_name = dir.substr(dir.rfind('/') + 1);
+        ImageStackDirectoryDatasource::writeMetaDataFile(dir.substr(0, dir.rfind('/') + 1) + "metadata.xml",
+                                                         {-30.f, 45.5f}, {base_name + "_p0.tif", base_name + "_p1.tif"},
+                                                         ScannerGeometry::mrcBase(6, 5), {{6, 6, 4}});
+        ImageStackDirectoryDatasource ds(dir.substr(0, dir.rfind('/')));
+        const std::vector<float> pr = ds.loadProjections();
+        std::printf("stack %u %u %u %g %g %g %g\n", ds.getNumberOfProjections(), ds.getResolution()[0],
+                    ds.getResolution()[1], ds.tiltAngles()[0], ds.tiltAngles()[1], pr[7], pr[30 + 7]);
+        uint32_t w = 0, h = 0;
+        const std::vector<float> t0 = readTiff(dir + "_p0.tif", 0, &w, &h);
+        std::printf("tiff %u %u %g\n", w, h, t0[29]);
+        const std::string xml = dir + "_run.xml";
+        if (FILE* f = std::fopen(xml.c_str(), "w")) {
+            std::fputs("<?xml version=\"1.0\"?>\n<algorithm value=\"sirt\"><numberOfIterations value=\"4\"/>"
+                       "<lambda value=\"0.5\"/></algorithm><input><projections value=\"sub\\dir\"/></input>\n",
+                       f);
+            std::fclose(f);
+        }
+        XMLParameterSource src(xml);
+        const auto p = AlgebraicParameterSet::fromConfig(src.values());
+        const std::string proj = src.getPathParameter("input.projections");
+        std::printf("xml %s %u %g %s\n", p.algorithm.c_str(), p.iterations, p.lambda,
+                    proj.substr(proj.size() - 8).c_str());
     }
     try {
         Framework fw(0);

@@ -47,6 +47,9 @@ def test_cpp_shim_host_side(tmp_path):
     assert lines["config missing"][2:4] == ["error", "1"]
     assert lines["mrc"][1:] == ["ok", "0", "23"]
     assert lines["mrc_missing"][1:] == ["error", "1"]
+    assert lines["stack"][1:] == ["2", "6", "5", "-30", "45.5", "1.75", "-1.75"]
+    assert lines["tiff"][1:] == ["6", "5", "7.25"]
+    assert lines["xml"][1:] == ["sirt", "4", "0.5", "/sub/dir"]
     import torch
     if torch.cuda.is_available():
         assert lines["framework"][1] == "ok"
