@@ -61,7 +61,9 @@ def parse():
                          "bf16 shadow; c4: 64 batched series of uneven sizes")
     ap.add_argument("--ncu-case", action="store_true",
                     help="small profiling case for ncu: 512x512x256 volume, 8 views, one SART iteration "
-                         "launched kernel by kernel (8 forward + 8 back projections), then per-kernel times")
+                         "launched kernel by kernel, then per-kernel times of the unfused kernels")
+    ap.add_argument("--ncu-res", default="512,512,256",
+                    help="volume of the --ncu-case (x,y,z; the detector is x by y)")
     return ap.parse_args()
 
 
@@ -238,12 +240,14 @@ def make_problem(ctx, seed: int):
 def algorithmic_bytes():
     """Per launch, FP32 storage: forward projection of one view reads the volume once,
     reads b and writes (r, L); back projection of a one-view block read-modify-writes
-    the volume and reads (r, L)."""
+    the volume and reads (r, L); the fused SART step read-modify-writes the volume once,
+    reads view p's (r, L) and view p + 1's b, and writes view p + 1's (r, L)."""
     V = RES[0] * RES[1] * RES[2]
     P = DET[0] * DET[1]
     fp = V * 4 + P * 4 + P * 8
     bp = 2 * V * 4 + P * 8
-    return fp, bp
+    fused = 2 * V * 4 + P * 8 + P * 4 + P * 8
+    return fp, bp, fused
 
 
 # DRAM bytes per voxel of one launch, dram__bytes_read.sum + dram__bytes_write.sum from an
@@ -254,12 +258,16 @@ def algorithmic_bytes():
 # (at most the L2 size, about 63 MB in that capture).
 FP_DRAM_BYTES_PER_VOXEL = (269974272 + 5381120) / 67108864
 BP_DRAM_BYTES_PER_VOXEL = (270639104 + 205491712) / 67108864
+# sart_fused_kernel, ncu capture of the 1024x1024x256 case (python bench.py --ncu-case
+# --ncu-res 1024,1024,256: the bench's own volume and detector, 268,435,456 voxels):
+# dram__bytes_read.sum + dram__bytes_write.sum per launch.
+FUSED_DRAM_BYTES_PER_VOXEL = (1086500000 + 1021966000) / 268435456
 
 
 def dram_traffic():
-    """Measured DRAM bytes per launch scaled to the bench volume (forward, back)."""
+    """Measured DRAM bytes per launch scaled to the bench volume (forward, back, fused)."""
     V = RES[0] * RES[1] * RES[2]
-    return FP_DRAM_BYTES_PER_VOXEL * V, BP_DRAM_BYTES_PER_VOXEL * V
+    return FP_DRAM_BYTES_PER_VOXEL * V, BP_DRAM_BYTES_PER_VOXEL * V, FUSED_DRAM_BYTES_PER_VOXEL * V
 
 
 # ------------------------------------------------------------------ CPU baseline (oracle)
@@ -384,9 +392,11 @@ def run_ours(args, rank, world, local):
     ms_per_step = ms_total / args.steps
     value = TARGET_ITERS * ms_per_step / 1e3
     d1 = rec.data_residual_sq()
-    # ---- per-kernel device times (one more real iteration, launch by launch) ----
-    fp_ms, bp_ms, nf, nb = rec.profile_iteration()
-    fp_bytes, bp_bytes = algorithmic_bytes()
+    # ---- per-step device times (one more real iteration, issued as run() issues it,
+    # CUDA events around every step on the library stream) ----
+    steps = rec.profile_steps()
+    fp_bytes, bp_bytes, fused_bytes = algorithmic_bytes()
+    fp_traffic, bp_traffic, fused_traffic = dram_traffic()
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -394,20 +404,25 @@ def run_ours(args, rank, world, local):
         pass
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    fp_avg, bp_avg = fp_ms / max(nf, 1), bp_ms / max(nb, 1)
-    fp_gbs = fp_bytes / (fp_avg * 1e-3) / 1e9
-    bp_gbs = bp_bytes / (bp_avg * 1e-3) / 1e9
-    dominant = "back_project" if bp_ms >= fp_ms else "forward_project"
-    ach = bp_gbs if dominant == "back_project" else fp_gbs
-    fp_traffic, bp_traffic = dram_traffic()
-    roofline = {"bound": "hbm", "kernel": dominant, "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
-                "frac": ach / hbm_peak, "peak_source": peak_src,
-                "traffic": bp_traffic if dominant == "back_project" else fp_traffic,
-                "traffic_source": "ncu dram bytes of the 512x512x256 case, scaled by voxel count",
-                "per_kernel": {"forward_project": {"avg_ms": fp_avg, "launches": nf, "algorithmic_bytes": fp_bytes,
-                                                   "gbs": fp_gbs, "frac": fp_gbs / hbm_peak, "traffic": fp_traffic},
-                               "back_project": {"avg_ms": bp_avg, "launches": nb, "algorithmic_bytes": bp_bytes,
-                                                "gbs": bp_gbs, "frac": bp_gbs / hbm_peak, "traffic": bp_traffic}}}
+    per_kernel = {}
+    for kind, name, byts, traffic in (("fused", "sart_fused_step", fused_bytes, fused_traffic),
+                                      ("forward", "forward_project", fp_bytes, fp_traffic),
+                                      ("back", "back_project", bp_bytes, bp_traffic)):
+        ts = [t for k, t, _ in steps if k == kind]
+        if not ts:
+            continue
+        avg = sum(ts) / len(ts)
+        gbs = byts / (avg * 1e-3) / 1e9
+        per_kernel[name] = {"avg_ms": avg, "launches": sum(l for k, _, l in steps if k == kind),
+                            "total_ms": sum(ts), "algorithmic_bytes": byts, "gbs": gbs, "frac": gbs / hbm_peak,
+                            "traffic": traffic}
+    dominant = max(per_kernel, key=lambda n: per_kernel[n]["total_ms"])
+    dk = per_kernel[dominant]
+    roofline = {"bound": "hbm", "kernel": dominant, "achieved": dk["gbs"], "peak": hbm_peak, "unit": "GB/s",
+                "frac": dk["frac"], "peak_source": peak_src, "traffic": dk["traffic"],
+                "traffic_source": ("ncu dram bytes per launch of the 1024x1024x256 case" if dominant == "sart_fused_step"
+                                   else "ncu dram bytes of the 512x512x256 case, scaled by voxel count"),
+                "per_kernel": per_kernel}
     rec.close()
     vol.close()
     # ---- e2e: one-call host-buffer reconstruction through the C ABI ----
@@ -441,12 +456,12 @@ def run_ours(args, rank, world, local):
     ctx.close()
 
 
-def run_ncu_case():
-    """A case small enough for an ncu capture (256 MB volume, larger than L2)."""
+def run_ncu_case(res=(512, 512, 256)):
+    """A case small enough for an ncu capture (by default a 256 MB volume, larger than L2)."""
     from ettention_b200 import _abi
     from ettention_b200.operators import (AlgebraicParameterSet, BlockIterativeReconstructionOperator, Context,
                                           GPUMappedVolume, mrc_base_geometry)
-    X, Y, Z = 512, 512, 256
+    X, Y, Z = res
     ctx = Context(0)
     rng = np.random.Generator(np.random.PCG64(0))
     vol = GPUMappedVolume(ctx, (X, Y, Z))
@@ -457,7 +472,7 @@ def run_ncu_case():
     rec = BlockIterativeReconstructionOperator(vol, geoms, projs, p, use_graph=False)
     rec.runNiterations(1)
     f, b, nf, nb = rec.profile_iteration()
-    print(json.dumps({"ncu_case": "512x512x256 f32, 8 views, SART", "forward_ms": f / nf, "back_ms": b / nb}))
+    print(json.dumps({"ncu_case": f"{X}x{Y}x{Z} f32, 8 views, SART", "forward_ms": f / nf, "back_ms": b / nb}))
     rec.close()
     vol.close()
     ctx.close()
@@ -661,7 +676,7 @@ def run_c3(args):
 def main():
     args = parse()
     if args.ncu_case:
-        run_ncu_case()
+        run_ncu_case(tuple(int(v) for v in args.ncu_res.split(",")))
         return
     if args.workload == "c4":
         run_c4(args)

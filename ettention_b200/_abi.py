@@ -117,6 +117,7 @@ _SIG = {
     "etcu_recon_launches_per_iteration": (_U, [_P]),
     "etcu_recon_profile_iteration": (_S, [_P, ctypes.POINTER(_F), ctypes.POINTER(_F), ctypes.POINTER(_U),
                                          ctypes.POINTER(_U)]),
+    "etcu_recon_profile_steps": (_S, [_P, _P, _P, _P, _U, ctypes.POINTER(_U)]),
     "etcu_reconstruct": (_S, [_P, ctypes.POINTER(VolumeDesc), _I, ctypes.POINTER(View), _U, _P,
                               ctypes.POINTER(ReconParams), _U, _P]),
     "etcu_projection_order": (_S, [_I, _U, _P, _U, _P, ctypes.POINTER(_U)]),

@@ -39,6 +39,7 @@ struct etcu_context {
     uint32_t pair_w = 0, pair_h = 0;
     cudaTextureObject_t pair_tex = 0;
     bool bp_column = true;  // column-pipelined single-view back projection (ETCU_BP_COLUMN=0 disables)
+    bool fused_step = true; // fused SART step BP(p) + FP(p + 1) (ETCU_FUSED=0 disables)
 };
 
 struct etcu_volume {
@@ -82,6 +83,12 @@ struct etcu_recon {
     std::vector<uint8_t> row_const; // per view id
     std::vector<ViewConst> hvc;     // host copy of the view constants, [slab][view id]
     std::vector<float4> hsamples;   // host copy of the sample patterns, [view id][sample]
+    // fused SART step (sart_fused_kernel): per view id its tap window, per (view id,
+    // volume row) the detector rows of its rays
+    bool fused = false;
+    std::vector<int> fuse_x0lo, fuse_ntaps;
+    int2* d_jrange = nullptr;
+    size_t fuse_smem = 0;
 };
 
 namespace {
@@ -617,6 +624,7 @@ extern "C" etcu_status etcu_context_create(int device, etcu_context** out) {
         return fail(nullptr, ETCU_ERR_CUDA, "cudaStreamCreate failed");
     c->stream = c->own_stream;
     if (const char* env = getenv("ETCU_BP_COLUMN")) c->bp_column = atoi(env) != 0;
+    if (const char* env = getenv("ETCU_FUSED")) c->fused_step = atoi(env) != 0;
     *out = c.release();
     return ETCU_OK;
 }
@@ -1009,6 +1017,7 @@ void recon_free(etcu_recon* r) {
     dfree(ctx, r->rl_raw, r->rl_slot * r->slots * sizeof(float2) + ctx->tex_align);
     dfree(ctx, r->d_texs, r->slots * sizeof(cudaTextureObject_t));
     dfree(ctx, r->d_resid, sizeof(double));
+    dfree(ctx, r->d_jrange, (size_t)r->n_input * (r->vol->slabs.empty() ? 0 : r->vol->slabs[0].ry) * sizeof(int2));
 }
 
 // Forward projection of `count` views starting at order position `first`
@@ -1043,7 +1052,8 @@ uint32_t issue_forward(etcu_recon* r, uint32_t first, uint32_t count, cudaStream
 
 // Back projection of the block's views, slabs in reverse order
 // (BlockIterativeReconstructionOperator.cpp:130-142), lambda / blockSize.
-uint32_t issue_backward(etcu_recon* r, uint32_t first, uint32_t count, cudaStream_t st) {
+uint32_t issue_backward(etcu_recon* r, uint32_t first, uint32_t count, cudaStream_t st,
+                        const float2* rl = nullptr) {
     etcu_volume* vol = r->vol;
     const uint32_t S = (uint32_t)vol->slabs.size();
     uint32_t n = 0;
@@ -1057,7 +1067,7 @@ uint32_t issue_backward(etcu_recon* r, uint32_t first, uint32_t count, cudaStrea
         a.first = first;
         a.nviews = (int)count;
         a.texs = r->d_texs;
-        a.rl = r->rl;
+        a.rl = rl ? rl : r->rl;
         a.rl_pitch = r->rl_pitch;
         a.rl_slot = r->rl_slot;
         a.W = (int)r->W;
@@ -1079,12 +1089,147 @@ uint32_t issue_backward(etcu_recon* r, uint32_t first, uint32_t count, cudaStrea
     return n;
 }
 
+// SART with the fused step: FP of the first view into slot 0, then for every order
+// position p the fused BP(p) + FP(p + 1) (slots alternate), then the BP of the last
+// view.  Same operations in the same order as the unfused sequence.
+void launch_fused_step(etcu_recon* r, uint32_t p, cudaStream_t st) {
+    etcu_volume* vol = r->vol;
+    const SlabConst& g = vol->slabs[0];
+    const uint32_t vb = r->order[p];
+    FuseArgs a{};
+    a.vol = vol->master;
+    a.slab = g;
+    a.views = r->d_views;
+    a.order = r->d_order;
+    a.p = p;
+    a.samples = r->d_samples;
+    a.rl_in = r->rl + (size_t)(p & 1) * r->rl_slot;
+    a.rl_out = r->rl + (size_t)((p + 1) & 1) * r->rl_slot;
+    a.rl_pitch = r->rl_pitch;
+    a.W = (int)r->W;
+    a.H = (int)r->H;
+    a.lambda = r->params.lambda;  // block size 1
+    a.x0lo = r->fuse_x0lo[vb];
+    a.ntaps = r->fuse_ntaps[vb];
+    a.jrange = r->d_jrange;
+    a.real = r->d_proj;
+    a.resid_sq = r->d_resid;
+    a.loc = r->params.use_long_object_compensation ? 1 : 0;
+    sart_fused_kernel<<<g.ry, kFuseThreads, fuse_smem_bytes(g.rx, g.rz, a.ntaps), st>>>(a);
+}
+
+uint32_t issue_fused_iteration(etcu_recon* r, cudaStream_t st) {
+    const uint32_t M = (uint32_t)r->order.size();
+    uint32_t n = issue_forward(r, 0, 1, st);
+    for (uint32_t p = 0; p + 1 < M; ++p) {
+        launch_fused_step(r, p, st);
+        ++n;
+    }
+    // the last view's back projection reads the slot its FP wrote
+    const uint32_t last = M - 1;
+    n += issue_backward(r, last, 1, st, r->rl + (size_t)(last & 1) * r->rl_slot);
+    return n;
+}
+
+void fuse_limits(int dev, size_t smem, int& per_sm) {
+    static std::mutex mu;
+    static std::vector<char> opted;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if ((int)opted.size() <= dev) opted.resize(dev + 1, 0);
+        if (!opted[dev]) {
+            cudaDeviceProp prop;
+            if (cudaGetDeviceProperties(&prop, dev) == cudaSuccess)
+                cudaFuncSetAttribute(sart_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)prop.sharedMemPerBlockOptin);
+            cudaGetLastError();
+            opted[dev] = 1;
+        }
+    }
+    per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sart_fused_kernel, kFuseThreads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        per_sm = 0;
+    }
+}
+
+// Whether every SART step of this reconstruction can run fused (sart_fused_kernel):
+// SART on one FP32 sub-volume without mask, one sample each way, 1/256 sampling,
+// parallel views tilted about y (ray.y == 0, hpitch.y == 0, detector row constant
+// in y), x rows of an even number of at most 2 * kFuseThreads voxels, walks that
+// cannot reach the step cap, at most kFuseRays * kFuseThreads rays per volume row,
+// and a tap window per view (plan_bp_col).  Builds the per-view tap windows and the
+// (view, volume row) -> detector rows table.
+etcu_status plan_fused(etcu_recon* r, const std::vector<ViewConst>& vc, bool& ok) {
+    ok = false;
+    etcu_volume* vol = r->vol;
+    etcu_context* ctx = r->ctx;
+    const uint32_t N = r->n_input;
+    if (!ctx->fused_step || r->persp || vol->slabs.size() != 1 || r->block != 1 || r->order.size() < 2) return ETCU_OK;
+    if (vol->type != ETCU_VOXEL_FLOAT32 || vol->mask || r->params.sampling != ETCU_SAMPLING_Q8) return ETCU_OK;
+    if (r->params.fp_samples > 1 || r->params.bp_samples != 1 || r->hsamples.size() < N) return ETCU_OK;
+    const SlabConst& g = vol->slabs[0];
+    if (g.rx % 2 != 0 || g.rx > 2 * kFuseThreads || g.rx + g.rz - 1 > kMaxDdaIterations) return ETCU_OK;
+    std::vector<int> x0lo(N), ntaps(N);
+    size_t smem = 0;
+    for (uint32_t v = 0; v < N; ++v) {
+        const ViewConst& c = vc[v];
+        if (!c.fast2d || !row_constant(c) || c.hpitch.y != 0.f) return ETCU_OK;
+        BpColPlan plan;
+        if (!plan_bp_col(vol, g, c, r->hsamples[v], plan)) return ETCU_OK;
+        x0lo[v] = plan.x0lo;
+        ntaps[v] = plan.ntaps;
+        smem = std::max(smem, fuse_smem_bytes(g.rx, g.rz, plan.ntaps));
+    }
+    int per_sm = 0;
+    fuse_limits(ctx->device, smem, per_sm);
+    if (per_sm < 1) return ETCU_OK;
+    // detector rows of every (view, volume row)
+    const size_t T = (size_t)N * (size_t)g.ry;
+    int *jb = nullptr, *je = nullptr;
+    etcu_status s;
+    if ((s = dalloc(ctx, (void**)&jb, T * sizeof(int))) != ETCU_OK) return s;
+    if ((s = dalloc(ctx, (void**)&je, T * sizeof(int))) != ETCU_OK) {
+        dfree(ctx, jb, T * sizeof(int));
+        return s;
+    }
+    std::vector<int> hb(T), he(T);
+    cudaMemsetAsync(jb, 0x7f, T * sizeof(int), ctx->stream);
+    cudaMemsetAsync(je, 0, T * sizeof(int), ctx->stream);
+    fuse_rows_kernel<<<dim3((r->H + 127) / 128, N), 128, 0, ctx->stream>>>(r->d_views, g, (int)r->H, jb, je);
+    cudaMemcpyAsync(hb.data(), jb, T * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+    cudaMemcpyAsync(he.data(), je, T * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+    const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    dfree(ctx, jb, T * sizeof(int));
+    dfree(ctx, je, T * sizeof(int));
+    CK(ctx, e);
+    std::vector<int2> table(T);
+    for (size_t i = 0; i < T; ++i) {
+        const int b = hb[i], n = he[i] > b ? he[i] - b : 0;
+        if ((long long)n * r->W > (long long)kFuseRays * kFuseThreads) return ETCU_OK;
+        table[i] = make_int2(n ? b : 0, n ? he[i] : 0);
+    }
+    if ((s = dalloc(ctx, (void**)&r->d_jrange, T * sizeof(int2))) != ETCU_OK) return s;
+    CK(ctx, cudaMemcpyAsync(r->d_jrange, table.data(), T * sizeof(int2), cudaMemcpyHostToDevice, ctx->stream));
+    r->fuse_x0lo = std::move(x0lo);
+    r->fuse_ntaps = std::move(ntaps);
+    r->fuse_smem = smem;
+    ok = true;
+    return ETCU_OK;
+}
+
 // One iteration (BlockIterativeReconstructionOperator.cpp:92-103).
 etcu_status issue_iteration(etcu_recon* r, cudaStream_t st, uint32_t* launches) {
     etcu_context* ctx = r->ctx;
     const uint32_t M = (uint32_t)r->order.size();
     uint32_t n = 0;
     CK(ctx, cudaMemsetAsync(r->d_resid, 0, sizeof(double), st));
+    if (r->fused) {
+        n = issue_fused_iteration(r, st);
+        CKL(ctx);
+        if (launches) *launches = n;
+        return ETCU_OK;
+    }
     for (uint32_t b = 0; b < r->nblocks; ++b) {
         const uint32_t first = b * r->block;
         const uint32_t bs = (b < r->nblocks - 1) ? r->block : M - first;  // BlockIterativeProjectionAccess.cpp:55-70
@@ -1190,6 +1335,12 @@ etcu_status recon_build(etcu_volume* vol, const etcu_view* views, uint32_t n_vie
     } else {
         r->nsamples = 0;
     }
+    {
+        bool fused = false;
+        if ((s = plan_fused(r.get(), vc, fused)) != ETCU_OK) return s;
+        r->fused = fused;
+        if (fused) r->slots = std::max<uint32_t>(r->slots, 2);  // the fused steps alternate two images
+    }
     // per-slot interleaved (residual, length) images, padded by kPad zero texels, and
     // their textures (texture-unit sampling mode)
     const size_t pw = (size_t)W + 2 * kPad, ph = (size_t)H + 2 * kPad;
@@ -1229,7 +1380,7 @@ etcu_status recon_build(etcu_volume* vol, const etcu_view* views, uint32_t n_vie
         CK(ctx, cudaGraphInstantiate(&r->exec, g, 0));
         r->launches = n;
     } else {
-        r->launches = (uint32_t)(2 * S * r->nblocks);
+        r->launches = r->fused ? M + 1 : (uint32_t)(2 * S * r->nblocks);
     }
     *out = r.release();
     return ETCU_OK;
@@ -1338,6 +1489,51 @@ extern "C" etcu_status etcu_recon_profile_iteration(etcu_recon* r, float* fp_ms,
     *bp_ms = tb;
     *fp_n = nf;
     *bp_n = nb;
+    return ETCU_OK;
+}
+
+// Runs one iteration as issue_iteration does, timing every step: kind 0 forward
+// projection, 1 back projection, 2 fused step; launches per step.
+extern "C" etcu_status etcu_recon_profile_steps(etcu_recon* r, float* ms, uint32_t* kinds, uint32_t* launches,
+                                                uint32_t capacity, uint32_t* count) {
+    if (!r || !count) return fail(r ? r->ctx : nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    etcu_context* ctx = r->ctx;
+    cudaStream_t st = ctx->stream;
+    const uint32_t M = (uint32_t)r->order.size();
+    const uint32_t steps = r->fused ? M + 1 : 2 * r->nblocks;
+    *count = steps;
+    if (!ms || !kinds || !launches) return ETCU_OK;
+    if (capacity < steps) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "capacity %u < %u steps", capacity, steps);
+    std::vector<cudaEvent_t> ev(steps + 1);
+    for (auto& e : ev) CK(ctx, cudaEventCreate(&e));
+    CK(ctx, cudaMemsetAsync(r->d_resid, 0, sizeof(double), st));
+    uint32_t k = 0;
+    auto mark = [&](uint32_t kind, uint32_t n) {
+        kinds[k] = kind;
+        launches[k] = n;
+        cudaEventRecord(ev[++k], st);
+    };
+    cudaEventRecord(ev[0], st);
+    if (r->fused) {
+        mark(0, issue_forward(r, 0, 1, st));
+        for (uint32_t p = 0; p + 1 < M; ++p) {
+            launch_fused_step(r, p, st);
+            mark(2, 1);
+        }
+        const uint32_t last = M - 1;
+        mark(1, issue_backward(r, last, 1, st, r->rl + (size_t)(last & 1) * r->rl_slot));
+    } else {
+        for (uint32_t b = 0; b < r->nblocks; ++b) {
+            const uint32_t first = b * r->block;
+            const uint32_t bs = (b < r->nblocks - 1) ? r->block : M - first;
+            mark(0, issue_forward(r, first, bs, st));
+            mark(1, issue_backward(r, first, bs, st));
+        }
+    }
+    CKL(ctx);
+    CK(ctx, cudaStreamSynchronize(st));
+    for (uint32_t i = 0; i < steps; ++i) cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]);
+    for (auto& e : ev) cudaEventDestroy(e);
     return ETCU_OK;
 }
 

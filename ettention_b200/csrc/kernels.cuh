@@ -996,6 +996,9 @@ __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
 }
+__device__ __forceinline__ void cp_async8(uint32_t dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -1153,6 +1156,299 @@ __global__ void __launch_bounds__(kBpColThreads, 4) bp_sart_column_kernel(const 
         }
     }
     cp_async_wait<0>();
+}
+
+// ---- fused SART step: back projection of one view, forward projection of the next ----
+// SART alternates BP(view p) and FP(view p + 1) (BlockIterativeReconstructionOperator.cpp:
+// 92-142 with blockSize 1).  For parallel views tilted about y both touch one xz plane
+// of the volume per volume row y: the BP of row y reads only the detector rows its
+// voxels project to, and every ray of the next view stays in the volume row its
+// detector row maps to.  One block owns a volume row and streams it once, z chunk by
+// z chunk through shared memory: it applies the BP update of view p to the chunk
+// (as bp_sart_column_kernel: same tap window, same arithmetic), writes the chunk
+// back, and advances the rays of view p + 1 that lie in the row through the updated
+// chunk.  Chunks are taken in the direction the rays travel in z, and each ray
+// keeps its walk state (voxel, remaining distances, sums) between chunks, so its
+// steps and its sums are those of dda_walk_xz in the same order.  After the last
+// chunk the block writes the (residual, length) pairs of its rays, as fp_store does
+// for one sample and one sub-volume.  The volume then crosses HBM once per view
+// (read + write) instead of twice for the BP and once more for the FP.
+constexpr int kFuseThreads = 512;
+constexpr int kFuseZc = 8;    // z rows per chunk
+constexpr int kFuseRays = 2;  // detector pixels per thread: at most 1024 rays per volume row
+
+struct FuseArgs {
+    float* vol;                 // FP32 volume, x-fastest [z][y][x], one sub-volume
+    SlabConst slab;
+    const ViewConst* views;     // by view id
+    const uint32_t* order;
+    uint32_t p;                 // order position of the back-projected view; p + 1 is projected
+    const float4* samples;      // one (x, y, z, chord) per view id
+    const float2* rl_in;        // texel (0, 0) of view p's padded (residual, length) image
+    float2* rl_out;             // texel (0, 0) of view p + 1's image
+    size_t rl_pitch;            // float2 units
+    int W, H;
+    float lambda;
+    int x0lo, ntaps;            // view p's tap window (plan_bp_col)
+    const int2* jrange;         // [view id * ry + y]: detector rows [x, y) whose rays lie in volume row y
+    const float* real;          // measured projections, view id * W * H
+    double* resid_sq;           // sum of residual^2 (FP64), or nullptr
+    int loc;                    // long-object compensation
+};
+
+__host__ __device__ constexpr size_t fuse_smem_bytes(int rx, int rz, int ntaps) {
+    return (size_t)bp_col_tap_slots(ntaps) * 16 + ((size_t)rz * 4 + 15) / 16 * 16 + 2 * (size_t)kFuseZc * rx * 4;
+}
+
+// Each thread owns two consecutive x voxels of the row and two rays.  Requires
+// rx % 2 == 0, rx <= 2 * kFuseThreads, rx + rz - 1 <= kMaxDdaIterations (the walk cap is
+// never reached), at most kFuseRays * kFuseThreads rays per volume row.
+__global__ void __launch_bounds__(kFuseThreads, 2) sart_fused_kernel(const __grid_constant__ FuseArgs a) {
+    extern __shared__ __align__(16) unsigned char fuse_smem[];
+    const SlabConst& g = a.slab;
+    const int rx = g.rx, ry = g.ry, rz = g.rz, tid = threadIdx.x;
+    const int y = blockIdx.x;
+    float4* taps = (float4*)fuse_smem;
+    float* K = (float*)(taps + bp_col_tap_slots(a.ntaps));
+    float* buf = (float*)(fuse_smem + (size_t)bp_col_tap_slots(a.ntaps) * 16 + ((size_t)rz * 4 + 15) / 16 * 16);
+    const size_t chunk_elems = (size_t)kFuseZc * rx;
+
+    // ---- back projection constants of view p (bp_sart_column_kernel, one item = row y)
+    const uint32_t vb = a.order[a.p];
+    const ViewConst& vc = a.views[vb];
+    const float4 s = a.samples[vb];
+    for (int z = tid; z < rz; z += kFuseThreads)
+        K[z] = fmul(vc.mat[8], fadd(fadd(g.bmin.z, fmul(fadd((float)z, 0.5f), g.vs.z)), s.z));
+    const int x2 = 2 * tid;
+    const bool on = x2 < rx;
+    float A[2];
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+        A[j] = fmul(vc.mat[0], fadd(fadd(g.bmin.x, fmul(fadd((float)(x2 + j), 0.5f), g.vs.x)), s.x));
+    const float lamd = fmul(a.lambda, s.w);
+    const float2 m12 = splat(vc.mat[12]);
+    const float px0 = fadd(fadd(g.bmin.x, fmul(0.5f, g.vs.x)), s.x);
+    {
+        const float py = fadd(fadd(g.bmin.y, fmul(fadd((float)y, 0.5f), g.vs.y)), s.y);
+        const float av = fadd(fmul(vc.mat[1], px0), fmul(vc.mat[5], py));
+        int y0;
+        float b;
+        split_coord<kSampleQ8>(fadd(av, vc.mat[13]), a.H, y0, b);
+        const float omb = fsub(1.f, b);
+        const float2* r0 = a.rl_in + (ptrdiff_t)y0 * (ptrdiff_t)a.rl_pitch;
+        const float2* r1 = r0 + a.rl_pitch;
+        const float2 zero = make_float2(0.f, 0.f);
+        for (int e = tid; e < a.ntaps; e += kFuseThreads) {
+            const int x0 = a.x0lo + e;
+            const bool in0 = x0 >= -kPad && x0 < a.W + kPad, in1 = x0 + 1 >= -kPad && x0 + 1 < a.W + kPad;
+            const float2 p0 = in0 ? __ldg(r0 + x0) : zero, q0 = in1 ? __ldg(r0 + x0 + 1) : zero;
+            const float2 p1 = in0 ? __ldg(r1 + x0) : zero, q1 = in1 ? __ldg(r1 + x0 + 1) : zero;
+            const float2 P0 = make_float2(fadd(fmul(omb, p0.x), fmul(b, p1.x)), fadd(fmul(omb, p0.y), fmul(b, p1.y)));
+            const float2 P1 = make_float2(fadd(fmul(omb, q0.x), fmul(b, q1.x)), fadd(fmul(omb, q0.y), fmul(b, q1.y)));
+            taps[e + (e >> 3)] = make_float4(fmul(P0.x, lamd), P0.y, fmul(fsub(P1.x, P0.x), lamd), fsub(P1.y, P0.y));
+        }
+        const float cy4 = fmul(vc.mat[4], py);
+        A[0] = fadd(A[0], cy4);
+        A[1] = fadd(A[1], cy4);
+    }
+    const float2 au = f2(A[0], A[1]);
+
+    // ---- rays of view p + 1 in volume row y (fp_pixel with one sample, dda_setup)
+    const uint32_t vf = a.order[a.p + 1];
+    const ViewConst& fc = a.views[vf];
+    const int2 jr = a.jrange[(size_t)vf * ry + y];
+    const int nrays = jr.y > jr.x ? (jr.y - jr.x) * a.W : 0;
+    const float3 ray = make_float3(fc.ray.x, fc.ray.y, fc.ray.z);
+    const float3 inv = make_float3(fc.inv.x, fc.inv.y, fc.inv.z);
+    int rix[kFuseRays], riz[kFuseRays];
+    float rrx[kFuseRays], rrz[kFuseRays], acc[kFuseRays], accl[kFuseRays];
+    bool walking[kFuseRays];
+    // the step differences and directions are the view's (dda_setup; every ray of the
+    // view has the same direction), so the chunk order is uniform over the block
+    const float sgx = clsign(ray.x), sgz = clsign(ray.z);
+    const float sdx = fmul(fmul(g.vs.x, inv.x), sgx), sdz = fmul(fmul(g.vs.z, inv.z), sgz);
+    const int sx = (int)sgx, sz = (int)sgz;
+    {
+        const float sdist = fdiv(1.f, 1.f), off = fdiv(sdist, 2.f);
+#pragma unroll
+        for (int i = 0; i < kFuseRays; ++i) {
+            const int k = tid + i * kFuseThreads;
+            acc[i] = 0.f;
+            accl[i] = 0.f;
+            walking[i] = false;
+            rix[i] = riz[i] = 0;
+            rrx[i] = rrz[i] = 0.f;
+            if (k < nrays) {
+                const int gy = jr.x + k / a.W, gx = k - (k / a.W) * a.W;
+                const float fx = fadd(fadd((float)gx, off), fmul(sdist, 0.f));
+                const float fy = fadd(fadd((float)gy, off), fmul(sdist, 0.f));
+                const float3 src = make_float3(fadd(fadd(fc.source.x, fmul(fc.hpitch.x, fx)), fmul(fc.vpitch.x, fy)),
+                                               fadd(fadd(fc.source.y, fmul(fc.hpitch.y, fx)), fmul(fc.vpitch.y, fy)),
+                                               fadd(fadd(fc.source.z, fmul(fc.hpitch.z, fx)), fmul(fc.vpitch.z, fy)));
+                DdaStart st;
+                if (dda_setup(src, ray, inv, g, st)) {
+                    walking[i] = true;
+                    rix[i] = st.ix;
+                    riz[i] = st.iz;
+                    rrx[i] = st.res.x;
+                    rrz[i] = st.res.z;
+                }
+            }
+        }
+    }
+    const bool up = sz >= 0;
+    const int nchunks = (rz + kFuseZc - 1) / kFuseZc;
+    const size_t plane = (size_t)rx * (size_t)ry;
+
+    // chunk c (in walk order) -> its first z row
+    auto chunk_z0 = [&](int c) { return (up ? c : nchunks - 1 - c) * kFuseZc; };
+    auto fetch = [&](int c) {
+        if (c < nchunks && on) {
+            const int z0 = chunk_z0(c), z1 = min(rz, z0 + kFuseZc);
+            float* dst = buf + (size_t)(c & 1) * chunk_elems + x2;
+            const float* src = a.vol + ((size_t)z0 * ry + y) * rx + x2;
+            for (int z = z0; z < z1; ++z, dst += rx, src += plane) cp_async8(smem_addr(dst), src);
+        }
+        cp_async_commit();
+    };
+    // BP update of chunk c in place (this thread's two columns), written back to the volume
+    auto update = [&](int c) {
+        if (c >= nchunks || !on) return;
+        const int z0 = chunk_z0(c), z1 = min(rz, z0 + kFuseZc);
+        float* cb = buf + (size_t)(c & 1) * chunk_elems;
+        float* dst = a.vol + ((size_t)z0 * ry + y) * rx + x2;
+        for (int z = z0; z < z1; ++z, dst += plane) {
+            float2* slot = reinterpret_cast<float2*>(cb + (size_t)(z - z0) * rx + x2);
+            const float2 v = *slot;
+            const float vin[2] = {v.x, v.y};
+            float vout[2];
+            // u = (au + m8 * pz) + m12 and the column split, two voxels per instruction
+            const float2 u = add2(add2(au, splat(K[z])), m12);
+            const float2 f = __fadd2_rd(fma2(u, splat(256.f), splat(-127.5f)), splat(12582912.0f));
+            int e0, e1;
+            float a0, a1;
+            q8_tap_bits(f.x, a.x0lo, e0, a0);
+            q8_tap_bits(f.y, a.x0lo, e1, a1);
+            const float2 ax = add2(f2(a0, a1), splat(-1.f));
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int eq = q ? e1 : e0;
+                const float4 t = taps[eq + (eq >> 3)];
+                const float w = q ? ax.y : ax.x;
+                const float R = fmaf(w, t.z, t.x), L = fmaf(w, t.w, t.y);
+                // ParallelBeamsBackProjection.cl:40-50: v + r * lambda * d / L where L > eps
+                const float cc = fmul(R, rcp_approx(L));
+                vout[q] = L > kEps ? fadd(vin[q], cc) : vin[q];
+            }
+            const float2 o = make_float2(vout[0], vout[1]);
+            *reinterpret_cast<float2*>(dst) = o;
+            *slot = o;
+        }
+    };
+    // FP walk of the rays through the updated chunk c (dda_walk_xz's steps, chunk-local
+    // offsets): x may take nxr more steps before the ray leaves the volume, z nzr more
+    // before it leaves the chunk; blocks of 4 steps run unchecked while both budgets allow.
+    auto walk = [&](int c) {
+        const int z0 = chunk_z0(c), z1 = min(rz, z0 + kFuseZc);
+        const float* cb = buf + (size_t)(c & 1) * chunk_elems;
+        const int dzo = sz * rx;
+#pragma unroll
+        for (int i = 0; i < kFuseRays; ++i) {
+            if (!walking[i] || riz[i] < z0 || riz[i] >= z1) continue;
+            const int ix = rix[i], iz = riz[i];
+            const int nxr = sx > 0 ? rx - ix : (sx < 0 ? ix + 1 : 0x3fffffff);
+            const int nzr = sz > 0 ? z1 - iz : (sz < 0 ? iz - z0 + 1 : 0x3fffffff);
+            float rxv = rrx[i], rzv = rrz[i], av = acc[i], al = accl[i];
+            int off = (iz - z0) * rx + ix, nxs = 0, nzs = 0;
+            auto step = [&]() {
+                const float dt = fminf(rxv, rzv);
+                const bool bx = rxv <= rzv;
+                av = fmaf(dt, cb[off], av);
+                al += dt;
+                rxv = bx ? sdx : fsub(rxv, dt);
+                rzv = bx ? fsub(rzv, dt) : sdz;
+                off += bx ? sx : dzo;
+                nxs += bx ? 1 : 0;
+                nzs += bx ? 0 : 1;
+            };
+            while (min(nxr - nxs, nzr - nzs) >= 4) {
+                step();
+                step();
+                step();
+                step();
+            }
+            while (nxs < nxr && nzs < nzr) step();
+            rix[i] = ix + sx * nxs;
+            riz[i] = iz + sz * nzs;
+            // x ran out: the ray left the volume; z ran out: it continues in the next chunk
+            // unless it left the volume in z
+            walking[i] = nxs < nxr && riz[i] >= 0 && riz[i] < rz;
+            rrx[i] = rxv;
+            rrz[i] = rzv;
+            acc[i] = av;
+            accl[i] = al;
+        }
+    };
+
+    // Skewed pipeline, one barrier per chunk: while the rays walk chunk c, chunk c + 1
+    // is in flight; it is then updated in place, and the barrier publishes it (and
+    // frees chunk c's buffer for chunk c + 2).
+    fetch(0);
+    cp_async_wait<0>();
+    __syncthreads();  // K and the taps are staged
+    update(0);
+    __syncthreads();  // chunk 0 is updated
+    for (int c = 0; c < nchunks; ++c) {
+        fetch(c + 1);
+        walk(c);
+        cp_async_wait<0>();  // this thread's rows of chunk c + 1 have landed
+        update(c + 1);
+        __syncthreads();
+    }
+    cp_async_wait<0>();
+
+    // ---- epilogue of view p + 1 (fp_store, mode kFpPairResidual, one sample, one sub-volume)
+    double r2 = 0.0;
+#pragma unroll
+    for (int i = 0; i < kFuseRays; ++i) {
+        const int k = tid + i * kFuseThreads;
+        if (k < nrays) {
+            const int gy = jr.x + k / a.W, gx = k - (k / a.W) * a.W;
+            // fp_pixel sums its one sub-ray into zero, fp_store divides by the count
+            const float pv = fdiv(fadd(0.f, acc[i]), 1.f), pl = fdiv(fadd(0.f, accl[i]), 1.f);
+            float vv = fadd(0.f, pv), ll = fadd(0.f, pl);
+            if (a.loc) {
+                vv = ll > kEps ? fdiv(fmul(vv, fc.loc_length), ll) : 0.f;
+                ll = fc.loc_length;
+            }
+            const size_t pix = (size_t)gy * (size_t)a.W + (size_t)gx;
+            const float r = fsub(a.real[(size_t)vf * (size_t)a.W * (size_t)a.H + pix], vv);
+            a.rl_out[(size_t)gy * a.rl_pitch + (size_t)gx] = make_float2(r, ll);
+            r2 += (double)r * (double)r;
+        }
+    }
+    if (a.resid_sq) {
+        for (int o = 16; o > 0; o >>= 1) r2 += __shfl_down_sync(0xffffffffu, r2, o);
+        if ((tid & 31) == 0 && r2 != 0.0) atomicAdd(a.resid_sq, r2);
+    }
+}
+
+// Detector rows per volume row for the fused step: the rays of detector row j of a
+// parallel view with ray.y == 0 and hpitch.y == 0 stay in the volume row dda_setup
+// assigns them (the clamp of the source's y); jb / je receive the first and one past
+// the last detector row of every (view, volume row).
+__global__ void fuse_rows_kernel(const ViewConst* views, SlabConst g, int H, int* jb, int* je) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
+    if (j >= H) return;
+    const ViewConst& vc = views[v];
+    const float sdist = fdiv(1.f, 1.f), off = fdiv(sdist, 2.f);
+    const float fx = fadd(fadd(0.f, off), fmul(sdist, 0.f));
+    const float fy = fadd(fadd((float)j, off), fmul(sdist, 0.f));
+    const float sy = fadd(fadd(vc.source.y, fmul(vc.hpitch.y, fx)), fmul(vc.vpitch.y, fy));
+    const float py = clclamp(sy, g.bmin.y, g.bmax.y);
+    const int iy = min(max((int)fmul(fsub(py, g.bmin.y), g.ivs.y), 0), g.ry - 1);
+    atomicMin(jb + (size_t)v * g.ry + iy, j);
+    atomicMax(je + (size_t)v * g.ry + iy, j + 1);
 }
 
 // PerspectiveBeamsBackProjection.cl:10-17 getRayLengthInVoxel

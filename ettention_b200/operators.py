@@ -849,6 +849,19 @@ class BlockIterativeReconstructionOperator:
     def launches_per_iteration(self) -> int:
         return int(lib().etcu_recon_launches_per_iteration(self.handle))
 
+    def profile_steps(self):
+        """Runs one iteration as run() does, each step timed: [(kind, ms, launches)],
+        kind 'forward', 'back' or 'fused' (etcu_recon_profile_steps)."""
+        n = ctypes.c_uint32()
+        self.volume.ctx.check(lib().etcu_recon_profile_steps(self.handle, None, None, None, 0, ctypes.byref(n)))
+        ms = np.zeros(n.value, np.float32)
+        kinds = np.zeros(n.value, np.uint32)
+        launches = np.zeros(n.value, np.uint32)
+        self.volume.ctx.check(lib().etcu_recon_profile_steps(self.handle, ms.ctypes.data, kinds.ctypes.data,
+                                                             launches.ctypes.data, n.value, ctypes.byref(n)))
+        names = ("forward", "back", "fused")
+        return [(names[int(k)], float(t), int(l)) for k, t, l in zip(kinds, ms, launches)]
+
     def profile_iteration(self):
         """Runs one iteration with per-launch CUDA events: (fp_ms, bp_ms, fp_launches, bp_launches)."""
         f, b = ctypes.c_float(), ctypes.c_float()

@@ -225,6 +225,13 @@ ETCU_API etcu_status etcu_recon_view_order(const etcu_recon* rec, uint32_t* out,
  * LR/gpu/opencl/CLAbstractionLayer.cpp:295-324.) */
 ETCU_API etcu_status etcu_recon_profile_iteration(etcu_recon* rec, float* fp_ms, float* bp_ms, uint32_t* fp_launches,
                                                   uint32_t* bp_launches);
+/* One iteration as etcu_recon_run issues it, each step timed with CUDA events on the
+ * context's stream: kinds[i] = 0 forward projection, 1 back projection, 2 fused SART
+ * step (back projection of one view and forward projection of the next in one pass);
+ * launches[i] = kernel launches of the step.  *count = the number of steps; with NULL
+ * arrays only the count is returned. */
+ETCU_API etcu_status etcu_recon_profile_steps(etcu_recon* rec, float* ms, uint32_t* kinds, uint32_t* launches,
+                                              uint32_t capacity, uint32_t* count);
 /* Kernel launches one iteration issues (graph nodes when captured). */
 ETCU_API uint32_t etcu_recon_launches_per_iteration(const etcu_recon* rec);
 
