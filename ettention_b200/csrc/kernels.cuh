@@ -1291,7 +1291,7 @@ __global__ void __launch_bounds__(kFuseThreads, 2) sart_fused_kernel(const __gri
                     rix[i] = st.ix;
                     riz[i] = st.iz;
                     rrx[i] = st.res.x;
-                    rrz[i] = st.res.z;
+                    rrz[i] = -st.res.z;  // kept negated by the walk
                 }
             }
         }
@@ -1335,10 +1335,10 @@ __global__ void __launch_bounds__(kFuseThreads, 2) sart_fused_kernel(const __gri
                 const int eq = q ? e1 : e0;
                 const float4 t = taps[eq + (eq >> 3)];
                 const float w = q ? ax.y : ax.x;
-                const float R = fmaf(w, t.z, t.x), L = fmaf(w, t.w, t.y);
+                const float2 RL = fma2(splat(w), f2(t.z, t.w), f2(t.x, t.y));  // (R, L), one fma each
                 // ParallelBeamsBackProjection.cl:40-50: v + r * lambda * d / L where L > eps
-                const float cc = fmul(R, rcp_approx(L));
-                vout[q] = L > kEps ? fadd(vin[q], cc) : vin[q];
+                const float cc = fmul(RL.x, rcp_approx(RL.y));
+                vout[q] = RL.y > kEps ? fadd(vin[q], cc) : vin[q];
             }
             const float2 o = make_float2(vout[0], vout[1]);
             *reinterpret_cast<float2*>(dst) = o;
@@ -1346,45 +1346,54 @@ __global__ void __launch_bounds__(kFuseThreads, 2) sart_fused_kernel(const __gri
         }
     };
     // FP walk of the rays through the updated chunk c (dda_walk_xz's steps, chunk-local
-    // offsets): x may take nxr more steps before the ray leaves the volume, z nzr more
-    // before it leaves the chunk; blocks of 4 steps run unchecked while both budgets allow.
+    // byte offsets): x may take nxr more steps before the ray leaves the volume, z nzr
+    // more before it leaves the chunk; blocks of 4 steps run unchecked while both
+    // budgets allow.  The remaining z distance is kept negated (nz = -rz): s = rx + nz
+    // is fsub(rx, rz), whose sign decides the axis (rx <= rz iff s <= 0) and which is
+    // the new remaining distance of the axis that did not step (rx - rz, or
+    // -(rz - rx)); dt = min(rx, -nz).  Same values as dda_walk_xz's updates.
+    const float nsdz = -sdz;
     auto walk = [&](int c) {
         const int z0 = chunk_z0(c), z1 = min(rz, z0 + kFuseZc);
-        const float* cb = buf + (size_t)(c & 1) * chunk_elems;
-        const int dzo = sz * rx;
+        const unsigned char* cb = (const unsigned char*)(buf + (size_t)(c & 1) * chunk_elems);
+        const int dxo = 4 * sx, dzo = 4 * sz * rx;
 #pragma unroll
         for (int i = 0; i < kFuseRays; ++i) {
             if (!walking[i] || riz[i] < z0 || riz[i] >= z1) continue;
             const int ix = rix[i], iz = riz[i];
             const int nxr = sx > 0 ? rx - ix : (sx < 0 ? ix + 1 : 0x3fffffff);
             const int nzr = sz > 0 ? z1 - iz : (sz < 0 ? iz - z0 + 1 : 0x3fffffff);
-            float rxv = rrx[i], rzv = rrz[i], av = acc[i], al = accl[i];
-            int off = (iz - z0) * rx + ix, nxs = 0, nzs = 0;
+            float rxv = rrx[i], nzv = rrz[i], av = acc[i], al = accl[i];
+            int off = 4 * ((iz - z0) * rx + ix), nxs = 0, n = 0;
             auto step = [&]() {
-                const float dt = fminf(rxv, rzv);
-                const bool bx = rxv <= rzv;
-                av = fmaf(dt, cb[off], av);
+                const float sdiff = rxv + nzv;
+                const bool bx = sdiff <= 0.f;
+                const float dt = fminf(rxv, -nzv);
+                av = fmaf(dt, *(const float*)(cb + off), av);
                 al += dt;
-                rxv = bx ? sdx : fsub(rxv, dt);
-                rzv = bx ? fsub(rzv, dt) : sdz;
-                off += bx ? sx : dzo;
+                rxv = bx ? sdx : sdiff;
+                nzv = bx ? sdiff : nsdz;
+                off += bx ? dxo : dzo;
                 nxs += bx ? 1 : 0;
-                nzs += bx ? 0 : 1;
             };
-            while (min(nxr - nxs, nzr - nzs) >= 4) {
+            while (min(nxr - nxs, nzr - (n - nxs)) >= 4) {
                 step();
                 step();
                 step();
                 step();
+                n += 4;
             }
-            while (nxs < nxr && nzs < nzr) step();
+            while (nxs < nxr && n - nxs < nzr) {
+                step();
+                ++n;
+            }
             rix[i] = ix + sx * nxs;
-            riz[i] = iz + sz * nzs;
+            riz[i] = iz + sz * (n - nxs);
             // x ran out: the ray left the volume; z ran out: it continues in the next chunk
             // unless it left the volume in z
             walking[i] = nxs < nxr && riz[i] >= 0 && riz[i] < rz;
             rrx[i] = rxv;
-            rrz[i] = rzv;
+            rrz[i] = nzv;
             acc[i] = av;
             accl[i] = al;
         }
