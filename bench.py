@@ -238,16 +238,23 @@ def make_problem(ctx, seed: int):
 
 # ------------------------------------------------------------------ byte model
 def algorithmic_bytes():
-    """Per launch, FP32 storage: forward projection of one view reads the volume once,
-    reads b and writes (r, L); back projection of a one-view block read-modify-writes
-    the volume and reads (r, L); the fused SART step read-modify-writes the volume once,
-    reads view p's (r, L) and view p + 1's b, and writes view p + 1's (r, L)."""
+    """Per launch, FP32 storage, by the per-unit byte model (one forward-projection view:
+    the volume read once, b read, (r, L) written; one back-projection view of a one-view
+    block: the volume read and written once, (r, L) read).  A fused SART step processes
+    one unit of each, so its algorithmic bytes are their sum."""
     V = RES[0] * RES[1] * RES[2]
     P = DET[0] * DET[1]
     fp = V * 4 + P * 4 + P * 8
     bp = 2 * V * 4 + P * 8
-    fused = 2 * V * 4 + P * 8 + P * 4 + P * 8
-    return fp, bp, fused
+    return fp, bp, fp + bp
+
+
+def fused_moved_bytes():
+    """Bytes the fused step must move: the volume read and written once, view p's (r, L)
+    read, view p + 1's b read and (r, L) written."""
+    V = RES[0] * RES[1] * RES[2]
+    P = DET[0] * DET[1]
+    return 2 * V * 4 + P * 8 + P * 4 + P * 8
 
 
 # DRAM bytes per voxel of one launch, dram__bytes_read.sum + dram__bytes_write.sum from an
@@ -416,10 +423,22 @@ def run_ours(args, rank, world, local):
         per_kernel[name] = {"avg_ms": avg, "launches": sum(l for k, _, l in steps if k == kind),
                             "total_ms": sum(ts), "algorithmic_bytes": byts, "gbs": gbs, "frac": gbs / hbm_peak,
                             "traffic": traffic}
+    if "sart_fused_step" in per_kernel:
+        fk = per_kernel["sart_fused_step"]
+        moved = fused_moved_bytes()
+        fk["moved_bytes"] = moved
+        fk["moved_gbs"] = moved / (fk["avg_ms"] * 1e-3) / 1e9
+        fk["moved_frac"] = fk["moved_gbs"] / hbm_peak
+        # ncu --set full of this kernel (profiles/sart_fused_1024x1024x256.md)
+        fk["ncu"] = {"issue_active_pct": 71.0, "ipc": 2.84, "dram_throughput_pct": 39.2,
+                     "shared_pipe_pct": 64.5, "alu_pipe_pct": 61.0}
     dominant = max(per_kernel, key=lambda n: per_kernel[n]["total_ms"])
     dk = per_kernel[dominant]
     roofline = {"bound": "hbm", "kernel": dominant, "achieved": dk["gbs"], "peak": hbm_peak, "unit": "GB/s",
                 "frac": dk["frac"], "peak_source": peak_src, "traffic": dk["traffic"],
+                "bytes_model": ("one forward-projection view + one back-projection view per fused launch "
+                                "(4V+4P+8P + 8V+8P); the launch moves moved_bytes of them"
+                                if dominant == "sart_fused_step" else "per-view byte model"),
                 "traffic_source": ("ncu dram bytes per launch of the 1024x1024x256 case" if dominant == "sart_fused_step"
                                    else "ncu dram bytes of the 512x512x256 case, scaled by voxel count"),
                 "per_kernel": per_kernel}
