@@ -136,6 +136,8 @@ _SIG = {
     "etcu_image_stack_write_metadata": (_S, [ctypes.c_char_p, _P, ctypes.POINTER(ctypes.c_char_p), _U,
                                              ctypes.POINTER(View), _P]),
     "etcu_xml_config_read": (_S, [ctypes.c_char_p, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+    "etcu_wbp": (_S, [_P, ctypes.POINTER(View), _U, _P, _F, _U, _I]),
+    "etcu_wbp_filter": (_S, [_P, _P, _P, _U, _U, _U]),
     "etcu_batch_create": (_S, [_P, ctypes.POINTER(BatchSeries), _U, ctypes.POINTER(ReconParams), ctypes.POINTER(_P)]),
     "etcu_batch_destroy": (_S, [_P]),
     "etcu_batch_run": (_S, [_P, _U]),

@@ -1537,6 +1537,165 @@ extern "C" etcu_status etcu_recon_profile_steps(etcu_recon* r, float* ms, uint32
     return ETCU_OK;
 }
 
+// ================================================================ weighted back projection
+namespace {
+
+// GenerateRamLakKernel.cl: taps at positions gid - fres / 2 in float arithmetic; the
+// nonzero ones (position 0 and the odd positions) with their positions.
+void ramlak_taps(uint32_t fres, std::vector<float>& taps, std::vector<int>& pos) {
+    const float pi_f = 3.14159274101257324f;  // M_PI_F
+    const float pi2 = pi_f * pi_f;
+    taps.clear();
+    pos.clear();
+    for (uint32_t gid = 0; gid < fres; ++gid) {
+        const int p = (int)gid - (int)(fres / 2);
+        float v;
+        if (p == 0) v = 1.0f / 4.0f;
+        else if (p % 2 == 0) v = 0.0f;
+        else v = -1.0f / ((float)(p * p) * pi2);
+        if (v != 0.0f) {
+            taps.push_back(v);
+            pos.push_back(p);
+        }
+    }
+}
+
+uint32_t next_pow2(uint32_t v) {  // NumericalAlgorithms::nearestPowerOfTwo
+    v--;
+    v |= v >> 1;
+    v |= v >> 2;
+    v |= v >> 4;
+    v |= v >> 8;
+    v |= v >> 16;
+    return v + 1;
+}
+
+// PaddingForFFT.cl mirrors at most (nu - n) / 2 pixels into the image on each side; for a
+// narrower image the reference reads outside its buffer.
+bool wbp_padding_fits(uint32_t n, uint32_t nu) {
+    const long long b = ((long long)nu - n) / 2, e = ((long long)nu + n) / 2;
+    return b <= (long long)n - 1 && (long long)n + e - 1 - ((long long)nu - 1) >= 0;
+}
+
+struct WbpFilter {
+    float* taps = nullptr;
+    int* pos = nullptr;
+    int ntaps = 0;
+    etcu_context* ctx = nullptr;
+    ~WbpFilter() {
+        if (ctx) {
+            dfree(ctx, taps, ntaps * sizeof(float));
+            dfree(ctx, pos, ntaps * sizeof(int));
+        }
+    }
+    etcu_status init(etcu_context* c, uint32_t fres) {
+        ctx = c;
+        // rows of up to 16384 padded pixels: 64 KB of shared memory
+        CK(ctx, cudaFuncSetAttribute(wbp_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 16384 * 4));
+        std::vector<float> t;
+        std::vector<int> p;
+        ramlak_taps(fres, t, p);
+        ntaps = (int)t.size();
+        etcu_status s;
+        if ((s = dalloc(ctx, (void**)&taps, t.size() * sizeof(float))) != ETCU_OK) return s;
+        if ((s = dalloc(ctx, (void**)&pos, p.size() * sizeof(int))) != ETCU_OK) return s;
+        CK(ctx, cudaMemcpyAsync(taps, t.data(), t.size() * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+        CK(ctx, cudaMemcpyAsync(pos, p.data(), p.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+        return ETCU_OK;
+    }
+    void launch(WbpArgs a, uint32_t fres, cudaStream_t st) const {
+        a.Wu = (int)next_pow2(std::max<uint32_t>((uint32_t)a.W, fres));
+        a.Hu = (int)next_pow2((uint32_t)a.H);
+        a.ntaps = ntaps;
+        a.taps = taps;
+        a.tap_pos = pos;
+        wbp_filter_kernel<<<a.H, 256, (size_t)a.Wu * sizeof(float), st>>>(a);
+    }
+};
+
+}  // namespace
+
+extern "C" etcu_status etcu_wbp_filter(etcu_context* ctx, const float* d_in, float* d_out, uint32_t width,
+                                       uint32_t height, uint32_t filter_width) {
+    if (!ctx || !d_in || !d_out) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (width == 0 || height == 0 || filter_width == 0)
+        return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "empty image or filter");
+    if (next_pow2(std::max(width, filter_width)) > 16384)
+        return fail(ctx, ETCU_ERR_UNSUPPORTED, "images up to 16384 pixels wide are filtered");
+    if (!wbp_padding_fits(width, next_pow2(std::max(width, filter_width))) ||
+        !wbp_padding_fits(height, next_pow2(height)))
+        return fail(ctx, ETCU_ERR_UNSUPPORTED, "a %u x %u image is too small for the mirrored padding to %u x %u",
+                    width, height, next_pow2(std::max(width, filter_width)), next_pow2(height));
+    WbpFilter f;
+    etcu_status s;
+    if ((s = f.init(ctx, filter_width)) != ETCU_OK) return s;
+    WbpArgs a{};
+    a.proj = d_in;
+    a.out_f = d_out;
+    a.W = (int)width;
+    a.H = (int)height;
+    f.launch(a, filter_width, ctx->stream);
+    CKL(ctx);
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    return ETCU_OK;
+}
+
+// WBP::WBP + WBP::runNiterations (WBPPlugin/src/reconstruction/WBP.cpp:22-86): every
+// projection filtered, its ray lengths through the complete volume computed, and all
+// views back projected with lambda / n_views (the operator's block size is the number
+// of projections), in view order.
+extern "C" etcu_status etcu_wbp(etcu_volume* vol, const etcu_view* views, uint32_t n_views,
+                                const float* host_projections, float lambda, uint32_t bp_samples,
+                                etcu_sampling sampling) {
+    etcu_context* ctx = vol ? vol->ctx : nullptr;
+    if (!vol || !views || !host_projections || n_views == 0)
+        return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "NULL argument or no projections");
+    for (uint32_t i = 0; i < n_views; ++i)
+        if (views[i].perspective)
+            return fail(ctx, ETCU_ERR_UNSUPPORTED, "WBP uses a parallel scanner geometry");
+    const uint32_t fres = 128;  // WBP.cpp:40 filterSize
+    if (next_pow2(std::max(views[0].width, fres)) > 16384)
+        return fail(ctx, ETCU_ERR_UNSUPPORTED, "images up to 16384 pixels wide are filtered");
+    if (!wbp_padding_fits(views[0].width, next_pow2(std::max(views[0].width, fres))) ||
+        !wbp_padding_fits(views[0].height, next_pow2(views[0].height)))
+        return fail(ctx, ETCU_ERR_UNSUPPORTED, "a %u x %u projection is too small for the mirrored padding",
+                    views[0].width, views[0].height);
+    etcu_recon_params p{};
+    p.lambda = lambda;
+    p.block_size = ETCU_BLOCK_ALL;
+    p.fp_samples = 1;
+    p.bp_samples = bp_samples;
+    p.order = ETCU_ORDER_IDENTITY;
+    p.sampling = sampling;
+    p.use_graph = 0;
+    etcu_recon* r = nullptr;
+    etcu_status s = recon_build(vol, views, n_views, host_projections, nullptr, &p, &r);
+    if (s != ETCU_OK) return s;
+    WbpFilter f;
+    if ((s = f.init(ctx, fres)) != ETCU_OK) {
+        etcu_recon_destroy(r);
+        return s;
+    }
+    const SlabConst& full = vol->slabs[0];
+    for (uint32_t v = 0; v < n_views; ++v) {
+        WbpArgs a{};
+        a.proj = r->d_proj + (size_t)v * r->W * r->H;
+        a.out = r->rl + (size_t)v * r->rl_slot;
+        a.pitch = r->rl_pitch;
+        a.W = (int)r->W;
+        a.H = (int)r->H;
+        a.vc = r->hvc[v];
+        a.g = full;  // cmin / cmax: the complete box
+        f.launch(a, fres, ctx->stream);
+    }
+    issue_backward(r, 0, n_views, ctx->stream);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    etcu_recon_destroy(r);
+    if (e != cudaSuccess) return fail(ctx, ETCU_ERR_CUDA, "weighted back projection: %s", cudaGetErrorString(e));
+    return ETCU_OK;
+}
+
 // ================================================================ batched series
 struct etcu_batch {
     etcu_context* ctx = nullptr;

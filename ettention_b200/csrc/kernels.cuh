@@ -1571,6 +1571,74 @@ __global__ void __launch_bounds__(256) bp_perspective_kernel(const __grid_consta
     }
 }
 
+// ---------------------------------------------------------------- weighted back projection
+// WBP (WBPPlugin/src/reconstruction/WBP.cpp:22-86) filters every projection with the
+// RamLak kernel of GenerateRamLakKernel.cl (fres taps, value at position p = tap -
+// fres / 2: 1/4 at 0, 0 at even p, -1 / (p^2 pi^2) at odd p) through
+// ConvolutionFourierSpaceImplementation: the projection is padded to the power-of-two
+// grid (Wu, Hu) (PaddingForFFT.cl computePaddedCopyForFourierSpace: centred, mirrored
+// at the edges), the kernel is zero-padded centred and its origin moved to (0, 0)
+// (MoveOriginToCenter.cl), the two are multiplied in Fourier space (a circular
+// convolution) and the result is cropped centred (CroppingForFFT.cl).  The kernel row
+// sits at row (Hu - 1) / 2 and is moved by Hu / 2, so for an even Hu the filtered row y
+// comes from padded row y + 1 (mod Hu).  This kernel evaluates that circular
+// convolution directly, one output row per block: the padded source row is staged in
+// shared memory and every output pixel sums the nonzero taps.  It also writes the
+// pixel's ray length through the complete volume (ComputeRayLength.cl) beside the
+// filtered value, the (residual, length) pair the back projector reads.
+struct WbpArgs {
+    const float* proj;  // H x W projection
+    float2* out;        // texel (0, 0) of the padded pair image, or nullptr:
+    float* out_f;       //   the filtered image alone, H x W
+    size_t pitch;       // float2 units
+    int W, H, Wu, Hu;
+    int ntaps;          // nonzero taps
+    const float* taps;  // device: tap values
+    const int* tap_pos; // device: tap positions p
+    ViewConst vc;
+    SlabConst g;        // complete bounding box in cmin / cmax
+};
+
+__device__ __forceinline__ int wbp_pad_index(int i, int n, int nu) {
+    const int b = (nu - n) / 2, e = (nu + n) / 2;
+    if (i >= b && i < e) return i - b;
+    return i < e ? b - i : (n + e - 1) - i;
+}
+
+__global__ void __launch_bounds__(256) wbp_filter_kernel(const __grid_constant__ WbpArgs a) {
+    extern __shared__ float wbp_row[];  // Wu floats: the padded source row
+    const int y = blockIdx.x;
+    const int yy = y + (a.Hu / 2 - a.H / 2);                          // row of the padded result
+    const int ys = a.Hu > 1 ? a.Hu - 1 : 0;                           // the kernel row after the origin move
+    const int sy = wbp_pad_index(((yy - ys) % a.Hu + a.Hu) % a.Hu, a.H, a.Hu);
+    const float* src = a.proj + (size_t)sy * a.W;
+    for (int x = threadIdx.x; x < a.Wu; x += blockDim.x) wbp_row[x] = src[wbp_pad_index(x, a.W, a.Wu)];
+    __syncthreads();
+    const int cx = a.Wu / 2 - a.W / 2;
+    for (int x = threadIdx.x; x < a.W; x += blockDim.x) {
+        const int xx = x + cx;
+        float acc = 0.f;
+        for (int k = 0; k < a.ntaps; ++k) {
+            const int xs = ((xx - a.tap_pos[k]) % a.Wu + a.Wu) % a.Wu;
+            acc = fmaf(a.taps[k], wbp_row[xs], acc);
+        }
+        if (!a.out) {
+            a.out_f[(size_t)y * a.W + x] = acc;
+            continue;
+        }
+        // ComputeRayLength.cl:21-33: chord of the pixel-centre ray through the complete box
+        const ViewConst& vc = a.vc;
+        const float fx = fadd((float)x, 0.5f), fy = fadd((float)y, 0.5f);
+        const float3 s = make_float3(fadd(fadd(vc.source.x, fmul(vc.hpitch.x, fx)), fmul(vc.vpitch.x, fy)),
+                                     fadd(fadd(vc.source.y, fmul(vc.hpitch.y, fx)), fmul(vc.vpitch.y, fy)),
+                                     fadd(fadd(vc.source.z, fmul(vc.hpitch.z, fx)), fmul(vc.vpitch.z, fy)));
+        float tin, tout;
+        slab_test(make_float3(a.g.cmin.x, a.g.cmin.y, a.g.cmin.z), make_float3(a.g.cmax.x, a.g.cmax.y, a.g.cmax.z), s,
+                  make_float3(vc.inv.x, vc.inv.y, vc.inv.z), tin, tout);
+        a.out[(size_t)y * a.pitch + x] = make_float2(acc, fmaxf(fsub(tout, tin), 0.f));
+    }
+}
+
 // ---------------------------------------------------------------- small kernels
 __global__ void compare_kernel(const float* real, const float* virt, float* res, size_t n) {
     size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;

@@ -384,7 +384,7 @@ def reconstruct_from_config(config, device: int = 0, write_output: bool = True) 
     volume.initFileOrientation, XZY by default; BlockIterativeConfiguration.cpp:36-40,
     :155-198) and priorknowledge.maskVolumeFilename (MRC read in file order, values
     cast to 8 bits; :46-50), the iterations of BlockIterativeReconstructionOperator
-    on the GPU, and Framework::writeFinalVolume to output.filename (float32 MRC,
+    on the GPU (or, for algorithm "wbp", the WBP plugin's weighted back projection), and Framework::writeFinalVolume to output.filename (float32 MRC,
     output.options.orientation xyz_order or xzy_order, XZY by default).  Returns the
     (z, y, x) volume."""
     cfg = config.config() if isinstance(config, XMLParameterSource) else dict(config)
@@ -421,9 +421,13 @@ def reconstruct_from_config(config, device: int = 0, write_output: bool = True) 
             vol.upload(init)
         if mask is not None:
             vol.set_mask(mask)
-        rec = BlockIterativeReconstructionOperator(vol, views, data, p)
-        rec.run()
-        v = rec.getReconstructedVolume()
+        if p.algorithm == "wbp":  # the WBP plugin's algorithm (WBPPlugin.cpp)
+            WBPOperator(vol, views, data, p).run()
+            v = vol.download()
+        else:
+            rec = BlockIterativeReconstructionOperator(vol, views, data, p)
+            rec.run()
+            v = rec.getReconstructedVolume()
     finally:
         ctx.close()
         if isinstance(stack, ImageStackDirectoryDatasource):
@@ -869,6 +873,35 @@ class BlockIterativeReconstructionOperator:
         self.volume.ctx.check(lib().etcu_recon_profile_iteration(self.handle, ctypes.byref(f), ctypes.byref(b),
                                                                  ctypes.byref(nf), ctypes.byref(nb)))
         return float(f.value), float(b.value), int(nf.value), int(nb.value)
+
+
+def wbp_filter(ctx: "Context", image, out, filter_width: int = 128) -> None:
+    """The WBP plugin's RamLak filtering of one device image (etcu_wbp_filter)."""
+    H, W = int(image.shape[-2]), int(image.shape[-1])
+    ctx.check(lib().etcu_wbp_filter(ctx.handle, _dptr(image), _dptr(out), W, H, int(filter_width)))
+
+
+class WBPOperator:
+    """WBP plugin (plugins/WBPPlugin/src/reconstruction/WBP.cpp): every projection
+    RamLak-filtered, back projected with its ray lengths and lambda / N; ``run`` adds
+    the weighted back projection of all views to the volume."""
+
+    def __init__(self, volume: GPUMappedVolume, geometries: Sequence[ScannerGeometry], projections: np.ndarray,
+                 params: AlgebraicParameterSet):
+        self.volume = volume
+        self.params = params
+        self._views = (View * len(geometries))(*[g.to_view() for g in geometries])
+        self._host = np.ascontiguousarray(projections, np.float32)
+        if self._host.shape[0] != len(geometries):
+            raise EttentionError(_abi.ERR_INVALID_ARGUMENT, "one projection per geometry")
+
+    def run(self) -> None:
+        p = self.params
+        self.volume.ctx.check(lib().etcu_wbp(self.volume.handle, self._views, len(self._views), self._host.ctypes.data,
+                                             float(p.lam), int(p.bp_samples), int(p.sampling)))
+
+    def getReconstructedVolume(self) -> np.ndarray:
+        return self.volume.download()
 
 
 class BatchReconstructionOperator:

@@ -323,6 +323,22 @@ ETCU_API etcu_status etcu_image_stack_write_metadata(const char* path, const flo
  * (XMLParameterSource.cpp:24-35); resolving them is the caller's. */
 ETCU_API etcu_status etcu_xml_config_read(const char* path, char* out, size_t capacity, size_t* needed);
 
+/* ---------------------------------------------------------------- weighted back projection */
+/* WBP plugin (plugins/WBPPlugin/src/reconstruction/WBP.cpp:22-86): each projection is
+ * filtered with the RamLak kernel of 128 taps (ocl_src/GenerateRamLakKernel.cl) as
+ * ConvolutionFourierSpaceImplementation does it (power-of-two grid, mirrored padding,
+ * origin-moved kernel, circular convolution, centred crop; for an even grid height the
+ * filtered row y is taken from padded row y + 1), its ray lengths through the complete
+ * volume are computed (ComputeRayLength.cl), and every view is back projected into vol
+ * with lambda / n_views, in view order.  vol is not cleared first.  Parallel views only.
+ * host_projections: n_views x height x width floats. */
+ETCU_API etcu_status etcu_wbp(etcu_volume* vol, const etcu_view* views, uint32_t n_views,
+                              const float* host_projections, float lambda, uint32_t bp_samples,
+                              etcu_sampling sampling);
+/* The RamLak filtering of one device image (height x width floats) with filter_width taps. */
+ETCU_API etcu_status etcu_wbp_filter(etcu_context* ctx, const float* d_in, float* d_out, uint32_t width,
+                                     uint32_t height, uint32_t filter_width);
+
 /* ---------------------------------------------------------------- batched series */
 /* Many independent tilt series of uneven sizes reconstructed together: every SART
  * step runs one forward-projection launch and one back-projection launch over all

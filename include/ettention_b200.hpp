@@ -20,6 +20,7 @@
  *   ImageStackDirectoryDatasource,         LR/io/datasource/ImageStackDirectoryDatasource.cpp,
  *   readTiff, writeTiff                    LR/io/deserializer/ImageDeserializer.cpp, ImageSerializer.cpp
  *   XMLParameterSource                     LR/setup/parametersource/XMLParameterSource.cpp
+ *   WBP                                    plugins/WBPPlugin/src/reconstruction/WBP.cpp
  *   BatchReconstructionOperator            many series per launch (no counterpart in the reference)
  * Errors: every non-OK status of the ABI is rethrown as ettention::b200::Exception
  * (validation) or GPUException (device errors), with the library's message, as
@@ -552,6 +553,29 @@ public:
 private:
     std::string filename_;
     std::map<std::string, std::string> values_;
+};
+
+// WBP plugin (plugins/WBPPlugin/src/reconstruction/WBP.cpp): RamLak-filtered projections
+// back projected with their ray lengths and lambda / N into the volume.
+class WBP {
+public:
+    WBP(GPUMappedVolume& volume, const std::vector<ScannerGeometry>& views, const float* host_projections,
+        const AlgebraicParameterSet& p)
+        : vol_(&volume), host_(host_projections), p_(p) {
+        for (const auto& g : views) views_.push_back(g.view());
+    }
+    void run() {
+        check(etcu_wbp(vol_->handle(), views_.data(), (uint32_t)views_.size(), host_, p_.lambda, p_.bpSamples,
+                       p_.sampling),
+              vol_->framework().handle());
+    }
+    std::vector<float> getReconstructedVolume() const { return vol_->download(); }
+
+private:
+    GPUMappedVolume* vol_;
+    std::vector<etcu_view> views_;
+    const float* host_;
+    AlgebraicParameterSet p_;
 };
 
 // Many independent tilt series reconstructed together with SART (etcu_batch_*): one

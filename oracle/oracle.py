@@ -376,6 +376,72 @@ def ray_length(vg: VolumeGeometry, g: ScannerGeometry, prec: int = 32) -> np.nda
     return out
 
 
+# ----------------------------------------------------------------------------
+# Weighted back projection (plugins/WBPPlugin/src/reconstruction/WBP.cpp)
+# ----------------------------------------------------------------------------
+def ramlak_kernel(resolution: int = 128) -> np.ndarray:
+    """ocl_src/GenerateRamLakKernel.cl: value at position gid - resolution/2, float32."""
+    out = np.zeros(resolution, np.float32)
+    pi2 = np.float32(np.float32(np.pi) * np.float32(np.pi))
+    for gid in range(resolution):
+        pos = gid - resolution // 2
+        if pos == 0:
+            out[gid] = np.float32(0.25)
+        elif pos % 2 != 0:
+            out[gid] = np.float32(-1.0) / np.float32(np.float32(pos * pos) * pi2)
+    return out
+
+
+def _next_pow2(n: int) -> int:
+    """framework/NumericalAlgorithms.cpp:20-31."""
+    v = n - 1
+    for k in (1, 2, 4, 8, 16):
+        v |= v >> k
+    return v + 1
+
+
+def _pad_index(i: np.ndarray, n: int, nu: int) -> np.ndarray:
+    """ocl_src/PaddingForFFT.cl computePaddedCopyForFourierSpace, one axis."""
+    b, e = (nu - n) // 2, (nu + n) // 2
+    out = np.where((i >= b) & (i < e), i - b, np.where(i < e, b - i, (n + e - 1) - i))
+    if out.min() < 0 or out.max() >= n:  # the reference would read outside the image
+        raise ValueError(f"mirrored padding of {n} to {nu} leaves the image")
+    return out
+
+
+def wbp_filter(image: np.ndarray, filter_resolution: int = 128) -> np.ndarray:
+    """algorithm/imagemanipulation/convolution/ConvolutionFourierSpaceImplementation.cpp
+    with kernelRequiresOriginShifting (WBP.cpp:40-42): source padded (mirrored, centred)
+    to the power-of-two grid, kernel zero-padded centred (PaddingForFFT.cl) and its origin
+    moved (MoveOriginToCenter.cl), product of the FFTs, inverse FFT with 1/N, centred crop
+    (CroppingForFFT.cl).  FP64 FFT here; float32 out."""
+    img = np.asarray(image, np.float64)
+    H, W = img.shape
+    Wu, Hu = _next_pow2(max(W, filter_resolution)), _next_pow2(max(H, 1))
+    ys = _pad_index(np.arange(Hu), H, Hu)
+    xs = _pad_index(np.arange(Wu), W, Wu)
+    src = img[ys][:, xs]
+    padded = np.zeros((Hu, Wu))
+    bx, by = (Wu - filter_resolution) // 2, (Hu - 1) // 2
+    padded[by, bx:bx + filter_resolution] = ramlak_kernel(filter_resolution)
+    shifted = np.roll(np.roll(padded, -(Hu // 2), axis=0), -(Wu // 2), axis=1)
+    full = np.real(np.fft.ifft2(np.fft.fft2(src) * np.fft.fft2(shifted)))
+    cx, cy = Wu // 2 - W // 2, Hu // 2 - H // 2
+    return full[cy:cy + H, cx:cx + W].astype(np.float32)
+
+
+def wbp(projections: np.ndarray, geometries, vg: "VolumeGeometry", lam: float = 1.0, samples: int = 1,
+        prec: int = 32, weights: int = WEIGHTS_Q8, volume: Optional[np.ndarray] = None) -> np.ndarray:
+    """WBP::runNiterations (WBP.cpp:72-83): per view the filtered projection and its ray
+    lengths through the complete volume are back projected with lambda / N."""
+    X, Y, Z = vg.resolution
+    vol = np.zeros((Z, Y, X), np.float32) if volume is None else volume
+    lamb = np.float32(lam) / np.float32(len(geometries))
+    for i, g in enumerate(geometries):
+        back_project(vol, vg, g, wbp_filter(projections[i]), ray_length(vg, g, prec), lamb, samples, prec, weights)
+    return vol
+
+
 def long_object_compensation(proj: np.ndarray, length: np.ndarray, constant_length: float):
     p = np.ascontiguousarray(proj, np.float32).copy()
     l = np.ascontiguousarray(length, np.float32).copy()

@@ -87,6 +87,13 @@ int main(int argc, char** argv) {
         rec.run();
         save(dir, "sart_volume.bin", rec.getReconstructedVolume().data(), rvol.voxelCount());
         std::printf("residual %.17g\n", rec.lastResidualSq());
+        // weighted back projection of the same projections (the WBP plugin's algorithm)
+        GPUMappedVolume wvol(fw, {X, Y, Z});
+        WBP wbp(wvol, views, projs.data(),
+                AlgebraicParameterSet::fromConfig(
+                    {{"algorithm", "wbp"}, {"algorithm.numberOfIterations", "1"}, {"algorithm.lambda", "1.0"}}));
+        wbp.run();
+        save(dir, "wbp_volume.bin", wbp.getReconstructedVolume().data(), wvol.voxelCount());
         cudaFree(dv);
         cudaFree(dl);
         cudaFree(dr);

@@ -45,3 +45,5 @@ def test_cpp_shim_projectors_and_sart_match_oracle(tmp_path):
     vo = np.zeros((Z, Y, X), np.float32)
     O.block_iterative(setup, vo, 2, 32)
     assert O.rel_l2(load("sart_volume.bin", (Z, Y, X)), vo) <= 1e-3
+    vw = O.wbp(projs, [oracle_geometry(q) for q in geoms], vg)
+    assert O.rel_l2(load("wbp_volume.bin", (Z, Y, X)), vw) <= 1e-4
