@@ -1493,24 +1493,45 @@ __global__ void __launch_bounds__(256) bp_perspective_kernel(const __grid_consta
     const float cx = fadd(g.bmin.x, fmul(fadd((float)x, 0.5f), g.vs.x));
     const float cy = fadd(g.bmin.y, fmul(fadd((float)y, 0.5f), g.vs.y));
     if (n == 1) {
-        // One sample per voxel, at its centre: the column's x / y projection terms are
-        // hoisted, the perspective divide takes one refined reciprocal of w, and the
-        // chord of a ray through the voxel's centre is vs_i * |d| / |d_i| minimised over
-        // the axes (the slab test of getRayLengthInVoxel for that ray).
+        // One sample per voxel, at its centre.  The views run outermost and the thread's
+        // z voxels innermost, so every term that depends on the column and the view only
+        // is formed once: the x / y parts of the three projection rows, (dx, dy), dx^2 + dy^2
+        // and the x / y bounds of the chord.  The perspective divide takes one refined
+        // reciprocal of w, and the chord of a ray through the voxel's centre is
+        // vs_i * |d| / |d_i| minimised over the axes (the slab test of
+        // getRayLengthInVoxel for that ray).  Same operations, in the same order per voxel,
+        // as evaluating everything per voxel.
         const float px = fadd(fsub(cx, fmul(0.5f, g.vs.x)), fmul(g.vs.x, 0.5f));
         const float py = fadd(fsub(cy, fmul(0.5f, g.vs.y)), fmul(g.vs.y, 0.5f));
-        for (int j = 0; j < nzc; ++j) {
-            const size_t idx = base + (size_t)j * plane;
-            const float cz = fadd(g.bmin.z, fmul(fadd((float)(z0 + j), 0.5f), g.vs.z));
-            const float pz = fadd(fsub(cz, fmul(0.5f, g.vs.z)), fmul(g.vs.z, 0.5f));
-            float val = bp_load<kStore>(a, idx);
-            const float mw = kMask ? mask_weight(a.mask + idx) : 1.f;
-            for (int p = 0; p < a.nviews; ++p) {
-                const BpView& V = sv[p];
-                const float2* img = a.rl + (size_t)p * a.rl_slot;
-                float u = fadd(fadd(fadd(fmul(V.mu[0], px), fmul(V.mu[1], py)), fmul(V.mu[2], pz)), V.mu[3]);
-                float v = fadd(fadd(fadd(fmul(V.mv[0], px), fmul(V.mv[1], py)), fmul(V.mv[2], pz)), V.mv[3]);
-                const float w = fadd(fadd(fadd(fmul(V.mw[0], px), fmul(V.mw[1], py)), fmul(V.mw[2], pz)), V.mw[3]);
+        float val[kBpZPersp], pz[kBpZPersp], mw[kBpZPersp];
+#pragma unroll
+        for (int j = 0; j < kBpZPersp; ++j) {
+            val[j] = 0.f;
+            pz[j] = 0.f;
+            mw[j] = 1.f;
+            if (j < nzc) {
+                const size_t idx = base + (size_t)j * plane;
+                const float cz = fadd(g.bmin.z, fmul(fadd((float)(z0 + j), 0.5f), g.vs.z));
+                pz[j] = fadd(fsub(cz, fmul(0.5f, g.vs.z)), fmul(g.vs.z, 0.5f));
+                val[j] = bp_load<kStore>(a, idx);
+                if (kMask) mw[j] = mask_weight(a.mask + idx);
+            }
+        }
+        for (int p = 0; p < a.nviews; ++p) {
+            const BpView& V = sv[p];
+            const float2* img = a.rl + (size_t)p * a.rl_slot;
+            const float cu = fadd(fmul(V.mu[0], px), fmul(V.mu[1], py));
+            const float cv = fadd(fmul(V.mv[0], px), fmul(V.mv[1], py));
+            const float cw = fadd(fmul(V.mw[0], px), fmul(V.mw[1], py));
+            const float dx = fsub(px, V.src[0]), dy = fsub(py, V.src[1]);
+            const float dxy = fadd(fmul(dx, dx), fmul(dy, dy));
+            const float lxy = fminf(fmul(g.vs.x, rcp_approx(fabsf(dx))), fmul(g.vs.y, rcp_approx(fabsf(dy))));
+#pragma unroll
+            for (int j = 0; j < kBpZPersp; ++j) {
+                if (j >= nzc) continue;
+                float u = fadd(fadd(cu, fmul(V.mu[2], pz[j])), V.mu[3]);
+                float v = fadd(fadd(cv, fmul(V.mv[2], pz[j])), V.mv[3]);
+                const float w = fadd(fadd(cw, fmul(V.mw[2], pz[j])), V.mw[3]);
                 float rw = rcp_approx(w);
                 rw = fmaf(rw, fmaf(-w, rw, 1.f), rw);
                 u = fmul(u, rw);
@@ -1518,19 +1539,21 @@ __global__ void __launch_bounds__(256) bp_perspective_kernel(const __grid_consta
                 const float2 rl = sample_pair<kSampling>(img, a.rl_pitch, a.W, a.H, V.tex, u, v);
                 float value = 0.f;
                 if (rl.y >= kEps) {
-                    const float dx = fsub(px, V.src[0]), dy = fsub(py, V.src[1]), dz = fsub(pz, V.src[2]);
-                    const float nd = __fsqrt_rn(fadd(fadd(fmul(dx, dx), fmul(dy, dy)), fmul(dz, dz)));
-                    const float l = fmul(nd, fminf(fminf(fmul(g.vs.x, rcp_approx(fabsf(dx))), fmul(g.vs.y, rcp_approx(fabsf(dy)))),
-                                                   fmul(g.vs.z, rcp_approx(fabsf(dz)))));
+                    const float dz = fsub(pz[j], V.src[2]);
+                    const float nd = __fsqrt_rn(fadd(dxy, fmul(dz, dz)));
+                    const float l = fmul(nd, fminf(lxy, fmul(g.vs.z, rcp_approx(fabsf(dz)))));
                     value = fmul(fmul(rl.x, l), rcp_approx(rl.y));
                 }
-                val = fadd(val, fmul(fmul(a.lambda, value), mw));
-                if (a.use_min) val = fmaxf(a.vmin, val);
-                if (a.use_max) val = fminf(a.vmax, val);
-                if (kStore == 1) val = __half2float(__float2half_rn(val));
+                float vj = fadd(val[j], fmul(fmul(a.lambda, value), mw[j]));
+                if (a.use_min) vj = fmaxf(a.vmin, vj);
+                if (a.use_max) vj = fminf(a.vmax, vj);
+                if (kStore == 1) vj = __half2float(__float2half_rn(vj));
+                val[j] = vj;
             }
-            bp_store<kStore>(a, idx, val);
         }
+#pragma unroll
+        for (int j = 0; j < kBpZPersp; ++j)
+            if (j < nzc) bp_store<kStore>(a, base + (size_t)j * plane, val[j]);
         return;
     }
     for (int j = 0; j < nzc; ++j) {
