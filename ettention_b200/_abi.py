@@ -68,6 +68,10 @@ class ImageStackInfo(ctypes.Structure):
                 ("base", View)]
 
 
+class BlobParams(ctypes.Structure):
+    _fields_ = [("support_radius", ctypes.c_float), ("degree", ctypes.c_uint32), ("density_falloff", ctypes.c_float)]
+
+
 class BatchSeries(ctypes.Structure):
     _fields_ = [("volume", ctypes.c_void_p), ("views", ctypes.POINTER(View)), ("n_views", ctypes.c_uint32),
                 ("host_projections", ctypes.c_void_p)]
@@ -138,6 +142,20 @@ _SIG = {
     "etcu_xml_config_read": (_S, [ctypes.c_char_p, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
     "etcu_wbp": (_S, [_P, ctypes.POINTER(View), _U, _P, _F, _U, _I]),
     "etcu_wbp_filter": (_S, [_P, _P, _P, _U, _U, _U]),
+    "etcu_blob_ray_integration_samples": (_S, [ctypes.POINTER(BlobParams), _U, _P]),
+    "etcu_blob_voxelization_kernel": (_S, [ctypes.POINTER(BlobParams), _P, _U, ctypes.POINTER(_U)]),
+    "etcu_forward_project_blobs": (_S, [_P, ctypes.POINTER(View), _U, ctypes.POINTER(BlobParams), _U, _P, _P]),
+    "etcu_back_project_blobs": (_S, [_P, ctypes.POINTER(View), _U, ctypes.POINTER(BlobParams), _F, _U, _P, _P]),
+    "etcu_blob_voxelize": (_S, [_P, _P, ctypes.POINTER(BlobParams)]),
+    "etcu_blob_recon_create": (_S, [_P, ctypes.POINTER(View), _U, _P, ctypes.POINTER(ReconParams),
+                                    ctypes.POINTER(BlobParams), ctypes.POINTER(_P)]),
+    "etcu_blob_recon_create_device": (_S, [_P, ctypes.POINTER(View), _U, _P, ctypes.POINTER(ReconParams),
+                                           ctypes.POINTER(BlobParams), ctypes.POINTER(_P)]),
+    "etcu_blob_recon_run": (_S, [_P, _U]),
+    "etcu_blob_recon_last_residual_sq": (_S, [_P, ctypes.POINTER(ctypes.c_double)]),
+    "etcu_blob_recon_view_order": (_S, [_P, _P, _U, ctypes.POINTER(_U)]),
+    "etcu_blob_recon_launches_per_iteration": (_U, [_P]),
+    "etcu_blob_recon_destroy": (_S, [_P]),
     "etcu_batch_create": (_S, [_P, ctypes.POINTER(BatchSeries), _U, ctypes.POINTER(ReconParams), ctypes.POINTER(_P)]),
     "etcu_batch_destroy": (_S, [_P]),
     "etcu_batch_run": (_S, [_P, _U]),

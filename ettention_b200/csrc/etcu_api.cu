@@ -21,6 +21,7 @@
 #include "ettention_b200.h"
 #include "geometry.hpp"
 #include "kernels.cuh"
+#include "blobs.cuh"
 
 using namespace etcu;
 
@@ -1693,6 +1694,542 @@ extern "C" etcu_status etcu_wbp(etcu_volume* vol, const etcu_view* views, uint32
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     etcu_recon_destroy(r);
     if (e != cudaSuccess) return fail(ctx, ETCU_ERR_CUDA, "weighted back projection: %s", cudaGetErrorString(e));
+    return ETCU_OK;
+}
+
+// ================================================================ blob basis functions
+namespace {
+
+// model/blobs/BlobParameters.cpp: Kaiser-Bessel blob of support radius a, degree m and
+// density fall-off alpha (float members, evaluated in double).
+struct BlobP {
+    double a, alpha;
+    unsigned m;
+};
+
+double uint_pow(double base, unsigned e) {  // NumericalAlgorithms::uintPow
+    if (e == 0) return 1.0;
+    if (e == 1) return base;
+    const double f = uint_pow(base, e / 2);
+    return f * f * (e % 2 == 0 ? 1.0 : base);
+}
+
+unsigned long long factorial(unsigned n) { return n < 2 ? 1ull : (unsigned long long)n * factorial(n - 1); }
+
+// evaluateModifiedBessel: I_m(x) by 40 terms of its series (m = the degree).
+double kb_bessel(const BlobP& p, double x) {
+    double sum = 0.0, summand = uint_pow(0.5 * x, p.m) / (double)factorial(p.m);
+    for (unsigned k = 0; k < 40; ++k) {
+        sum += summand;
+        summand *= 0.25 * x * x / (double)((k + 1) * (k + p.m + 1));
+    }
+    return sum;
+}
+
+double kb_evaluate(const BlobP& p, double x) {  // BlobParameters::evaluate (Lewitt 1992)
+    if (0 <= x && x <= p.a) {
+        const double root = std::sqrt(1.0 - (x * x) / (p.a * p.a));
+        return 1.0 / kb_bessel(p, p.alpha) * uint_pow(root, p.m) * kb_bessel(p, p.alpha * root);
+    }
+    return 0.0;
+}
+
+etcu_status blob_params(etcu_context* ctx, const etcu_blob_params* in, BlobP& out) {
+    if (!in) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "NULL blob parameters");
+    if (!(in->support_radius > 0.f) || in->degree > 20)
+        return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "invalid blob parameters");
+    out.a = (double)in->support_radius;
+    out.alpha = (double)in->density_falloff;
+    out.m = in->degree;
+    return ETCU_OK;
+}
+
+// BlobRayIntegrationSampler::generateSamples: the line integral through the blob at
+// distance w = i a / (count - 1), 1000 steps.
+void blob_table(const BlobP& p, unsigned count, std::vector<float>& out) {
+    out.resize(count);
+    for (unsigned i = 0; i < count; ++i) {
+        const double w = (double)i * p.a / (double)(count - 1);
+        const double d = std::sqrt(p.a * p.a - w * w), delta = d / 1000.0;
+        double sum = 0.0;
+        for (unsigned k = 1; k <= 1000; ++k) sum += kb_evaluate(p, std::sqrt(w * w + (double)(k * k) * delta * delta));
+        out[i] = (float)(delta * (2.0 * sum + kb_evaluate(p, w)));
+    }
+}
+
+// BlobVoxelizationKernelValues::generateValues: the blob integrated over every voxel of
+// the (2 ceil(a) + 1)^3 neighbourhood with 20^3 samples, [dz][dy][dx].
+void blob_voxel_kernel(const BlobP& p, std::vector<float>& out, int& ks) {
+    const int r = (int)std::ceil((float)p.a);
+    ks = 2 * r + 1;
+    out.clear();
+    for (int dz = -r; dz <= r; ++dz)
+        for (int dy = -r; dy <= r; ++dy)
+            for (int dx = -r; dx <= r; ++dx) {
+                double val = 0.0;
+                for (int sz = 0; sz < 20; ++sz)
+                    for (int sy = 0; sy < 20; ++sy)
+                        for (int sx = 0; sx < 20; ++sx) {
+                            const double px = (double)dx - 0.5 + ((double)sx + 0.5) / 20.0;
+                            const double py = (double)dy - 0.5 + ((double)sy + 0.5) / 20.0;
+                            const double pz = (double)dz - 0.5 + ((double)sz + 0.5) / 20.0;
+                            val += kb_evaluate(p, std::sqrt(px * px + py * py + pz * pz));
+                        }
+                out.push_back((float)(val / 8000.0));
+            }
+}
+
+// framework/math/Matrix4x4.cpp in float, step by step: the blob kernels take the
+// projection matrix and its inverse as the reference forms them (cofactor inverse in
+// float), which for perspective views differs visibly from an exact inverse.
+struct FMat {
+    float v[16] = {};  // value 4 * column + row
+    float at(int c, int r) const { return v[4 * c + r]; }
+    float minor(int dc, int dr) const {
+        int c[3], r[3];
+        for (int i = 0; i < 3; ++i) {
+            c[i] = i < dc ? i : i + 1;
+            r[i] = i < dr ? i : i + 1;
+        }
+        const float t1 = at(c[1], r[1]) * at(c[2], r[2]) - at(c[1], r[2]) * at(c[2], r[1]);
+        const float t2 = at(c[1], r[0]) * at(c[2], r[2]) - at(c[1], r[2]) * at(c[2], r[0]);
+        const float t3 = at(c[1], r[0]) * at(c[2], r[1]) - at(c[1], r[1]) * at(c[2], r[0]);
+        return at(c[0], r[0]) * t1 - at(c[0], r[1]) * t2 + at(c[0], r[2]) * t3;
+    }
+    bool inverse(FMat& out) const {
+        const float det = at(0, 0) * minor(0, 0) - at(0, 1) * minor(0, 1) + at(0, 2) * minor(0, 2) -
+                          at(0, 3) * minor(0, 3);
+        if (std::fabs(det) == 0.0f) return false;
+        const float o = 1.0f / det;
+        for (int c = 0; c < 4; ++c)
+            for (int r = 0; r < 4; ++r) {
+                float x = minor(c, r) * o;
+                if ((r + c) % 2 == 1) x *= -1.0f;
+                out.v[4 * r + c] = x;
+            }
+        return true;
+    }
+};
+
+FMat fmat_cols(const float c0[4], const float c1[4], const float c2[4], const float c3[4]) {
+    FMat m;
+    const float* cs[4] = {c0, c1, c2, c3};
+    for (int c = 0; c < 4; ++c)
+        for (int r = 0; r < 4; ++r) m.v[4 * c + r] = cs[c][r];
+    return m;
+}
+
+FMat fmat_mul(const FMat& a, const FMat& b) {  // Matrix4x4.cpp multiply
+    FMat m;
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) {
+            float v = 0.0f;
+            for (int k = 0; k < 4; ++k) v += a.at(k, j) * b.at(i, k);
+            m.v[4 * i + j] = v;
+        }
+    return m;
+}
+
+// Matrix4x4::getPerspectiveProjection (Matrix4x4.cpp:376-399) in float, and its inverse.
+bool float_perspective(const etcu_view& g, FMat& w2p, FMat& p2w) {
+    float dc[3];
+    for (int i = 0; i < 3; ++i)
+        dc[i] = g.detector[i] + 0.5f * ((float)g.width * g.hpitch[i] + (float)g.height * g.vpitch[i]);
+    const float c0[4] = {g.hpitch[0], g.hpitch[1], g.hpitch[2], 0.f};
+    const float c1[4] = {g.vpitch[0], g.vpitch[1], g.vpitch[2], 0.f};
+    const float c2[4] = {dc[0] - g.source[0], dc[1] - g.source[1], dc[2] - g.source[2], 0.f};
+    const float c3[4] = {g.source[0], g.source[1], g.source[2], 1.f};
+    FMat view;
+    if (!fmat_cols(c0, c1, c2, c3).inverse(view)) return false;
+    const float zn = 1e-2f;
+    const float p0[4] = {1, 0, 0, 0}, p1[4] = {0, 1, 0, 0}, p2[4] = {0, 0, 1.0f / (1.0f - zn), 1.0f},
+                p3[4] = {0, 0, -zn / (1.0f - zn), 0};
+    const float t3[4] = {0.5f * (float)g.width, 0.5f * (float)g.height, 0.f, 1.f};
+    const float e2[4] = {0, 0, 1, 0};
+    w2p = fmat_mul(fmat_mul(fmat_cols(p0, p1, e2, t3), fmat_cols(p0, p1, p2, p3)), view);
+    return w2p.inverse(p2w);
+}
+
+// The projection factories have blob kernels for perspective beams only
+// (DefaultForwardProjectionCreator.cpp:30-62, DefaultBackProjectionCreator.cpp:28-63).
+etcu_status blob_view(etcu_context* ctx, const etcu_view* view, FMat& w2p, FMat& p2w, const char* kind) {
+    etcu_status s = check_view(ctx, view);
+    if (s != ETCU_OK) return s;
+    if (!view->perspective) return fail(ctx, ETCU_ERR_UNSUPPORTED, "No fitting %s projection kernel found!", kind);
+    if (!float_perspective(*view, w2p, p2w)) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "matrix not invertible");
+    return ETCU_OK;
+}
+
+struct DevBuf {  // a device buffer owned for one call
+    etcu_context* ctx;
+    void* p = nullptr;
+    size_t n = 0;
+    explicit DevBuf(etcu_context* c) : ctx(c) {}
+    ~DevBuf() { dfree(ctx, p, n); }
+    etcu_status alloc_copy(const void* host, size_t bytes) {
+        n = bytes;
+        etcu_status s = dalloc(ctx, &p, bytes);
+        if (s != ETCU_OK) return s;
+        CK(ctx, cudaMemcpyAsync(p, host, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        return ETCU_OK;
+    }
+};
+
+constexpr int kBlobFpTable = 256;  // DefaultForwardProjectionCreator.cpp:56
+constexpr int kBlobBpTable = 256;  // PerspectiveBeamsBackProjectionWithBlobsKernel.cpp:29
+
+// one slab's forward projection of one view (BlobTraverseRay: blobRadius *= voxelSize.x)
+void launch_blob_fp(const etcu_volume* vol, const SlabConst& g, const etcu_view& view, const FMat& p2w,
+                    float support_radius, const float* table, int ntable, float* proj, float* len,
+                    cudaStream_t st) {
+    BlobFpArgs a{};
+    a.vol = vol->master + slab_offset_elems(vol, g);
+    a.rx = g.rx;
+    a.ry = g.ry;
+    a.rz = g.rz;
+    a.bmin = g.bmin;
+    a.vs = g.vs;
+    std::memcpy(a.p2w.v, p2w.v, sizeof(a.p2w.v));
+    a.source = make_float4(view.source[0], view.source[1], view.source[2], 0.f);
+    a.R = support_radius * g.vs.x;
+    a.grid = (int)ceilf(1.415f * a.R / g.vs.x);
+    a.table = table;
+    a.ntable = ntable;
+    a.W = (int)view.width;
+    a.H = (int)view.height;
+    a.proj = proj;
+    a.len = len;
+    blob_fp_kernel<<<dim3((a.W + 127) / 128, a.H), 128, (size_t)ntable * sizeof(float), st>>>(a);
+}
+
+// one slab's back projection of one view with lambda already divided by the block size
+// (BackProjectionKernel.cpp:94)
+void launch_blob_bp(etcu_volume* vol, const SlabConst& g, const etcu_view& view, const FMat& w2p, const FMat& p2w,
+                    float support_radius, const float* table, int ntable, const float* residual,
+                    const float* raylength, float lambda, cudaStream_t st) {
+    BlobBpArgs a{};
+    const size_t off = slab_offset_elems(vol, g);
+    a.vol = vol->master + off;
+    a.rx = g.rx;
+    a.ry = g.ry;
+    a.rz = g.rz;
+    a.bmin = g.bmin;
+    a.vs = g.vs;
+    std::memcpy(a.w2p.v, w2p.v, sizeof(a.w2p.v));
+    std::memcpy(a.p2w.v, p2w.v, sizeof(a.p2w.v));
+    a.source = make_float4(view.source[0], view.source[1], view.source[2], 0.f);
+    a.detector = make_float4(view.detector[0], view.detector[1], view.detector[2], 0.f);
+    a.hpitch = make_float4(view.hpitch[0], view.hpitch[1], view.hpitch[2], 0.f);
+    a.vpitch = make_float4(view.vpitch[0], view.vpitch[1], view.vpitch[2], 0.f);
+    a.R = support_radius * g.vs.x;
+    a.table = table;
+    a.ntable = ntable;
+    a.residual = residual;
+    a.raylength = raylength;
+    a.W = (int)view.width;
+    a.H = (int)view.height;
+    a.lambda = lambda;
+    a.mask = vol->mask ? vol->mask + off : nullptr;
+    blob_bp_kernel<<<dim3((g.rx + 127) / 128, g.ry, g.rz), 128, 0, st>>>(a);
+}
+
+etcu_status blob_volume_ok(etcu_context* ctx, const etcu_volume* vol) {
+    if (vol->type != ETCU_VOXEL_FLOAT32) return fail(ctx, ETCU_ERR_UNSUPPORTED, "blob coefficients are FP32 volumes");
+    for (const SlabConst& g : vol->slabs)
+        if (g.ry > 65535 || g.rz > 65535)
+            return fail(ctx, ETCU_ERR_UNSUPPORTED, "sub-volume of %d x %d x %d exceeds the launch grid", g.rx, g.ry,
+                        g.rz);
+    return ETCU_OK;
+}
+
+}  // namespace
+
+extern "C" etcu_status etcu_blob_ray_integration_samples(const etcu_blob_params* params, uint32_t count, float* out) {
+    BlobP p;
+    etcu_status s = blob_params(nullptr, params, p);
+    if (s != ETCU_OK) return s;
+    if (count < 2 || !out) return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT, "at least two samples and an output");
+    std::vector<float> t;
+    blob_table(p, count, t);
+    std::memcpy(out, t.data(), count * sizeof(float));
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_blob_voxelization_kernel(const etcu_blob_params* params, float* out, uint32_t capacity,
+                                                     uint32_t* size_per_dim) {
+    BlobP p;
+    etcu_status s = blob_params(nullptr, params, p);
+    if (s != ETCU_OK) return s;
+    if (!size_per_dim) return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    const int ks = 2 * (int)std::ceil((float)p.a) + 1;
+    *size_per_dim = (uint32_t)ks;
+    if (!out) return ETCU_OK;
+    if (capacity < (uint32_t)(ks * ks * ks))
+        return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT, "output holds %u of %d values", capacity, ks * ks * ks);
+    std::vector<float> k;
+    int n;
+    blob_voxel_kernel(p, k, n);
+    std::memcpy(out, k.data(), k.size() * sizeof(float));
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_forward_project_blobs(etcu_volume* vol, const etcu_view* view, uint32_t subvolume,
+                                                  const etcu_blob_params* params, uint32_t sample_count,
+                                                  float* d_projection, float* d_traversal) {
+    etcu_context* ctx = vol ? vol->ctx : nullptr;
+    if (!vol || !d_projection || !d_traversal) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (subvolume != ETCU_ALL_SUBVOLUMES && subvolume >= vol->slabs.size())
+        return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "subvolume %u out of range", subvolume);
+    if (sample_count < 2 || sample_count > 8192) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "2 to 8192 table samples");
+    BlobP p;
+    FMat w2p, p2w;
+    etcu_status s;
+    if ((s = blob_volume_ok(ctx, vol)) != ETCU_OK || (s = blob_params(ctx, params, p)) != ETCU_OK ||
+        (s = blob_view(ctx, view, w2p, p2w, "forward")) != ETCU_OK)
+        return s;
+    std::vector<float> table;
+    blob_table(p, sample_count, table);
+    DevBuf dt(ctx);
+    if ((s = dt.alloc_copy(table.data(), table.size() * sizeof(float))) != ETCU_OK) return s;
+    for (size_t i = 0; i < vol->slabs.size(); ++i)
+        if (subvolume == ETCU_ALL_SUBVOLUMES || i == subvolume)
+            launch_blob_fp(vol, vol->slabs[i], *view, p2w, params->support_radius, (const float*)dt.p,
+                           (int)sample_count, d_projection, d_traversal, ctx->stream);
+    CKL(ctx);
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_back_project_blobs(etcu_volume* vol, const etcu_view* view, uint32_t subvolume,
+                                               const etcu_blob_params* params, float lambda, uint32_t block_size,
+                                               const float* d_residual, const float* d_raylength) {
+    etcu_context* ctx = vol ? vol->ctx : nullptr;
+    if (!vol || !d_residual || !d_raylength) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (block_size == 0) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "Illegal ProjectionBlockSize!");
+    if (subvolume != ETCU_ALL_SUBVOLUMES && subvolume >= vol->slabs.size())
+        return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "subvolume %u out of range", subvolume);
+    BlobP p;
+    FMat w2p, p2w;
+    etcu_status s;
+    if ((s = blob_volume_ok(ctx, vol)) != ETCU_OK || (s = blob_params(ctx, params, p)) != ETCU_OK ||
+        (s = blob_view(ctx, view, w2p, p2w, "back")) != ETCU_OK)
+        return s;
+    std::vector<float> table;
+    blob_table(p, kBlobBpTable, table);
+    DevBuf dt(ctx);
+    if ((s = dt.alloc_copy(table.data(), table.size() * sizeof(float))) != ETCU_OK) return s;
+    for (size_t i = 0; i < vol->slabs.size(); ++i)
+        if (subvolume == ETCU_ALL_SUBVOLUMES || i == subvolume)
+            launch_blob_bp(vol, vol->slabs[i], *view, w2p, p2w, params->support_radius, (const float*)dt.p,
+                           kBlobBpTable, d_residual, d_raylength, lambda / (float)block_size, ctx->stream);
+    CKL(ctx);
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    return ETCU_OK;
+}
+
+// ---------------------------------------------------------------- blob block iterations
+// BlockIterativeReconstructionOperator.cpp:84-160 with algorithm.basisFunctions = blobs:
+// tables and matrices formed once, the tilt series device-resident, per block the forward
+// projection of every view into cleared images, the residual, then the back projection
+// of every view with lambda / block size; iterations stream-ordered, one sync per run.
+struct etcu_blob_recon {
+    etcu_volume* vol = nullptr;
+    etcu_context* ctx = nullptr;
+    float lambda = 1.f, support_radius = 2.f;
+    uint32_t W = 0, H = 0, n_input = 0, block = 1;
+    std::vector<uint32_t> order;
+    std::vector<etcu_view> views;
+    std::vector<FMat> w2p, p2w;
+    float* d_proj = nullptr;
+    bool own_proj = false;
+    float* d_img = nullptr;  // virtual, traversal, residual: 3 x block x W x H
+    float* d_tables = nullptr;  // forward table, back table
+    double* d_rsq = nullptr;
+    double last_rsq = 0.0;
+    uint32_t launches = 0;
+};
+
+namespace {
+void blob_recon_free(etcu_blob_recon* r) {
+    etcu_context* ctx = r->ctx;
+    const size_t P = (size_t)r->W * r->H;
+    if (r->own_proj) dfree(ctx, r->d_proj, P * r->n_input * sizeof(float));
+    dfree(ctx, r->d_img, 3 * P * r->block * sizeof(float));
+    dfree(ctx, r->d_tables, (kBlobFpTable + kBlobBpTable) * sizeof(float));
+    dfree(ctx, r->d_rsq, sizeof(double));
+}
+
+etcu_status blob_recon_build(etcu_volume* vol, const etcu_view* views, uint32_t n_views, const float* host_proj,
+                             const float* dev_proj, const etcu_recon_params* params, const etcu_blob_params* blob,
+                             etcu_blob_recon** out) {
+    etcu_context* ctx = vol ? vol->ctx : nullptr;
+    if (!vol || !views || !params || !out || (!host_proj && !dev_proj))
+        return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (n_views == 0) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "no projections");
+    if (params->block_size == 0) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "Illegal ProjectionBlockSize!");
+    if (params->use_long_object_compensation)
+        return fail(ctx, ETCU_ERR_INVALID_ARGUMENT,
+                    "Calculation of traversal length is only supported for parallel scanner geometry!");
+    BlobP p;
+    etcu_status s;
+    if ((s = blob_volume_ok(ctx, vol)) != ETCU_OK || (s = blob_params(ctx, blob, p)) != ETCU_OK) return s;
+    std::unique_ptr<etcu_blob_recon, void (*)(etcu_blob_recon*)> r(new etcu_blob_recon(), [](etcu_blob_recon* q) {
+        blob_recon_free(q);
+        delete q;
+    });
+    r->vol = vol;
+    r->ctx = ctx;
+    r->lambda = params->lambda;
+    r->support_radius = blob->support_radius;
+    r->n_input = n_views;
+    r->W = views[0].width;
+    r->H = views[0].height;
+    r->views.assign(views, views + n_views);
+    r->w2p.resize(n_views);
+    r->p2w.resize(n_views);
+    for (uint32_t i = 0; i < n_views; ++i) {
+        if (views[i].width != r->W || views[i].height != r->H)
+            return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "all projections must share one resolution");
+        if ((s = blob_view(ctx, &views[i], r->w2p[i], r->p2w[i], "forward")) != ETCU_OK) return s;
+    }
+    r->order = projection_order(params->order, n_views, params->skip, params->skip ? params->skip_count : 0);
+    const uint32_t M = (uint32_t)r->order.size();
+    if (M == 0) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "After applying SkipProjectionList no projections are left!");
+    r->block = params->block_size == ETCU_BLOCK_ALL ? M : std::min(params->block_size, M);
+    const size_t P = (size_t)r->W * r->H;
+    if (dev_proj) {
+        r->d_proj = const_cast<float*>(dev_proj);
+    } else {
+        if ((s = dalloc(ctx, (void**)&r->d_proj, P * n_views * sizeof(float))) != ETCU_OK) return s;
+        r->own_proj = true;
+        CK(ctx, cudaMemcpyAsync(r->d_proj, host_proj, P * n_views * sizeof(float), cudaMemcpyHostToDevice,
+                                ctx->stream));
+    }
+    if ((s = dalloc(ctx, (void**)&r->d_img, 3 * P * r->block * sizeof(float))) != ETCU_OK) return s;
+    std::vector<float> tables, t;
+    blob_table(p, kBlobFpTable, tables);
+    blob_table(p, kBlobBpTable, t);
+    tables.insert(tables.end(), t.begin(), t.end());
+    if ((s = dalloc(ctx, (void**)&r->d_tables, tables.size() * sizeof(float))) != ETCU_OK) return s;
+    CK(ctx, cudaMemcpyAsync(r->d_tables, tables.data(), tables.size() * sizeof(float), cudaMemcpyHostToDevice,
+                            ctx->stream));
+    if ((s = dalloc(ctx, (void**)&r->d_rsq, sizeof(double))) != ETCU_OK) return s;
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    *out = r.release();
+    return ETCU_OK;
+}
+
+uint32_t issue_blob_iteration(etcu_blob_recon* r) {
+    etcu_volume* vol = r->vol;
+    cudaStream_t st = r->ctx->stream;
+    const size_t P = (size_t)r->W * r->H;
+    const uint32_t M = (uint32_t)r->order.size();
+    const float* fpt = r->d_tables;
+    const float* bpt = r->d_tables + kBlobFpTable;
+    uint32_t launches = 0;
+    cudaMemsetAsync(r->d_rsq, 0, sizeof(double), st);
+    for (uint32_t b0 = 0; b0 < M; b0 += r->block) {
+        const uint32_t n = std::min(r->block, M - b0);
+        float* virt = r->d_img;
+        float* trav = r->d_img + (size_t)r->block * P;
+        float* res = r->d_img + 2 * (size_t)r->block * P;
+        // BlockIterativeState::setCurrentBlockIndex clears the block's images
+        cudaMemsetAsync(virt, 0, n * P * sizeof(float), st);
+        cudaMemsetAsync(trav, 0, n * P * sizeof(float), st);
+        for (size_t sl = 0; sl < vol->slabs.size(); ++sl)
+            for (uint32_t j = 0; j < n; ++j) {
+                const uint32_t v = r->order[b0 + j];
+                launch_blob_fp(vol, vol->slabs[sl], r->views[v], r->p2w[v], r->support_radius, fpt, kBlobFpTable,
+                               virt + j * P, trav + j * P, st);
+                ++launches;
+            }
+        for (uint32_t j = 0; j < n; ++j) {
+            const uint32_t v = r->order[b0 + j];
+            const int blocks = (int)std::min<size_t>((P + 255) / 256, 148 * 8);
+            blob_residual_kernel<<<blocks, 256, 0, st>>>(r->d_proj + (size_t)v * P, virt + j * P, res + j * P, P,
+                                                         r->d_rsq);
+            ++launches;
+        }
+        for (size_t k = vol->slabs.size(); k-- > 0;)  // doBackProjectionForBlock: sub-volumes last to first
+            for (uint32_t j = 0; j < n; ++j) {
+                const uint32_t v = r->order[b0 + j];
+                launch_blob_bp(vol, vol->slabs[k], r->views[v], r->w2p[v], r->p2w[v], r->support_radius, bpt,
+                               kBlobBpTable, res + j * P, trav + j * P, r->lambda / (float)n, st);
+                ++launches;
+            }
+    }
+    return launches;
+}
+}  // namespace
+
+extern "C" etcu_status etcu_blob_recon_create(etcu_volume* vol, const etcu_view* views, uint32_t n_views,
+                                              const float* host_projections, const etcu_recon_params* params,
+                                              const etcu_blob_params* blob, etcu_blob_recon** out) {
+    return blob_recon_build(vol, views, n_views, host_projections, nullptr, params, blob, out);
+}
+
+extern "C" etcu_status etcu_blob_recon_create_device(etcu_volume* vol, const etcu_view* views, uint32_t n_views,
+                                                     const float* d_projections, const etcu_recon_params* params,
+                                                     const etcu_blob_params* blob, etcu_blob_recon** out) {
+    return blob_recon_build(vol, views, n_views, nullptr, d_projections, params, blob, out);
+}
+
+extern "C" etcu_status etcu_blob_recon_run(etcu_blob_recon* r, uint32_t iterations) {
+    if (!r) return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL reconstruction");
+    etcu_context* ctx = r->ctx;
+    for (uint32_t it = 0; it < iterations; ++it) r->launches = issue_blob_iteration(r);
+    CKL(ctx);
+    if (iterations) {
+        CK(ctx, cudaMemcpyAsync(&r->last_rsq, r->d_rsq, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_blob_recon_last_residual_sq(const etcu_blob_recon* r, double* out) {
+    if (!r || !out) return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = r->last_rsq;
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_blob_recon_view_order(const etcu_blob_recon* r, uint32_t* out, uint32_t capacity,
+                                                  uint32_t* count) {
+    if (!r || !count) return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    *count = (uint32_t)r->order.size();
+    if (out) std::memcpy(out, r->order.data(), std::min<size_t>(capacity, r->order.size()) * sizeof(uint32_t));
+    return ETCU_OK;
+}
+
+extern "C" uint32_t etcu_blob_recon_launches_per_iteration(const etcu_blob_recon* r) { return r ? r->launches : 0; }
+
+extern "C" etcu_status etcu_blob_recon_destroy(etcu_blob_recon* r) {
+    if (!r) return ETCU_OK;
+    blob_recon_free(r);
+    delete r;
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_blob_voxelize(etcu_volume* blobs, etcu_volume* voxels, const etcu_blob_params* params) {
+    etcu_context* ctx = blobs ? blobs->ctx : nullptr;
+    if (!blobs || !voxels) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "NULL volume");
+    if (blobs->type != ETCU_VOXEL_FLOAT32 || voxels->type != ETCU_VOXEL_FLOAT32)
+        return fail(ctx, ETCU_ERR_UNSUPPORTED, "blob voxelisation takes FP32 volumes");
+    for (int i = 0; i < 3; ++i)
+        if (blobs->desc.resolution[i] != voxels->desc.resolution[i])
+            return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "Input and output volume resolutions for VolumeConvolutionKernel differ!");
+    BlobP p;
+    etcu_status s = blob_params(ctx, params, p);
+    if (s != ETCU_OK) return s;
+    std::vector<float> k;
+    int ks;
+    blob_voxel_kernel(p, k, ks);
+    DevBuf dk(ctx);
+    if ((s = dk.alloc_copy(k.data(), k.size() * sizeof(float))) != ETCU_OK) return s;
+    const int X = (int)blobs->desc.resolution[0], Y = (int)blobs->desc.resolution[1], Z = (int)blobs->desc.resolution[2];
+    blob_voxelize_kernel<<<dim3((X + 127) / 128, Y, Z), 128, 0, ctx->stream>>>(blobs->master, voxels->master, X, Y, Z,
+                                                                               (const float*)dk.p, ks);
+    CKL(ctx);
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
     return ETCU_OK;
 }
 

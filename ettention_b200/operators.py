@@ -12,6 +12,8 @@ Names, argument meaning and error behaviour follow the reference
                                     LR/algorithm/reconstruction/blockiterative/
                                     BlockIterativeReconstructionOperator.cpp
   AlgebraicParameterSet.from_config LR/setup/parameterset/*ParameterSet.cpp (same config keys)
+  BlobParameters, BlobRayIntegrationSampler, BlobVoxelizationKernelValues,
+  BlobVoxelizerOperator             LR/model/blobs, LR/algorithm/blobs (blob basis functions)
 
 Every compute call goes through ``libettention_b200.so``; device images are
 CUDA ``torch.Tensor`` objects (float32, contiguous) used as plain device
@@ -582,9 +584,12 @@ class ForwardProjectionOperator:
     """ForwardProjectionOperator (ForwardProjectionOperator.cpp:11-55): SetOutput + Execute(subVolume).
     The outputs are ACCUMULATED (+=), as in the reference."""
 
-    def __init__(self, volume: GPUMappedVolume, samples: int = 1):
+    def __init__(self, volume: GPUMappedVolume, samples: int = 1, blob_parameters: Optional["BlobParameters"] = None,
+                 blob_samples: int = 256):
         self.volume = volume
         self.samples = samples
+        self.blob_parameters = blob_parameters  # algorithm.basisFunctions = blobs
+        self.blob_samples = blob_samples
         self.geometry: Optional[ScannerGeometry] = None
         self.virtual = None
         self.traversal = None
@@ -608,6 +613,10 @@ class ForwardProjectionOperator:
         g = self.geometry
         if tuple(self.virtual.shape) != (g.height, g.width):
             raise EttentionError(_abi.ERR_INVALID_ARGUMENT, "output image does not match the detector resolution")
+        if self.blob_parameters is not None:
+            forward_project_blobs(self.volume, g, self.blob_parameters, self.virtual, self.traversal, subvolume,
+                                  self.blob_samples)
+            return
         v = g.to_view()
         self.volume.ctx.check(lib().etcu_forward_project(self.volume.handle, ctypes.byref(v), int(subvolume),
                                                          int(self.samples), _dptr(self.virtual),
@@ -622,8 +631,9 @@ class BackProjectionOperator:
     ALL_SUB_VOLUMES = _abi.ALL_SUBVOLUMES
 
     def __init__(self, volume: GPUMappedVolume, lam: float, samples: int = 1,
-                 sampling: int = _abi.SAMPLING_Q8):
+                 sampling: int = _abi.SAMPLING_Q8, blob_parameters: Optional["BlobParameters"] = None):
         self.volume = volume
+        self.blob_parameters = blob_parameters  # algorithm.basisFunctions = blobs
         self.lam = float(lam)
         self.samples = int(samples)
         self.sampling = sampling
@@ -647,6 +657,10 @@ class BackProjectionOperator:
         if self.residual is None:
             raise EttentionError(_abi.ERR_STATE, "Residual and traversalLength images must both be provided via "
                                  "SetInput() before kernel launch!")
+        if self.blob_parameters is not None:
+            back_project_blobs(self.volume, self.geometry, self.blob_parameters, self.residual, self.traversal,
+                               self.lam, self.block_size, subvolume)
+            return
         v = self.geometry.to_view()
         self.volume.ctx.check(lib().etcu_back_project(self.volume.handle, ctypes.byref(v), int(subvolume),
                                                       self.samples, self.lam, self.block_size,
@@ -675,6 +689,185 @@ def compute_ray_length(volume: GPUMappedVolume, g: ScannerGeometry, out) -> None
     volume.ctx.synchronize()
 
 
+# ----------------------------------------------------------------------------- blob basis functions
+@dataclass
+class BlobParameters:
+    """model/blobs/BlobParameters.cpp: Kaiser-Bessel blob of support radius a (voxels),
+    degree m and density fall-off alpha; createDefault() = (2.0, 2, 3.6)."""
+    support_radius: float = 2.0
+    degree: int = 2
+    density_falloff: float = 3.6
+
+    @classmethod
+    def createDefault(cls) -> "BlobParameters":
+        return cls()
+
+    @classmethod
+    def createWithParameters(cls, support_radius: float, degree: int, density_falloff: float) -> "BlobParameters":
+        return cls(float(support_radius), int(degree), float(density_falloff))
+
+    @classmethod
+    def from_config(cls, cfg: Dict[str, str]) -> "BlobParameters":
+        """BlobParameterSet.cpp:7-29: blobs.supportRadius, blobs.degree, blobs.densityFalloff."""
+        return cls(float(cfg.get("blobs.supportRadius", 2.0)), int(cfg.get("blobs.degree", 2)),
+                   float(cfg.get("blobs.densityFalloff", 3.6)))
+
+    def getSupportRadius(self) -> float:
+        return self.support_radius
+
+    def getDegree(self) -> int:
+        return self.degree
+
+    def getDensityFallOff(self) -> float:
+        return self.density_falloff
+
+    def to_c(self) -> "_abi.BlobParams":
+        return _abi.BlobParams(float(self.support_radius), int(self.degree), float(self.density_falloff))
+
+
+class BlobRayIntegrationSampler:
+    """algorithm/blobs/BlobRayIntegrationSampler.cpp: the blob's line integral at
+    ``count`` distances from 0 to a (etcu_blob_ray_integration_samples)."""
+
+    def __init__(self, params: BlobParameters, count: int):
+        self.params = params
+        self.samples = np.zeros(int(count), np.float32)
+        c = params.to_c()
+        check(lib().etcu_blob_ray_integration_samples(ctypes.byref(c), int(count), self.samples.ctypes.data))
+
+    def getSamples(self) -> np.ndarray:
+        return self.samples
+
+    def getSampleCount(self) -> int:
+        return int(self.samples.shape[0])
+
+    def getParameters(self) -> BlobParameters:
+        return self.params
+
+
+class BlobVoxelizationKernelValues:
+    """algorithm/blobs/BlobVoxelizationKernelValues.cpp: the blob integrated over every
+    voxel of its (2 ceil(a) + 1)^3 neighbourhood, [dz][dy][dx]."""
+
+    def __init__(self, params: BlobParameters):
+        c = params.to_c()
+        n = ctypes.c_uint32()
+        check(lib().etcu_blob_voxelization_kernel(ctypes.byref(c), None, 0, ctypes.byref(n)))
+        k = int(n.value)
+        self.values = np.zeros((k, k, k), np.float32)
+        check(lib().etcu_blob_voxelization_kernel(ctypes.byref(c), self.values.ctypes.data, k ** 3, ctypes.byref(n)))
+
+    def getValuesPerDimension(self) -> int:
+        return int(self.values.shape[0])
+
+    def getKernelValues(self) -> np.ndarray:
+        return self.values
+
+
+def forward_project_blobs(volume: "GPUMappedVolume", g: ScannerGeometry, params: BlobParameters, projection,
+                          traversal, subvolume: int = _abi.ALL_SUBVOLUMES, sample_count: int = 256) -> None:
+    """PerspectiveBeamsForwardProjectionWithBlobsKernel: ADDS the blob line integrals of the
+    coefficients and their weights into two device images."""
+    v, c = g.to_view(), params.to_c()
+    volume.ctx.check(lib().etcu_forward_project_blobs(volume.handle, ctypes.byref(v), int(subvolume), ctypes.byref(c),
+                                                      int(sample_count), _dptr(projection), _dptr(traversal)))
+
+
+def back_project_blobs(volume: "GPUMappedVolume", g: ScannerGeometry, params: BlobParameters, residual, traversal,
+                       lam: float, block_size: int = 1, subvolume: int = _abi.ALL_SUBVOLUMES) -> None:
+    """PerspectiveBeamsBackProjectionWithBlobsKernel: every blob takes lambda / block size times
+    the weighted mean of residual / ray length over the pixels whose rays pass within its radius."""
+    v, c = g.to_view(), params.to_c()
+    volume.ctx.check(lib().etcu_back_project_blobs(volume.handle, ctypes.byref(v), int(subvolume), ctypes.byref(c),
+                                                   float(lam), int(block_size), _dptr(residual), _dptr(traversal)))
+
+
+class BlobVoxelizerOperator:
+    """algorithm/blobs/BlobVoxelizerOperator.cpp: the blob coefficients convolved with the
+    voxelisation kernel into a second volume of the same resolution and box."""
+
+    def __init__(self, volume: "GPUMappedVolume", params: BlobParameters):
+        self.volume = volume
+        self.params = params
+        self.voxels = GPUMappedVolume(volume.ctx, volume.resolution, volume.bbox_min, volume.bbox_max)
+
+    def voxelize(self) -> None:
+        c = self.params.to_c()
+        self.volume.ctx.check(lib().etcu_blob_voxelize(self.volume.handle, self.voxels.handle, ctypes.byref(c)))
+
+    def getVoxelVolume(self) -> "GPUMappedVolume":
+        return self.voxels
+
+
+class _BlobBlockIterations:
+    """BlockIterativeReconstructionOperator.cpp:84-160 with blob basis functions
+    (algorithm.basisFunctions = blobs, etcu_blob_recon_*): per block, the blob forward
+    projection of every view into cleared images, residual = measured - virtual, then the
+    blob back projection of every view with lambda / block size.  With
+    output.options.enableVoxelization the coefficients are voxelised after every
+    runNiterations (:66-79) and the voxel volume is the result."""
+
+    def __init__(self, volume: "GPUMappedVolume", geometries: Sequence[ScannerGeometry], projections,
+                 params: "AlgebraicParameterSet"):
+        self.volume = volume
+        self.params = params
+        self._views = (View * len(geometries))(*[g.to_view() for g in geometries])
+        rp = params.recon_params(False)
+        self._skip = (ctypes.c_uint32 * max(1, len(params.skip)))(*[int(s) for s in params.skip])
+        if len(params.skip):
+            rp.skip = ctypes.cast(self._skip, ctypes.POINTER(ctypes.c_uint32))
+            rp.skip_count = len(params.skip)
+        blob = params.blob.to_c()
+        h = ctypes.c_void_p()
+        if isinstance(projections, np.ndarray):
+            host = np.ascontiguousarray(projections, np.float32)
+            if host.shape[0] != len(geometries):
+                raise EttentionError(_abi.ERR_INVALID_ARGUMENT, "one projection per geometry")
+            volume.ctx.check(lib().etcu_blob_recon_create(volume.handle, self._views, len(geometries), host.ctypes.data,
+                                                          ctypes.byref(rp), ctypes.byref(blob), ctypes.byref(h)))
+        else:
+            self._dev = projections
+            volume.ctx.check(lib().etcu_blob_recon_create_device(volume.handle, self._views, len(geometries),
+                                                                 _dptr(projections), ctypes.byref(rp),
+                                                                 ctypes.byref(blob), ctypes.byref(h)))
+        self.handle = h
+        self.voxelizer = BlobVoxelizerOperator(volume, params.blob) if params.enable_voxelization else None
+
+    @property
+    def order(self) -> List[int]:
+        n = len(self._views)
+        out = np.zeros(n, np.uint32)
+        cnt = ctypes.c_uint32()
+        self.volume.ctx.check(lib().etcu_blob_recon_view_order(self.handle, out.ctypes.data, n, ctypes.byref(cnt)))
+        return [int(i) for i in out[: cnt.value]]
+
+    @property
+    def residual_sq(self) -> float:
+        r = ctypes.c_double()
+        self.volume.ctx.check(lib().etcu_blob_recon_last_residual_sq(self.handle, ctypes.byref(r)))
+        return float(r.value)
+
+    @property
+    def launches(self) -> int:
+        return int(lib().etcu_blob_recon_launches_per_iteration(self.handle))
+
+    def run(self, n: int) -> None:
+        self.volume.ctx.check(lib().etcu_blob_recon_run(self.handle, int(n)))
+        if self.voxelizer is not None:
+            self.voxelizer.voxelize()
+
+    def result(self) -> np.ndarray:
+        return (self.voxelizer.getVoxelVolume() if self.voxelizer is not None else self.volume).download()
+
+    def close(self) -> None:
+        if self.voxelizer is not None:
+            self.voxelizer.voxels.close()
+            self.voxelizer = None
+        if getattr(self, "handle", None):
+            lib().etcu_blob_recon_destroy(self.handle)
+            self.handle = None
+
+
 # ----------------------------------------------------------------------------- parameters
 @dataclass
 class AlgebraicParameterSet:
@@ -700,6 +893,9 @@ class AlgebraicParameterSet:
     vmin: Optional[float] = None
     vmax: Optional[float] = None
     sampling: int = _abi.SAMPLING_Q8
+    basis_functions: str = "voxels"
+    blob: BlobParameters = field(default_factory=BlobParameters)
+    enable_voxelization: bool = False
 
     @classmethod
     def from_config(cls, cfg: Dict[str, str]) -> "AlgebraicParameterSet":
@@ -722,12 +918,14 @@ class AlgebraicParameterSet:
         p.lam = float(cfg["algorithm.lambda"])
         p.use_long_object_compensation = str(cfg.get("algorithm.useLongObjectCompensation", "false")).lower() in (
             "true", "1", "yes")
-        basis = cfg.get("algorithm.basisFunctions", "voxels")
-        if basis == "blobs":
-            raise EttentionError(_abi.ERR_UNSUPPORTED, "blob basis functions are not part of the voxel hot path")
-        if basis != "voxels":
+        basis = cfg.get("algorithm.basisFunctions", "voxels")  # AlgorithmParameterSet.cpp:34-45
+        if basis not in ("voxels", "blobs"):
             raise EttentionError(_abi.ERR_INVALID_ARGUMENT,
                                  f'Illegal value for parameter "algorithm.basisFunctions": {basis}!')
+        p.basis_functions = basis
+        p.blob = BlobParameters.from_config(cfg)
+        p.enable_voxelization = str(cfg.get("output.options.enableVoxelization", "false")).lower() in (
+            "true", "1", "yes")
         p.fp_samples = int(cfg.get("forwardProjection.samples", 1))
         p.bp_samples = int(cfg.get("backProjection.samples", 1))
         vt = cfg.get("optimization.internalVoxelRepresentationType", "float")
@@ -788,6 +986,12 @@ class BlockIterativeReconstructionOperator:
                  params: AlgebraicParameterSet, use_graph: bool = True):
         self.volume = volume
         self.params = params
+        self.handle = None
+        self._blobs = None
+        if params.basis_functions == "blobs":
+            self._blobs = _BlobBlockIterations(volume, geometries, projections, params)
+            volume.ctx._adopt(self)
+            return
         self._views = (View * len(geometries))(*[g.to_view() for g in geometries])
         rp = params.recon_params(use_graph)
         self._skip = (ctypes.c_uint32 * max(1, len(params.skip)))(*[int(s) for s in params.skip])
@@ -810,6 +1014,9 @@ class BlockIterativeReconstructionOperator:
         volume.ctx._adopt(self)
 
     def close(self) -> None:
+        if getattr(self, "_blobs", None) is not None:
+            self._blobs.close()
+            self._blobs = None
         if getattr(self, "handle", None):
             lib().etcu_recon_destroy(self.handle)
             self.handle = None
@@ -820,7 +1027,14 @@ class BlockIterativeReconstructionOperator:
         except Exception:
             pass
 
+    def _voxels_only(self, what: str) -> None:
+        if self._blobs is not None:
+            raise EttentionError(_abi.ERR_UNSUPPORTED, f"{what} is reported for voxel basis functions only")
+
     def runNiterations(self, n: int = 1) -> None:
+        if self._blobs is not None:
+            self._blobs.run(n)
+            return
         self.volume.ctx.check(lib().etcu_recon_run(self.handle, int(n)))
 
     def run(self) -> None:
@@ -830,19 +1044,26 @@ class BlockIterativeReconstructionOperator:
         self.runNiterations(1)
 
     def getReconstructedVolume(self) -> np.ndarray:
+        if self._blobs is not None:
+            return self._blobs.result()
         return self.volume.download()
 
     def last_residual_sq(self) -> float:
+        if self._blobs is not None:
+            return self._blobs.residual_sq
         r = ctypes.c_double()
         self.volume.ctx.check(lib().etcu_recon_last_residual_sq(self.handle, ctypes.byref(r)))
         return float(r.value)
 
     def data_residual_sq(self) -> float:
+        self._voxels_only("the data residual")
         r = ctypes.c_double()
         self.volume.ctx.check(lib().etcu_recon_data_residual_sq(self.handle, ctypes.byref(r)))
         return float(r.value)
 
     def view_order(self) -> List[int]:
+        if self._blobs is not None:
+            return list(self._blobs.order)
         n = len(self._views)
         out = np.zeros(n, np.uint32)
         cnt = ctypes.c_uint32()
@@ -851,11 +1072,14 @@ class BlockIterativeReconstructionOperator:
 
     @property
     def launches_per_iteration(self) -> int:
+        if self._blobs is not None:
+            return self._blobs.launches
         return int(lib().etcu_recon_launches_per_iteration(self.handle))
 
     def profile_steps(self):
         """Runs one iteration as run() does, each step timed: [(kind, ms, launches)],
         kind 'forward', 'back' or 'fused' (etcu_recon_profile_steps)."""
+        self._voxels_only("the step profile")
         n = ctypes.c_uint32()
         self.volume.ctx.check(lib().etcu_recon_profile_steps(self.handle, None, None, None, 0, ctypes.byref(n)))
         ms = np.zeros(n.value, np.float32)
@@ -868,6 +1092,7 @@ class BlockIterativeReconstructionOperator:
 
     def profile_iteration(self):
         """Runs one iteration with per-launch CUDA events: (fp_ms, bp_ms, fp_launches, bp_launches)."""
+        self._voxels_only("the iteration profile")
         f, b = ctypes.c_float(), ctypes.c_float()
         nf, nb = ctypes.c_uint32(), ctypes.c_uint32()
         self.volume.ctx.check(lib().etcu_recon_profile_iteration(self.handle, ctypes.byref(f), ctypes.byref(b),

@@ -339,6 +339,62 @@ ETCU_API etcu_status etcu_wbp(etcu_volume* vol, const etcu_view* views, uint32_t
 ETCU_API etcu_status etcu_wbp_filter(etcu_context* ctx, const float* d_in, float* d_out, uint32_t width,
                                      uint32_t height, uint32_t filter_width);
 
+/* ---------------------------------------------------------------- blob basis functions */
+/* Kaiser-Bessel blobs (model/blobs/BlobParameters.cpp; createDefault = 2.0, 2, 3.6) as the
+ * basis of perspective projection (ocl_src/BlobRaytracer.hl,
+ * PerspectiveBeams{Forward,Back}ProjectionWithBlobs.cl) and their voxelisation
+ * (algorithm/blobs/BlobVoxelizerOperator.cpp).  The kernels take the projection matrix and
+ * its inverse as the reference forms them: Matrix4x4 arithmetic in float with a cofactor
+ * inverse. */
+typedef struct {
+    float support_radius;  /* a, in voxels */
+    uint32_t degree;       /* m */
+    float density_falloff; /* alpha */
+} etcu_blob_params;
+/* BlobRayIntegrationSampler: the blob's line integral at count distances 0 .. a. */
+ETCU_API etcu_status etcu_blob_ray_integration_samples(const etcu_blob_params* params, uint32_t count, float* out);
+/* BlobVoxelizationKernelValues: the blob integrated over each voxel of the
+ * (2 ceil(a) + 1)^3 neighbourhood, [dz][dy][dx]; *size_per_dim = 2 ceil(a) + 1 (out may be
+ * NULL to ask for it). */
+ETCU_API etcu_status etcu_blob_voxelization_kernel(const etcu_blob_params* params, float* out, uint32_t capacity,
+                                                  uint32_t* size_per_dim);
+/* PerspectiveBeamsForwardProjectionWithBlobsKernel: ADDS the blob line integrals of the
+ * coefficients in vol (FP32) and their weights into device images (height x width floats);
+ * table of sample_count entries (the reference's callers use 128). */
+ETCU_API etcu_status etcu_forward_project_blobs(etcu_volume* vol, const etcu_view* view, uint32_t subvolume,
+                                               const etcu_blob_params* params, uint32_t sample_count,
+                                               float* d_projection, float* d_traversal);
+/* PerspectiveBeamsBackProjectionWithBlobsKernel: each blob takes lambda / block_size times the
+ * weighted mean of residual / ray length over the pixels whose rays pass within its radius
+ * (pixels with a nonzero residual and a ray length above 1). */
+ETCU_API etcu_status etcu_back_project_blobs(etcu_volume* vol, const etcu_view* view, uint32_t subvolume,
+                                            const etcu_blob_params* params, float lambda, uint32_t block_size,
+                                            const float* d_residual, const float* d_raylength);
+/* Block-iterative reconstruction with blob basis functions (algorithm.basisFunctions =
+ * blobs; BlockIterativeReconstructionOperator.cpp:84-160 with the blob kernels that
+ * DefaultForwardProjectionCreator.cpp:53-60 and DefaultBackProjectionCreator.cpp:51-59
+ * pick for perspective beams, tables of 256 samples).  Same parameters as etcu_recon_create
+ * (lambda, block_size, order, skip; long-object compensation is rejected as for every
+ * perspective series); the coefficients live in vol (FP32).  Voxelise them with
+ * etcu_blob_voxelize after etcu_blob_recon_run when output.options.enableVoxelization is set. */
+typedef struct etcu_blob_recon etcu_blob_recon;
+ETCU_API etcu_status etcu_blob_recon_create(etcu_volume* vol, const etcu_view* views, uint32_t n_views,
+                                           const float* host_projections, const etcu_recon_params* params,
+                                           const etcu_blob_params* blob, etcu_blob_recon** out);
+ETCU_API etcu_status etcu_blob_recon_create_device(etcu_volume* vol, const etcu_view* views, uint32_t n_views,
+                                                  const float* d_projections, const etcu_recon_params* params,
+                                                  const etcu_blob_params* blob, etcu_blob_recon** out);
+ETCU_API etcu_status etcu_blob_recon_run(etcu_blob_recon* rec, uint32_t iterations);
+/* sum of the squared residuals of the last iteration (each view against the volume of its block) */
+ETCU_API etcu_status etcu_blob_recon_last_residual_sq(const etcu_blob_recon* rec, double* out);
+ETCU_API etcu_status etcu_blob_recon_view_order(const etcu_blob_recon* rec, uint32_t* out, uint32_t capacity,
+                                               uint32_t* count);
+ETCU_API uint32_t etcu_blob_recon_launches_per_iteration(const etcu_blob_recon* rec);
+ETCU_API etcu_status etcu_blob_recon_destroy(etcu_blob_recon* rec);
+/* BlobVoxelizerOperator::voxelize: voxels = the blob coefficients convolved with the
+ * voxelisation kernel (zero outside the volume); both FP32, same resolution. */
+ETCU_API etcu_status etcu_blob_voxelize(etcu_volume* blobs, etcu_volume* voxels, const etcu_blob_params* params);
+
 /* ---------------------------------------------------------------- batched series */
 /* Many independent tilt series of uneven sizes reconstructed together: every SART
  * step runs one forward-projection launch and one back-projection launch over all

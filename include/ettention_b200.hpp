@@ -21,6 +21,8 @@
  *   readTiff, writeTiff                    LR/io/deserializer/ImageDeserializer.cpp, ImageSerializer.cpp
  *   XMLParameterSource                     LR/setup/parametersource/XMLParameterSource.cpp
  *   WBP                                    plugins/WBPPlugin/src/reconstruction/WBP.cpp
+ *   BlobParameters, BlobVoxelizerOperator  LR/model/blobs/BlobParameters.cpp, LR/algorithm/blobs
+ *                                          (algorithm.basisFunctions = blobs, perspective beams)
  *   BatchReconstructionOperator            many series per launch (no counterpart in the reference)
  * Errors: every non-OK status of the ABI is rethrown as ettention::b200::Exception
  * (validation) or GPUException (device errors), with the library's message, as
@@ -35,6 +37,7 @@
 #include <array>
 #include <cstdint>
 #include <map>
+#include <memory>
 #include <sstream>
 #include <stdexcept>
 #include <string>
@@ -190,9 +193,33 @@ private:
     etcu_volume* vol_ = nullptr;
 };
 
+// LR/model/blobs/BlobParameters.cpp: Kaiser-Bessel blob (support radius in voxels, degree,
+// density fall-off); BlobParameterSet.cpp:7-29 reads blobs.supportRadius / degree /
+// densityFalloff.
+struct BlobParameters {
+    float supportRadius = 2.0f;
+    uint32_t degree = 2;
+    float densityFalloff = 3.6f;
+
+    static BlobParameters createDefault() { return BlobParameters(); }
+    static BlobParameters createWithParameters(float a, uint32_t m, float alpha) { return {a, m, alpha}; }
+    etcu_blob_params c() const { return etcu_blob_params{supportRadius, degree, densityFalloff}; }
+    // BlobRayIntegrationSampler: the blob's line integral at count distances 0 .. a.
+    std::vector<float> rayIntegrationSamples(uint32_t count) const {
+        std::vector<float> out(count);
+        const etcu_blob_params b = c();
+        check(etcu_blob_ray_integration_samples(&b, count, out.data()), nullptr);
+        return out;
+    }
+};
+
 class ForwardProjectionOperator {
 public:
     ForwardProjectionOperator(GPUMappedVolume& vol, uint32_t samples = 1) : vol_(&vol), samples_(samples) {}
+    // algorithm.basisFunctions = blobs: the perspective blob kernel with a table of
+    // blob_samples entries (DefaultForwardProjectionCreator.cpp:53-60 uses 256).
+    ForwardProjectionOperator(GPUMappedVolume& vol, const BlobParameters& blob, uint32_t blob_samples = 256)
+        : vol_(&vol), samples_(1), blobs_(true), blob_(blob), blobSamples_(blob_samples) {}
     void setScannerGeometry(const ScannerGeometry& g) { geo_ = g; }
     void SetOutput(float* d_virtual, float* d_traversal) {
         virt_ = d_virtual;
@@ -201,13 +228,22 @@ public:
     // Adds the sub-volume's line integrals into the outputs (the caller clears them).
     void Execute(uint32_t subvolume) {
         etcu_context* ctx = vol_->framework().handle();
-        check(etcu_forward_project(vol_->handle(), &geo_.view(), subvolume, samples_, virt_, trav_), ctx);
+        if (blobs_) {
+            const etcu_blob_params b = blob_.c();
+            check(etcu_forward_project_blobs(vol_->handle(), &geo_.view(), subvolume, &b, blobSamples_, virt_, trav_),
+                  ctx);
+        } else {
+            check(etcu_forward_project(vol_->handle(), &geo_.view(), subvolume, samples_, virt_, trav_), ctx);
+        }
         vol_->framework().synchronize();
     }
 
 private:
     GPUMappedVolume* vol_;
     uint32_t samples_;
+    bool blobs_ = false;
+    BlobParameters blob_;
+    uint32_t blobSamples_ = 256;
     ScannerGeometry geo_;
     float* virt_ = nullptr;
     float* trav_ = nullptr;
@@ -220,6 +256,9 @@ public:
     BackProjectionOperator(GPUMappedVolume& vol, float lambda, uint32_t samples = 1,
                            etcu_sampling sampling = ETCU_SAMPLING_Q8)
         : vol_(&vol), lambda_(lambda), samples_(samples), sampling_(sampling) {}
+    // algorithm.basisFunctions = blobs (DefaultBackProjectionCreator.cpp:51-59).
+    BackProjectionOperator(GPUMappedVolume& vol, float lambda, const BlobParameters& blob)
+        : vol_(&vol), lambda_(lambda), samples_(1), sampling_(ETCU_SAMPLING_Q8), blobs_(true), blob_(blob) {}
     void setScannerGeometry(const ScannerGeometry& g) { geo_ = g; }
     void setInput(const float* d_residual, const float* d_traversal, uint32_t block_size) {
         res_ = d_residual;
@@ -229,9 +268,15 @@ public:
     // Updates with lambda / blockSize (BackProjectionKernel.cpp:94).
     void execute(uint32_t subvolume = ALL_SUB_VOLUMES) {
         etcu_context* ctx = vol_->framework().handle();
-        check(etcu_back_project(vol_->handle(), &geo_.view(), subvolume, samples_, lambda_, block_, res_, trav_,
-                                sampling_),
-              ctx);
+        if (blobs_) {
+            const etcu_blob_params b = blob_.c();
+            check(etcu_back_project_blobs(vol_->handle(), &geo_.view(), subvolume, &b, lambda_, block_, res_, trav_),
+                  ctx);
+        } else {
+            check(etcu_back_project(vol_->handle(), &geo_.view(), subvolume, samples_, lambda_, block_, res_, trav_,
+                                    sampling_),
+                  ctx);
+        }
         vol_->framework().synchronize();
     }
 
@@ -240,10 +285,34 @@ private:
     float lambda_;
     uint32_t samples_;
     etcu_sampling sampling_;
+    bool blobs_ = false;
+    BlobParameters blob_;
     ScannerGeometry geo_;
     const float* res_ = nullptr;
     const float* trav_ = nullptr;
     uint32_t block_ = 1;
+};
+
+// LR/algorithm/blobs/BlobVoxelizerOperator.cpp: the blob coefficients convolved with the
+// voxelisation kernel into a second volume of the same resolution and box.
+class BlobVoxelizerOperator {
+public:
+    BlobVoxelizerOperator(GPUMappedVolume& blobs, const BlobParameters& p)
+        : blobs_(&blobs),
+          p_(p),
+          voxels_(blobs.framework(), blobs.resolution(),
+                  {blobs.description().bbox_min[0], blobs.description().bbox_min[1], blobs.description().bbox_min[2]},
+                  {blobs.description().bbox_max[0], blobs.description().bbox_max[1], blobs.description().bbox_max[2]}) {}
+    void voxelize() {
+        const etcu_blob_params b = p_.c();
+        check(etcu_blob_voxelize(blobs_->handle(), voxels_.handle(), &b), blobs_->framework().handle());
+    }
+    GPUMappedVolume& getVoxelVolume() { return voxels_; }
+
+private:
+    GPUMappedVolume* blobs_;
+    BlobParameters p_;
+    GPUMappedVolume voxels_;
 };
 
 // The reference's configuration keys of the block-iterative reconstruction.
@@ -257,6 +326,9 @@ struct AlgebraicParameterSet {
     etcu_voxel_type voxelType = ETCU_VOXEL_FLOAT32;
     etcu_order order = ETCU_ORDER_RANDOM;  // optimization.projectionIteration default
     etcu_sampling sampling = ETCU_SAMPLING_Q8;
+    std::string basisFunctions = "voxels";  // algorithm.basisFunctions
+    BlobParameters blob;                    // blobs.*
+    bool enableVoxelization = false;        // output.options.enableVoxelization
     uint32_t subVolumeCount = 1;
     std::array<uint32_t, 3> resolution{{0, 0, 0}};
     std::array<float, 3> dimension{{0.f, 0.f, 0.f}};
@@ -296,11 +368,15 @@ struct AlgebraicParameterSet {
         const std::string loc = get("algorithm.useLongObjectCompensation", "false");
         p.useLongObjectCompensation = loc == "true" || loc == "1" || loc == "yes";
         const std::string basis = get("algorithm.basisFunctions", "voxels");
-        if (basis == "blobs")
-            throw Exception(ETCU_ERR_UNSUPPORTED, "blob basis functions are not part of the voxel hot path");
-        if (basis != "voxels")
+        if (basis != "voxels" && basis != "blobs")
             throw Exception(ETCU_ERR_INVALID_ARGUMENT,
                             "Illegal value for parameter \"algorithm.basisFunctions\": " + basis + "!");
+        p.basisFunctions = basis;
+        p.blob.supportRadius = std::stof(get("blobs.supportRadius", "2.0"));
+        p.blob.degree = (uint32_t)std::stoul(get("blobs.degree", "2"));
+        p.blob.densityFalloff = std::stof(get("blobs.densityFalloff", "3.6"));
+        const std::string vox = get("output.options.enableVoxelization", "false");
+        p.enableVoxelization = vox == "true" || vox == "1" || vox == "yes";
         p.fpSamples = (uint32_t)std::stoul(get("forwardProjection.samples", "1"));
         p.bpSamples = (uint32_t)std::stoul(get("backProjection.samples", "1"));
         const std::string vt = get("optimization.internalVoxelRepresentationType", "float");
@@ -367,24 +443,48 @@ public:
         v.reserve(views.size());
         for (const auto& g : views) v.push_back(g.view());
         const etcu_recon_params rp = p.reconParams(use_graph);
+        if (p.basisFunctions == "blobs") {  // the blob kernels of the projection factories
+            const etcu_blob_params b = p.blob.c();
+            check(etcu_blob_recon_create(vol.handle(), v.data(), (uint32_t)v.size(), host_projections, &rp, &b,
+                                         &blobRec_),
+                  vol.framework().handle());
+            if (p.enableVoxelization) voxelizer_.reset(new BlobVoxelizerOperator(vol, p.blob));
+            return;
+        }
         check(etcu_recon_create(vol.handle(), v.data(), (uint32_t)v.size(), host_projections, &rp, &rec_),
               vol.framework().handle());
     }
-    ~BlockIterativeReconstructionOperator() { etcu_recon_destroy(rec_); }
+    ~BlockIterativeReconstructionOperator() {
+        etcu_recon_destroy(rec_);
+        etcu_blob_recon_destroy(blobRec_);
+    }
     BlockIterativeReconstructionOperator(const BlockIterativeReconstructionOperator&) = delete;
     BlockIterativeReconstructionOperator& operator=(const BlockIterativeReconstructionOperator&) = delete;
 
     void run() { runNiterations(params_.iterations); }
     void runSingleIteration() { runNiterations(1); }
     void runNiterations(uint32_t n) {
-        check(etcu_recon_run(rec_, n), vol_->framework().handle());
+        if (blobRec_) {
+            check(etcu_blob_recon_run(blobRec_, n), vol_->framework().handle());
+            if (voxelizer_) voxelizer_->voxelize();  // BlockIterativeReconstructionOperator.cpp:75-78
+        } else {
+            check(etcu_recon_run(rec_, n), vol_->framework().handle());
+        }
         vol_->framework().synchronize();
     }
-    void getReconstructedVolume(float* host) const { vol_->download(host); }
-    std::vector<float> getReconstructedVolume() const { return vol_->download(); }
+    // the voxelised volume when blobs are voxelised (:82-90), else the volume
+    void getReconstructedVolume(float* host) const {
+        (voxelizer_ ? voxelizer_->getVoxelVolume() : *vol_).download(host);
+    }
+    std::vector<float> getReconstructedVolume() const {
+        return (voxelizer_ ? voxelizer_->getVoxelVolume() : *vol_).download();
+    }
     double lastResidualSq() const {
         double r = 0.0;
-        check(etcu_recon_last_residual_sq(rec_, &r), vol_->framework().handle());
+        if (blobRec_)
+            check(etcu_blob_recon_last_residual_sq(blobRec_, &r), vol_->framework().handle());
+        else
+            check(etcu_recon_last_residual_sq(rec_, &r), vol_->framework().handle());
         return r;
     }
     double dataResidualSq() const {
@@ -395,7 +495,11 @@ public:
     std::vector<uint32_t> viewOrder() const {
         std::vector<uint32_t> out(1u << 16);
         uint32_t n = 0;
-        check(etcu_recon_view_order(rec_, out.data(), (uint32_t)out.size(), &n), vol_->framework().handle());
+        if (blobRec_)
+            check(etcu_blob_recon_view_order(blobRec_, out.data(), (uint32_t)out.size(), &n),
+                  vol_->framework().handle());
+        else
+            check(etcu_recon_view_order(rec_, out.data(), (uint32_t)out.size(), &n), vol_->framework().handle());
         out.resize(n);
         return out;
     }
@@ -404,6 +508,8 @@ private:
     GPUMappedVolume* vol_;
     AlgebraicParameterSet params_;
     etcu_recon* rec_ = nullptr;
+    etcu_blob_recon* blobRec_ = nullptr;
+    std::unique_ptr<BlobVoxelizerOperator> voxelizer_;
 };
 
 // LR/io/datasource/MRCStack.cpp: a tilt series in an MRC file (modes 0/1/2/6) with an

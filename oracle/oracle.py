@@ -18,7 +18,7 @@ import ctypes
 import math
 import os
 from dataclasses import dataclass, field
-from typing import List, Optional, Sequence
+from typing import Dict, List, Optional, Sequence
 
 import numpy as np
 
@@ -440,6 +440,361 @@ def wbp(projections: np.ndarray, geometries, vg: "VolumeGeometry", lam: float = 
     for i, g in enumerate(geometries):
         back_project(vol, vg, g, wbp_filter(projections[i]), ray_length(vg, g, prec), lamb, samples, prec, weights)
     return vol
+
+
+# ----------------------------------------------------------------------------
+# Blob basis functions (model/blobs, algorithm/blobs, ocl_src/BlobRaytracer.hl)
+# ----------------------------------------------------------------------------
+@dataclass
+class BlobParameters:
+    """model/blobs/BlobParameters.cpp: Kaiser-Bessel blob (support radius a, degree m,
+    density fall-off alpha); createDefault() = (2.0, 2, 3.6)."""
+    support_radius: float = 2.0
+    degree: int = 2
+    density_falloff: float = 3.6
+
+    def _bessel(self, x: float, n: int = 40) -> float:
+        """evaluateModifiedBessel: I_m(x) by 40 series terms (m = the degree)."""
+        m = self.degree
+        total, summand = 0.0, _uint_pow(0.5 * x, m) / float(math.factorial(m))
+        for k in range(n):
+            total += summand
+            summand *= 0.25 * x * x / float((k + 1) * (k + m + 1))
+        return total
+
+    def evaluate(self, x: float) -> float:
+        """BlobParameters::evaluate (Lewitt 1992)."""
+        a, m, alpha = float(np.float32(self.support_radius)), self.degree, float(np.float32(self.density_falloff))
+        if 0 <= x <= a:
+            root = math.sqrt(1.0 - (x * x) / (a * a))
+            return 1.0 / self._bessel(alpha) * _uint_pow(root, m) * self._bessel(alpha * root)
+        return 0.0
+
+
+def _uint_pow(base: float, e: int) -> float:
+    """framework/NumericalAlgorithms.cpp uintPow (square and multiply)."""
+    if e == 0:
+        return 1.0
+    if e == 1:
+        return base
+    f = _uint_pow(base, e // 2)
+    return f * f * (1.0 if e % 2 == 0 else base)
+
+
+_BLOB_TABLES: Dict[tuple, np.ndarray] = {}
+
+
+def blob_ray_integration_samples(p: BlobParameters, count: int) -> np.ndarray:
+    """algorithm/blobs/BlobRayIntegrationSampler.cpp: line integral through the blob at
+    distance w = i * a / (count - 1), trapezoid-like sum of 1000 steps (kept per
+    parameters and count: the sums take seconds in Python)."""
+    key = (float(p.support_radius), int(p.degree), float(p.density_falloff), int(count))
+    if key not in _BLOB_TABLES:
+        _BLOB_TABLES[key] = _blob_ray_integration_samples(p, count)
+    return _BLOB_TABLES[key].copy()
+
+
+def _blob_ray_integration_samples(p: BlobParameters, count: int) -> np.ndarray:
+    a = float(np.float32(p.support_radius))
+    out = np.zeros(count, np.float32)
+    n = 1000
+    for i in range(count):
+        w = float(i) * a / float(count - 1)
+        d = math.sqrt(a * a - w * w)
+        delta = d / n
+        total = sum(p.evaluate(math.sqrt(w * w + float(k * k) * delta * delta)) for k in range(1, n + 1))
+        out[i] = np.float32(delta * (2.0 * total + p.evaluate(w)))
+    return out
+
+
+def blob_voxelization_kernel(p: BlobParameters) -> np.ndarray:
+    """algorithm/blobs/BlobVoxelizationKernelValues.cpp:49-67: the blob integrated over each
+    voxel of the (2 ceil(a) + 1)^3 neighbourhood with 20^3 samples summed one after another
+    in double (z, y, x order; a cumulative sum keeps that order), float32, [dz][dy][dx]."""
+    r = int(math.ceil(float(np.float32(p.support_radius))))
+    s = (np.arange(20) + 0.5) / 20.0
+    out = np.zeros((2 * r + 1,) * 3, np.float32)
+    ev = np.vectorize(p.evaluate)
+    for dz in range(-r, r + 1):
+        for dy in range(-r, r + 1):
+            for dx in range(-r, r + 1):
+                zz, yy, xx = np.meshgrid(dz - 0.5 + s, dy - 0.5 + s, dx - 0.5 + s, indexing="ij")
+                vals = ev(np.sqrt(xx * xx + yy * yy + zz * zz)).ravel()
+                out[dz + r, dy + r, dx + r] = np.float32(np.cumsum(vals)[-1] / 8000.0)
+    return out
+
+
+def blob_voxelize(blobs: np.ndarray, kernel: np.ndarray) -> np.ndarray:
+    """BlobVoxelizerOperator: VolumeConvolution.cl over the blob coefficients with a zero
+    border of the kernel radius (VolumeConvolutionOperator.cpp:30-37); float32 sums in
+    kernel order z, y, x."""
+    Z, Y, X = blobs.shape
+    r = kernel.shape[0] // 2
+    pad = np.zeros((Z + 2 * r, Y + 2 * r, X + 2 * r), np.float32)
+    pad[r:r + Z, r:r + Y, r:r + X] = blobs
+    out = np.zeros_like(blobs, dtype=np.float32)
+    for kz in range(kernel.shape[0]):
+        for ky in range(kernel.shape[1]):
+            for kx in range(kernel.shape[2]):
+                out = (out + kernel[kz, ky, kx] * pad[kz:kz + Z, ky:ky + Y, kx:kx + X]).astype(np.float32)
+    return out
+
+
+def _sample_blob(samples: np.ndarray, t: np.ndarray) -> np.ndarray:
+    """BlobRaytracer.hl SampleBlob: linear interpolation of the ray-integration table."""
+    n = samples.shape[0]
+    # OpenCL clamp(t, 0, 1) = min(max(t, 0), 1); a NaN distance (sqrt of a rounded-negative
+    # square) becomes 0 as fmax / fmin return the non-NaN operand
+    coord = (np.fmin(np.fmax(t, np.float32(0.0)), np.float32(1.0)) * np.float32(n - 1)).astype(np.float32)
+    left = np.floor(coord).astype(np.int64)
+    lv = samples[left]
+    rv = samples[np.minimum(n - 1, left + 1)]
+    f = (coord - left.astype(np.float32)).astype(np.float32)
+    return (lv + (rv - lv) * f).astype(np.float32)
+
+
+class _FloatMat4:
+    """framework/math/Matrix4x4.cpp in float32, step by step: at(column, row), multiply
+    (:312-328), determinantOfMinor / determinant / inverse by cofactors (:90-119, :208-220)."""
+
+    def __init__(self, cols=None):
+        self.v = [np.float32(0)] * 16
+        if cols is not None:
+            for c in range(4):
+                for r in range(4):
+                    self.v[4 * c + r] = np.float32(cols[c][r])
+
+    def at(self, c, r):
+        return self.v[4 * c + r]
+
+    def minor(self, dc, dr):
+        f = np.float32
+        c = [i if i < dc else i + 1 for i in range(3)]
+        r = [i if i < dr else i + 1 for i in range(3)]
+        a = self.at
+        t1 = f(f(a(c[1], r[1]) * a(c[2], r[2])) - f(a(c[1], r[2]) * a(c[2], r[1])))
+        t2 = f(f(a(c[1], r[0]) * a(c[2], r[2])) - f(a(c[1], r[2]) * a(c[2], r[0])))
+        t3 = f(f(a(c[1], r[0]) * a(c[2], r[1])) - f(a(c[1], r[1]) * a(c[2], r[0])))
+        return f(f(f(a(c[0], r[0]) * t1) - f(a(c[0], r[1]) * t2)) + f(a(c[0], r[2]) * t3))
+
+    def inverse(self):
+        f = np.float32
+        a = self.at
+        det = f(f(f(f(a(0, 0) * self.minor(0, 0)) - f(a(0, 1) * self.minor(0, 1))) + f(a(0, 2) * self.minor(0, 2)))
+                - f(a(0, 3) * self.minor(0, 3)))
+        o = f(f(1.0) / det)
+        out = _FloatMat4()
+        for c in range(4):
+            for r in range(4):
+                x = f(self.minor(c, r) * o)
+                if (r + c) % 2 == 1:
+                    x = f(x * f(-1.0))
+                out.v[4 * r + c] = x
+        return out
+
+    def __matmul__(self, b):
+        out = _FloatMat4()
+        for i in range(4):
+            for j in range(4):
+                v = np.float32(0)
+                for k in range(4):
+                    v = np.float32(v + np.float32(self.at(k, j) * b.at(i, k)))
+                out.v[4 * i + j] = v
+        return out
+
+
+def float_perspective_projection(g: ScannerGeometry) -> "_FloatMat4":
+    """Matrix4x4::getPerspectiveProjection (Matrix4x4.cpp:376-399) in float32."""
+    f = np.float32
+    src, det = _f32(g.source).astype(f), _f32(g.detector).astype(f)
+    hp, vp = _f32(g.hpitch).astype(f), _f32(g.vpitch).astype(f)
+    dc = (det + f(0.5) * (f(g.width) * hp + f(g.height) * vp)).astype(f)
+    view = _FloatMat4([list(hp) + [0], list(vp) + [0], list((dc - src).astype(f)) + [0], list(src) + [1]]).inverse()
+    zn = f(1e-2)
+    proj = _FloatMat4([[1, 0, 0, 0], [0, 1, 0, 0], [0, 0, f(f(1) / f(f(1) - zn)), 1], [0, 0, f(-zn / f(f(1) - zn)), 0]])
+    tr = _FloatMat4([[1, 0, 0, 0], [0, 1, 0, 0], [0, 0, 1, 0], [f(0.5) * f(g.width), f(0.5) * f(g.height), 0, 1]])
+    return tr @ proj @ view
+
+
+def projection_to_world(g: ScannerGeometry) -> np.ndarray:
+    """The blob kernels' projection2world: world2projection.inverse() of the float
+    perspective projection (PerspectiveBeamsForwardProjectionWithBlobsKernel.cpp:39-41),
+    as a row-major 4x4 float32 array."""
+    return np.array(float_perspective_projection(g).inverse().v, np.float32).reshape(4, 4).T
+
+
+def forward_project_blobs(volume: np.ndarray, vg: "VolumeGeometry", g: ScannerGeometry, p: BlobParameters,
+                          sample_count: int = 128) -> tuple:
+    """PerspectiveBeamsForwardProjectionWithBlobs.cl + BlobRaytracer.hl BlobTraverseRay:
+    the ray through pixel (x, y) (TransformCoordG of (x, y, 1) by projection_to_world)
+    steps slice by slice along its dominant axis; every voxel within
+    ceil(1.415 R / vs) of the pierced voxel whose centre is closer than R = a * vs.x to the
+    ray adds table(dist / R) * value (and table(dist / R) to the traversal length).
+    Vectorised over the rays, float32."""
+    f32 = np.float32
+    samples = blob_ray_integration_samples(p, sample_count)
+    inv = projection_to_world(g)
+    H, W = g.height, g.width
+    yy, xx = np.meshgrid(np.arange(H, dtype=np.float32), np.arange(W, dtype=np.float32), indexing="ij")
+    v = np.stack([xx.ravel(), yy.ravel(), np.ones(H * W, np.float32), np.ones(H * W, np.float32)])
+    wp = (inv @ v).astype(np.float32)
+    world = (wp[:3] / wp[3]).astype(np.float32)
+    src = _f32(g.source).astype(np.float32)[:, None]
+    d = (world - src).astype(np.float32)
+    ray = (d / np.sqrt((d * d).sum(0))).astype(np.float32)
+    X, Y, Z = vg.resolution
+    res = np.array([X, Y, Z])
+    vs = np.asarray(vg.voxel_size, np.float32)[:, None]
+    bmin = np.asarray(vg.bmin, np.float32)[:, None]
+    R = f32(f32(p.support_radius) * vs[0, 0])
+    grid = int(math.ceil(f32(1.415) * R / vs[0, 0]))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        tmin = ((bmin + f32(0.5) * vs - src) / ray).astype(np.float32)
+    absr = np.abs(ray)
+    axis = np.where((absr[0] >= np.maximum(absr[1], absr[2])), 0, np.where(absr[1] >= np.maximum(absr[0], absr[2]), 1, 2))
+    val = np.zeros(H * W, np.float32)
+    length = np.zeros(H * W, np.float32)
+    vol = np.asarray(volume, np.float32)
+    for ax in (0, 1, 2):
+        sel = np.nonzero(axis == ax)[0]
+        if sel.size == 0:
+            continue
+        r_ = ray[:, sel]
+        point = (src + tmin[ax, sel] * r_).astype(np.float32)
+        step = (r_ / r_[ax] * vs).astype(np.float32)
+        ex, ey = [(1, 2), (2, 0), (0, 1)][ax]
+        for _ in range(res[ax]):
+            base = np.floor((point - bmin) / vs).astype(np.int64)
+            for dy in range(-grid, grid + 1):
+                for dx in range(-grid, grid + 1):
+                    gc = base.copy()
+                    gc[ex] += dx
+                    gc[ey] += dy
+                    inside = np.all((gc >= 0) & (gc < res[:, None]), axis=0)
+                    if not inside.any():
+                        continue
+                    gci = gc[:, inside]
+                    ids = sel[inside]
+                    centre = (bmin + f32(0.5) * vs + gci.astype(np.float32) * vs).astype(np.float32)
+                    rr = r_[:, inside]
+                    sc = (src - centre).astype(np.float32)
+                    t = (-(sc * rr).sum(0)).astype(np.float32)
+                    c2r = (src + t * rr - centre).astype(np.float32)
+                    d2 = (c2r * c2r).sum(0).astype(np.float32)
+                    hit = d2 < R * R
+                    if not hit.any():
+                        continue
+                    wgt = _sample_blob(samples, (np.sqrt(d2[hit]) / R).astype(np.float32))
+                    gh = gci[:, hit]
+                    np.add.at(val, ids[hit], wgt * vol[gh[2], gh[1], gh[0]])
+                    np.add.at(length, ids[hit], wgt)
+            point = (point + step).astype(np.float32)
+    return val.reshape(H, W), length.reshape(H, W)
+
+
+def back_project_blobs(volume: np.ndarray, vg: "VolumeGeometry", g: ScannerGeometry, residual: np.ndarray,
+                       raylength: np.ndarray, lam: float, p: BlobParameters, sample_count: int = 256,
+                       mask: Optional[np.ndarray] = None) -> np.ndarray:
+    """PerspectiveBeamsBackProjectionWithBlobs.cl correct(), in place: every blob centre is
+    projected, the detector window its footprint can reach is bounded (asin / acos / sin of
+    the view angles), and every pixel of the window with a nonzero residual and a ray
+    length above 1 whose ray passes closer than R = a * vs.x to the centre adds
+    residual * table(dist / R) / length; the blob takes lambda * sum / sum(table) when the
+    weights exceed 1e-2, times mask / 255 with a prior-knowledge mask (uint8).  Vectorised
+    over the voxels, float32."""
+    f = np.float32
+    table = blob_ray_integration_samples(p, sample_count)
+    X, Y, Z = vg.resolution
+    vs = np.asarray(vg.voxel_size, f)
+    R = f(f(p.support_radius) * vs[0])
+    fp = float_perspective_projection(g)
+    w2p = np.array(fp.v, f).reshape(4, 4).T  # the float projection matrix, row-major
+    p2w = np.array(fp.inverse().v, f).reshape(4, 4).T
+    src = _f32(g.source).astype(f)
+    det = _f32(g.detector).astype(f)
+    hp, vp = _f32(g.hpitch).astype(f), _f32(g.vpitch).astype(f)
+    zz, yy, xx = np.meshgrid(np.arange(Z), np.arange(Y), np.arange(X), indexing="ij")
+    centre = np.stack([np.asarray(vg.bmin, f)[i] + (g_.astype(f) + f(0.5)) * vs[i]
+                       for i, g_ in enumerate((xx.ravel(), yy.ravel(), zz.ravel()))]).astype(f)
+    c4 = np.vstack([centre, np.ones((1, centre.shape[1]), f)])
+    proj = (w2p @ c4).astype(f)
+    params = (proj[:2] / proj[3]).astype(f)
+    ok = proj[3] > 0
+    pv = (det[:, None] + params[0] * hp[:, None] + params[1] * vp[:, None] - src[:, None]).astype(f)
+    q = (centre - src[:, None]).astype(f)
+    lp = np.sqrt((pv * pv).sum(0)).astype(f)
+    lq = np.sqrt((q * q).sum(0)).astype(f)
+    ldx, ldy = f(np.sqrt((hp * hp).sum())), f(np.sqrt((vp * vp).sum()))
+    r = (R * lp / lq).astype(f)
+    alpha = np.arcsin(R / lq).astype(f)
+    bx = np.arccos(((hp[:, None] * pv).sum(0) / (ldx * lp)).astype(f)).astype(f)
+    by = np.arccos(((vp[:, None] * pv).sum(0) / (ldy * lp)).astype(f)).astype(f)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        wx = (np.maximum(r / np.sin(bx - alpha), r / np.sin(bx + alpha)) / ldx).astype(f)
+        wy = (np.maximum(r / np.sin(by - alpha), r / np.sin(by + alpha)) / ldy).astype(f)
+    ok &= (wx < 4096) & (wy < 4096)  # windows that are not finite or wider than any detector: skipped
+    sx = np.where(ok, np.ceil(np.where(ok, wx, 0)), 0).astype(np.int64)
+    sy = np.where(ok, np.ceil(np.where(ok, wy, 0)), 0).astype(np.int64)
+    base = np.trunc(params + f(0.5) * np.sign(params)).astype(np.int64)
+    H, W = residual.shape
+    val = np.zeros(centre.shape[1], f)
+    acc = np.zeros(centre.shape[1], f)
+    R2 = f(R * R)
+    for dy in range(-int(sy.max()), int(sy.max()) + 1):
+        for dx in range(-int(sx.max()), int(sx.max()) + 1):
+            use = ok & (np.abs(dx) <= sx) & (np.abs(dy) <= sy)
+            px, py = base[0] + dx, base[1] + dy
+            use &= (px >= 0) & (py >= 0) & (px < W) & (py < H)
+            ids = np.nonzero(use)[0]
+            if ids.size == 0:
+                continue
+            pxs, pys = px[ids], py[ids]
+            ln = raylength[pys, pxs]
+            res = residual[pys, pxs]
+            take = (res != 0) & (ln > 1.0)
+            ids, pxs, pys, ln, res = ids[take], pxs[take], pys[take], ln[take], res[take]
+            if ids.size == 0:
+                continue
+            pc = (p2w @ np.vstack([pxs.astype(f), pys.astype(f), np.ones_like(ln), np.ones_like(ln)])).astype(f)
+            d = (pc[:3] / pc[3] - src[:, None]).astype(f)
+            d = (d / np.sqrt((d * d).sum(0))).astype(f)
+            s2b = q[:, ids]
+            t0 = (d * s2b).sum(0).astype(f)
+            dist2 = ((s2b * s2b).sum(0) - t0 * t0).astype(f)
+            hit = R2 > dist2
+            with np.errstate(invalid="ignore"):
+                wgt = _sample_blob(table, np.sqrt(dist2[hit] / R2).astype(f))
+            np.add.at(acc, ids[hit], wgt)
+            np.add.at(val, ids[hit], (res[hit] * wgt / ln[hit]).astype(f))
+    upd = acc > f(1e-2)
+    flat = volume.reshape(-1)
+    step = (f(lam) * val[upd]).astype(f)
+    if mask is not None:
+        step = (step * (mask.reshape(-1)[upd].astype(f) / f(255.0)).astype(f)).astype(f)
+    flat[upd] = (flat[upd] + step / acc[upd]).astype(f)
+    return volume
+
+
+def blob_block_iterations(volume: np.ndarray, vg: "VolumeGeometry", geometries, projections: np.ndarray,
+                          order, block_size: int, lam: float, p: BlobParameters, iterations: int = 1) -> float:
+    """BlockIterativeReconstructionOperator.cpp:84-160 with blob basis functions, in place:
+    per block of ``order``, the blob forward projection (256-entry table,
+    DefaultForwardProjectionCreator.cpp:56) of every view into cleared images, residual =
+    measured - virtual, then the blob back projection of every view with lambda / block
+    size.  Returns the sum of squared residuals of the last iteration."""
+    order = list(order)
+    rsq = 0.0
+    for _ in range(iterations):
+        rsq = 0.0
+        for b0 in range(0, len(order), block_size):
+            blk = order[b0:b0 + block_size]
+            fps = [forward_project_blobs(volume, vg, geometries[i], p, 256) for i in blk]
+            res = [(projections[i] - fps[j][0]).astype(np.float32) for j, i in enumerate(blk)]
+            rsq += float(sum((r.astype(np.float64) ** 2).sum() for r in res))
+            for j, i in enumerate(blk):
+                back_project_blobs(volume, vg, geometries[i], res[j], fps[j][1],
+                                   float(np.float32(lam) / np.float32(len(blk))), p)
+    return rsq
 
 
 def long_object_compensation(proj: np.ndarray, length: np.ndarray, constant_length: float):

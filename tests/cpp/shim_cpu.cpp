@@ -78,6 +78,8 @@ int main(int argc, char** argv) {
                        f);
             std::fclose(f);
         }
+        const std::vector<float> blob = BlobParameters::createDefault().rayIntegrationSamples(4);
+        std::printf("blob %.6f %.6f %.6f\n", blob[0], blob[1], blob[3]);
         XMLParameterSource src(xml);
         const auto p = AlgebraicParameterSet::fromConfig(src.values());
         const std::string proj = src.getPathParameter("input.projections");

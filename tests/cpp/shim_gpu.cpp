@@ -94,6 +94,48 @@ int main(int argc, char** argv) {
                     {{"algorithm", "wbp"}, {"algorithm.numberOfIterations", "1"}, {"algorithm.lambda", "1.0"}}));
         wbp.run();
         save(dir, "wbp_volume.bin", wbp.getReconstructedVolume().data(), wvol.voxelCount());
+        // blob basis functions: perspective views of a 24^3 phantom, blob SART from the
+        // configuration keys with voxelisation of the result
+        {
+            const uint32_t B = 24, D = 32, BV = 4;
+            std::vector<float> ph(B * B * B);
+            for (uint32_t i = 0; i < ph.size(); ++i) ph[i] = (float)((i * 7 + (i / B) * 13) % 11) / 10.f;
+            GPUMappedVolume pvol(fw, {B, B, B});
+            pvol.upload(ph.data());
+            etcu_view base{};
+            const float pitch = 0.1f / (float)D;
+            const float src[3] = {0.f, 0.f, -160.f}, det[3] = {-0.05f, -0.05f, -159.f};
+            for (int i = 0; i < 3; ++i) {
+                base.source[i] = src[i];
+                base.detector[i] = det[i];
+                base.hpitch[i] = i == 0 ? pitch : 0.f;
+                base.vpitch[i] = i == 1 ? pitch : 0.f;
+            }
+            base.width = base.height = D;
+            base.perspective = 1;
+            std::vector<ScannerGeometry> bviews;
+            std::vector<float> bprojs(BV * D * D);
+            ForwardProjectionOperator bfp(pvol, BlobParameters::createDefault());
+            for (uint32_t i = 0; i < BV; ++i) {
+                bviews.push_back(ScannerGeometry(base).rotated(-45.f + 30.f * (float)i));
+                bfp.setScannerGeometry(bviews.back());
+                cuda(cudaMemset(dv, 0, D * D * 4));
+                cuda(cudaMemset(dl, 0, D * D * 4));
+                bfp.SetOutput(dv, dl);
+                bfp.Execute(0);
+                cuda(cudaMemcpy(bprojs.data() + i * D * D, dv, D * D * 4, cudaMemcpyDeviceToHost));
+            }
+            save(dir, "blob_projections.bin", bprojs.data(), bprojs.size());
+            const AlgebraicParameterSet bp2 = AlgebraicParameterSet::fromConfig(
+                {{"algorithm", "sart"}, {"algorithm.numberOfIterations", "1"}, {"algorithm.lambda", "0.5"},
+                 {"optimization.projectionIteration", "identity"}, {"algorithm.basisFunctions", "blobs"},
+                 {"output.options.enableVoxelization", "true"}});
+            GPUMappedVolume bvol2(fw, {B, B, B});
+            BlockIterativeReconstructionOperator brec(bvol2, bviews, bprojs.data(), bp2);
+            brec.run();
+            save(dir, "blob_coefficients.bin", bvol2.download().data(), bvol2.voxelCount());
+            save(dir, "blob_voxels.bin", brec.getReconstructedVolume().data(), bvol2.voxelCount());
+        }
         cudaFree(dv);
         cudaFree(dl);
         cudaFree(dr);

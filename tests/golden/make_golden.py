@@ -19,6 +19,9 @@ Fixtures (reference test that uses each one):
               virtual_projection_reference}.tif (test/src/unit/LongObjectCompensationTest.cpp:129-164)
   persp.npz   perspective/{projection,intersection_lengths}_reference.tif
               (ForwardProjectionTest.cpp:163-183, :267-304)
+  blobs.npz   blobs/voxelized_reference.mrc (test/src/unit/BlobTest.cpp:113-131) and
+              perspective/intersection_lengths_blobs_reference.tif
+              (ForwardProjectionTest.cpp:238-265, :306-338)
   synth.npz   synthetic_3_parallel/ground_truth.mrc plus five of its 180 projections
               (test/src/integration/SyntheticReconstruction.cpp:66-172); the other
               projections are forward projections of ground_truth and are regenerated.
@@ -70,6 +73,9 @@ def main(root: str) -> None:
     np.savez_compressed(os.path.join(OUT, "persp.npz"),
                         projection=read_tif(os.path.join(pe, "projection_reference.tif")),
                         intersection_lengths=read_tif(os.path.join(pe, "intersection_lengths_reference.tif")))
+    np.savez_compressed(os.path.join(OUT, "blobs.npz"),
+                        voxelized=read_mrc(os.path.join(d, "blobs", "voxelized_reference.mrc")),
+                        intersection_lengths=read_tif(os.path.join(pe, "intersection_lengths_blobs_reference.tif")))
     sy = os.path.join(d, "synthetic_3_parallel")
     syn = {"ground_truth": read_mrc(os.path.join(sy, "ground_truth.mrc")),
            "angles": np.array(SYNTH_ANGLES, np.float32)}

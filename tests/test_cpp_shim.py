@@ -50,6 +50,9 @@ def test_cpp_shim_host_side(tmp_path):
     assert lines["stack"][1:] == ["2", "6", "5", "-30", "45.5", "1.75", "-1.75"]
     assert lines["tiff"][1:] == ["6", "5", "7.25"]
     assert lines["xml"][1:] == ["sirt", "4", "0.5", "/sub/dir"]
+    from oracle import oracle as O
+    blob = O.blob_ray_integration_samples(O.BlobParameters(), 4)
+    assert [float(v) for v in lines["blob"][1:]] == pytest.approx([blob[0], blob[1], blob[3]], abs=1e-6)
     import torch
     if torch.cuda.is_available():
         assert lines["framework"][1] == "ok"

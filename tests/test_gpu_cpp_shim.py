@@ -47,3 +47,20 @@ def test_cpp_shim_projectors_and_sart_match_oracle(tmp_path):
     assert O.rel_l2(load("sart_volume.bin", (Z, Y, X)), vo) <= 1e-3
     vw = O.wbp(projs, [oracle_geometry(q) for q in geoms], vg)
     assert O.rel_l2(load("wbp_volume.bin", (Z, Y, X)), vw) <= 1e-4
+    # blob basis functions: forward projections, one blob SART iteration, voxelisation
+    from ettention_b200.operators import ScannerGeometry
+    B, D = 24, 32
+    i = np.arange(B ** 3, dtype=np.int64)
+    ph = (((i * 7 + (i // B) * 13) % 11).astype(np.float32) / np.float32(10.0)).reshape(B, B, B)
+    base = ScannerGeometry([0.0, 0.0, -160.0], [-0.05, -0.05, -159.0], [0.1 / D, 0, 0], [0, 0.1 / D, 0], D, D, True)
+    bgeoms = [oracle_geometry(base.rotated(-45.0 + 30.0 * k)) for k in range(4)]
+    bvg = O.VolumeGeometry.centered((B, B, B))
+    bprojs = load("blob_projections.bin", (4, D, D))
+    want = np.stack([O.forward_project_blobs(ph, bvg, q, O.BlobParameters(), 256)[0] for q in bgeoms])
+    assert O.rel_l2(bprojs, want) <= 1e-5
+    coeff = np.zeros((B, B, B), np.float32)
+    O.blob_block_iterations(coeff, bvg, bgeoms, bprojs, [0, 1, 2, 3], 1, 0.5, O.BlobParameters())
+    got = load("blob_coefficients.bin", (B, B, B))
+    assert O.rel_l2(got, coeff) <= 1e-4
+    vox = O.blob_voxelize(got, O.blob_voxelization_kernel(O.BlobParameters()))
+    assert np.array_equal(load("blob_voxels.bin", (B, B, B)), vox)
