@@ -155,6 +155,7 @@ _SIG = {
     "etcu_blob_recon_last_residual_sq": (_S, [_P, ctypes.POINTER(ctypes.c_double)]),
     "etcu_blob_recon_view_order": (_S, [_P, _P, _U, ctypes.POINTER(_U)]),
     "etcu_blob_recon_launches_per_iteration": (_U, [_P]),
+    "etcu_blob_recon_profile_iteration": (_S, [_P, _P, _P]),
     "etcu_blob_recon_destroy": (_S, [_P]),
     "etcu_batch_create": (_S, [_P, ctypes.POINTER(BatchSeries), _U, ctypes.POINTER(ReconParams), ctypes.POINTER(_P)]),
     "etcu_batch_destroy": (_S, [_P]),

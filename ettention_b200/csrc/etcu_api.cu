@@ -2119,7 +2119,10 @@ etcu_status blob_recon_build(etcu_volume* vol, const etcu_view* views, uint32_t 
     return ETCU_OK;
 }
 
-uint32_t issue_blob_iteration(etcu_blob_recon* r) {
+// ev (optional): one event pair per launch of kind 0 forward, 1 residual, 2 back, recorded
+// around it on the stream; kinds gets the kind of every launch.
+uint32_t issue_blob_iteration(etcu_blob_recon* r, std::vector<std::pair<cudaEvent_t, cudaEvent_t>>* ev = nullptr,
+                              std::vector<int>* kinds = nullptr) {
     etcu_volume* vol = r->vol;
     cudaStream_t st = r->ctx->stream;
     const size_t P = (size_t)r->W * r->H;
@@ -2139,22 +2142,37 @@ uint32_t issue_blob_iteration(etcu_blob_recon* r) {
         for (size_t sl = 0; sl < vol->slabs.size(); ++sl)
             for (uint32_t j = 0; j < n; ++j) {
                 const uint32_t v = r->order[b0 + j];
+                if (ev) cudaEventRecord((*ev)[launches].first, st);
                 launch_blob_fp(vol, vol->slabs[sl], r->views[v], r->p2w[v], r->support_radius, fpt, kBlobFpTable,
                                virt + j * P, trav + j * P, st);
+                if (ev) {
+                    cudaEventRecord((*ev)[launches].second, st);
+                    kinds->push_back(0);
+                }
                 ++launches;
             }
         for (uint32_t j = 0; j < n; ++j) {
             const uint32_t v = r->order[b0 + j];
             const int blocks = (int)std::min<size_t>((P + 255) / 256, 148 * 8);
+            if (ev) cudaEventRecord((*ev)[launches].first, st);
             blob_residual_kernel<<<blocks, 256, 0, st>>>(r->d_proj + (size_t)v * P, virt + j * P, res + j * P, P,
                                                          r->d_rsq);
+            if (ev) {
+                cudaEventRecord((*ev)[launches].second, st);
+                kinds->push_back(1);
+            }
             ++launches;
         }
         for (size_t k = vol->slabs.size(); k-- > 0;)  // doBackProjectionForBlock: sub-volumes last to first
             for (uint32_t j = 0; j < n; ++j) {
                 const uint32_t v = r->order[b0 + j];
+                if (ev) cudaEventRecord((*ev)[launches].first, st);
                 launch_blob_bp(vol, vol->slabs[k], r->views[v], r->w2p[v], r->p2w[v], r->support_radius, bpt,
                                kBlobBpTable, res + j * P, trav + j * P, r->lambda / (float)n, st);
+                if (ev) {
+                    cudaEventRecord((*ev)[launches].second, st);
+                    kinds->push_back(2);
+                }
                 ++launches;
             }
     }
@@ -2183,6 +2201,38 @@ extern "C" etcu_status etcu_blob_recon_run(etcu_blob_recon* r, uint32_t iteratio
         CK(ctx, cudaMemcpyAsync(&r->last_rsq, r->d_rsq, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     }
     CK(ctx, cudaStreamSynchronize(ctx->stream));
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_blob_recon_profile_iteration(etcu_blob_recon* r, float* ms_by_kind, uint32_t* n_by_kind) {
+    if (!r || !ms_by_kind || !n_by_kind) return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    etcu_context* ctx = r->ctx;
+    // per view: a forward and a back projection per sub-volume and one residual launch
+    const uint32_t n = (uint32_t)r->order.size() * (2 * (uint32_t)r->vol->slabs.size() + 1);
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev(n);
+    for (auto& e : ev) {
+        CK(ctx, cudaEventCreate(&e.first));
+        CK(ctx, cudaEventCreate(&e.second));
+    }
+    std::vector<int> kinds;
+    r->launches = issue_blob_iteration(r, &ev, &kinds);
+    CKL(ctx);
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    for (int k = 0; k < 3; ++k) {
+        ms_by_kind[k] = 0.f;
+        n_by_kind[k] = 0;
+    }
+    for (size_t i = 0; i < kinds.size(); ++i) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev[i].first, ev[i].second);
+        ms_by_kind[kinds[i]] += ms;
+        ++n_by_kind[kinds[i]];
+    }
+    for (auto& e : ev) {
+        cudaEventDestroy(e.first);
+        cudaEventDestroy(e.second);
+    }
+    CK(ctx, cudaMemcpy(&r->last_rsq, r->d_rsq, sizeof(double), cudaMemcpyDeviceToHost));
     return ETCU_OK;
 }
 

@@ -851,6 +851,14 @@ class _BlobBlockIterations:
     def launches(self) -> int:
         return int(lib().etcu_blob_recon_launches_per_iteration(self.handle))
 
+    def profile_iteration(self):
+        """One iteration with CUDA events around every launch:
+        {kind: (total ms, launches)} for 'forward', 'residual', 'back'."""
+        ms = np.zeros(3, np.float32)
+        cnt = np.zeros(3, np.uint32)
+        self.volume.ctx.check(lib().etcu_blob_recon_profile_iteration(self.handle, ms.ctypes.data, cnt.ctypes.data))
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(("forward", "residual", "back"))}
+
     def run(self, n: int) -> None:
         self.volume.ctx.check(lib().etcu_blob_recon_run(self.handle, int(n)))
         if self.voxelizer is not None:
@@ -1092,7 +1100,9 @@ class BlockIterativeReconstructionOperator:
 
     def profile_iteration(self):
         """Runs one iteration with per-launch CUDA events: (fp_ms, bp_ms, fp_launches, bp_launches)."""
-        self._voxels_only("the iteration profile")
+        if self._blobs is not None:
+            k = self._blobs.profile_iteration()
+            return k["forward"][0], k["back"][0], k["forward"][1], k["back"][1]
         f, b = ctypes.c_float(), ctypes.c_float()
         nf, nb = ctypes.c_uint32(), ctypes.c_uint32()
         self.volume.ctx.check(lib().etcu_recon_profile_iteration(self.handle, ctypes.byref(f), ctypes.byref(b),

@@ -390,6 +390,10 @@ ETCU_API etcu_status etcu_blob_recon_last_residual_sq(const etcu_blob_recon* rec
 ETCU_API etcu_status etcu_blob_recon_view_order(const etcu_blob_recon* rec, uint32_t* out, uint32_t capacity,
                                                uint32_t* count);
 ETCU_API uint32_t etcu_blob_recon_launches_per_iteration(const etcu_blob_recon* rec);
+/* Runs one iteration as etcu_blob_recon_run does with CUDA events around every launch:
+ * ms_by_kind[3] / n_by_kind[3] = total device milliseconds and launches of the forward
+ * projections, the residual launches and the back projections. */
+ETCU_API etcu_status etcu_blob_recon_profile_iteration(etcu_blob_recon* rec, float* ms_by_kind, uint32_t* n_by_kind);
 ETCU_API etcu_status etcu_blob_recon_destroy(etcu_blob_recon* rec);
 /* BlobVoxelizerOperator::voxelize: voxels = the blob coefficients convolved with the
  * voxelisation kernel (zero outside the volume); both FP32, same resolution. */

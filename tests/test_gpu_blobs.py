@@ -189,6 +189,8 @@ def test_blob_recon_vs_oracle(torch, ctx, block):
     got = rec.getReconstructedVolume()
     rsq = rec.last_residual_sq()
     assert rec.launches_per_iteration == 3 * len(geoms)
+    fp_ms, bp_ms, nf, nb = rec.profile_iteration()  # one more iteration, timed per launch
+    assert nf == nb == len(geoms) and fp_ms > 0 and bp_ms > 0
     rec.close()
     vol.close()
     want = np.zeros((24, 24, 24), np.float32)
