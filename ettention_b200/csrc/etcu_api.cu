@@ -41,6 +41,7 @@ struct etcu_context {
     cudaTextureObject_t pair_tex = 0;
     bool bp_column = true;  // column-pipelined single-view back projection (ETCU_BP_COLUMN=0 disables)
     bool fused_step = true; // fused SART step BP(p) + FP(p + 1) (ETCU_FUSED=0 disables)
+    bool fused_persist = true; // all fused steps of an iteration in one launch (ETCU_PERSIST=0 disables)
 };
 
 struct etcu_volume {
@@ -90,6 +91,11 @@ struct etcu_recon {
     std::vector<int> fuse_x0lo, fuse_ntaps;
     int2* d_jrange = nullptr;
     size_t fuse_smem = 0;
+    // every fused step of an iteration in one launch (sart_fused_persistent_kernel)
+    bool fuse_persist = false;
+    int fuse_window = 0, fuse_grid = 0;
+    int2* d_tapwin = nullptr;     // per view id
+    uint32_t* d_fuse_ctl = nullptr;  // unit counter + steps finished per row, then the error word
 };
 
 namespace {
@@ -626,6 +632,7 @@ extern "C" etcu_status etcu_context_create(int device, etcu_context** out) {
     c->stream = c->own_stream;
     if (const char* env = getenv("ETCU_BP_COLUMN")) c->bp_column = atoi(env) != 0;
     if (const char* env = getenv("ETCU_FUSED")) c->fused_step = atoi(env) != 0;
+    if (const char* env = getenv("ETCU_PERSIST")) c->fused_persist = atoi(env) != 0;
     *out = c.release();
     return ETCU_OK;
 }
@@ -1018,7 +1025,10 @@ void recon_free(etcu_recon* r) {
     dfree(ctx, r->rl_raw, r->rl_slot * r->slots * sizeof(float2) + ctx->tex_align);
     dfree(ctx, r->d_texs, r->slots * sizeof(cudaTextureObject_t));
     dfree(ctx, r->d_resid, sizeof(double));
-    dfree(ctx, r->d_jrange, (size_t)r->n_input * (r->vol->slabs.empty() ? 0 : r->vol->slabs[0].ry) * sizeof(int2));
+    const size_t ry = r->vol->slabs.empty() ? 0 : r->vol->slabs[0].ry;
+    dfree(ctx, r->d_jrange, (size_t)r->n_input * ry * sizeof(int2));
+    dfree(ctx, r->d_tapwin, (size_t)r->n_input * sizeof(int2));
+    dfree(ctx, r->d_fuse_ctl, (ry + 2) * sizeof(uint32_t));
 }
 
 // Forward projection of `count` views starting at order position `first`
@@ -1119,12 +1129,48 @@ void launch_fused_step(etcu_recon* r, uint32_t p, cudaStream_t st) {
     sart_fused_kernel<<<g.ry, kFuseThreads, fuse_smem_bytes(g.rx, g.rz, a.ntaps), st>>>(a);
 }
 
+// All M - 1 fused steps in one launch; the row counters are cleared first.
+void launch_fused_persistent(etcu_recon* r, cudaStream_t st) {
+    etcu_volume* vol = r->vol;
+    const SlabConst& g = vol->slabs[0];
+    const uint32_t M = (uint32_t)r->order.size();
+    cudaMemsetAsync(r->d_fuse_ctl, 0, ((size_t)g.ry + 1) * sizeof(uint32_t), st);
+    FuseArgs a{};
+    a.vol = vol->master;
+    a.slab = g;
+    a.views = r->d_views;
+    a.order = r->d_order;
+    a.samples = r->d_samples;
+    a.rl_pitch = r->rl_pitch;
+    a.W = (int)r->W;
+    a.H = (int)r->H;
+    a.lambda = r->params.lambda;
+    a.jrange = r->d_jrange;
+    a.real = r->d_proj;
+    a.resid_sq = r->d_resid;
+    a.loc = r->params.use_long_object_compensation ? 1 : 0;
+    FusePersist q{};
+    q.tapwin = r->d_tapwin;
+    q.rl0 = r->rl;
+    q.rl_slot = r->rl_slot;
+    q.steps = M - 1;
+    q.ctl = r->d_fuse_ctl;
+    q.error = r->d_fuse_ctl + g.ry + 1;
+    q.window = r->fuse_window;
+    sart_fused_persistent_kernel<<<r->fuse_grid, kFuseThreads, r->fuse_smem, st>>>(a, q);
+}
+
 uint32_t issue_fused_iteration(etcu_recon* r, cudaStream_t st) {
     const uint32_t M = (uint32_t)r->order.size();
     uint32_t n = issue_forward(r, 0, 1, st);
-    for (uint32_t p = 0; p + 1 < M; ++p) {
-        launch_fused_step(r, p, st);
+    if (r->fuse_persist) {
+        launch_fused_persistent(r, st);
         ++n;
+    } else {
+        for (uint32_t p = 0; p + 1 < M; ++p) {
+            launch_fused_step(r, p, st);
+            ++n;
+        }
     }
     // the last view's back projection reads the slot its FP wrote
     const uint32_t last = M - 1;
@@ -1132,26 +1178,82 @@ uint32_t issue_fused_iteration(etcu_recon* r, cudaStream_t st) {
     return n;
 }
 
-void fuse_limits(int dev, size_t smem, int& per_sm) {
+void fuse_limits(int dev, size_t smem, int& per_sm, int& persist_per_sm, int& sms) {
     static std::mutex mu;
     static std::vector<char> opted;
+    cudaDeviceProp prop;
+    const bool have_prop = cudaGetDeviceProperties(&prop, dev) == cudaSuccess;
+    if (!have_prop) cudaGetLastError();
     {
         std::lock_guard<std::mutex> lock(mu);
         if ((int)opted.size() <= dev) opted.resize(dev + 1, 0);
         if (!opted[dev]) {
-            cudaDeviceProp prop;
-            if (cudaGetDeviceProperties(&prop, dev) == cudaSuccess)
+            if (have_prop) {
                 cudaFuncSetAttribute(sart_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)prop.sharedMemPerBlockOptin);
+                cudaFuncSetAttribute(sart_fused_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)prop.sharedMemPerBlockOptin - 16);
+            }
             cudaGetLastError();
             opted[dev] = 1;
         }
     }
-    per_sm = 0;
+    sms = have_prop ? prop.multiProcessorCount : 0;
+    per_sm = persist_per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sart_fused_kernel, kFuseThreads, smem) != cudaSuccess) {
         cudaGetLastError();
         per_sm = 0;
     }
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&persist_per_sm, sart_fused_persistent_kernel, kFuseThreads,
+                                                      smem) != cudaSuccess) {
+        cudaGetLastError();
+        persist_per_sm = 0;
+    }
+}
+
+constexpr int kFuseMaxWindow = 16;
+
+// Dependency window of the persistent fused steps: the largest distance between a volume
+// row and a row that owns (under any view) one of the two detector rows the row's back
+// projection samples (under any view).  Covers both the residual a step reads (written
+// by the owners in the step before) and the residual slot it overwrites (read by the
+// samplers two steps before).  window = -1 when it exceeds kFuseMaxWindow.
+etcu_status fuse_window(etcu_recon* r, const std::vector<int2>& jrange, int& window) {
+    etcu_context* ctx = r->ctx;
+    const SlabConst& g = r->vol->slabs[0];
+    const uint32_t N = r->n_input;
+    const int H = (int)r->H;
+    const size_t T = (size_t)N * g.ry;
+    int* d_y0 = nullptr;
+    etcu_status s;
+    if ((s = dalloc(ctx, (void**)&d_y0, T * sizeof(int))) != ETCU_OK) return s;
+    std::vector<int> y0(T);
+    fuse_bp_rows_kernel<<<dim3((g.ry + 127) / 128, N), 128, 0, ctx->stream>>>(r->d_views, r->d_samples, g, H, d_y0);
+    cudaMemcpyAsync(y0.data(), d_y0, T * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+    const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    dfree(ctx, d_y0, T * sizeof(int));
+    CK(ctx, e);
+    std::vector<int> omin(H, INT32_MAX), omax(H, -1);
+    for (uint32_t v = 0; v < N; ++v)
+        for (int y = 0; y < g.ry; ++y) {
+            const int2 jr = jrange[(size_t)v * g.ry + y];
+            for (int j = jr.x; j < jr.y; ++j) {
+                omin[j] = std::min(omin[j], y);
+                omax[j] = std::max(omax[j], y);
+            }
+        }
+    window = 0;
+    for (uint32_t v = 0; v < N; ++v)
+        for (int y = 0; y < g.ry; ++y)
+            for (int j = y0[(size_t)v * g.ry + y]; j <= y0[(size_t)v * g.ry + y] + 1; ++j) {
+                if (j < 0 || j >= H || omax[j] < 0) continue;  // padding, or a row no ray writes
+                window = std::max(window, std::max(std::abs(omin[j] - y), std::abs(omax[j] - y)));
+                if (window > kFuseMaxWindow) {
+                    window = -1;
+                    return ETCU_OK;
+                }
+            }
+    return ETCU_OK;
 }
 
 // Whether every SART step of this reconstruction can run fused (sart_fused_kernel):
@@ -1182,8 +1284,8 @@ etcu_status plan_fused(etcu_recon* r, const std::vector<ViewConst>& vc, bool& ok
         ntaps[v] = plan.ntaps;
         smem = std::max(smem, fuse_smem_bytes(g.rx, g.rz, plan.ntaps));
     }
-    int per_sm = 0;
-    fuse_limits(ctx->device, smem, per_sm);
+    int per_sm = 0, persist_per_sm = 0, sms = 0;
+    fuse_limits(ctx->device, smem, per_sm, persist_per_sm, sms);
     if (per_sm < 1) return ETCU_OK;
     // detector rows of every (view, volume row)
     const size_t T = (size_t)N * (size_t)g.ry;
@@ -1212,10 +1314,26 @@ etcu_status plan_fused(etcu_recon* r, const std::vector<ViewConst>& vc, bool& ok
     }
     if ((s = dalloc(ctx, (void**)&r->d_jrange, T * sizeof(int2))) != ETCU_OK) return s;
     CK(ctx, cudaMemcpyAsync(r->d_jrange, table.data(), T * sizeof(int2), cudaMemcpyHostToDevice, ctx->stream));
-    r->fuse_x0lo = std::move(x0lo);
-    r->fuse_ntaps = std::move(ntaps);
     r->fuse_smem = smem;
     ok = true;
+    if (ctx->fused_persist && persist_per_sm >= 1 && sms > 0) {
+        int window = 0;
+        if ((s = fuse_window(r, table, window)) != ETCU_OK) return s;
+        if (window >= 0 && window <= kFuseMaxWindow) {
+            std::vector<int2> tw(N);
+            for (uint32_t v = 0; v < N; ++v) tw[v] = make_int2(x0lo[v], ntaps[v]);
+            if ((s = dalloc(ctx, (void**)&r->d_tapwin, N * sizeof(int2))) != ETCU_OK) return s;
+            CK(ctx, cudaMemcpyAsync(r->d_tapwin, tw.data(), N * sizeof(int2), cudaMemcpyHostToDevice, ctx->stream));
+            if ((s = dalloc(ctx, (void**)&r->d_fuse_ctl, ((size_t)g.ry + 2) * sizeof(uint32_t))) != ETCU_OK) return s;
+            CK(ctx, cudaMemsetAsync(r->d_fuse_ctl, 0, ((size_t)g.ry + 2) * sizeof(uint32_t), ctx->stream));
+            r->fuse_window = window;
+            r->fuse_grid = (int)std::min<long long>((long long)persist_per_sm * sms,
+                                                    (long long)(r->order.size() - 1) * g.ry);
+            r->fuse_persist = true;
+        }
+    }
+    r->fuse_x0lo = std::move(x0lo);
+    r->fuse_ntaps = std::move(ntaps);
     return ETCU_OK;
 }
 
@@ -1381,7 +1499,7 @@ etcu_status recon_build(etcu_volume* vol, const etcu_view* views, uint32_t n_vie
         CK(ctx, cudaGraphInstantiate(&r->exec, g, 0));
         r->launches = n;
     } else {
-        r->launches = r->fused ? M + 1 : (uint32_t)(2 * S * r->nblocks);
+        r->launches = r->fused ? (r->fuse_persist ? 3 : M + 1) : (uint32_t)(2 * S * r->nblocks);
     }
     *out = r.release();
     return ETCU_OK;
@@ -1409,6 +1527,22 @@ extern "C" etcu_status etcu_recon_destroy(etcu_recon* rec) {
     return ETCU_OK;
 }
 
+// The persistent fused steps' error word (a wait that gave up), read after the stream's
+// work; cleared for the next run.
+etcu_status check_fused_waits(etcu_recon* r) {
+    if (!r->fuse_persist) return ETCU_OK;
+    etcu_context* ctx = r->ctx;
+    uint32_t* err = r->d_fuse_ctl + r->vol->slabs[0].ry + 1;
+    uint32_t h = 0;
+    CK(ctx, cudaMemcpyAsync(&h, err, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    if (h) {
+        CK(ctx, cudaMemsetAsync(err, 0, sizeof(uint32_t), ctx->stream));
+        return fail(ctx, ETCU_ERR_CUDA, "a fused SART step waited longer than its limit for its neighbour rows");
+    }
+    return ETCU_OK;
+}
+
 extern "C" etcu_status etcu_recon_run(etcu_recon* r, uint32_t iterations) {
     if (!r) return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL reconstruction");
     etcu_context* ctx = r->ctx;
@@ -1421,7 +1555,7 @@ extern "C" etcu_status etcu_recon_run(etcu_recon* r, uint32_t iterations) {
         }
     }
     CKL(ctx);
-    return ETCU_OK;
+    return check_fused_waits(r);
 }
 
 extern "C" etcu_status etcu_recon_last_residual_sq(etcu_recon* r, double* out) {
@@ -1501,7 +1635,7 @@ extern "C" etcu_status etcu_recon_profile_steps(etcu_recon* r, float* ms, uint32
     etcu_context* ctx = r->ctx;
     cudaStream_t st = ctx->stream;
     const uint32_t M = (uint32_t)r->order.size();
-    const uint32_t steps = r->fused ? M + 1 : 2 * r->nblocks;
+    const uint32_t steps = r->fused ? (r->fuse_persist ? 3 : M + 1) : 2 * r->nblocks;
     *count = steps;
     if (!ms || !kinds || !launches) return ETCU_OK;
     if (capacity < steps) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "capacity %u < %u steps", capacity, steps);
@@ -1517,9 +1651,14 @@ extern "C" etcu_status etcu_recon_profile_steps(etcu_recon* r, float* ms, uint32
     cudaEventRecord(ev[0], st);
     if (r->fused) {
         mark(0, issue_forward(r, 0, 1, st));
-        for (uint32_t p = 0; p + 1 < M; ++p) {
-            launch_fused_step(r, p, st);
+        if (r->fuse_persist) {
+            launch_fused_persistent(r, st);
             mark(2, 1);
+        } else {
+            for (uint32_t p = 0; p + 1 < M; ++p) {
+                launch_fused_step(r, p, st);
+                mark(2, 1);
+            }
         }
         const uint32_t last = M - 1;
         mark(1, issue_backward(r, last, 1, st, r->rl + (size_t)(last & 1) * r->rl_slot));
@@ -1535,7 +1674,7 @@ extern "C" etcu_status etcu_recon_profile_steps(etcu_recon* r, float* ms, uint32
     CK(ctx, cudaStreamSynchronize(st));
     for (uint32_t i = 0; i < steps; ++i) cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]);
     for (auto& e : ev) cudaEventDestroy(e);
-    return ETCU_OK;
+    return check_fused_waits(r);
 }
 
 // ================================================================ weighted back projection

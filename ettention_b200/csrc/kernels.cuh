@@ -1200,21 +1200,32 @@ __host__ __device__ constexpr size_t fuse_smem_bytes(int rx, int rz, int ntaps) 
     return (size_t)bp_col_tap_slots(ntaps) * 16 + ((size_t)rz * 4 + 15) / 16 * 16 + 2 * (size_t)kFuseZc * rx * 4;
 }
 
-// Each thread owns two consecutive x voxels of the row and two rays.  Requires
+// Global loads of data that other blocks of the same launch write (the persistent
+// step's residual images): plain loads, not the read-only path.
+template <bool kCoherent>
+__device__ __forceinline__ float2 ld_rl(const float2* p) {
+    if (kCoherent) return *p;
+    return __ldg(p);
+}
+
+// One fused step of volume row y: BP of the view at order position p, FP of the view at
+// p + 1.  Each thread owns two consecutive x voxels of the row and two rays.  Requires
 // rx % 2 == 0, rx <= 2 * kFuseThreads, rx + rz - 1 <= kMaxDdaIterations (the walk cap is
-// never reached), at most kFuseRays * kFuseThreads rays per volume row.
-__global__ void __launch_bounds__(kFuseThreads, 2) sart_fused_kernel(const __grid_constant__ FuseArgs a) {
-    extern __shared__ __align__(16) unsigned char fuse_smem[];
+// never reached), at most kFuseRays * kFuseThreads rays per volume row.  kCoherent: the
+// residual images may have been written by other blocks of the same launch.
+template <bool kCoherent>
+__device__ __forceinline__ void fused_row_step(const FuseArgs& a, uint32_t p, int y, int x0lo, int ntaps,
+                                               const float2* rl_in, float2* rl_out,
+                                               unsigned char* fuse_smem) {
     const SlabConst& g = a.slab;
     const int rx = g.rx, ry = g.ry, rz = g.rz, tid = threadIdx.x;
-    const int y = blockIdx.x;
     float4* taps = (float4*)fuse_smem;
-    float* K = (float*)(taps + bp_col_tap_slots(a.ntaps));
-    float* buf = (float*)(fuse_smem + (size_t)bp_col_tap_slots(a.ntaps) * 16 + ((size_t)rz * 4 + 15) / 16 * 16);
+    float* K = (float*)(taps + bp_col_tap_slots(ntaps));
+    float* buf = (float*)(fuse_smem + (size_t)bp_col_tap_slots(ntaps) * 16 + ((size_t)rz * 4 + 15) / 16 * 16);
     const size_t chunk_elems = (size_t)kFuseZc * rx;
 
     // ---- back projection constants of view p (bp_sart_column_kernel, one item = row y)
-    const uint32_t vb = a.order[a.p];
+    const uint32_t vb = a.order[p];
     const ViewConst& vc = a.views[vb];
     const float4 s = a.samples[vb];
     for (int z = tid; z < rz; z += kFuseThreads)
@@ -1235,14 +1246,14 @@ __global__ void __launch_bounds__(kFuseThreads, 2) sart_fused_kernel(const __gri
         float b;
         split_coord<kSampleQ8>(fadd(av, vc.mat[13]), a.H, y0, b);
         const float omb = fsub(1.f, b);
-        const float2* r0 = a.rl_in + (ptrdiff_t)y0 * (ptrdiff_t)a.rl_pitch;
+        const float2* r0 = rl_in + (ptrdiff_t)y0 * (ptrdiff_t)a.rl_pitch;
         const float2* r1 = r0 + a.rl_pitch;
         const float2 zero = make_float2(0.f, 0.f);
-        for (int e = tid; e < a.ntaps; e += kFuseThreads) {
-            const int x0 = a.x0lo + e;
+        for (int e = tid; e < ntaps; e += kFuseThreads) {
+            const int x0 = x0lo + e;
             const bool in0 = x0 >= -kPad && x0 < a.W + kPad, in1 = x0 + 1 >= -kPad && x0 + 1 < a.W + kPad;
-            const float2 p0 = in0 ? __ldg(r0 + x0) : zero, q0 = in1 ? __ldg(r0 + x0 + 1) : zero;
-            const float2 p1 = in0 ? __ldg(r1 + x0) : zero, q1 = in1 ? __ldg(r1 + x0 + 1) : zero;
+            const float2 p0 = in0 ? ld_rl<kCoherent>(r0 + x0) : zero, q0 = in1 ? ld_rl<kCoherent>(r0 + x0 + 1) : zero;
+            const float2 p1 = in0 ? ld_rl<kCoherent>(r1 + x0) : zero, q1 = in1 ? ld_rl<kCoherent>(r1 + x0 + 1) : zero;
             const float2 P0 = make_float2(fadd(fmul(omb, p0.x), fmul(b, p1.x)), fadd(fmul(omb, p0.y), fmul(b, p1.y)));
             const float2 P1 = make_float2(fadd(fmul(omb, q0.x), fmul(b, q1.x)), fadd(fmul(omb, q0.y), fmul(b, q1.y)));
             taps[e + (e >> 3)] = make_float4(fmul(P0.x, lamd), P0.y, fmul(fsub(P1.x, P0.x), lamd), fsub(P1.y, P0.y));
@@ -1254,7 +1265,7 @@ __global__ void __launch_bounds__(kFuseThreads, 2) sart_fused_kernel(const __gri
     const float2 au = f2(A[0], A[1]);
 
     // ---- rays of view p + 1 in volume row y (fp_pixel with one sample, dda_setup)
-    const uint32_t vf = a.order[a.p + 1];
+    const uint32_t vf = a.order[p + 1];
     const ViewConst& fc = a.views[vf];
     const int2 jr = a.jrange[(size_t)vf * ry + y];
     const int nrays = jr.y > jr.x ? (jr.y - jr.x) * a.W : 0;
@@ -1327,8 +1338,8 @@ __global__ void __launch_bounds__(kFuseThreads, 2) sart_fused_kernel(const __gri
             const float2 f = __fadd2_rd(fma2(u, splat(256.f), splat(-127.5f)), splat(12582912.0f));
             int e0, e1;
             float a0, a1;
-            q8_tap_bits(f.x, a.x0lo, e0, a0);
-            q8_tap_bits(f.y, a.x0lo, e1, a1);
+            q8_tap_bits(f.x, x0lo, e0, a0);
+            q8_tap_bits(f.y, x0lo, e1, a1);
             const float2 ax = add2(f2(a0, a1), splat(-1.f));
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
@@ -1432,7 +1443,7 @@ __global__ void __launch_bounds__(kFuseThreads, 2) sart_fused_kernel(const __gri
             }
             const size_t pix = (size_t)gy * (size_t)a.W + (size_t)gx;
             const float r = fsub(a.real[(size_t)vf * (size_t)a.W * (size_t)a.H + pix], vv);
-            a.rl_out[(size_t)gy * a.rl_pitch + (size_t)gx] = make_float2(r, ll);
+            rl_out[(size_t)gy * a.rl_pitch + (size_t)gx] = make_float2(r, ll);
             r2 += (double)r * (double)r;
         }
     }
@@ -1440,6 +1451,114 @@ __global__ void __launch_bounds__(kFuseThreads, 2) sart_fused_kernel(const __gri
         for (int o = 16; o > 0; o >>= 1) r2 += __shfl_down_sync(0xffffffffu, r2, o);
         if ((tid & 31) == 0 && r2 != 0.0) atomicAdd(a.resid_sq, r2);
     }
+}
+
+__global__ void __launch_bounds__(kFuseThreads, 2) sart_fused_kernel(const __grid_constant__ FuseArgs a) {
+    extern __shared__ __align__(16) unsigned char fuse_smem[];
+    fused_row_step<false>(a, a.p, (int)blockIdx.x, a.x0lo, a.ntaps, a.rl_in, a.rl_out, fuse_smem);
+}
+
+// All fused steps of one SART iteration in one launch.  With parallel views tilted about
+// y, step p of volume row y reads and writes only row y of the volume, the detector rows
+// of row y's rays (written) and the two detector rows its back projection samples (read);
+// those belong to rows y - window .. y + window.  Blocks take (step, row) units from a
+// counter in step-major order and start a unit once those rows have finished the step
+// before, so rows run ahead of one another instead of every step waiting for the whole
+// volume (and its last partial wave of blocks).  A unit only waits on units taken before
+// it by running blocks, so the waits end; each is still bounded by kFuseWaitNs, after which
+// the block sets the error word and leaves, and every block leaves once it is set.
+struct FusePersist {
+    const int2* tapwin;   // per view id: (x0lo, ntaps) of its back projection
+    float2* rl0;          // texel (0, 0) of residual slot 0; slot 1 follows at rl_slot
+    size_t rl_slot;       // float2 units
+    uint32_t steps;       // fused steps per iteration (views - 1)
+    uint32_t* ctl;        // [0] unit counter, [1 + y] steps row y has finished (zeroed per iteration)
+    uint32_t* error;      // nonzero once a wait gave up (sticky)
+    int window;
+};
+
+constexpr unsigned long long kFuseWaitNs = 1000000000ull;
+
+__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_u32(uint32_t* p, uint32_t v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__global__ void __launch_bounds__(kFuseThreads, 2)
+    sart_fused_persistent_kernel(const __grid_constant__ FuseArgs a, const __grid_constant__ FusePersist q) {
+    extern __shared__ __align__(16) unsigned char fuse_smem[];
+    __shared__ uint32_t unit_s;
+    const uint32_t ry = (uint32_t)a.slab.ry;
+    const uint32_t total = q.steps * ry;
+    uint32_t* done = q.ctl + 1;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            uint32_t u = total;
+            if (ld_acquire_u32(q.error) == 0) {
+                u = atomicAdd(q.ctl, 1u);
+                if (u < total) {
+                    const uint32_t p = u / ry;
+                    const int y = (int)(u - p * ry);
+                    if (p > 0) {
+                        const int lo = max(0, y - q.window), hi = min((int)ry - 1, y + q.window);
+                        const unsigned long long t0 = global_ns();
+                        for (int yy = lo; yy <= hi && u < total; ++yy)
+                            while (ld_acquire_u32(done + yy) < p) {
+                                if (global_ns() - t0 > kFuseWaitNs) {
+                                    atomicExch(q.error, 1u);
+                                    u = total;
+                                    break;
+                                }
+                                __nanosleep(128);
+                            }
+                    }
+                } else {
+                    u = total;
+                }
+            }
+            unit_s = u;
+        }
+        __syncthreads();
+        const uint32_t u = unit_s;
+        if (u >= total) return;
+        const uint32_t p = u / ry;
+        const int y = (int)(u - p * ry);
+        const int2 tw = q.tapwin[a.order[p]];
+        fused_row_step<true>(a, p, y, tw.x, tw.y, q.rl0 + (size_t)(p & 1) * q.rl_slot,
+                             q.rl0 + (size_t)((p + 1) & 1) * q.rl_slot, fuse_smem);
+        __syncthreads();  // the unit's stores are issued and its shared memory is free
+        if (threadIdx.x == 0) {
+            __threadfence();
+            st_release_u32(done + y, p + 1);
+        }
+    }
+}
+
+// Detector row pair (y0, y0 + 1) the fused back projection of view v samples for volume
+// row y (the same arithmetic as fused_row_step), for the dependency window.
+__global__ void fuse_bp_rows_kernel(const ViewConst* views, const float4* samples, SlabConst g, int H, int* y0out) {
+    const int y = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
+    if (y >= g.ry) return;
+    const ViewConst& vc = views[v];
+    const float4 s = samples[v];
+    const float px0 = fadd(fadd(g.bmin.x, fmul(0.5f, g.vs.x)), s.x);
+    const float py = fadd(fadd(g.bmin.y, fmul(fadd((float)y, 0.5f), g.vs.y)), s.y);
+    const float av = fadd(fmul(vc.mat[1], px0), fmul(vc.mat[5], py));
+    int y0;
+    float b;
+    split_coord<kSampleQ8>(fadd(av, vc.mat[13]), H, y0, b);
+    y0out[(size_t)v * g.ry + y] = y0;
 }
 
 // Detector rows per volume row for the fused step: the rays of detector row j of a

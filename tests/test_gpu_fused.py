@@ -1,9 +1,11 @@
-"""The fused SART step (sart_fused_kernel: back projection of view p and forward projection
-of view p + 1 in one pass over each volume row) against the unfused kernels
-(bp_sart_column_kernel + the xz forward projector): the volumes and residual sums must
-be bit-identical, since the fused kernel performs the same operations in the same
-order; the fused path must be the one that ran (M + 1 launches per iteration instead of
-2 M); and one case is held to the oracle within the column kernel's tolerance."""
+"""The fused SART step (back projection of view p and forward projection of view p + 1 in
+one pass over each volume row), launched per step (sart_fused_kernel) and as one
+persistent launch per iteration (sart_fused_persistent_kernel), against the unfused
+kernels (bp_sart_column_kernel + the xz forward projector): the volumes and residual sums
+must be bit-identical, since the fused kernels perform the same operations in the same
+order; the fused paths must be the ones that ran (3 launches per iteration persistent,
+M + 1 per step, 2 M unfused); and one case is held to the oracle within the column
+kernel's tolerance."""
 import os
 
 import numpy as np
@@ -12,13 +14,21 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _context(fused):
+MODES = {"persistent": ("1", "1"), "step": ("1", "0"), "unfused": ("0", "0")}
+
+
+def _context(mode):
+    """persistent: all fused steps of an iteration in one launch (sart_fused_persistent_kernel);
+    step: one launch per fused step (sart_fused_kernel); unfused: the column BP and xz FP."""
     from ettention_b200.operators import Context
-    os.environ["ETCU_FUSED"] = "1" if fused else "0"
+    if mode in (True, False):
+        mode = "persistent" if mode else "unfused"
+    os.environ["ETCU_FUSED"], os.environ["ETCU_PERSIST"] = MODES[mode]
     try:
         return Context(0)
     finally:
         del os.environ["ETCU_FUSED"]
+        del os.environ["ETCU_PERSIST"]
 
 
 def _run(fused, res, geoms, projs, params, iters):
@@ -38,41 +48,56 @@ def _run(fused, res, geoms, projs, params, iters):
     return v, last, launches
 
 
-def _problem(res, det, angles, seed):
+def _problem(res, det, angles, seed, vpitch=1.0):
     from oracle import oracle as O
-    from ettention_b200.operators import mrc_base_geometry
+    from ettention_b200.operators import ScannerGeometry, mrc_base_geometry
     from tests.helpers import ellipsoid_phantom, oracle_geometry
     X, Y, Z = res
     truth = ellipsoid_phantom(res, 6, seed=seed)
     vg = O.VolumeGeometry.centered(res)
     base = mrc_base_geometry(*det)
+    if vpitch != 1.0:  # detector rows vpitch volume rows apart (rows of rays skip volume rows)
+        h = 0.5 * det[1] * vpitch
+        base = ScannerGeometry([base.source[0], -h, base.source[2]], [base.detector[0], -h, base.detector[2]],
+                               list(base.hpitch), [0.0, vpitch, 0.0], det[0], det[1], False)
     geoms = [base.rotated(float(a)) for a in angles]
     projs = np.stack([O.forward_project(truth, vg, oracle_geometry(g), 1, 32)[0] for g in geoms]).astype(np.float32)
     return geoms, projs
 
 
 CASES = [
-    # volume, detector, angles, order, long-object compensation
-    ((128, 64, 48), (128, 64), list(np.linspace(-70, 70, 15)) + [90.0, 0.0], "identity", True),
-    ((256, 32, 40), (200, 32), list(np.linspace(-60, 60, 9)), "random", False),
-    ((96, 16, 130), (96, 16), [-89.0, -45.0, -1.0, 0.0, 33.3, 60.0, 91.0, 180.0], "maxangle", True),
+    # volume, detector, angles, order, long-object compensation, detector row pitch
+    ((128, 64, 48), (128, 64), list(np.linspace(-70, 70, 15)) + [90.0, 0.0], "identity", True, 1.0),
+    ((256, 32, 40), (200, 32), list(np.linspace(-60, 60, 9)), "random", False, 1.0),
+    ((96, 16, 130), (96, 16), [-89.0, -45.0, -1.0, 0.0, 33.3, 60.0, 91.0, 180.0], "maxangle", True, 1.0),
+    ((64, 40, 24), (64, 16), list(np.linspace(-50, 50, 7)), "random", False, 2.5),
 ]
 
 
 @pytest.mark.parametrize("case", range(len(CASES)))
 def test_fused_step_is_bit_identical_to_unfused(case):
+    """The persistent launch, the per-step launches and the unfused kernels give the same
+    volume bit for bit (the steps of a volume row wait for the rows whose detector rows
+    they read or overwrite, so every row sees the same data as in step order)."""
     from ettention_b200.operators import AlgebraicParameterSet, ORDERS
-    res, det, angles, order, loc = CASES[case]
-    geoms, projs = _problem(res, det, angles, seed=100 + case)
+    res, det, angles, order, loc, vpitch = CASES[case]
+    geoms, projs = _problem(res, det, angles, seed=100 + case, vpitch=vpitch)
     p = AlgebraicParameterSet(algorithm="sart", block_size=1, iterations=2, lam=0.3, order=ORDERS[order],
                               use_long_object_compensation=loc)
-    vf, lf, nf = _run(True, res, geoms, projs, p, 2)
-    vu, lu, nu = _run(False, res, geoms, projs, p, 2)
+    vp, lp, np_ = _run("persistent", res, geoms, projs, p, 2)
+    vf, lf, nf = _run("step", res, geoms, projs, p, 2)
+    vu, lu, nu = _run("unfused", res, geoms, projs, p, 2)
     M = len(angles)
-    assert nf == M + 1 and nu == 2 * M, (nf, nu)
+    assert nu == 2 * M
+    if vpitch == 1.0:
+        assert nf == M + 1 and np_ == 3, (np_, nf, nu)
+    else:
+        assert (nf, np_) in ((M + 1, 3), (2 * M, 2 * M)), (np_, nf, nu)
     assert np.abs(vu).max() > 0
     assert np.array_equal(vf, vu)
+    assert np.array_equal(vp, vu)
     assert lf == pytest.approx(lu, rel=1e-12)  # FP64 sums of the same residuals, atomics in another order
+    assert lp == pytest.approx(lu, rel=1e-12)
 
 
 def test_fused_step_against_oracle():
@@ -85,7 +110,7 @@ def test_fused_step_against_oracle():
     geoms, projs = _problem(res, det, angles, seed=7)
     p = AlgebraicParameterSet(algorithm="sart", block_size=1, iterations=2, lam=0.5, order=_abi.ORDER_IDENTITY)
     v, _, n = _run(True, res, geoms, projs, p, 2)
-    assert n == len(angles) + 1
+    assert n == 3  # FP of the first view, the persistent fused steps, BP of the last view
     vg = O.VolumeGeometry.centered(res)
     setup = O.ReconstructionSetup(vg, [oracle_geometry(g) for g in geoms], projs, 0.5, 1, 1, 1)
     vo = np.zeros((res[2], res[1], res[0]), np.float32)
