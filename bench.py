@@ -267,8 +267,10 @@ FP_DRAM_BYTES_PER_VOXEL = (269974272 + 5381120) / 67108864
 BP_DRAM_BYTES_PER_VOXEL = (270639104 + 205491712) / 67108864
 # sart_fused_kernel, ncu capture of the 1024x1024x256 case (python bench.py --ncu-case
 # --ncu-res 1024,1024,256: the bench's own volume and detector, 268,435,456 voxels):
-# dram__bytes_read.sum + dram__bytes_write.sum per launch.
+# dram__bytes_read.sum + dram__bytes_write.sum per fused step: one launch of the per-step
+# kernel, and the persistent kernel's launch of the 8-view case (7 steps) divided by 7.
 FUSED_DRAM_BYTES_PER_VOXEL = (1086500000 + 1021966000) / 268435456
+PERSIST_DRAM_BYTES_PER_VOXEL = (7603772000 + 7516285000) / 7 / 268435456
 
 
 def dram_traffic():
@@ -417,6 +419,8 @@ def run_ours(args, rank, world, local):
     fused_launches = sum(l for k, _, l in steps if k == "fused")
     pairs = (N_VIEWS - 1) // fused_launches if fused_launches else 1
     fused_bytes *= pairs
+    if pairs > 1:
+        fused_traffic = PERSIST_DRAM_BYTES_PER_VOXEL * RES[0] * RES[1] * RES[2]
     fused_traffic *= pairs
     for kind, name, byts, traffic in (("fused", "sart_fused_step", fused_bytes, fused_traffic),
                                       ("forward", "forward_project", fp_bytes, fp_traffic),
@@ -437,9 +441,14 @@ def run_ours(args, rank, world, local):
         fk["moved_bytes"] = moved
         fk["moved_gbs"] = moved / (fk["avg_ms"] * 1e-3) / 1e9
         fk["moved_frac"] = fk["moved_gbs"] / hbm_peak
-        # ncu --set full of this kernel (profiles/sart_fused_1024x1024x256.md)
-        fk["ncu"] = {"issue_active_pct": 71.0, "ipc": 2.84, "dram_throughput_pct": 39.2,
-                     "shared_pipe_pct": 64.5, "alu_pipe_pct": 61.0}
+        # ncu --set full of the kernel that ran (profiles/sart_fused_persistent_1024x1024x256.md,
+        # profiles/sart_fused_1024x1024x256.md)
+        if pairs > 1:
+            fk["ncu"] = {"issue_active_pct": 72.7, "ipc": 2.91, "dram_throughput_pct": 41.2,
+                         "lsu_pipe_pct": 70.8, "alu_pipe_pct": 65.4, "warp_inst_per_step": 530.0e6}
+        else:
+            fk["ncu"] = {"issue_active_pct": 71.0, "ipc": 2.84, "dram_throughput_pct": 39.2,
+                         "lsu_pipe_pct": 70.2, "alu_pipe_pct": 61.0, "warp_inst_per_step": 515.6e6}
     dominant = max(per_kernel, key=lambda n: per_kernel[n]["total_ms"])
     dk = per_kernel[dominant]
     roofline = {"bound": "hbm", "kernel": dominant, "achieved": dk["gbs"], "peak": hbm_peak, "unit": "GB/s",
@@ -447,7 +456,8 @@ def run_ours(args, rank, world, local):
                 "bytes_model": ("one forward-projection view + one back-projection view per fused step "
                                 "(4V+4P+8P + 8V+8P) x view_pairs_per_launch; the launch moves moved_bytes of them"
                                 if dominant == "sart_fused_step" else "per-view byte model"),
-                "traffic_source": ("ncu dram bytes per launch of the 1024x1024x256 case" if dominant == "sart_fused_step"
+                "traffic_source": ("ncu dram bytes per fused step of the 1024x1024x256 case x view_pairs_per_launch"
+                                   if dominant == "sart_fused_step"
                                    else "ncu dram bytes of the 512x512x256 case, scaled by voxel count"),
                 "per_kernel": per_kernel}
     rec.close()
