@@ -42,6 +42,7 @@ struct etcu_context {
     bool bp_column = true;  // column-pipelined single-view back projection (ETCU_BP_COLUMN=0 disables)
     bool fused_step = true; // fused SART step BP(p) + FP(p + 1) (ETCU_FUSED=0 disables)
     bool fused_persist = true; // all fused steps of an iteration in one launch (ETCU_PERSIST=0 disables)
+    int fuse_withhold_row = -1; // tests of the bounded waits (ETCU_TEST_WITHHOLD_ROW)
 };
 
 struct etcu_volume {
@@ -633,6 +634,7 @@ extern "C" etcu_status etcu_context_create(int device, etcu_context** out) {
     if (const char* env = getenv("ETCU_BP_COLUMN")) c->bp_column = atoi(env) != 0;
     if (const char* env = getenv("ETCU_FUSED")) c->fused_step = atoi(env) != 0;
     if (const char* env = getenv("ETCU_PERSIST")) c->fused_persist = atoi(env) != 0;
+    if (const char* env = getenv("ETCU_TEST_WITHHOLD_ROW")) c->fuse_withhold_row = atoi(env);
     *out = c.release();
     return ETCU_OK;
 }
@@ -1157,6 +1159,7 @@ void launch_fused_persistent(etcu_recon* r, cudaStream_t st) {
     q.ctl = r->d_fuse_ctl;
     q.error = r->d_fuse_ctl + g.ry + 1;
     q.window = r->fuse_window;
+    q.withhold_row = r->ctx->fuse_withhold_row;
     sart_fused_persistent_kernel<<<r->fuse_grid, kFuseThreads, r->fuse_smem, st>>>(a, q);
 }
 

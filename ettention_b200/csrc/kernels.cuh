@@ -1475,6 +1475,7 @@ struct FusePersist {
     uint32_t* ctl;        // [0] unit counter, [1 + y] steps row y has finished (zeroed per iteration)
     uint32_t* error;      // nonzero once a wait gave up (sticky)
     int window;
+    int withhold_row;     // tests of the bounded waits: this row never reports step 0 (else -1)
 };
 
 constexpr unsigned long long kFuseWaitNs = 1000000000ull;
@@ -1520,6 +1521,10 @@ __global__ void __launch_bounds__(kFuseThreads, 2)
                                     u = total;
                                     break;
                                 }
+                                if (ld_acquire_u32(q.error) != 0) {  // another block gave up
+                                    u = total;
+                                    break;
+                                }
                                 __nanosleep(128);
                             }
                     }
@@ -1538,7 +1543,7 @@ __global__ void __launch_bounds__(kFuseThreads, 2)
         fused_row_step<true>(a, p, y, tw.x, tw.y, q.rl0 + (size_t)(p & 1) * q.rl_slot,
                              q.rl0 + (size_t)((p + 1) & 1) * q.rl_slot, fuse_smem);
         __syncthreads();  // the unit's stores are issued and its shared memory is free
-        if (threadIdx.x == 0) {
+        if (threadIdx.x == 0 && !(p == 0 && y == q.withhold_row)) {
             __threadfence();
             st_release_u32(done + y, p + 1);
         }

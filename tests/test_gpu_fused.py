@@ -133,3 +133,46 @@ def test_ineligible_reconstructions_fall_back():
     q = AlgebraicParameterSet(algorithm="sirt", block_size=3, iterations=1, lam=0.3, order=ORDERS["identity"])
     _, _, n = _run(True, res, geoms, projs, q, 1)
     assert n == 2
+
+
+def test_persistent_wait_gives_up_and_context_survives():
+    """The persistent launch's waits are bounded: with one row's first step never reported
+    (ETCU_TEST_WITHHOLD_ROW, a flag nothing sets), the units that need it wait out their
+    limit (1 s), the run returns an error status instead of hanging, and the same context
+    then runs another reconstruction with results equal to a fresh context's."""
+    import time
+    from ettention_b200 import _abi
+    from ettention_b200._abi import EttentionError
+    from ettention_b200.operators import (AlgebraicParameterSet, BlockIterativeReconstructionOperator, Context,
+                                          GPUMappedVolume)
+    res, det = (64, 32, 24), (64, 32)
+    geoms, projs = _problem(res, det, list(np.linspace(-60, 60, 11)), seed=9)
+    p = AlgebraicParameterSet(algorithm="sart", block_size=1, iterations=1, lam=0.5, order=_abi.ORDER_IDENTITY)
+    os.environ["ETCU_FUSED"], os.environ["ETCU_PERSIST"], os.environ["ETCU_TEST_WITHHOLD_ROW"] = "1", "1", "3"
+    try:
+        ctx = Context(0)
+    finally:
+        for k in ("ETCU_FUSED", "ETCU_PERSIST", "ETCU_TEST_WITHHOLD_ROW"):
+            del os.environ[k]
+    try:
+        vol = GPUMappedVolume(ctx, res)
+        rec = BlockIterativeReconstructionOperator(vol, geoms, projs, p)
+        assert rec.launches_per_iteration == 3
+        t0 = time.time()
+        with pytest.raises(EttentionError, match="waited longer than its limit"):
+            rec.runNiterations(1)
+        assert time.time() - t0 < 30
+        rec.close()
+        vol.close()
+        q = AlgebraicParameterSet(algorithm="sirt", block_size=_abi.BLOCK_ALL, iterations=2, lam=0.5,
+                                  order=_abi.ORDER_IDENTITY)
+        vol = GPUMappedVolume(ctx, res)
+        rec = BlockIterativeReconstructionOperator(vol, geoms, projs, q)
+        rec.run()
+        after = rec.getReconstructedVolume()
+        rec.close()
+        vol.close()
+    finally:
+        ctx.close()
+    fresh, _, _ = _run("unfused", res, geoms, projs, q, 2)
+    assert np.abs(fresh).max() > 0 and np.array_equal(after, fresh)
