@@ -279,6 +279,37 @@ def dram_traffic():
     return FP_DRAM_BYTES_PER_VOXEL * V, BP_DRAM_BYTES_PER_VOXEL * V, FUSED_DRAM_BYTES_PER_VOXEL * V
 
 
+def work_units(geoms):
+    """Algorithmic work of one iteration in the survey's units: forward-projection ray-voxel
+    steps (every ray of every view counted from the voxels it enters and leaves the volume
+    in: 1 + x cells crossed + z cells crossed; the views are tilted about y, so every
+    detector row repeats its rays' xz path) and back-projection voxel-view updates."""
+    X, Y, Z = RES
+    lo = np.array([-0.5 * X, -0.5 * Y, -0.5 * Z])
+    hi = -lo
+    steps = 0
+    for g in geoms:
+        src, det = np.asarray(g.source, np.float64), np.asarray(g.detector, np.float64)
+        hp, vp = np.asarray(g.hpitch, np.float64), np.asarray(g.vpitch, np.float64)
+        d = det - src
+        d /= np.linalg.norm(d)
+        i = np.arange(g.width, dtype=np.float64) + 0.5
+        o = src[None, :] + i[:, None] * hp[None, :] + (0.5 * g.height) * vp[None, :]
+        with np.errstate(divide="ignore", invalid="ignore"):
+            t0 = np.where(d != 0, (lo - o) / d, -np.inf)
+            t1 = np.where(d != 0, (hi - o) / d, np.inf)
+        tin = np.max(np.minimum(t0, t1), axis=1)
+        tout = np.min(np.maximum(t0, t1), axis=1)
+        hit = tout > tin
+        pin = o + tin[:, None] * d
+        pout = o + tout[:, None] * d
+        cin = np.clip(np.floor(pin - lo), 0, np.array(RES) - 1)
+        cout = np.clip(np.floor(pout - lo - 1e-9 * np.sign(d)), 0, np.array(RES) - 1)
+        n = 1 + np.abs(cout[:, 0] - cin[:, 0]) + np.abs(cout[:, 2] - cin[:, 2])
+        steps += int(n[hit].sum()) * g.height
+    return steps, X * Y * Z * len(geoms)
+
+
 # ------------------------------------------------------------------ CPU baseline (oracle)
 def cpu_sample_seconds(threads: int, views: int = 1):
     """Times the FP32 CPU restatement of the reference kernels (oracle/) on `views` views
@@ -476,6 +507,7 @@ def run_ours(args, rank, world, local):
                "sample": "1 of 61 views (FP + residual + BP) at full size, FP32 oracle, scaled x61 views x30 "
                          "iterations"}
     if rank == 0:
+        fp_steps, bp_updates = work_units(geoms)
         line = {"metric": "SART s to reach plain 30-iter residual", "value": value, "unit": "s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
                 "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -487,6 +519,9 @@ def run_ours(args, rank, world, local):
                 "e2e": e2e,
                 "gpu_launches": launches_per_iter * args.steps,
                 "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks.summary(),
+                "work": {"fp_ray_voxel_steps": fp_steps, "bp_voxel_view_updates": bp_updates,
+                         "units_per_s": (fp_steps + bp_updates) / (ms_per_step * 1e-3),
+                         "fp_steps_source": "entry and exit voxels of every ray of the 61 views"},
                 "residual_sq": {"before": d0, "after_warmup_and_timed": d1},
                 "learned_warm_start": "not built: plain SART only"}
         print(json.dumps(line), flush=True)
