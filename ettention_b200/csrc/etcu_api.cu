@@ -1221,17 +1221,15 @@ constexpr int kFuseMaxWindow = 16;
 // projection samples (under any view).  Covers both the residual a step reads (written
 // by the owners in the step before) and the residual slot it overwrites (read by the
 // samplers two steps before).  window = -1 when it exceeds kFuseMaxWindow.
-etcu_status fuse_window(etcu_recon* r, const std::vector<int2>& jrange, int& window) {
-    etcu_context* ctx = r->ctx;
-    const SlabConst& g = r->vol->slabs[0];
-    const uint32_t N = r->n_input;
-    const int H = (int)r->H;
+etcu_status fuse_window_of(etcu_context* ctx, const ViewConst* d_views, const float4* d_samples, const SlabConst& g,
+                           uint32_t N, uint32_t height, const std::vector<int2>& jrange, int& window) {
+    const int H = (int)height;
     const size_t T = (size_t)N * g.ry;
     int* d_y0 = nullptr;
     etcu_status s;
     if ((s = dalloc(ctx, (void**)&d_y0, T * sizeof(int))) != ETCU_OK) return s;
     std::vector<int> y0(T);
-    fuse_bp_rows_kernel<<<dim3((g.ry + 127) / 128, N), 128, 0, ctx->stream>>>(r->d_views, r->d_samples, g, H, d_y0);
+    fuse_bp_rows_kernel<<<dim3((g.ry + 127) / 128, N), 128, 0, ctx->stream>>>(d_views, d_samples, g, H, d_y0);
     cudaMemcpyAsync(y0.data(), d_y0, T * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
     const cudaError_t e = cudaStreamSynchronize(ctx->stream);
     dfree(ctx, d_y0, T * sizeof(int));
@@ -1256,6 +1254,44 @@ etcu_status fuse_window(etcu_recon* r, const std::vector<int2>& jrange, int& win
                     return ETCU_OK;
                 }
             }
+    return ETCU_OK;
+}
+
+etcu_status fuse_window(etcu_recon* r, const std::vector<int2>& jrange, int& window) {
+    return fuse_window_of(r->ctx, r->d_views, r->d_samples, r->vol->slabs[0], r->n_input, r->H, jrange, window);
+}
+
+// The (view, volume row) -> detector rows table of the fused steps (fuse_rows_kernel
+// evaluates dda_setup's row assignment on the device); ok = false when some volume row
+// has more than kFuseRays * kFuseThreads rays.
+etcu_status fuse_row_table(etcu_context* ctx, const ViewConst* d_views, const SlabConst& g, uint32_t N, uint32_t W,
+                           uint32_t H, std::vector<int2>& table, bool& ok) {
+    ok = false;
+    const size_t T = (size_t)N * (size_t)g.ry;
+    int *jb = nullptr, *je = nullptr;
+    etcu_status s;
+    if ((s = dalloc(ctx, (void**)&jb, T * sizeof(int))) != ETCU_OK) return s;
+    if ((s = dalloc(ctx, (void**)&je, T * sizeof(int))) != ETCU_OK) {
+        dfree(ctx, jb, T * sizeof(int));
+        return s;
+    }
+    std::vector<int> hb(T), he(T);
+    cudaMemsetAsync(jb, 0x7f, T * sizeof(int), ctx->stream);
+    cudaMemsetAsync(je, 0, T * sizeof(int), ctx->stream);
+    fuse_rows_kernel<<<dim3((H + 127) / 128, N), 128, 0, ctx->stream>>>(d_views, g, (int)H, jb, je);
+    cudaMemcpyAsync(hb.data(), jb, T * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+    cudaMemcpyAsync(he.data(), je, T * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+    const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    dfree(ctx, jb, T * sizeof(int));
+    dfree(ctx, je, T * sizeof(int));
+    CK(ctx, e);
+    table.assign(T, make_int2(0, 0));
+    for (size_t i = 0; i < T; ++i) {
+        const int b = hb[i], n = he[i] > b ? he[i] - b : 0;
+        if ((long long)n * W > (long long)kFuseRays * kFuseThreads) return ETCU_OK;
+        table[i] = make_int2(n ? b : 0, n ? he[i] : 0);
+    }
+    ok = true;
     return ETCU_OK;
 }
 
@@ -1292,29 +1328,11 @@ etcu_status plan_fused(etcu_recon* r, const std::vector<ViewConst>& vc, bool& ok
     if (per_sm < 1) return ETCU_OK;
     // detector rows of every (view, volume row)
     const size_t T = (size_t)N * (size_t)g.ry;
-    int *jb = nullptr, *je = nullptr;
+    std::vector<int2> table;
+    bool rows_ok = false;
     etcu_status s;
-    if ((s = dalloc(ctx, (void**)&jb, T * sizeof(int))) != ETCU_OK) return s;
-    if ((s = dalloc(ctx, (void**)&je, T * sizeof(int))) != ETCU_OK) {
-        dfree(ctx, jb, T * sizeof(int));
-        return s;
-    }
-    std::vector<int> hb(T), he(T);
-    cudaMemsetAsync(jb, 0x7f, T * sizeof(int), ctx->stream);
-    cudaMemsetAsync(je, 0, T * sizeof(int), ctx->stream);
-    fuse_rows_kernel<<<dim3((r->H + 127) / 128, N), 128, 0, ctx->stream>>>(r->d_views, g, (int)r->H, jb, je);
-    cudaMemcpyAsync(hb.data(), jb, T * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
-    cudaMemcpyAsync(he.data(), je, T * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
-    const cudaError_t e = cudaStreamSynchronize(ctx->stream);
-    dfree(ctx, jb, T * sizeof(int));
-    dfree(ctx, je, T * sizeof(int));
-    CK(ctx, e);
-    std::vector<int2> table(T);
-    for (size_t i = 0; i < T; ++i) {
-        const int b = hb[i], n = he[i] > b ? he[i] - b : 0;
-        if ((long long)n * r->W > (long long)kFuseRays * kFuseThreads) return ETCU_OK;
-        table[i] = make_int2(n ? b : 0, n ? he[i] : 0);
-    }
+    if ((s = fuse_row_table(ctx, r->d_views, g, N, r->W, r->H, table, rows_ok)) != ETCU_OK) return s;
+    if (!rows_ok) return ETCU_OK;
     if ((s = dalloc(ctx, (void**)&r->d_jrange, T * sizeof(int2))) != ETCU_OK) return s;
     CK(ctx, cudaMemcpyAsync(r->d_jrange, table.data(), T * sizeof(int2), cudaMemcpyHostToDevice, ctx->stream));
     r->fuse_smem = smem;
@@ -2442,6 +2460,14 @@ struct etcu_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     uint32_t launches = 0;
+    // the whole iteration of every series in one launch (sart_fused_batch_kernel)
+    bool persist = false;
+    FuseSeries* d_series = nullptr;
+    FuseSegment* d_segs = nullptr;
+    uint32_t nsegs = 0, total_units = 0, ctl_words = 0;
+    uint32_t* d_ctl = nullptr;  // [0] unit counter, then every series' row counters, then the error word
+    int grid = 0, threads = 0;
+    size_t smem = 0;
 };
 
 namespace {
@@ -2485,8 +2511,186 @@ void issue_batch_step(const etcu_batch* b, int step, cudaStream_t st) {
 etcu_status issue_batch_iteration(etcu_batch* b, cudaStream_t st) {
     etcu_context* ctx = b->ctx;
     CK(ctx, cudaMemsetAsync(b->d_resid, 0, sizeof(double) * b->n, st));
+    if (b->persist) {
+        CK(ctx, cudaMemsetAsync(b->d_ctl, 0, (size_t)(b->ctl_words - 1) * sizeof(uint32_t), st));
+        uint32_t* err = b->d_ctl + b->ctl_words - 1;
+        if (b->threads == 128)
+            sart_fused_batch_kernel<128><<<b->grid, 128, b->smem, st>>>(b->d_series, b->d_segs, b->nsegs,
+                                                                        b->total_units, b->d_ctl, err);
+        else
+            sart_fused_batch_kernel<kFuseThreads><<<b->grid, kFuseThreads, b->smem, st>>>(
+                b->d_series, b->d_segs, b->nsegs, b->total_units, b->d_ctl, err);
+        CKL(ctx);
+        return ETCU_OK;
+    }
     for (int k = 0; k < b->max_steps; ++k) issue_batch_step(b, k, st);
     CKL(ctx);
+    return ETCU_OK;
+}
+
+// One series as the persistent batch plan needs it (host view constants, samples and
+// the device copies made for the per-step path).
+struct BatchSeriesRec {
+    etcu_volume* vol;
+    SlabConst slab;
+    std::vector<ViewConst> vc;
+    std::vector<float4> hs;
+    const ViewConst* d_views;
+    const uint32_t* d_order;
+    const float4* d_samples;
+    const float* d_proj;
+    uint32_t W, H, M;
+};
+
+// Whether every series can run the fused SART steps (the conditions of plan_fused, series
+// by series); if so, builds the persistent batch: per series its tap windows, row table,
+// dependency window, two residual slots and row counters; the (step, series) segments in
+// step-major order.  Otherwise the batch keeps its per-step launches.
+etcu_status plan_batch_persistent(etcu_batch* b, const std::vector<BatchSeriesRec>& recs,
+                                  const etcu_recon_params* params) {
+    etcu_context* ctx = b->ctx;
+    if (!ctx->fused_step || !ctx->fused_persist || params->sampling != ETCU_SAMPLING_Q8 || params->fp_samples > 1 ||
+        params->bp_samples != 1)
+        return ETCU_OK;
+    const uint32_t n = (uint32_t)recs.size();
+    std::vector<FuseSeries> fs(n);
+    std::vector<std::vector<int2>> tables(n), tapwins(n);
+    std::vector<int> windows(n);
+    size_t smem = 0;
+    bool narrow = true;  // every row fits a block of 128 threads (256 voxels, 256 rays)
+    etcu_status s;
+    for (uint32_t i = 0; i < n; ++i) {
+        const BatchSeriesRec& rc = recs[i];
+        const SlabConst& g = rc.slab;
+        if (g.rx % 2 != 0 || g.rx > 2 * kFuseThreads || g.rx + g.rz - 1 > kMaxDdaIterations || g.ry > 65535 ||
+            rc.M > 65534)
+            return ETCU_OK;
+        const uint32_t N = (uint32_t)rc.vc.size();
+        tapwins[i].resize(N);
+        for (uint32_t v = 0; v < N; ++v) {
+            const ViewConst& c = rc.vc[v];
+            if (!c.fast2d || !row_constant(c) || c.hpitch.y != 0.f) return ETCU_OK;
+            BpColPlan plan;
+            if (!plan_bp_col(rc.vol, g, c, rc.hs[v], plan)) return ETCU_OK;
+            tapwins[i][v] = make_int2(plan.x0lo, plan.ntaps);
+            smem = std::max(smem, fuse_smem_bytes(g.rx, g.rz, plan.ntaps));
+        }
+        bool ok = false;
+        if ((s = fuse_row_table(ctx, rc.d_views, g, N, rc.W, rc.H, tables[i], ok)) != ETCU_OK) return s;
+        if (!ok) return ETCU_OK;
+        narrow &= g.rx <= 2 * 128;
+        for (const int2& jr : tables[i]) narrow &= (long long)(jr.y - jr.x) * rc.W <= (long long)kFuseRays * 128;
+        if ((s = fuse_window_of(ctx, rc.d_views, rc.d_samples, g, N, rc.H, tables[i], windows[i])) != ETCU_OK) return s;
+        if (windows[i] < 0 || windows[i] > kFuseMaxWindow) return ETCU_OK;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, ctx->device) != cudaSuccess) {
+        cudaGetLastError();
+        return ETCU_OK;
+    }
+    const int threads = narrow ? 128 : kFuseThreads;
+    const void* kern = narrow ? (const void*)sart_fused_batch_kernel<128>
+                              : (const void*)sart_fused_batch_kernel<kFuseThreads>;
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, kern) != cudaSuccess) {
+        cudaGetLastError();
+        return ETCU_OK;
+    }
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(prop.sharedMemPerBlockOptin - fa.sharedSizeBytes));
+    cudaGetLastError();
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return ETCU_OK;
+    }
+    if (per_sm < 1) return ETCU_OK;
+    // segments: unit steps 0 .. M of every series, step-major
+    uint32_t max_m = 0;
+    for (const auto& rc : recs) max_m = std::max(max_m, rc.M);
+    std::vector<FuseSegment> segs;
+    unsigned long long start = 0;
+    for (uint32_t st = 0; st <= max_m; ++st)
+        for (uint32_t i = 0; i < n; ++i)
+            if (st <= recs[i].M) {
+                segs.push_back(FuseSegment{(uint32_t)start, i, st});
+                start += (unsigned long long)recs[i].slab.ry;
+            }
+    if (start >= 0xffffffffull) return ETCU_OK;
+    // device data
+    uint32_t words = 1;
+    std::vector<uint32_t> done_off(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        done_off[i] = words;
+        words += (uint32_t)recs[i].slab.ry;
+    }
+    words += 1;  // the error word
+    if ((s = batch_alloc(b, (void**)&b->d_ctl, (size_t)words * sizeof(uint32_t))) != ETCU_OK) return s;
+    CK(ctx, cudaMemsetAsync(b->d_ctl, 0, (size_t)words * sizeof(uint32_t), ctx->stream));
+    for (uint32_t i = 0; i < n; ++i) {
+        const BatchSeriesRec& rc = recs[i];
+        const SlabConst& g = rc.slab;
+        const uint32_t N = (uint32_t)rc.vc.size();
+        int2 *d_jr, *d_tw;
+        if ((s = batch_alloc(b, (void**)&d_jr, tables[i].size() * sizeof(int2))) != ETCU_OK) return s;
+        if ((s = batch_alloc(b, (void**)&d_tw, N * sizeof(int2))) != ETCU_OK) return s;
+        CK(ctx, cudaMemcpyAsync(d_jr, tables[i].data(), tables[i].size() * sizeof(int2), cudaMemcpyHostToDevice,
+                                ctx->stream));
+        CK(ctx, cudaMemcpyAsync(d_tw, tapwins[i].data(), N * sizeof(int2), cudaMemcpyHostToDevice, ctx->stream));
+        const size_t pw = (size_t)rc.W + 2 * kPad, ph = (size_t)rc.H + 2 * kPad, slot = pw * ph;
+        float2* rl_base;
+        if ((s = batch_alloc(b, (void**)&rl_base, 2 * slot * sizeof(float2))) != ETCU_OK) return s;
+        CK(ctx, cudaMemsetAsync(rl_base, 0, 2 * slot * sizeof(float2), ctx->stream));
+        FuseSeries& f = fs[i];
+        f = FuseSeries{};
+        f.a.vol = rc.vol->master + slab_offset_elems(rc.vol, g);
+        f.a.slab = g;
+        f.a.views = rc.d_views;
+        f.a.order = rc.d_order;
+        f.a.samples = rc.d_samples;
+        f.a.rl_pitch = pw;
+        f.a.W = (int)rc.W;
+        f.a.H = (int)rc.H;
+        f.a.lambda = params->lambda;  // block size 1
+        f.a.jrange = d_jr;
+        f.a.real = rc.d_proj;
+        f.a.resid_sq = b->d_resid + i;
+        f.a.loc = params->use_long_object_compensation ? 1 : 0;
+        f.tapwin = d_tw;
+        f.rl0 = rl_base + kPad * pw + kPad;
+        f.rl_slot = slot;
+        f.done = b->d_ctl + done_off[i];
+        f.views = rc.M;
+        f.window = windows[i];
+    }
+    if ((s = batch_alloc(b, (void**)&b->d_series, n * sizeof(FuseSeries))) != ETCU_OK) return s;
+    if ((s = batch_alloc(b, (void**)&b->d_segs, segs.size() * sizeof(FuseSegment))) != ETCU_OK) return s;
+    CK(ctx, cudaMemcpyAsync(b->d_series, fs.data(), n * sizeof(FuseSeries), cudaMemcpyHostToDevice, ctx->stream));
+    CK(ctx, cudaMemcpyAsync(b->d_segs, segs.data(), segs.size() * sizeof(FuseSegment), cudaMemcpyHostToDevice,
+                            ctx->stream));
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    b->nsegs = (uint32_t)segs.size();
+    b->total_units = (uint32_t)start;
+    b->ctl_words = words;
+    b->smem = smem;
+    b->grid = (int)std::min<long long>((long long)per_sm * prop.multiProcessorCount, (long long)start);
+    b->threads = threads;
+    b->persist = true;
+    return ETCU_OK;
+}
+
+// The persistent batch's error word (a wait that gave up), read after the stream's work.
+etcu_status check_batch_waits(etcu_batch* b) {
+    if (!b->persist) return ETCU_OK;
+    etcu_context* ctx = b->ctx;
+    uint32_t* err = b->d_ctl + b->ctl_words - 1;
+    uint32_t h = 0;
+    CK(ctx, cudaMemcpyAsync(&h, err, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    if (h) {
+        CK(ctx, cudaMemsetAsync(err, 0, sizeof(uint32_t), ctx->stream));
+        return fail(ctx, ETCU_ERR_CUDA, "a fused SART step waited longer than its limit for its neighbour rows");
+    }
     return ETCU_OK;
 }
 
@@ -2503,6 +2707,8 @@ etcu_status batch_build(etcu_context* ctx, const etcu_batch_series* series, uint
     b->sampling = params->sampling;
     std::vector<FpArgs> fp(n);
     std::vector<BpArgs> bp(n);
+    std::vector<BatchSeriesRec> recs;
+    recs.reserve(n);
     bool all_fast2d = true, all_nocap = true;
     etcu_status s;
     for (uint32_t i = 0; i < n; ++i) {
@@ -2596,6 +2802,13 @@ etcu_status batch_build(etcu_context* ctx, const etcu_batch_series* series, uint
         g.lambda = params->lambda;  // block size 1 (BackProjectionKernel.cpp:94)
         g.samples = d_samples;
         g.nsamples = 1;
+        {
+            BatchSeriesRec rc{vol, slab, vc, std::vector<float4>(sr.n_views), d_views, d_order,
+                              reinterpret_cast<const float4*>(d_samples), d_proj, W, H, (uint32_t)order.size()};
+            for (uint32_t v = 0; v < sr.n_views; ++v)
+                rc.hs[v] = make_float4(pat[4 * v], pat[4 * v + 1], pat[4 * v + 2], pat[4 * v + 3]);
+            recs.push_back(std::move(rc));
+        }
         b->vols.push_back(vol);
         b->steps.push_back((int)order.size());
         b->max_steps = std::max(b->max_steps, (int)order.size());
@@ -2615,7 +2828,8 @@ etcu_status batch_build(etcu_context* ctx, const etcu_batch_series* series, uint
     CK(ctx, cudaMemcpyAsync(b->d_steps, b->steps.data(), sizeof(int) * n, cudaMemcpyHostToDevice, ctx->stream));
     CK(ctx, cudaMemsetAsync(b->d_resid, 0, sizeof(double) * n, ctx->stream));
     CK(ctx, cudaStreamSynchronize(ctx->stream));
-    b->launches = 2u * (uint32_t)b->max_steps;
+    if ((s = plan_batch_persistent(b, recs, params)) != ETCU_OK) return s;
+    b->launches = b->persist ? 1u : 2u * (uint32_t)b->max_steps;
     if (params->use_graph) {
         cudaStream_t cs = ctx->stream;
         CK(ctx, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
@@ -2672,7 +2886,7 @@ extern "C" etcu_status etcu_batch_run(etcu_batch* b, uint32_t iterations) {
         }
     }
     CKL(ctx);
-    return ETCU_OK;
+    return check_batch_waits(b);
 }
 
 extern "C" etcu_status etcu_batch_last_residual_sq(etcu_batch* b, double* out) {

@@ -1208,15 +1208,25 @@ __device__ __forceinline__ float2 ld_rl(const float2* p) {
     return __ldg(p);
 }
 
+// Unit kinds of fused_row_step: the fused step (BP of p, FP of p + 1), the forward
+// projection alone (the first view of an iteration, p + 1 = 0), the back projection alone
+// (the last view).
+constexpr int kUnitFused = 0, kUnitForward = 1, kUnitBack = 2;
+
 // One fused step of volume row y: BP of the view at order position p, FP of the view at
 // p + 1.  Each thread owns two consecutive x voxels of the row and two rays.  Requires
 // rx % 2 == 0, rx <= 2 * kFuseThreads, rx + rz - 1 <= kMaxDdaIterations (the walk cap is
-// never reached), at most kFuseRays * kFuseThreads rays per volume row.  kCoherent: the
-// residual images may have been written by other blocks of the same launch.
-template <bool kCoherent>
+// never reached), at most kFuseRays * kFuseThreads rays per volume row (kThreads in place of
+// kFuseThreads for a block of kThreads threads).  kCoherent: the
+// residual images may have been written by other blocks of the same launch.  kKind
+// kUnitForward skips the back projection (the volume is only read; p + 1 is the view),
+// kUnitBack the forward projection; each half performs the same operations as in the
+// fused step.
+template <bool kCoherent, int kKind = kUnitFused, int kThreads = kFuseThreads>
 __device__ __forceinline__ void fused_row_step(const FuseArgs& a, uint32_t p, int y, int x0lo, int ntaps,
                                                const float2* rl_in, float2* rl_out,
                                                unsigned char* fuse_smem) {
+    constexpr bool kBP = kKind != kUnitForward, kFP = kKind != kUnitBack;
     const SlabConst& g = a.slab;
     const int rx = g.rx, ry = g.ry, rz = g.rz, tid = threadIdx.x;
     float4* taps = (float4*)fuse_smem;
@@ -1225,11 +1235,12 @@ __device__ __forceinline__ void fused_row_step(const FuseArgs& a, uint32_t p, in
     const size_t chunk_elems = (size_t)kFuseZc * rx;
 
     // ---- back projection constants of view p (bp_sart_column_kernel, one item = row y)
-    const uint32_t vb = a.order[p];
+    const uint32_t vb = kBP ? a.order[p] : a.order[p + 1];
     const ViewConst& vc = a.views[vb];
     const float4 s = a.samples[vb];
-    for (int z = tid; z < rz; z += kFuseThreads)
-        K[z] = fmul(vc.mat[8], fadd(fadd(g.bmin.z, fmul(fadd((float)z, 0.5f), g.vs.z)), s.z));
+    if (kBP)
+        for (int z = tid; z < rz; z += kThreads)
+            K[z] = fmul(vc.mat[8], fadd(fadd(g.bmin.z, fmul(fadd((float)z, 0.5f), g.vs.z)), s.z));
     const int x2 = 2 * tid;
     const bool on = x2 < rx;
     float A[2];
@@ -1249,7 +1260,7 @@ __device__ __forceinline__ void fused_row_step(const FuseArgs& a, uint32_t p, in
         const float2* r0 = rl_in + (ptrdiff_t)y0 * (ptrdiff_t)a.rl_pitch;
         const float2* r1 = r0 + a.rl_pitch;
         const float2 zero = make_float2(0.f, 0.f);
-        for (int e = tid; e < ntaps; e += kFuseThreads) {
+        for (int e = tid; kBP && e < ntaps; e += kThreads) {
             const int x0 = x0lo + e;
             const bool in0 = x0 >= -kPad && x0 < a.W + kPad, in1 = x0 + 1 >= -kPad && x0 + 1 < a.W + kPad;
             const float2 p0 = in0 ? ld_rl<kCoherent>(r0 + x0) : zero, q0 = in1 ? ld_rl<kCoherent>(r0 + x0 + 1) : zero;
@@ -1265,9 +1276,9 @@ __device__ __forceinline__ void fused_row_step(const FuseArgs& a, uint32_t p, in
     const float2 au = f2(A[0], A[1]);
 
     // ---- rays of view p + 1 in volume row y (fp_pixel with one sample, dda_setup)
-    const uint32_t vf = a.order[p + 1];
+    const uint32_t vf = kFP ? a.order[p + 1] : vb;
     const ViewConst& fc = a.views[vf];
-    const int2 jr = a.jrange[(size_t)vf * ry + y];
+    const int2 jr = kFP ? a.jrange[(size_t)vf * ry + y] : make_int2(0, 0);
     const int nrays = jr.y > jr.x ? (jr.y - jr.x) * a.W : 0;
     const float3 ray = make_float3(fc.ray.x, fc.ray.y, fc.ray.z);
     const float3 inv = make_float3(fc.inv.x, fc.inv.y, fc.inv.z);
@@ -1283,7 +1294,7 @@ __device__ __forceinline__ void fused_row_step(const FuseArgs& a, uint32_t p, in
         const float sdist = fdiv(1.f, 1.f), off = fdiv(sdist, 2.f);
 #pragma unroll
         for (int i = 0; i < kFuseRays; ++i) {
-            const int k = tid + i * kFuseThreads;
+            const int k = tid + i * kThreads;
             acc[i] = 0.f;
             accl[i] = 0.f;
             walking[i] = false;
@@ -1324,7 +1335,7 @@ __device__ __forceinline__ void fused_row_step(const FuseArgs& a, uint32_t p, in
     };
     // BP update of chunk c in place (this thread's two columns), written back to the volume
     auto update = [&](int c) {
-        if (c >= nchunks || !on) return;
+        if (!kBP || c >= nchunks || !on) return;
         const int z0 = chunk_z0(c), z1 = min(rz, z0 + kFuseZc);
         float* cb = buf + (size_t)(c & 1) * chunk_elems;
         float* dst = a.vol + ((size_t)z0 * ry + y) * rx + x2;
@@ -1431,7 +1442,7 @@ __device__ __forceinline__ void fused_row_step(const FuseArgs& a, uint32_t p, in
     double r2 = 0.0;
 #pragma unroll
     for (int i = 0; i < kFuseRays; ++i) {
-        const int k = tid + i * kFuseThreads;
+        const int k = tid + i * kThreads;
         if (k < nrays) {
             const int gy = jr.x + k / a.W, gx = k - (k / a.W) * a.W;
             // fp_pixel sums its one sub-ray into zero, fp_store divides by the count
@@ -1546,6 +1557,110 @@ __global__ void __launch_bounds__(kFuseThreads, 2)
         if (threadIdx.x == 0 && !(p == 0 && y == q.withhold_row)) {
             __threadfence();
             st_release_u32(done + y, p + 1);
+        }
+    }
+}
+
+// Many independent series in one launch per SART iteration.  Per series and volume row
+// the unit steps are 0 (forward projection of the first view), 1 .. M - 1 (the fused
+// steps) and M (back projection of the last view); units are numbered step-major over
+// all series (segments of (step, series) in that order), so a unit waits only on units
+// of smaller numbers, as in sart_fused_persistent_kernel, with the same bounded waits.
+struct FuseSeries {
+    FuseArgs a;           // p, rl_in, rl_out, x0lo and ntaps unused
+    const int2* tapwin;   // per view id: (x0lo, ntaps)
+    float2* rl0;          // texel (0, 0) of residual slot 0; slot 1 follows at rl_slot
+    size_t rl_slot;       // float2 units
+    uint32_t* done;       // per volume row: unit steps finished (zeroed per iteration)
+    uint32_t views;       // M
+    int window;
+};
+
+struct FuseSegment {
+    uint32_t start;       // first unit number
+    uint32_t series;
+    uint32_t step;        // unit step
+};
+
+// kThreads = 512 for rows of up to 1024 voxels, 128 for batches whose rows are at most 256
+// voxels wide with at most 256 rays each (two voxels and two rays per thread either way).
+template <int kThreads>
+__global__ void __launch_bounds__(kThreads, 1024 / kThreads)
+    sart_fused_batch_kernel(const FuseSeries* series, const FuseSegment* segs, uint32_t nsegs, uint32_t total,
+                            uint32_t* counter, uint32_t* error) {
+    extern __shared__ __align__(16) unsigned char fuse_smem[];
+    __shared__ __align__(16) FuseSeries cur;
+    __shared__ uint32_t unit_s[3];
+    for (;;) {
+        if (threadIdx.x == 0) {
+            uint32_t u = total, si = 0, st = 0, y = 0;
+            if (ld_acquire_u32(error) == 0) {
+                u = atomicAdd(counter, 1u);
+                if (u < total) {
+                    uint32_t lo = 0, hi = nsegs - 1;  // last segment with start <= u
+                    while (lo < hi) {
+                        const uint32_t mid = (lo + hi + 1) / 2;
+                        if (segs[mid].start <= u) lo = mid;
+                        else hi = mid - 1;
+                    }
+                    si = segs[lo].series;
+                    st = segs[lo].step;
+                    y = u - segs[lo].start;
+                    if (st > 0) {
+                        const FuseSeries& f = series[si];
+                        const int ry = f.a.slab.ry, w = f.window;
+                        const int yl = max(0, (int)y - w), yh = min(ry - 1, (int)y + w);
+                        const unsigned long long t0 = global_ns();
+                        for (int yy = yl; yy <= yh && u < total; ++yy)
+                            while (ld_acquire_u32(f.done + yy) < st) {
+                                if (global_ns() - t0 > kFuseWaitNs) {
+                                    atomicExch(error, 1u);
+                                    u = total;
+                                    break;
+                                }
+                                if (ld_acquire_u32(error) != 0) {
+                                    u = total;
+                                    break;
+                                }
+                                __nanosleep(128);
+                            }
+                    }
+                } else {
+                    u = total;
+                }
+            }
+            unit_s[0] = u;
+            unit_s[1] = si;
+            unit_s[2] = (st << 16) | y;
+        }
+        __syncthreads();
+        const uint32_t u = unit_s[0];
+        if (u >= total) return;
+        const uint32_t si = unit_s[1], st = unit_s[2] >> 16;
+        const int y = (int)(unit_s[2] & 0xffffu);
+        // the unit's series arguments, staged in shared memory
+        {
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(series + si);
+            uint32_t* dst = reinterpret_cast<uint32_t*>(&cur);
+            for (int i = threadIdx.x; i < (int)(sizeof(FuseSeries) / 4); i += blockDim.x) dst[i] = src[i];
+        }
+        __syncthreads();
+        if (st == 0) {
+            fused_row_step<true, kUnitForward, kThreads>(cur.a, 0xffffffffu, y, 0, 0, cur.rl0, cur.rl0, fuse_smem);
+        } else {
+            const uint32_t p = st - 1;
+            const int2 tw = cur.tapwin[cur.a.order[p]];
+            const float2* rin = cur.rl0 + (size_t)(p & 1) * cur.rl_slot;
+            float2* rout = cur.rl0 + (size_t)((p + 1) & 1) * cur.rl_slot;
+            if (st < cur.views)
+                fused_row_step<true, kUnitFused, kThreads>(cur.a, p, y, tw.x, tw.y, rin, rout, fuse_smem);
+            else
+                fused_row_step<true, kUnitBack, kThreads>(cur.a, p, y, tw.x, tw.y, rin, rout, fuse_smem);
+        }
+        __syncthreads();  // the unit's stores are issued; its shared memory is free
+        if (threadIdx.x == 0) {
+            __threadfence();
+            st_release_u32(cur.done + y, st + 1);
         }
     }
 }

@@ -1141,8 +1141,9 @@ class WBPOperator:
 
 class BatchReconstructionOperator:
     """Many independent tilt series of uneven sizes reconstructed together with SART:
-    every step runs one forward-projection and one back-projection launch over all
-    series, each iteration one CUDA graph (etcu_batch_*).  No counterpart in the
+    each iteration of all series is one persistent launch when every series can run the
+    fused step, else every step runs one forward-projection and one back-projection
+    launch over all series, each iteration one CUDA graph (etcu_batch_*).  No counterpart in the
     reference, which reconstructs one series per run.
 
     ``series`` is a list of (GPUMappedVolume, [ScannerGeometry], projections (N, H, W)

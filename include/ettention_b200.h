@@ -400,10 +400,13 @@ ETCU_API etcu_status etcu_blob_recon_destroy(etcu_blob_recon* rec);
 ETCU_API etcu_status etcu_blob_voxelize(etcu_volume* blobs, etcu_volume* voxels, const etcu_blob_params* params);
 
 /* ---------------------------------------------------------------- batched series */
-/* Many independent tilt series of uneven sizes reconstructed together: every SART
- * step runs one forward-projection launch and one back-projection launch over all
- * series (series without a view at that step sit it out), and each iteration is one
- * CUDA graph.  Per series the result is the block-iterative reconstruction of
+/* Many independent tilt series of uneven sizes reconstructed together.  When every
+ * series can run the fused SART step (Q8 sampling, one sample each way, even rows of at
+ * most 1024 voxels), each iteration of all series is one persistent launch; otherwise
+ * every SART step runs one forward-projection launch and one back-projection launch
+ * over all series (series without a view at that step sit it out), and each iteration
+ * is one CUDA graph.  etcu_batch_run reports ETCU_ERR_CUDA if a step of the persistent
+ * launch waited longer than its limit (1 s) for neighbouring rows.  Per series the result is the block-iterative reconstruction of
  * etcu_recon_* with block size 1 (BlockIterativeReconstructionOperator.cpp:92-142).
  * No counterpart in the reference, which reconstructs one series per run.
  * Supported: SART (block_size 1), one back-projection sample, parallel views whose

@@ -116,3 +116,58 @@ def test_batch_refuses_what_it_does_not_cover(ctx, case):
         BatchReconstructionOperator([(vol, geoms, projs)], p)
     assert e.value.status == _abi.ERR_UNSUPPORTED
     vol.close()
+
+
+@pytest.mark.parametrize("wide", [False, True])
+def test_persistent_batch_equals_single_series(wide):
+    """With the fused steps available (the default context), the whole batched iteration is
+    one launch (sart_fused_batch_kernel: per series and volume row, the first view's forward
+    projection, the fused steps and the last view's back projection, taken as units in
+    step-major order; blocks of 128 threads while every row is at most 256 voxels and rays
+    wide, of 512 with the wide series).  Per series the volume equals the single-series
+    reconstruction bit for bit, including a series of one view, with long-object
+    compensation and the random order."""
+    from ettention_b200 import _abi
+    from ettention_b200.operators import (AlgebraicParameterSet, BatchReconstructionOperator,
+                                          BlockIterativeReconstructionOperator, Context, GPUMappedVolume,
+                                          mrc_base_geometry)
+    from oracle import oracle as O
+    from tests.helpers import ellipsoid_phantom, oracle_geometry
+    series = make_series(500)
+    truth = ellipsoid_phantom((32, 24, 16), 4, seed=77)
+    g1 = [mrc_base_geometry(32, 24).rotated(20.0)]
+    series.append(((32, 24, 16), g1, np.stack([O.forward_project(truth, O.VolumeGeometry.centered((32, 24, 16)),
+                                                                 oracle_geometry(g1[0]), 1, 32)[0]])))
+    if wide:
+        truth = ellipsoid_phantom((288, 16, 12), 4, seed=78)
+        gw = [mrc_base_geometry(288, 16).rotated(float(a)) for a in (-40.0, -10.0, 25.0, 50.0, 5.0)]
+        vw = O.VolumeGeometry.centered((288, 16, 12))
+        series.append(((288, 16, 12), gw, np.stack([O.forward_project(truth, vw, oracle_geometry(g), 1, 32)[0]
+                                                    for g in gw])))
+    ctx = Context(0)
+    try:
+        for order, loc in ((_abi.ORDER_IDENTITY, False), (_abi.ORDER_RANDOM, True)):
+            p = AlgebraicParameterSet(algorithm="sart", block_size=1, iterations=2, lam=0.3, order=order,
+                                      use_long_object_compensation=loc)
+            vols = [GPUMappedVolume(ctx, shape) for shape, _, _ in series]
+            batch = BatchReconstructionOperator([(v, g, pr) for v, (_, g, pr) in zip(vols, series)], p)
+            assert batch.launches_per_iteration == 1
+            batch.runNiterations(2)
+            got = batch.getReconstructedVolumes()
+            res = batch.last_residual_sq()
+            batch.close()
+            for v in vols:
+                v.close()
+            for i, (shape, geoms, projs) in enumerate(series):
+                vol = GPUMappedVolume(ctx, shape)
+                rec = BlockIterativeReconstructionOperator(vol, geoms, projs, p)
+                rec.runNiterations(2)
+                want = rec.getReconstructedVolume()
+                wres = rec.last_residual_sq()
+                rec.close()
+                vol.close()
+                assert np.abs(want).max() > 0
+                assert np.array_equal(got[i], want), (order, loc, i)
+                assert res[i] == pytest.approx(wres, rel=1e-12)
+    finally:
+        ctx.close()
