@@ -312,8 +312,10 @@ void launch_bp_t(const BpArgs& a, int device, cudaStream_t st) {
     const int zc = kPersp ? kBpZPersp : kBpZ;
     const int zchunks = (a.slab.rz + zc - 1) / zc;
     dim3 block(32, 8, 1);
-    // parallel: each block walks up to 4 z-chunks (grid-stride) to amortise its staging
-    dim3 grid((a.slab.rx + 31) / 32, (a.slab.ry + 7) / 8, kPersp ? zchunks : (zchunks + 3) / 4);
+    // parallel: each block walks up to 4 z-chunks (grid-stride) to amortise its staging;
+    // perspective: z chunks fastest, so the blocks in flight share their texels in L2
+    const dim3 grid = kPersp ? dim3(zchunks, (a.slab.rx + 31) / 32, (a.slab.ry + 7) / 8)
+                             : dim3((a.slab.rx + 31) / 32, (a.slab.ry + 7) / 8, (zchunks + 3) / 4);
     kern<<<grid, block, smem, st>>>(a);
 }
 

@@ -458,8 +458,12 @@ __device__ __forceinline__ void fp_pixel(const FpArgs& a, uint32_t first, int p)
     fp_reduce_resid(a, r2);
 }
 
+// Minimum resident blocks: 7 for the xz walks, 8 for perspective rays (their gathers are
+// latency-bound: 8 x 4 warps per SM cut the C3 forward projection by 19 % against 4),
+// 4 otherwise.
 template <typename VoxT, bool kMask, int kPath>
-__global__ void __launch_bounds__(128, (kPath == kFpPathXz || kPath == kFpPathXzNoCap) ? 7 : 4)
+__global__ void __launch_bounds__(128, (kPath == kFpPathXz || kPath == kFpPathXzNoCap) ? 7
+                                           : (kPath == kFpPathPerspective ? 8 : 4))
     forward_project_kernel(const __grid_constant__ FpArgs a) {
     fp_pixel<VoxT, kMask, kPath>(a, a.first, blockIdx.z);
 }
@@ -1719,9 +1723,11 @@ __global__ void __launch_bounds__(256) bp_perspective_kernel(const __grid_consta
     BpView* sv = (BpView*)bp_smem;
     bp_stage(a, sv, nullptr, false);
     const SlabConst& g = a.slab;
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int z0 = blockIdx.z * kBpZPersp;
+    // grid (z chunks, x tiles, y tiles): consecutive blocks take the z chunks of one
+    // column tile, whose texels they share
+    const int x = blockIdx.y * blockDim.x + threadIdx.x;
+    const int y = blockIdx.z * blockDim.y + threadIdx.y;
+    const int z0 = blockIdx.x * kBpZPersp;
     if (x >= g.rx || y >= g.ry) return;
     const int nzc = min(kBpZPersp, g.rz - z0);
     const size_t plane = (size_t)g.rx * (size_t)g.ry;
