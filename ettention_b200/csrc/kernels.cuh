@@ -634,7 +634,7 @@ __device__ __forceinline__ void bp_store(const BpArgs& a, size_t idx, float val)
 }
 
 constexpr int kBpZ = 8;  // voxels per thread along z (parallel)
-constexpr int kBpZPersp = 4;
+constexpr int kBpZPersp = 8;
 
 // Row-constant view, one sample, 1/256 weights: the per-voxel sequence reduced to the
 // column coordinate.  q = floor((u - 0.5) * 256 + 0.5) is the 1/256-rounded texel
