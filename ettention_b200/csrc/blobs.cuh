@@ -49,67 +49,93 @@ struct BlobFpArgs {
 // pixel through (x, y, 1) of the projection space, stepped slice by slice along its
 // dominant axis; every voxel of the slice neighbourhood whose centre is closer than R to
 // the ray adds table(dist / R) times its value (and the weight alone to the length).
-__global__ void __launch_bounds__(128) blob_fp_kernel(const __grid_constant__ BlobFpArgs a) {
+// A block is 32 pixels x kBlobFpParts threads: part k of a pixel walks its k-th run of
+// slices (its slice positions accumulated from the first slice exactly as one walker
+// would), and part 0 adds the parts' sums in order.  The sums within a part follow the
+// reference's order (slice, neighbour row, neighbour); the parts split the ray so that a
+// 256^2 detector fills the GPU.
+constexpr int kBlobFpParts = 4;
+
+__global__ void __launch_bounds__(32 * kBlobFpParts) blob_fp_kernel(const __grid_constant__ BlobFpArgs a) {
     extern __shared__ float blob_table[];
-    for (int i = threadIdx.x; i < a.ntable; i += blockDim.x) blob_table[i] = a.table[i];
+    __shared__ float part_val[kBlobFpParts][32], part_len[kBlobFpParts][32];
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    for (int i = tid; i < a.ntable; i += 32 * kBlobFpParts) blob_table[i] = a.table[i];
     __syncthreads();
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (x >= a.W || y >= a.H) return;
-    // TransformCoordG(projection2world, (x, y, 1))
-    const float4 wp = mat_mul(a.p2w, make_float4((float)x, (float)y, 1.f, 1.f));
-    const float3 world = make_float3(fdiv(wp.x, wp.w), fdiv(wp.y, wp.w), fdiv(wp.z, wp.w));
-    const float3 src = make_float3(a.source.x, a.source.y, a.source.z);
-    float3 d = make_float3(fsub(world.x, src.x), fsub(world.y, src.y), fsub(world.z, src.z));
-    const float nd = __fsqrt_rn(fadd(fadd(fmul(d.x, d.x), fmul(d.y, d.y)), fmul(d.z, d.z)));
-    const float3 ray = make_float3(fdiv(d.x, nd), fdiv(d.y, nd), fdiv(d.z, nd));
-    const float3 ar = make_float3(fabsf(ray.x), fabsf(ray.y), fabsf(ray.z));
-    int axis;
-    if (ar.x >= fmaxf(ar.y, ar.z)) axis = 0;
-    else if (ar.y >= fmaxf(ar.x, ar.z)) axis = 1;
-    else axis = 2;
-    const float rc[3] = {ray.x, ray.y, ray.z}, sc[3] = {src.x, src.y, src.z};
-    const float bm[3] = {a.bmin.x, a.bmin.y, a.bmin.z}, vsz[3] = {a.vs.x, a.vs.y, a.vs.z};
-    const int res[3] = {a.rx, a.ry, a.rz};
-    // pointOnRay = source + tMin[axis] * ray, tMin = (bBoxMin + vs / 2 - source) / ray
-    const float tmin = fdiv(fsub(fadd(bm[axis], fmul(0.5f, vsz[axis])), sc[axis]), rc[axis]);
-    float p[3] = {fadd(sc[0], fmul(tmin, rc[0])), fadd(sc[1], fmul(tmin, rc[1])), fadd(sc[2], fmul(tmin, rc[2]))};
-    const float st[3] = {fmul(fdiv(rc[0], rc[axis]), vsz[0]), fmul(fdiv(rc[1], rc[axis]), vsz[1]),
-                         fmul(fdiv(rc[2], rc[axis]), vsz[2])};
-    const int ex = axis == 0 ? 1 : (axis == 1 ? 2 : 0);  // slice axes: x -> (y, z), y -> (z, x), z -> (x, y)
-    const int ey = axis == 0 ? 2 : (axis == 1 ? 0 : 1);
-    const float R2 = fmul(a.R, a.R);
-    const size_t plane = (size_t)a.rx * (size_t)a.ry;
+    const int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y, part = threadIdx.y;
     float val = 0.f, lval = 0.f;
-    for (int slice = 0; slice < res[axis]; ++slice) {
-        int base[3];
-        for (int k = 0; k < 3; ++k) base[k] = (int)floorf(fdiv(fsub(p[k], bm[k]), vsz[k]));
-        for (int dy = -a.grid; dy <= a.grid; ++dy) {
-            for (int dx = -a.grid; dx <= a.grid; ++dx) {
-                int gc[3] = {base[0], base[1], base[2]};
-                gc[ex] += dx;
-                gc[ey] += dy;
-                if (gc[0] < 0 || gc[1] < 0 || gc[2] < 0 || gc[0] >= res[0] || gc[1] >= res[1] || gc[2] >= res[2])
-                    continue;
-                float cen[3];
-                for (int k = 0; k < 3; ++k) cen[k] = fadd(fadd(bm[k], fmul(0.5f, vsz[k])), fmul((float)gc[k], vsz[k]));
-                const float t = -fadd(fadd(fmul(fsub(sc[0], cen[0]), rc[0]), fmul(fsub(sc[1], cen[1]), rc[1])),
-                                      fmul(fsub(sc[2], cen[2]), rc[2]));
-                const float c0 = fsub(fadd(sc[0], fmul(t, rc[0])), cen[0]);
-                const float c1 = fsub(fadd(sc[1], fmul(t, rc[1])), cen[1]);
-                const float c2 = fsub(fadd(sc[2], fmul(t, rc[2])), cen[2]);
-                const float d2 = fadd(fadd(fmul(c0, c0), fmul(c1, c1)), fmul(c2, c2));
-                if (d2 < R2) {
-                    const float w = sample_blob(blob_table, a.ntable, fdiv(__fsqrt_rn(d2), a.R));
-                    val = fadd(val, fmul(w, a.vol[(size_t)gc[2] * plane + (size_t)gc[1] * a.rx + gc[0]]));
-                    lval = fadd(lval, w);
+    if (x < a.W && y < a.H) {
+        // TransformCoordG(projection2world, (x, y, 1))
+        const float4 wp = mat_mul(a.p2w, make_float4((float)x, (float)y, 1.f, 1.f));
+        const float3 world = make_float3(fdiv(wp.x, wp.w), fdiv(wp.y, wp.w), fdiv(wp.z, wp.w));
+        const float3 src = make_float3(a.source.x, a.source.y, a.source.z);
+        float3 d = make_float3(fsub(world.x, src.x), fsub(world.y, src.y), fsub(world.z, src.z));
+        const float nd = __fsqrt_rn(fadd(fadd(fmul(d.x, d.x), fmul(d.y, d.y)), fmul(d.z, d.z)));
+        const float3 ray = make_float3(fdiv(d.x, nd), fdiv(d.y, nd), fdiv(d.z, nd));
+        const float3 ar = make_float3(fabsf(ray.x), fabsf(ray.y), fabsf(ray.z));
+        int axis;
+        if (ar.x >= fmaxf(ar.y, ar.z)) axis = 0;
+        else if (ar.y >= fmaxf(ar.x, ar.z)) axis = 1;
+        else axis = 2;
+        const float rc[3] = {ray.x, ray.y, ray.z}, sc[3] = {src.x, src.y, src.z};
+        const float bm[3] = {a.bmin.x, a.bmin.y, a.bmin.z}, vsz[3] = {a.vs.x, a.vs.y, a.vs.z};
+        const int res[3] = {a.rx, a.ry, a.rz};
+        // pointOnRay = source + tMin[axis] * ray, tMin = (bBoxMin + vs / 2 - source) / ray
+        const float tmin = fdiv(fsub(fadd(bm[axis], fmul(0.5f, vsz[axis])), sc[axis]), rc[axis]);
+        float p[3] = {fadd(sc[0], fmul(tmin, rc[0])), fadd(sc[1], fmul(tmin, rc[1])), fadd(sc[2], fmul(tmin, rc[2]))};
+        const float st[3] = {fmul(fdiv(rc[0], rc[axis]), vsz[0]), fmul(fdiv(rc[1], rc[axis]), vsz[1]),
+                             fmul(fdiv(rc[2], rc[axis]), vsz[2])};
+        const int ex = axis == 0 ? 1 : (axis == 1 ? 2 : 0);  // slice axes: x -> (y, z), y -> (z, x), z -> (x, y)
+        const int ey = axis == 0 ? 2 : (axis == 1 ? 0 : 1);
+        const float R2 = fmul(a.R, a.R);
+        const size_t plane = (size_t)a.rx * (size_t)a.ry;
+        const int nslices = res[axis];
+        const int per = (nslices + kBlobFpParts - 1) / kBlobFpParts;
+        const int s0 = min(nslices, part * per), s1 = min(nslices, s0 + per);
+        for (int slice = 0; slice < s0; ++slice)
+            for (int k = 0; k < 3; ++k) p[k] = fadd(p[k], st[k]);
+        for (int slice = s0; slice < s1; ++slice) {
+            int base[3];
+            for (int k = 0; k < 3; ++k) base[k] = (int)floorf(fdiv(fsub(p[k], bm[k]), vsz[k]));
+            for (int dy = -a.grid; dy <= a.grid; ++dy) {
+                for (int dx = -a.grid; dx <= a.grid; ++dx) {
+                    int gc[3] = {base[0], base[1], base[2]};
+                    gc[ex] += dx;
+                    gc[ey] += dy;
+                    if (gc[0] < 0 || gc[1] < 0 || gc[2] < 0 || gc[0] >= res[0] || gc[1] >= res[1] || gc[2] >= res[2])
+                        continue;
+                    float cen[3];
+                    for (int k = 0; k < 3; ++k)
+                        cen[k] = fadd(fadd(bm[k], fmul(0.5f, vsz[k])), fmul((float)gc[k], vsz[k]));
+                    const float t = -fadd(fadd(fmul(fsub(sc[0], cen[0]), rc[0]), fmul(fsub(sc[1], cen[1]), rc[1])),
+                                          fmul(fsub(sc[2], cen[2]), rc[2]));
+                    const float c0 = fsub(fadd(sc[0], fmul(t, rc[0])), cen[0]);
+                    const float c1 = fsub(fadd(sc[1], fmul(t, rc[1])), cen[1]);
+                    const float c2 = fsub(fadd(sc[2], fmul(t, rc[2])), cen[2]);
+                    const float d2 = fadd(fadd(fmul(c0, c0), fmul(c1, c1)), fmul(c2, c2));
+                    if (d2 < R2) {
+                        const float w = sample_blob(blob_table, a.ntable, fdiv(__fsqrt_rn(d2), a.R));
+                        val = fadd(val, fmul(w, a.vol[(size_t)gc[2] * plane + (size_t)gc[1] * a.rx + gc[0]]));
+                        lval = fadd(lval, w);
+                    }
                 }
             }
+            for (int k = 0; k < 3; ++k) p[k] = fadd(p[k], st[k]);
         }
-        for (int k = 0; k < 3; ++k) p[k] = fadd(p[k], st[k]);
     }
-    const size_t i = (size_t)y * a.W + x;
-    a.proj[i] = fadd(a.proj[i], val);
-    a.len[i] = fadd(a.len[i], lval);
+    part_val[part][threadIdx.x] = val;
+    part_len[part][threadIdx.x] = lval;
+    __syncthreads();
+    if (part == 0 && x < a.W && y < a.H) {
+        float v = part_val[0][threadIdx.x], l = part_len[0][threadIdx.x];
+        for (int k = 1; k < kBlobFpParts; ++k) {
+            v = fadd(v, part_val[k][threadIdx.x]);
+            l = fadd(l, part_len[k][threadIdx.x]);
+        }
+        const size_t i = (size_t)y * a.W + x;
+        a.proj[i] = fadd(a.proj[i], v);
+        a.len[i] = fadd(a.len[i], l);
+    }
 }
 
 struct BlobBpArgs {

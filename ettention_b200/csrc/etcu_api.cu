@@ -2061,7 +2061,7 @@ void launch_blob_fp(const etcu_volume* vol, const SlabConst& g, const etcu_view&
     a.H = (int)view.height;
     a.proj = proj;
     a.len = len;
-    blob_fp_kernel<<<dim3((a.W + 127) / 128, a.H), 128, (size_t)ntable * sizeof(float), st>>>(a);
+    blob_fp_kernel<<<dim3((a.W + 31) / 32, a.H), dim3(32, kBlobFpParts), (size_t)ntable * sizeof(float), st>>>(a);
 }
 
 // one slab's back projection of one view with lambda already divided by the block size
