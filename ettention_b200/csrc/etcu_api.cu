@@ -2516,12 +2516,13 @@ etcu_status issue_batch_iteration(etcu_batch* b, cudaStream_t st) {
     if (b->persist) {
         CK(ctx, cudaMemsetAsync(b->d_ctl, 0, (size_t)(b->ctl_words - 1) * sizeof(uint32_t), st));
         uint32_t* err = b->d_ctl + b->ctl_words - 1;
+        const int withhold = ctx->fuse_withhold_row;
         if (b->threads == 128)
             sart_fused_batch_kernel<128><<<b->grid, 128, b->smem, st>>>(b->d_series, b->d_segs, b->nsegs,
-                                                                        b->total_units, b->d_ctl, err);
+                                                                        b->total_units, b->d_ctl, err, withhold);
         else
             sart_fused_batch_kernel<kFuseThreads><<<b->grid, kFuseThreads, b->smem, st>>>(
-                b->d_series, b->d_segs, b->nsegs, b->total_units, b->d_ctl, err);
+                b->d_series, b->d_segs, b->nsegs, b->total_units, b->d_ctl, err, withhold);
         CKL(ctx);
         return ETCU_OK;
     }

@@ -1591,7 +1591,7 @@ struct FuseSegment {
 template <int kThreads>
 __global__ void __launch_bounds__(kThreads, 1024 / kThreads)
     sart_fused_batch_kernel(const FuseSeries* series, const FuseSegment* segs, uint32_t nsegs, uint32_t total,
-                            uint32_t* counter, uint32_t* error) {
+                            uint32_t* counter, uint32_t* error, int withhold_row) {
     extern __shared__ __align__(16) unsigned char fuse_smem[];
     __shared__ __align__(16) FuseSeries cur;
     __shared__ uint32_t unit_s[3];
@@ -1662,7 +1662,8 @@ __global__ void __launch_bounds__(kThreads, 1024 / kThreads)
                 fused_row_step<true, kUnitBack, kThreads>(cur.a, p, y, tw.x, tw.y, rin, rout, fuse_smem);
         }
         __syncthreads();  // the unit's stores are issued; its shared memory is free
-        if (threadIdx.x == 0) {
+        // withhold_row (tests of the bounded waits): series 0 never reports that row's step 0
+        if (threadIdx.x == 0 && !(si == 0 && st == 0 && y == withhold_row)) {
             __threadfence();
             st_release_u32(cur.done + y, st + 1);
         }

@@ -171,3 +171,55 @@ def test_persistent_batch_equals_single_series(wide):
                 assert res[i] == pytest.approx(wres, rel=1e-12)
     finally:
         ctx.close()
+
+
+def test_persistent_batch_wait_gives_up_and_context_survives():
+    """The persistent batch's waits are bounded: with row 2 of the first series never
+    reporting its first step (ETCU_TEST_WITHHOLD_ROW, a flag nothing else sets), the units
+    that need it wait out their limit (1 s) and the run returns an error status instead of
+    hanging; the same context then reconstructs a series normally."""
+    import time
+    from ettention_b200 import _abi
+    from ettention_b200._abi import EttentionError
+    from ettention_b200.operators import (AlgebraicParameterSet, BatchReconstructionOperator,
+                                          BlockIterativeReconstructionOperator, Context, GPUMappedVolume)
+    series = make_series(700)[:2]
+    p = AlgebraicParameterSet(algorithm="sart", block_size=1, iterations=1, lam=0.3, order=_abi.ORDER_IDENTITY)
+    os.environ["ETCU_TEST_WITHHOLD_ROW"] = "2"
+    try:
+        ctx = Context(0)
+    finally:
+        del os.environ["ETCU_TEST_WITHHOLD_ROW"]
+    try:
+        vols = [GPUMappedVolume(ctx, shape) for shape, _, _ in series]
+        batch = BatchReconstructionOperator([(v, g, pr) for v, (_, g, pr) in zip(vols, series)], p)
+        assert batch.launches_per_iteration == 1
+        t0 = time.time()
+        with pytest.raises(EttentionError, match="waited longer than its limit"):
+            batch.runNiterations(1)
+        assert time.time() - t0 < 30
+        batch.close()
+        for v in vols:
+            v.close()
+        q = AlgebraicParameterSet(algorithm="sirt", block_size=_abi.BLOCK_ALL, iterations=1, lam=0.3,
+                                  order=_abi.ORDER_IDENTITY)
+        shape, geoms, projs = series[0]
+        vol = GPUMappedVolume(ctx, shape)
+        rec = BlockIterativeReconstructionOperator(vol, geoms, projs, q)
+        rec.run()
+        after = rec.getReconstructedVolume()
+        rec.close()
+        vol.close()
+    finally:
+        ctx.close()
+    ctx2 = Context(0)
+    try:
+        vol = GPUMappedVolume(ctx2, shape)
+        rec = BlockIterativeReconstructionOperator(vol, geoms, projs, q)
+        rec.run()
+        fresh = rec.getReconstructedVolume()
+        rec.close()
+        vol.close()
+    finally:
+        ctx2.close()
+    assert np.abs(fresh).max() > 0 and np.array_equal(after, fresh)
