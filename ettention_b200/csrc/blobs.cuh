@@ -199,16 +199,18 @@ __global__ void __launch_bounds__(128) blob_bp_kernel(const __grid_constant__ Bl
             const float len = a.raylength[pi], res = a.residual[pi];
             if (!(res != 0.f && len > 1.f)) continue;
             const float4 w = mat_mul(a.p2w, make_float4((float)px, (float)py, 1.f, 1.f));
-            float3 dd = make_float3(fsub(fdiv(w.x, w.w), a.source.x), fsub(fdiv(w.y, w.w), a.source.y),
-                                    fsub(fdiv(w.z, w.w), a.source.z));
+            // divisions of the window loop to within one ulp (reciprocal and one correction):
+            // the loop runs per (coefficient, pixel) and its IEEE divisions were most of it
+            float3 dd = make_float3(fsub(div_fast(w.x, w.w), a.source.x), fsub(div_fast(w.y, w.w), a.source.y),
+                                    fsub(div_fast(w.z, w.w), a.source.z));
             const float n = __fsqrt_rn(fadd(fadd(fmul(dd.x, dd.x), fmul(dd.y, dd.y)), fmul(dd.z, dd.z)));
-            dd = make_float3(fdiv(dd.x, n), fdiv(dd.y, n), fdiv(dd.z, n));
+            dd = make_float3(div_fast(dd.x, n), div_fast(dd.y, n), div_fast(dd.z, n));
             const float t0 = fadd(fadd(fmul(dd.x, q.x), fmul(dd.y, q.y)), fmul(dd.z, q.z));
             const float dist2 = fsub(fadd(fadd(fmul(q.x, q.x), fmul(q.y, q.y)), fmul(q.z, q.z)), fmul(t0, t0));
             if (R2 > dist2) {
-                const float wt = sample_blob(a.table, a.ntable, __fsqrt_rn(fdiv(dist2, R2)));
+                const float wt = sample_blob(a.table, a.ntable, __fsqrt_rn(div_fast(dist2, R2)));
                 acc = fadd(acc, wt);
-                val = fadd(val, fdiv(fmul(res, wt), len));
+                val = fadd(val, div_fast(fmul(res, wt), len));
             }
         }
     }
