@@ -54,7 +54,7 @@ struct BlobFpArgs {
 // would), and part 0 adds the parts' sums in order.  The sums within a part follow the
 // reference's order (slice, neighbour row, neighbour); the parts split the ray so that a
 // 256^2 detector fills the GPU.
-constexpr int kBlobFpParts = 4;
+constexpr int kBlobFpParts = 8;
 
 __global__ void __launch_bounds__(32 * kBlobFpParts) blob_fp_kernel(const __grid_constant__ BlobFpArgs a) {
     extern __shared__ float blob_table[];
