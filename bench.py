@@ -280,7 +280,7 @@ def dram_traffic():
 
 
 def work_units(geoms):
-    """Algorithmic work of one iteration in the survey's units: forward-projection ray-voxel
+    """Algorithmic work of one iteration in two units: forward-projection ray-voxel
     steps (every ray of every view counted from the voxels it enters and leaves the volume
     in: 1 + x cells crossed + z cells crossed; the views are tilted about y, so every
     detector row repeats its rays' xz path) and back-projection voxel-view updates."""
