@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "blobs"],
                     help="c2: the headline SART workload (default); c3: 2048^2 x 512 perspective, block 8, "
                          "bf16 shadow; c4: 64 batched series of uneven sizes")
+    ap.add_argument("--c3-res", default="2048,2048,512",
+                    help="volume (x,y,z) of --workload c3; the detector is x by y (smaller cases for ncu captures)")
     ap.add_argument("--ncu-case", action="store_true",
                     help="small profiling case for ncu: 512x512x256 volume, 8 views, one SART iteration "
                          "launched kernel by kernel, then per-kernel times of the unfused kernels")
@@ -660,15 +662,15 @@ C3_RES = (2048, 2048, 512)
 C3_VIEWS = 121
 
 
-def c3_geometry(tilt: float):
-    """Perspective view of a 2048^2 detector: source 10 x volume width above the volume
-    centre, detector plane one unit from the source with a pitch that spans the volume
-    at its centre (the reference's perspective convention, ProjectionTestBase.cpp:137-145),
-    rotated by -tilt about y."""
+def c3_geometry(tilt: float, res=C3_RES):
+    """Perspective view of a res[0] x res[1] detector (2048^2 for C3): source 10 x volume
+    width above the volume centre, detector plane one unit from the source with a pitch
+    that spans the volume at its centre (the reference's perspective convention,
+    ProjectionTestBase.cpp:137-145), rotated by -tilt about y."""
     from ettention_b200.operators import ScannerGeometry
-    D = 10.0 * C3_RES[0]
+    D = 10.0 * res[0]
     pitch = 1.0 / D
-    W, H = C3_RES[0], C3_RES[1]
+    W, H = res[0], res[1]
     base = ScannerGeometry([0.0, 0.0, D], [-0.5 * W * pitch, -0.5 * H * pitch, D - 1.0], [pitch, 0.0, 0.0],
                            [0.0, pitch, 0.0], W, H, True)
     return base.rotated(tilt)
@@ -684,10 +686,11 @@ def run_c3(args):
                                           ForwardProjectionOperator, GPUMappedVolume)
     ctx = Context(0)
     dev = torch.device("cuda", 0)
-    X, Y, Z = C3_RES
-    phantom = make_phantom_torch(3000, dev, C3_RES, count=500, axes=(8.0, 256.0))
-    geoms = [c3_geometry(float(a)) for a in np.linspace(-60.0, 60.0, C3_VIEWS)]
-    vol = GPUMappedVolume(ctx, C3_RES)
+    res = tuple(int(v) for v in args.c3_res.split(","))
+    X, Y, Z = res
+    phantom = make_phantom_torch(3000, dev, res, count=500, axes=(8.0 * X / 2048, 256.0 * X / 2048))
+    geoms = [c3_geometry(float(a), res) for a in np.linspace(-60.0, 60.0, C3_VIEWS)]
+    vol = GPUMappedVolume(ctx, res)
     vol.upload(phantom.cpu().numpy())
     del phantom
     fp = ForwardProjectionOperator(vol, 1)
@@ -706,7 +709,7 @@ def run_c3(args):
     torch.cuda.synchronize()
     p = AlgebraicParameterSet(algorithm="blockIterative", block_size=8, iterations=1, lam=0.2,
                               order=_abi.ORDER_RANDOM)
-    vol = GPUMappedVolume(ctx, C3_RES, voxel_type=_abi.VOXEL_BF16_MASTER)
+    vol = GPUMappedVolume(ctx, res, voxel_type=_abi.VOXEL_BF16_MASTER)
     rec = BlockIterativeReconstructionOperator(vol, geoms, b, p)
     stream = torch.cuda.ExternalStream(ctx.stream_handle)
     for _ in range(args.warmup):
@@ -737,7 +740,7 @@ def run_c3(args):
         "metric": "C3 block-iterative s per iteration", "value": ms / 1e3, "unit": "s", "higher_is_better": False,
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "dtype": "f32 math, bf16 shadow, f32 master",
         "data": "synthetic (seeded 500-ellipsoid phantom, CUDA-forward-projected, Poisson I0=200)",
-        "config": {"workload": "C3: 2048x2048x512, 121 perspective views -60..60 step 1, 2048^2 detector, "
+        "config": {"workload": f"C3: {X}x{Y}x{Z}, 121 perspective views -60..60 step 1, {X}x{Y} detector, "
                                "block 8, lambda 0.2, random order", "voxel_type": "bf16_master"},
         "per_kernel_ms": {"forward_project_total": fp_ms, "back_project_total": bp_ms,
                           "forward_launches": nf, "back_launches": nb},
