@@ -267,28 +267,51 @@ __device__ __forceinline__ void dda_walk3_fast(const DdaStart& st, const SlabCon
     const float sdx = st.sd.x, sdy = st.sd.y, sdz = st.sd.z;
     for (;;) {
         float dts[kUnroll], vals[kUnroll], mws[kUnroll];
+        if (min(min(nx, ny), min(nz, left)) >= kUnroll) {
+            // no axis can run out within the next kUnroll steps: every step is live
 #pragma unroll
-        for (int j = 0; j < kUnroll; ++j) {
-            const bool live = (nx > 0) & (ny > 0) & (nz > 0) & (left > 0);
-            const float dt = fminf(fminf(rx, ry), rz);
-            const bool bx = rx <= ry && rx <= rz;
-            const bool by = ry < rx && ry <= rz;
-            const bool bz = !bx && !by;  // rz < rx && rz < ry for finite values
-            dts[j] = live ? dt : 0.f;
-            vals[j] = 0.f;
-            mws[j] = 0.f;
-            if (live) {
+            for (int j = 0; j < kUnroll; ++j) {
+                const float dt = fminf(fminf(rx, ry), rz);
+                const bool bx = rx <= ry && rx <= rz;
+                const bool by = ry < rx && ry <= rz;
+                const bool bz = !bx && !by;
+                dts[j] = dt;
                 vals[j] = load_voxel(vol + off);
+                mws[j] = 0.f;
                 if (kMask) mws[j] = mask_weight(mask + off);
+                rx = bx ? sdx : fsub(rx, dt);
+                ry = by ? sdy : fsub(ry, dt);
+                rz = bz ? sdz : fsub(rz, dt);
+                off += bx ? dx : (by ? dy : dz);
+                nx -= bx ? 1 : 0;
+                ny -= by ? 1 : 0;
+                nz -= bz ? 1 : 0;
             }
-            rx = bx ? sdx : fsub(rx, dt);
-            ry = by ? sdy : fsub(ry, dt);
-            rz = bz ? sdz : fsub(rz, dt);
-            off += bx ? dx : (by ? dy : dz);
-            nx -= bx ? 1 : 0;
-            ny -= by ? 1 : 0;
-            nz -= bz ? 1 : 0;
-            left -= 1;
+            left -= kUnroll;
+        } else {
+#pragma unroll
+            for (int j = 0; j < kUnroll; ++j) {
+                const bool live = (nx > 0) & (ny > 0) & (nz > 0) & (left > 0);
+                const float dt = fminf(fminf(rx, ry), rz);
+                const bool bx = rx <= ry && rx <= rz;
+                const bool by = ry < rx && ry <= rz;
+                const bool bz = !bx && !by;  // rz < rx && rz < ry for finite values
+                dts[j] = live ? dt : 0.f;
+                vals[j] = 0.f;
+                mws[j] = 0.f;
+                if (live) {
+                    vals[j] = load_voxel(vol + off);
+                    if (kMask) mws[j] = mask_weight(mask + off);
+                }
+                rx = bx ? sdx : fsub(rx, dt);
+                ry = by ? sdy : fsub(ry, dt);
+                rz = bz ? sdz : fsub(rz, dt);
+                off += bx ? dx : (by ? dy : dz);
+                nx -= bx ? 1 : 0;
+                ny -= by ? 1 : 0;
+                nz -= bz ? 1 : 0;
+                left -= 1;
+            }
         }
 #pragma unroll
         for (int j = 0; j < kUnroll; ++j) {
