@@ -393,7 +393,21 @@ def run_e2e(args, ctx, geoms, b, params, world, lib_stream):
     e2e_ms = max_over_ranks(statistics.mean(e2e_times), world)
     h2d = host_proj.numel() * 4 + host_vol.numel() * 4
     d2h = host_vol.numel() * 4
-    return {"value": e2e_ms * 1e-3, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+    # the host link's own speed on this box, for reading the e2e figure: one pinned copy
+    # of the volume each way
+    dev_vol = torch.empty(host_vol.shape, dtype=torch.float32, device="cuda")
+    c0, c1, c2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    c0.record()
+    dev_vol.copy_(host_vol, non_blocking=True)
+    c1.record()
+    host_vol.copy_(dev_vol, non_blocking=True)
+    c2.record()
+    c2.synchronize()
+    link = {"h2d_gbs": host_vol.numel() * 4 / (c0.elapsed_time(c1) * 1e-3) / 1e9,
+            "d2h_gbs": host_vol.numel() * 4 / (c1.elapsed_time(c2) * 1e-3) / 1e9}
+    del dev_vol
+    return {"value": e2e_ms * 1e-3, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "host_link": link}
 
 
 # ------------------------------------------------------------------ ours
