@@ -1805,7 +1805,24 @@ __global__ void __launch_bounds__(256) bp_perspective_kernel(const __grid_consta
                 rw = fmaf(rw, fmaf(-w, rw, 1.f), rw);
                 u = fmul(u, rw);
                 v = fmul(v, rw);
-                const float2 rl = sample_pair<kSampling>(img, a.rl_pitch, a.W, a.H, V.tex, u, v);
+                float2 rl;
+                if (kSampling == kSampleQ8) {
+                    // the bilinear blend of (r, L) as paired FMAs: both channels per
+                    // instruction (weights as the 1/256 texture filter rounds them)
+                    int x0, y0;
+                    float wa, wb;
+                    split_coord<kSampling>(u, a.W, x0, wa);
+                    split_coord<kSampling>(v, a.H, y0, wb);
+                    float2 t00, t10, t01, t11;
+                    taps(img + (ptrdiff_t)y0 * (ptrdiff_t)a.rl_pitch, a.rl_pitch, x0, t00, t10, t01, t11);
+                    const float ob = fsub(1.f, wb), oa = fsub(1.f, wa);
+                    rl = __fmul2_rn(splat(fmul(oa, ob)), t00);
+                    rl = fma2(splat(fmul(wa, ob)), t10, rl);
+                    rl = fma2(splat(fmul(oa, wb)), t01, rl);
+                    rl = fma2(splat(fmul(wa, wb)), t11, rl);
+                } else {
+                    rl = sample_pair<kSampling>(img, a.rl_pitch, a.W, a.H, V.tex, u, v);
+                }
                 float value = 0.f;
                 if (rl.y >= kEps) {
                     const float dz = fsub(pz[j], V.src[2]);
@@ -1850,7 +1867,24 @@ __global__ void __launch_bounds__(256) bp_perspective_kernel(const __grid_consta
                 const float w = fadd(fadd(fadd(fmul(V.mw[0], px), fmul(V.mw[1], py)), fmul(V.mw[2], pz)), V.mw[3]);
                 u = div_fast(u, w);
                 v = div_fast(v, w);
-                const float2 rl = sample_pair<kSampling>(img, a.rl_pitch, a.W, a.H, V.tex, u, v);
+                float2 rl;
+                if (kSampling == kSampleQ8) {
+                    // the bilinear blend of (r, L) as paired FMAs: both channels per
+                    // instruction (weights as the 1/256 texture filter rounds them)
+                    int x0, y0;
+                    float wa, wb;
+                    split_coord<kSampling>(u, a.W, x0, wa);
+                    split_coord<kSampling>(v, a.H, y0, wb);
+                    float2 t00, t10, t01, t11;
+                    taps(img + (ptrdiff_t)y0 * (ptrdiff_t)a.rl_pitch, a.rl_pitch, x0, t00, t10, t01, t11);
+                    const float ob = fsub(1.f, wb), oa = fsub(1.f, wa);
+                    rl = __fmul2_rn(splat(fmul(oa, ob)), t00);
+                    rl = fma2(splat(fmul(wa, ob)), t10, rl);
+                    rl = fma2(splat(fmul(oa, wb)), t01, rl);
+                    rl = fma2(splat(fmul(wa, wb)), t11, rl);
+                } else {
+                    rl = sample_pair<kSampling>(img, a.rl_pitch, a.W, a.H, V.tex, u, v);
+                }
                 if (rl.y >= kEps) {
                     const float3 dir = make_float3(fsub(px, V.src[0]), fsub(py, V.src[1]), fsub(pz, V.src[2]));
                     const float l = chord_in_voxel(make_float3(px, py, pz), dir, c, vs);
