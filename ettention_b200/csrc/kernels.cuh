@@ -19,6 +19,7 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <cfloat>
+#include <type_traits>
 #include <stdint.h>
 
 namespace etcu {
@@ -1786,60 +1787,66 @@ __global__ void __launch_bounds__(256) bp_perspective_kernel(const __grid_consta
                 if (kMask) mw[j] = mask_weight(a.mask + idx);
             }
         }
-        for (int p = 0; p < a.nviews; ++p) {
-            const BpView& V = sv[p];
-            const float2* img = a.rl + (size_t)p * a.rl_slot;
-            const float cu = fadd(fmul(V.mu[0], px), fmul(V.mu[1], py));
-            const float cv = fadd(fmul(V.mv[0], px), fmul(V.mv[1], py));
-            const float cw = fadd(fmul(V.mw[0], px), fmul(V.mw[1], py));
-            const float dx = fsub(px, V.src[0]), dy = fsub(py, V.src[1]);
-            const float dxy = fadd(fmul(dx, dx), fmul(dy, dy));
-            const float lxy = fminf(fmul(g.vs.x, rcp_approx(fabsf(dx))), fmul(g.vs.y, rcp_approx(fabsf(dy))));
+        // full chunks (every z voxel of the thread inside the volume) skip the per-voxel test
+        auto views = [&](auto full_tag) {
+            constexpr bool kFull = decltype(full_tag)::value;
+            for (int p = 0; p < a.nviews; ++p) {
+                const BpView& V = sv[p];
+                const float2* img = a.rl + (size_t)p * a.rl_slot;
+                const float cu = fadd(fmul(V.mu[0], px), fmul(V.mu[1], py));
+                const float cv = fadd(fmul(V.mv[0], px), fmul(V.mv[1], py));
+                const float cw = fadd(fmul(V.mw[0], px), fmul(V.mw[1], py));
+                const float dx = fsub(px, V.src[0]), dy = fsub(py, V.src[1]);
+                const float dxy = fadd(fmul(dx, dx), fmul(dy, dy));
+                const float lxy = fminf(fmul(g.vs.x, rcp_approx(fabsf(dx))), fmul(g.vs.y, rcp_approx(fabsf(dy))));
 #pragma unroll
-            for (int j = 0; j < kBpZPersp; ++j) {
-                if (j >= nzc) continue;
-                float u = fadd(fadd(cu, fmul(V.mu[2], pz[j])), V.mu[3]);
-                float v = fadd(fadd(cv, fmul(V.mv[2], pz[j])), V.mv[3]);
-                const float w = fadd(fadd(cw, fmul(V.mw[2], pz[j])), V.mw[3]);
-                float rw = rcp_approx(w);
-                rw = fmaf(rw, fmaf(-w, rw, 1.f), rw);
-                u = fmul(u, rw);
-                v = fmul(v, rw);
-                float2 rl;
-                if (kSampling == kSampleQ8) {
-                    // the bilinear blend of (r, L) as paired FMAs: both channels per
-                    // instruction (weights as the 1/256 texture filter rounds them)
-                    int x0, y0;
-                    float wa, wb;
-                    split_coord<kSampling>(u, a.W, x0, wa);
-                    split_coord<kSampling>(v, a.H, y0, wb);
-                    float2 t00, t10, t01, t11;
-                    taps(img + (ptrdiff_t)y0 * (ptrdiff_t)a.rl_pitch, a.rl_pitch, x0, t00, t10, t01, t11);
-                    const float ob = fsub(1.f, wb), oa = fsub(1.f, wa);
-                    rl = __fmul2_rn(splat(fmul(oa, ob)), t00);
-                    rl = fma2(splat(fmul(wa, ob)), t10, rl);
-                    rl = fma2(splat(fmul(oa, wb)), t01, rl);
-                    rl = fma2(splat(fmul(wa, wb)), t11, rl);
-                } else {
-                    rl = sample_pair<kSampling>(img, a.rl_pitch, a.W, a.H, V.tex, u, v);
+                for (int j = 0; j < kBpZPersp; ++j) {
+                    if (!kFull && j >= nzc) continue;
+                    float u = fadd(fadd(cu, fmul(V.mu[2], pz[j])), V.mu[3]);
+                    float v = fadd(fadd(cv, fmul(V.mv[2], pz[j])), V.mv[3]);
+                    const float w = fadd(fadd(cw, fmul(V.mw[2], pz[j])), V.mw[3]);
+                    float rw = rcp_approx(w);
+                    rw = fmaf(rw, fmaf(-w, rw, 1.f), rw);
+                    u = fmul(u, rw);
+                    v = fmul(v, rw);
+                    float2 rl;
+                    if (kSampling == kSampleQ8) {
+                        // the bilinear blend of (r, L) as paired FMAs: both channels per
+                        // instruction (weights as the 1/256 texture filter rounds them)
+                        int x0, y0;
+                        float wa, wb;
+                        split_coord<kSampling>(u, a.W, x0, wa);
+                        split_coord<kSampling>(v, a.H, y0, wb);
+                        float2 t00, t10, t01, t11;
+                        taps(img + (ptrdiff_t)y0 * (ptrdiff_t)a.rl_pitch, a.rl_pitch, x0, t00, t10, t01, t11);
+                        const float ob = fsub(1.f, wb), oa = fsub(1.f, wa);
+                        rl = __fmul2_rn(splat(fmul(oa, ob)), t00);
+                        rl = fma2(splat(fmul(wa, ob)), t10, rl);
+                        rl = fma2(splat(fmul(oa, wb)), t01, rl);
+                        rl = fma2(splat(fmul(wa, wb)), t11, rl);
+                    } else {
+                        rl = sample_pair<kSampling>(img, a.rl_pitch, a.W, a.H, V.tex, u, v);
+                    }
+                    float value = 0.f;
+                    if (rl.y >= kEps) {
+                        const float dz = fsub(pz[j], V.src[2]);
+                        // |d| by reciprocal square root (within 2 ulp; the IEEE square root
+                        // cost 4 % of the kernel)
+                        const float nd2 = fadd(dxy, fmul(dz, dz));
+                        const float nd = fmul(nd2, rsqrtf(nd2));
+                        const float l = fmul(nd, fminf(lxy, fmul(g.vs.z, rcp_approx(fabsf(dz)))));
+                        value = fmul(fmul(rl.x, l), rcp_approx(rl.y));
+                    }
+                    float vj = fadd(val[j], fmul(fmul(a.lambda, value), mw[j]));
+                    if (a.use_min) vj = fmaxf(a.vmin, vj);
+                    if (a.use_max) vj = fminf(a.vmax, vj);
+                    if (kStore == 1) vj = __half2float(__float2half_rn(vj));
+                    val[j] = vj;
                 }
-                float value = 0.f;
-                if (rl.y >= kEps) {
-                    const float dz = fsub(pz[j], V.src[2]);
-                    // |d| by reciprocal square root (within 2 ulp; the IEEE square root
-                    // cost 4 % of the kernel)
-                    const float nd2 = fadd(dxy, fmul(dz, dz));
-                    const float nd = fmul(nd2, rsqrtf(nd2));
-                    const float l = fmul(nd, fminf(lxy, fmul(g.vs.z, rcp_approx(fabsf(dz)))));
-                    value = fmul(fmul(rl.x, l), rcp_approx(rl.y));
-                }
-                float vj = fadd(val[j], fmul(fmul(a.lambda, value), mw[j]));
-                if (a.use_min) vj = fmaxf(a.vmin, vj);
-                if (a.use_max) vj = fminf(a.vmax, vj);
-                if (kStore == 1) vj = __half2float(__float2half_rn(vj));
-                val[j] = vj;
             }
-        }
+        };
+        if (nzc == kBpZPersp) views(std::true_type{});
+        else views(std::false_type{});
 #pragma unroll
         for (int j = 0; j < kBpZPersp; ++j)
             if (j < nzc) bp_store<kStore>(a, base + (size_t)j * plane, val[j]);
