@@ -210,8 +210,9 @@ def make_phantom_torch(seed: int, device, res=None, count: int = 200, axes=(8.0,
     return vol
 
 
-def make_problem(ctx, seed: int):
-    """Phantom, tilt geometry and noisy projections (forward projected by the CUDA path)."""
+def make_problem(ctx, seed: int, keep_phantom: bool = False):
+    """Phantom, tilt geometry and noisy projections (forward projected by the CUDA path);
+    with keep_phantom also a host copy of the phantom."""
     import torch
     from ettention_b200.operators import ForwardProjectionOperator, GPUMappedVolume, mrc_base_geometry
     dev = torch.device("cuda", ctx.device)
@@ -220,7 +221,8 @@ def make_problem(ctx, seed: int):
     angles = np.linspace(-60.0, 60.0, N_VIEWS)
     geoms = [mrc_base_geometry(*DET).rotated(float(a)) for a in angles]
     vol = GPUMappedVolume(ctx, RES)
-    vol.upload(phantom.cpu().numpy())
+    host_phantom = phantom.cpu().numpy()
+    vol.upload(host_phantom)
     del phantom
     fp = ForwardProjectionOperator(vol, 1)
     projs = torch.zeros((N_VIEWS, DET[1], DET[0]), dtype=torch.float32, device=dev)
@@ -235,6 +237,8 @@ def make_problem(ctx, seed: int):
     counts = torch.poisson(I0 * torch.exp(-projs), generator=gen)
     b = -torch.log(torch.clamp(counts, min=1.0) / I0)
     torch.cuda.synchronize(dev)
+    if keep_phantom:
+        return geoms, b.contiguous(), host_phantom
     return geoms, b.contiguous()
 
 
@@ -259,26 +263,32 @@ def fused_moved_bytes():
     return 2 * V * 4 + P * 8 + P * 4 + P * 8
 
 
-# DRAM bytes per voxel of one launch, dram__bytes_read.sum + dram__bytes_write.sum from an
-# ncu capture of the 512x512x256 case (python bench.py --ncu-case, 67,108,864 voxels,
-# 512^2 detector): forward_project_kernel 269,974,272 + 5,381,120 B, bp_sart_column_kernel
-# 270,639,104 + 205,491,712 B.  Both grow with the voxel count; the back projector's
-# figure undercounts its writes by the dirty lines still in L2 when the launch ends
-# (at most the L2 size, about 63 MB in that capture).
-FP_DRAM_BYTES_PER_VOXEL = (269974272 + 5381120) / 67108864
-BP_DRAM_BYTES_PER_VOXEL = (270639104 + 205491712) / 67108864
-# sart_fused_kernel, ncu capture of the 1024x1024x256 case (python bench.py --ncu-case
-# --ncu-res 1024,1024,256: the bench's own volume and detector, 268,435,456 voxels):
-# dram__bytes_read.sum + dram__bytes_write.sum per fused step: one launch of the per-step
-# kernel, and the persistent kernel's launch of the 8-view case (7 steps) divided by 7.
-FUSED_DRAM_BYTES_PER_VOXEL = (1086500000 + 1021966000) / 268435456
-PERSIST_DRAM_BYTES_PER_VOXEL = (7603772000 + 7516285000) / 7 / 268435456
+def source_key() -> str:
+    """Hash of the CUDA sources that define the kernels: a DRAM-traffic figure recorded
+    from an ncu capture is used only while the library is built from the same sources."""
+    import hashlib
+    h = hashlib.sha256()
+    for f in ("kernels.cuh", "etcu_api.cu"):
+        with open(os.path.join(ROOT, "ettention_b200", "csrc", f), "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:16]
 
 
-def dram_traffic():
-    """Measured DRAM bytes per launch scaled to the bench volume (forward, back, fused)."""
-    V = RES[0] * RES[1] * RES[2]
-    return FP_DRAM_BYTES_PER_VOXEL * V, BP_DRAM_BYTES_PER_VOXEL * V, FUSED_DRAM_BYTES_PER_VOXEL * V
+def recorded_traffic(kernel: str):
+    """DRAM bytes per unit (`dram__bytes_read.sum + dram__bytes_write.sum` of one ncu
+    capture, per voxel of one step) recorded in a profile summary as
+    `traffic-key: <kernel> <source key> <bytes per voxel per step> <case>`, or None when no
+    summary matches this build's sources."""
+    key = source_key()
+    pdir = os.path.join(ROOT, "profiles")
+    for f in sorted(os.listdir(pdir)) if os.path.isdir(pdir) else ():
+        if not f.endswith(".md"):
+            continue
+        for ln in open(os.path.join(pdir, f)):
+            parts = ln.strip().strip("`").split()
+            if len(parts) >= 5 and parts[0] == "traffic-key:" and parts[1] == kernel and parts[2] == key:
+                return float(parts[3]), f"{f}: ncu capture of {parts[4]}"
+    return None
 
 
 def work_units(geoms):
@@ -313,45 +323,72 @@ def work_units(geoms):
 
 
 # ------------------------------------------------------------------ CPU baseline (oracle)
-def cpu_sample_seconds(threads: int, views: int = 1):
-    """Times the FP32 CPU restatement of the reference kernels (oracle/) on `views` views
-    of the same workload: forward projection + residual + back projection per view."""
-    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+CPU_SAMPLE_VIEWS = (0, 15, 30, 45, 60)  # -60, -30, 0, +30, +60 degrees of the 61-view series
+
+
+def cpu_sample_problem(phantom):
+    """The CPU sample's inputs: the views CPU_SAMPLE_VIEWS of the bench series and their
+    noisy projections (the oracle's line integrals of the phantom, Poisson at I0, -log),
+    made before the timed region."""
     from oracle import oracle as O
-    X, Y, Z = RES
-    rng = np.random.Generator(np.random.PCG64(5))
-    vol = (rng.uniform(0, 1, size=(Z, Y, X)).astype(np.float32) * MU_SCALE)
     vg = O.VolumeGeometry.centered(RES)
     base = O.mrc_base_geometry(*DET)
-    angles = np.linspace(-60.0, 60.0, N_VIEWS)[: views]
-    b = rng.uniform(0, 3, size=(DET[1], DET[0])).astype(np.float32)
+    angles = np.linspace(-60.0, 60.0, N_VIEWS)
+    rng = np.random.Generator(np.random.PCG64(7))
+    geoms, bs = [], []
+    for i in CPU_SAMPLE_VIEWS:
+        g = O.rotate_geometry(base, float(angles[i]))
+        p, _ = O.forward_project(phantom, vg, g, 1, 32)
+        counts = rng.poisson(I0 * np.exp(-p.astype(np.float64)))
+        geoms.append(g)
+        bs.append((-np.log(np.maximum(counts, 1) / I0)).astype(np.float32))
+    return vg, geoms, bs
+
+
+def cpu_sample_seconds(problem, threads: int):
+    """Seconds per SART view of the FP32 CPU restatement of the reference kernels (oracle/)
+    on `threads` host threads: forward projection, residual and back projection (texture
+    weights rounded to 1/256, the mode the GPU path runs) of the sampled views, in order,
+    from a zero volume as the first iteration starts."""
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    from oracle import oracle as O
+    vg, geoms, bs = problem
+    X, Y, Z = RES
+    vol = np.zeros((Z, Y, X), np.float32)
     t0 = time.perf_counter()
-    for a in angles:
-        g = O.rotate_geometry(base, float(a))
+    for g, b in zip(geoms, bs):
         p, l = O.forward_project(vol, vg, g, 1, 32)
         r = b - p
-        O.back_project(vol, vg, g, r, l, LAMBDA, 1, 32, O.WEIGHTS_EXACT)
-    return time.perf_counter() - t0
+        O.back_project(vol, vg, g, r, l, LAMBDA, 1, 32, O.WEIGHTS_Q8)
+    return (time.perf_counter() - t0) / len(geoms)
+
+
+CPU_SAMPLE_TEXT = ("5 of the 61 views (-60, -30, 0, +30, +60 deg; FP + residual + Q8 BP each) at full size on "
+                   "the bench phantom, FP32 oracle; seconds per view x61 views x30 iterations")
 
 
 def run_reference(args, rank, world):
     """Reference arm: the CPU restatement of the reference's path on all host cores."""
     if rank != 0:
         return
+    import torch
     threads = os.cpu_count() or 1
-    os.environ["OMP_NUM_THREADS"] = str(threads)
+    torch.set_num_threads(threads)
+    phantom = make_phantom_torch(series_seed(0), "cpu").numpy()
+    problem = cpu_sample_problem(phantom)
+    del phantom
     for _ in range(args.warmup):
-        cpu_sample_seconds(threads, 1)
-    ts = [cpu_sample_seconds(threads, 1) for _ in range(args.steps)]
+        cpu_sample_seconds(problem, threads)
+    ts = [cpu_sample_seconds(problem, threads) for _ in range(args.steps)]
     per_view = statistics.mean(ts)
     value = per_view * N_VIEWS * TARGET_ITERS
-    sample = "1 of 61 views (FP + residual + BP) per step at full size, scaled x61 views x30 iterations"
     line = {"impl": "reference", "metric": "SART s to reach plain 30-iter residual", "value": value, "unit": "s",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_view * 1e3,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": per_view * len(CPU_SAMPLE_VIEWS) * 1e3,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "config": {"workload": WORKLOAD, "step": "one view of one SART iteration",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "step": "5 sampled views of one SART iteration",
                                             "host_threads": threads},
-            "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "port", "sample": sample},
+            "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "port", "sample": CPU_SAMPLE_TEXT},
             "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "the reference's OpenCL build cannot be compiled or run on this box; this arm times the "
                     "FP32 CPU restatement of its kernels (oracle/) on all host threads"}
@@ -419,7 +456,11 @@ def run_ours(args, rank, world, local):
                                           GPUMappedVolume)
     torch.cuda.set_device(local)
     ctx = Context(local)
-    geoms, b = make_problem(ctx, series_seed(rank))
+    geoms, b, phantom = make_problem(ctx, series_seed(rank), keep_phantom=True)
+    cpu_problem = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu_problem = cpu_sample_problem(phantom)
+    del phantom
     params = AlgebraicParameterSet(algorithm="sart", block_size=1, iterations=TARGET_ITERS, lam=LAMBDA,
                                    order=_abi.ORDER_IDENTITY)
     vol = GPUMappedVolume(ctx, RES)
@@ -452,7 +493,6 @@ def run_ours(args, rank, world, local):
     # CUDA events around every step on the library stream) ----
     steps = rec.profile_steps()
     fp_bytes, bp_bytes, fused_bytes = algorithmic_bytes()
-    fp_traffic, bp_traffic, fused_traffic = dram_traffic()
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -460,52 +500,44 @@ def run_ours(args, rank, world, local):
         pass
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    V = RES[0] * RES[1] * RES[2]
     per_kernel = {}
     # the persistent fused kernel runs all N_VIEWS - 1 fused steps of an iteration in one
     # launch; the per-step kernel one step per launch
     fused_launches = sum(l for k, _, l in steps if k == "fused")
     pairs = (N_VIEWS - 1) // fused_launches if fused_launches else 1
     fused_bytes *= pairs
-    if pairs > 1:
-        fused_traffic = PERSIST_DRAM_BYTES_PER_VOXEL * RES[0] * RES[1] * RES[2]
-    fused_traffic *= pairs
-    for kind, name, byts, traffic in (("fused", "sart_fused_step", fused_bytes, fused_traffic),
-                                      ("forward", "forward_project", fp_bytes, fp_traffic),
-                                      ("back", "back_project", bp_bytes, bp_traffic)):
+    kernels = {"fused": "sart_fused_persistent_kernel" if pairs > 1 else "sart_fused_kernel",
+               "forward": "forward_project_kernel", "back": "bp_sart_column_kernel"}
+    for kind, name, byts, units in (("fused", "sart_fused_step", fused_bytes, pairs),
+                                    ("forward", "forward_project", fp_bytes, 1),
+                                    ("back", "back_project", bp_bytes, 1)):
         ts = [t for k, t, _ in steps if k == kind]
         if not ts:
             continue
         avg = sum(ts) / len(ts)
         gbs = byts / (avg * 1e-3) / 1e9
-        per_kernel[name] = {"avg_ms": avg, "launches": sum(l for k, _, l in steps if k == kind),
+        rec_t = recorded_traffic(kernels[kind])
+        per_kernel[name] = {"kernel": kernels[kind], "avg_ms": avg,
+                            "launches": sum(l for k, _, l in steps if k == kind),
                             "total_ms": sum(ts), "algorithmic_bytes": byts, "gbs": gbs, "frac": gbs / hbm_peak,
-                            "traffic": traffic}
+                            "traffic": rec_t[0] * V * units if rec_t else None,
+                            "traffic_source": rec_t[1] if rec_t else "no ncu capture recorded for this build"}
     if "sart_fused_step" in per_kernel:
         fk = per_kernel["sart_fused_step"]
         moved = fused_moved_bytes() * pairs
         fk["view_pairs_per_launch"] = pairs
-        fk["kernel"] = "sart_fused_persistent_kernel" if pairs > 1 else "sart_fused_kernel"
         fk["moved_bytes"] = moved
         fk["moved_gbs"] = moved / (fk["avg_ms"] * 1e-3) / 1e9
         fk["moved_frac"] = fk["moved_gbs"] / hbm_peak
-        # ncu --set full of the kernel that ran (profiles/sart_fused_persistent_1024x1024x256.md,
-        # profiles/sart_fused_1024x1024x256.md)
-        if pairs > 1:
-            fk["ncu"] = {"issue_active_pct": 72.7, "ipc": 2.91, "dram_throughput_pct": 41.2,
-                         "lsu_pipe_pct": 70.8, "alu_pipe_pct": 65.4, "warp_inst_per_step": 530.0e6}
-        else:
-            fk["ncu"] = {"issue_active_pct": 71.0, "ipc": 2.84, "dram_throughput_pct": 39.2,
-                         "lsu_pipe_pct": 70.2, "alu_pipe_pct": 61.0, "warp_inst_per_step": 515.6e6}
     dominant = max(per_kernel, key=lambda n: per_kernel[n]["total_ms"])
     dk = per_kernel[dominant]
-    roofline = {"bound": "hbm", "kernel": dominant, "achieved": dk["gbs"], "peak": hbm_peak, "unit": "GB/s",
+    roofline = {"bound": "hbm", "kernel": dk["kernel"], "achieved": dk["gbs"], "peak": hbm_peak, "unit": "GB/s",
                 "frac": dk["frac"], "peak_source": peak_src, "traffic": dk["traffic"],
                 "bytes_model": ("one forward-projection view + one back-projection view per fused step "
                                 "(4V+4P+8P + 8V+8P) x view_pairs_per_launch; the launch moves moved_bytes of them"
                                 if dominant == "sart_fused_step" else "per-view byte model"),
-                "traffic_source": ("ncu dram bytes per fused step of the 1024x1024x256 case x view_pairs_per_launch"
-                                   if dominant == "sart_fused_step"
-                                   else "ncu dram bytes of the 512x512x256 case, scaled by voxel count"),
+                "traffic_source": dk["traffic_source"], "source_key": source_key(),
                 "per_kernel": per_kernel}
     rec.close()
     vol.close()
@@ -518,10 +550,9 @@ def run_ours(args, rank, world, local):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        t = cpu_sample_seconds(threads, 1)
+        t = cpu_sample_seconds(cpu_problem, threads)
         cpu = {"value": t * N_VIEWS * TARGET_ITERS, "unit": "s", "cores": threads, "kind": "port",
-               "sample": "1 of 61 views (FP + residual + BP) at full size, FP32 oracle, scaled x61 views x30 "
-                         "iterations"}
+               "sample": CPU_SAMPLE_TEXT}
     if rank == 0:
         fp_steps, bp_updates = work_units(geoms)
         line = {"metric": "SART s to reach plain 30-iter residual", "value": value, "unit": "s",

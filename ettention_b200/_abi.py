@@ -19,6 +19,7 @@ SAMPLING_Q8, SAMPLING_EXACT, SAMPLING_HW_TEXTURE = 0, 1, 2
 ORDER_IDENTITY, ORDER_RANDOM, ORDER_MAXANGLE, ORDER_BUCKETS = 0, 1, 2, 3
 ALL_SUBVOLUMES = 0xFFFFFFFF
 NOALLOC_MAX_PIXELS = 1024 * 1024
+NOALLOC_SCRATCH_TEXELS = NOALLOC_MAX_PIXELS + 8208
 BLOCK_ALL = 0xFFFFFFFF
 
 

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -302,11 +303,13 @@ constexpr size_t kBpSmemBudget = 160 * 1024;
 template <bool kPersp, bool kMask, int kStore, int kSampling>
 void launch_bp_t(const BpArgs& a, int device, cudaStream_t st) {
     // Opt in to the large dynamic shared-memory carve-out once per device and instantiation.
-    static unsigned long long opted = 0;
+    // Host threads driving different devices may get here together: the set of opted-in
+    // devices is one atomic word (setting the attribute twice is harmless).
+    static std::atomic<unsigned long long> opted{0};
     auto kern = kPersp ? bp_perspective_kernel<kMask, kStore, kSampling> : bp_parallel_kernel<kMask, kStore, kSampling>;
-    if (device < 64 && !(opted & (1ull << device))) {
+    if (device < 64 && !(opted.load(std::memory_order_acquire) & (1ull << device))) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBpSmemBudget);
-        opted |= 1ull << device;
+        opted.fetch_or(1ull << device, std::memory_order_acq_rel);
     }
     const size_t smem = bp_smem_bytes(a.nviews, kPersp ? 0 : a.nsamples);
     const int zc = kPersp ? kBpZPersp : kBpZ;
@@ -2925,8 +2928,9 @@ extern "C" etcu_status etcu_reconstruct(etcu_context* ctx, const etcu_volume_des
 // Scratch of etcu_sart_view_update_noalloc: one interleaved (residual, length)
 // image and the FP64 residual accumulator, in static device memory.
 // (width + 2 kPad) x (height + 2 kPad) texels covers every detector of at most
-// 1024 x 1024 pixels.
-constexpr size_t kNoAllocScratchTexels = (size_t)ETCU_NOALLOC_MAX_PIXELS + 8 * 1024 + 16;
+// 1024 x 1024 pixels (1028 x 1028 = 1024^2 + 8208).
+constexpr size_t kNoAllocScratchTexels = ETCU_NOALLOC_SCRATCH_TEXELS;
+static_assert(kNoAllocScratchTexels >= (1024 + 2 * kPad) * (1024 + 2 * kPad), "scratch covers 1024^2 detectors");
 static __device__ __align__(256) float2 g_noalloc_pairs[kNoAllocScratchTexels];
 static __device__ __align__(256) double g_noalloc_resid[1];
 
@@ -2934,6 +2938,7 @@ namespace {
 struct NoAllocScratch {
     float2* pairs = nullptr;
     double* resid = nullptr;
+    void* context = nullptr;  // the driver context the addresses belong to
     bool ready = false;
 };
 NoAllocScratch g_noalloc[64];
@@ -2951,11 +2956,33 @@ etcu_status noalloc_fail(etcu_status st, const char* fmt, ...) {
     return st;
 }
 
-// Device addresses of the static scratch for the current device (looked up once).
+// The calling thread's current driver context (cuCtxGetCurrent through the runtime's
+// driver entry point, so the library needs no link against the driver library), or
+// NULL when none is current or the entry point is unavailable.
+void* current_driver_context() {
+    using CtxGetCurrent = int (*)(void**);
+    static CtxGetCurrent fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return (CtxGetCurrent)p;
+    }();
+    void* ctx = nullptr;
+    if (!fn || fn(&ctx) != 0) return nullptr;
+    return ctx;
+}
+
+// Device addresses of the static scratch for the current device: looked up once per
+// device and looked up again when the device's context changed since (the addresses of
+// a destroyed context are not valid in its successor).
 etcu_status noalloc_scratch(int dev, NoAllocScratch& out) {
     if (dev < 0 || dev >= 64) return noalloc_fail(ETCU_ERR_UNSUPPORTED, "device %d out of range", dev);
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
     NoAllocScratch& s = g_noalloc[dev];
+    void* ctx = current_driver_context();
+    if (s.ready && (ctx == nullptr || ctx != s.context)) s.ready = false;
     if (!s.ready) {
         cudaError_t e = cudaGetSymbolAddress((void**)&s.pairs, g_noalloc_pairs);
         if (e != cudaSuccess)
@@ -2963,7 +2990,9 @@ etcu_status noalloc_scratch(int dev, NoAllocScratch& out) {
         e = cudaGetSymbolAddress((void**)&s.resid, g_noalloc_resid);
         if (e != cudaSuccess)
             return noalloc_fail(ETCU_ERR_CUDA, "cudaGetSymbolAddress(residual) failed: %s", cudaGetErrorString(e));
-        s.ready = true;
+        // the lookup made the device's primary context current if none was
+        s.context = current_driver_context();
+        s.ready = s.context != nullptr;
     }
     out = s;
     return ETCU_OK;
@@ -2983,8 +3012,10 @@ extern "C" etcu_status etcu_sart_view_update_noalloc(const etcu_volume_desc* des
     if ((uint64_t)view->width * view->height > ETCU_NOALLOC_MAX_PIXELS ||
         ((uint64_t)view->width + 2 * kPad) * ((uint64_t)view->height + 2 * kPad) > kNoAllocScratchTexels)
         return noalloc_fail(ETCU_ERR_INVALID_ARGUMENT,
-                            "detector of %u x %u pixels exceeds the %u-pixel scratch of the allocation-free update",
-                            view->width, view->height, (unsigned)ETCU_NOALLOC_MAX_PIXELS);
+                            "detector of %u x %u pixels exceeds the scratch of the allocation-free update "
+                            "(at most %u pixels, and (width + 4) x (height + 4) <= %u texels)",
+                            view->width, view->height, (unsigned)ETCU_NOALLOC_MAX_PIXELS,
+                            (unsigned)ETCU_NOALLOC_SCRATCH_TEXELS);
     float mat[16];
     if (!projection_matrix(*view, mat)) return noalloc_fail(ETCU_ERR_INVALID_ARGUMENT, "matrix not invertible");
     if (desc->resolution[0] == 0 || desc->resolution[1] == 0 || desc->resolution[2] == 0)

@@ -439,17 +439,22 @@ ETCU_API uint32_t etcu_batch_launches_per_iteration(const etcu_batch* batch);
  * etcu_volume, one sub-volume), the measured projection of this view (device
  * pointer, height x width floats) and the stream to run on (NULL: the legacy
  * default stream).  The (residual, ray length) image lives in a static device
- * array of about ETCU_NOALLOC_MAX_PIXELS float2 (8 MiB) that every GPU loading
- * the library holds until the process exits; detectors of up to 1024 x 1024
- * pixels fit, larger ones are rejected.  The
- * first call on a device looks up that array's device address, so make the
- * first call before any stream capture.  All calls share the array and keep
+ * array of ETCU_NOALLOC_SCRATCH_TEXELS float2 (8 MiB) that every GPU loading
+ * the library holds until the process exits.  The image carries a two-texel zero
+ * border, so a detector fits when (width + 4) x (height + 4) <=
+ * ETCU_NOALLOC_SCRATCH_TEXELS and width x height <= ETCU_NOALLOC_MAX_PIXELS: every
+ * detector of up to 1024 x 1024 pixels fits, and so does, e.g., 2048 x 508; larger
+ * ones (also 4096 x 256, which needs 4100 x 260 texels) are rejected.  The first
+ * call on a device (and the first after that device's context was replaced, e.g.
+ * by cudaDeviceReset) looks up that array's device address, so make the first
+ * call before any stream capture.  All calls share the array and keep
  * the last call's contents: calls that overlap on the GPU (other streams or
  * threads on the same device) race and must be serialised by the caller.
  * residual_sq (optional, host) receives sum (b - Ax)^2 over the view, which
  * synchronises the stream.  Sampling is ETCU_SAMPLING_Q8.
  * No counterpart in the reference. */
 #define ETCU_NOALLOC_MAX_PIXELS (1024u * 1024u)
+#define ETCU_NOALLOC_SCRATCH_TEXELS (ETCU_NOALLOC_MAX_PIXELS + 8208u)
 ETCU_API etcu_status etcu_sart_view_update_noalloc(const etcu_volume_desc* desc, float* d_volume,
                                                    const float* d_projection, const etcu_view* view,
                                                    uint32_t fp_samples, uint32_t bp_samples, float lambda,

@@ -88,4 +88,7 @@ def main(root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("ETTENTION_REFERENCE", "")
+    if not ref:
+        sys.exit("usage: make_golden.py <reference checkout> (or set ETTENTION_REFERENCE)")
+    main(ref)

@@ -7,6 +7,15 @@ import numpy as np
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
+# The reference checkout (the directory holding `ettention/`), named by the environment
+# variable ETTENTION_REFERENCE; tests that read its files directly skip when it is unset.
+REFERENCE = os.environ.get("ETTENTION_REFERENCE", "")
+
+
+def reference_path(*parts: str) -> str:
+    """Path inside the reference checkout, or "" when ETTENTION_REFERENCE is unset."""
+    return os.path.join(REFERENCE, *parts) if REFERENCE else ""
+
 
 def golden(name: str) -> dict:
     with np.load(os.path.join(GOLDEN, f"{name}.npz")) as z:

@@ -55,6 +55,29 @@ def test_no_device_fails_loudly():
         Context(0)
 
 
+@pytest.mark.parametrize("w,h,fits", [(1024, 1024, True), (2048, 508, True), (4096, 256, False),
+                                       (2048, 1024, False), (1025, 1024, False)])
+def test_noalloc_scratch_bound(w, h, fits):
+    """The allocation-free update's static image holds (width + 4) x (height + 4) texels of
+    at most NOALLOC_SCRATCH_TEXELS and at most NOALLOC_MAX_PIXELS pixels; larger detectors
+    are rejected before the device is touched (the buffers below are never dereferenced)."""
+    assert ((w + 4) * (h + 4) <= _abi.NOALLOC_SCRATCH_TEXELS and w * h <= _abi.NOALLOC_MAX_PIXELS) == fits
+    if fits:
+        return
+    desc = _abi.VolumeDesc()
+    for i, r in enumerate((64, 64, 32)):
+        desc.resolution[i] = r
+        desc.bbox_min[i] = -0.5 * r
+        desc.bbox_max[i] = 0.5 * r
+    desc.subvolume_count = 1
+    view = mrc_base_geometry(w, h).to_view()
+    st = _abi.lib().etcu_sart_view_update_noalloc(ctypes.byref(desc), ctypes.c_void_p(256), ctypes.c_void_p(256),
+                                                  ctypes.byref(view), 1, 1, 0.3, None, None)
+    assert st == _abi.ERR_INVALID_ARGUMENT
+    msg = _abi.lib().etcu_last_error(None)
+    assert b"exceeds" in msg and str(_abi.NOALLOC_SCRATCH_TEXELS).encode() in msg
+
+
 @pytest.mark.parametrize("angle,xt", [(0.0, 0.0), (45.0, 0.0), (-60.0, 0.0), (225.0, 0.0), (37.5, 5.0)])
 def test_rotation_and_matrices_match_oracle(angle, xt):
     base = O.projection_test_geometry()

@@ -12,7 +12,9 @@ import struct
 import numpy as np
 import pytest
 
-REF_SYNTH = "/root/reference/ettention/test/data/synthetic_3_parallel"
+from tests.helpers import reference_path
+
+REF_SYNTH = reference_path("ettention", "test", "data", "synthetic_3_parallel")
 
 
 def _rand(shape, seed=0):
@@ -299,7 +301,7 @@ def test_init_and_mask_volumes(tmp_path):
 
 
 # ----------------------------------------------------------------------------- the reference's data set
-@pytest.mark.skipif(not os.path.isdir(REF_SYNTH), reason="reference checkout not mounted")
+@pytest.mark.skipif(not os.path.isdir(REF_SYNTH), reason="ETTENTION_REFERENCE (reference checkout) not set")
 def test_reference_synthetic_directory_stack():
     """synthetic_3_parallel: 180 LZW float projections, metadata.xml, sart/sirt/blockIterative
     parameter files, read through the native reader."""

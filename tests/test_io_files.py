@@ -10,8 +10,9 @@ import pytest
 
 from ettention_b200 import _abi
 from ettention_b200._abi import EttentionError
+from tests.helpers import reference_path
 
-REF_DATA = "/root/reference/ettention/test/data/jason_64_SART"
+REF_DATA = reference_path("ettention", "test", "data", "jason_64_SART")
 
 
 def write_stack(path, data, mode, extra=b""):
@@ -114,7 +115,7 @@ def test_volume_writer_orders_and_header(tmp_path, orientation):
     assert hdr[208:212] == b"MAP "
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_DATA), reason="reference checkout not present")
+@pytest.mark.skipif(not os.path.isdir(REF_DATA), reason="ETTENTION_REFERENCE (reference checkout) not set")
 def test_reference_jason64_stack_and_tilt_file():
     from ettention_b200.operators import MRCStack
     st = MRCStack(os.path.join(REF_DATA, "jason64.ali"), os.path.join(REF_DATA, "jason64.tlt"), logarithmize=True)

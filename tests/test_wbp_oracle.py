@@ -11,8 +11,9 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
+from tests.helpers import reference_path
 
-REF_WBP = "/root/reference/ettention/plugins/WBPPlugin/test/data/wbp_shepp_logan"
+REF_WBP = reference_path("ettention", "plugins", "WBPPlugin", "test", "data", "wbp_shepp_logan")
 
 
 def _direct_filter(img, fres=128):
@@ -62,7 +63,7 @@ def test_filter_of_a_delta_is_the_kernel_one_row_up():
     assert np.abs(f - want).max() <= 1e-7
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_WBP), reason="reference checkout not mounted")
+@pytest.mark.skipif(not os.path.isdir(REF_WBP), reason="ETTENTION_REFERENCE (reference checkout) not set")
 def test_oracle_wbp_meets_the_reference_test_bound():
     from ettention_b200.operators import MRCStack
     s = MRCStack(os.path.join(REF_WBP, "empiar_10009_128.mrc"), os.path.join(REF_WBP, "empiar_10009_128.tlt"))
