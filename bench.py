@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-reps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-c3", action="store_true",
+                    help="leave out the perspective (C3) record that the default 1-GPU run adds to its line")
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "blobs"],
                     help="c2: the headline SART workload (default); c3: 2048^2 x 512 perspective, block 8, "
                          "bf16 shadow; c4: 64 batched series of uneven sizes")
@@ -553,6 +555,16 @@ def run_ours(args, rank, world, local):
         t = cpu_sample_seconds(cpu_problem, threads)
         cpu = {"value": t * N_VIEWS * TARGET_ITERS, "unit": "s", "cores": threads, "kind": "port",
                "sample": CPU_SAMPLE_TEXT}
+    # ---- the perspective workload's record (1 GPU only): its own clocks, roofline and
+    # CPU sample, in the same line ----
+    ctx.close()
+    c3 = None
+    if rank == 0 and world == 1 and not args.no_c3:
+        torch.cuda.empty_cache()
+        try:
+            c3 = run_c3(args, steps=3, warmup=3, cpu_baseline=not args.no_cpu_baseline)
+        except Exception as exc:  # the headline line is printed either way
+            c3 = {"error": f"{type(exc).__name__}: {exc}"}
     if rank == 0:
         fp_steps, bp_updates = work_units(geoms)
         line = {"metric": "SART s to reach plain 30-iter residual", "value": value, "unit": "s",
@@ -570,9 +582,9 @@ def run_ours(args, rank, world, local):
                          "units_per_s": (fp_steps + bp_updates) / (ms_per_step * 1e-3),
                          "fp_steps_source": "entry and exit voxels of every ray of the 61 views"},
                 "residual_sq": {"before": d0, "after_warmup_and_timed": d1},
+                "c3": c3,
                 "learned_warm_start": "not built: plain SART only"}
         print(json.dumps(line), flush=True)
-    ctx.close()
 
 
 def run_ncu_case(res=(512, 512, 256)):
@@ -659,7 +671,8 @@ def run_c4(args):
     batch = BatchReconstructionOperator([(v, g, pr) for v, (_, g, pr) in zip(vols, problems)], p)
     for _ in range(args.warmup):
         batch.runNiterations(1)
-    batch_ms = timed(lambda: batch.runNiterations(1), args.steps)
+    with ClockSampler(0) as clk:
+        batch_ms = timed(lambda: batch.runNiterations(1), args.steps)
     launches = batch.launches_per_iteration
     batch.close()
     for v in vols:
@@ -698,7 +711,8 @@ def run_c4(args):
         "voxel_updates_per_s": updates / (batch_ms * 1e-3),
         "roofline": {"bound": "hbm", "achieved": byts / (batch_ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
                      "frac": byts / (batch_ms * 1e-3) / 1e9 / hbm,
-                     "bytes": "per view: 4V forward read + 8V back read+write + 20P"}}))
+                     "bytes": "per view: 4V forward read + 8V back read+write + 20P"},
+        "clocks": clk.summary()}))
     ctx.close()
 
 
@@ -721,14 +735,16 @@ def c3_geometry(tilt: float, res=C3_RES):
     return base.rotated(tilt)
 
 
-def run_c3(args):
+def run_c3(args, steps=None, warmup=None, cpu_baseline=True):
     """C3: 2048^2 x 512 volume, 121 perspective views (-60..60 step 1), block size 8,
     FP32 master + BF16 shadow, random order, Poisson I0 = 200; one block-iterative
-    iteration per step."""
+    iteration per step.  Returns the record (clocks, roofline, CPU sample)."""
     import torch
     from ettention_b200 import _abi
     from ettention_b200.operators import (AlgebraicParameterSet, BlockIterativeReconstructionOperator, Context,
                                           ForwardProjectionOperator, GPUMappedVolume)
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
     ctx = Context(0)
     dev = torch.device("cuda", 0)
     res = tuple(int(v) for v in args.c3_res.split(","))
@@ -736,7 +752,8 @@ def run_c3(args):
     phantom = make_phantom_torch(3000, dev, res, count=500, axes=(8.0 * X / 2048, 256.0 * X / 2048))
     geoms = [c3_geometry(float(a), res) for a in np.linspace(-60.0, 60.0, C3_VIEWS)]
     vol = GPUMappedVolume(ctx, res)
-    vol.upload(phantom.cpu().numpy())
+    host_phantom = phantom.cpu().numpy()
+    vol.upload(host_phantom)
     del phantom
     fp = ForwardProjectionOperator(vol, 1)
     projs = torch.zeros((C3_VIEWS, Y, X), dtype=torch.float32, device=dev)
@@ -752,45 +769,87 @@ def run_c3(args):
     b = (-torch.log(torch.clamp(counts, min=1.0) / 200.0)).contiguous()
     del counts, projs, scratch
     torch.cuda.synchronize()
+    cpu_view = None
+    if cpu_baseline:
+        mid = C3_VIEWS // 2
+        cpu_view = (geoms[mid], b[mid].cpu().numpy())
     p = AlgebraicParameterSet(algorithm="blockIterative", block_size=8, iterations=1, lam=0.2,
                               order=_abi.ORDER_RANDOM)
     vol = GPUMappedVolume(ctx, res, voxel_type=_abi.VOXEL_BF16_MASTER)
     rec = BlockIterativeReconstructionOperator(vol, geoms, b, p)
     stream = torch.cuda.ExternalStream(ctx.stream_handle)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         rec.runNiterations(1)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ctx.synchronize()
-    ev0.record(stream)
-    rec.runNiterations(args.steps)
-    ev1.record(stream)
-    ev1.synchronize()
-    ms = ev0.elapsed_time(ev1) / args.steps
+    with ClockSampler(0) as clk:
+        ev0.record(stream)
+        rec.runNiterations(steps)
+        ev1.record(stream)
+        ev1.synchronize()
+    ms = ev0.elapsed_time(ev1) / steps
     fp_ms, bp_ms, nf, nb = rec.profile_iteration()
     rec.close()
     vol.close()
     ctx.close()
+    del b
     V, P, N, B = X * Y * Z, X * Y, C3_VIEWS, 8
     nblocks = (N + B - 1) // B
     # byte model: FP reads the BF16 shadow, b, writes (r, L); BP read-modify-writes the
     # FP32 master once per block and rewrites the shadow; it reads (r, L) per view
-    byts = N * (V * 2 + P * 4 + P * 8) + nblocks * (2 * V * 4 + V * 2) + N * P * 8
+    fp_bytes = N * (V * 2 + P * 4 + P * 8)
+    bp_bytes = nblocks * (2 * V * 4 + V * 2) + N * P * 8
+    byts = fp_bytes + bp_bytes
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except OSError:
         pass
     hbm = float(peaks.get("hbm_gbs", 6650.0))
-    print(json.dumps({
+    cpu = None
+    if cpu_view is not None:
+        threads = os.cpu_count() or 1
+        t = c3_cpu_seconds_per_view(host_phantom, res, cpu_view, threads)
+        cpu = {"value": t * N, "unit": "s", "cores": threads, "kind": "port",
+               "sample": "1 of the 121 views (the 0 deg view: perspective FP + residual + Q8 perspective BP) at "
+                         "full size from a zero volume, FP32 oracle; seconds per view x121 views"}
+    del host_phantom
+    return {
         "metric": "C3 block-iterative s per iteration", "value": ms / 1e3, "unit": "s", "higher_is_better": False,
-        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "dtype": "f32 math, bf16 shadow, f32 master",
+        "n_gpus": 1, "steps": steps, "warmup": warmup, "dtype": "f32 math, bf16 shadow, f32 master",
         "data": "synthetic (seeded 500-ellipsoid phantom, CUDA-forward-projected, Poisson I0=200)",
         "config": {"workload": f"C3: {X}x{Y}x{Z}, 121 perspective views -60..60 step 1, {X}x{Y} detector, "
-                               "block 8, lambda 0.2, random order", "voxel_type": "bf16_master"},
+                               "block 8, lambda 0.2, random order", "voxel_type": "bf16_master",
+                   "l2": f"inputs larger than L2 ({V * 6 / 2**30:.1f} GiB volume)"},
         "per_kernel_ms": {"forward_project_total": fp_ms, "back_project_total": bp_ms,
                           "forward_launches": nf, "back_launches": nb},
         "roofline": {"bound": "hbm", "bytes_per_iteration": byts, "achieved": byts / (ms * 1e-3) / 1e9,
-                     "peak": hbm, "unit": "GB/s", "frac": byts / (ms * 1e-3) / 1e9 / hbm}}))
+                     "peak": hbm, "unit": "GB/s", "frac": byts / (ms * 1e-3) / 1e9 / hbm,
+                     "per_kernel": {
+                         "forward_project": {"kernel": "forward_project_kernel (perspective walk)",
+                                             "algorithmic_bytes": fp_bytes,
+                                             "frac": fp_bytes / (fp_ms * 1e-3) / 1e9 / hbm},
+                         "back_project": {"kernel": "bp_perspective_kernel", "algorithmic_bytes": bp_bytes,
+                                          "frac": bp_bytes / (bp_ms * 1e-3) / 1e9 / hbm}}},
+        "cpu_baseline": cpu, "clocks": clk.summary()}
+
+
+def c3_cpu_seconds_per_view(phantom, res, view, threads: int):
+    """Seconds for one C3 view of the FP32 CPU restatement of the reference kernels
+    (oracle/) on `threads` host threads: perspective forward projection of a zero volume,
+    residual, perspective back projection (texture weights rounded to 1/256)."""
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    from oracle import oracle as O
+    g, b = view
+    og = O.ScannerGeometry(np.asarray(g.source, np.float64), np.asarray(g.detector, np.float64),
+                           np.asarray(g.hpitch, np.float64), np.asarray(g.vpitch, np.float64), g.width, g.height, True)
+    vg = O.VolumeGeometry.centered(res)
+    vol = np.zeros_like(phantom)
+    t0 = time.perf_counter()
+    p, l = O.forward_project(vol, vg, og, 1, 32)
+    r = b - p
+    O.back_project(vol, vg, og, r, l, 0.2 / 8, 1, 32, O.WEIGHTS_Q8)
+    return time.perf_counter() - t0
 
 
 # ------------------------------------------------------------------ blob basis functions
@@ -879,7 +938,7 @@ def main():
         run_c4(args)
         return
     if args.workload == "c3":
-        run_c3(args)
+        print(json.dumps(run_c3(args)), flush=True)
         return
     if args.workload == "blobs":
         run_blobs(args)
