@@ -165,6 +165,16 @@ _SIG = {
     "etcu_batch_launches_per_iteration": (_U, [_P]),
     "etcu_sart_view_update_noalloc": (_S, [ctypes.POINTER(VolumeDesc), _P, _P, ctypes.POINTER(View), _U, _U, _F, _P,
                                            ctypes.POINTER(ctypes.c_double)]),
+    "etcu_warmstart_param_count": (_U, []),
+    "etcu_warmstart_layer_info": (_S, [_U, _P]),
+    "etcu_warmstart_create": (_S, [_P, _P, _U, ctypes.POINTER(_P)]),
+    "etcu_warmstart_destroy": (_S, [_P]),
+    "etcu_warmstart_set_params": (_S, [_P, _P, _F]),
+    "etcu_warmstart_get_params": (_S, [_P, _P, ctypes.POINTER(_F)]),
+    "etcu_warmstart_infer": (_S, [_P, _P, _P, _U]),
+    "etcu_warmstart_train_step": (_S, [_P, _P, _P, _U, _F, ctypes.POINTER(ctypes.c_double)]),
+    "etcu_warmstart_gradients": (_S, [_P, _P, _P, _U, _P, ctypes.POINTER(ctypes.c_double)]),
+    "etcu_warmstart_check": (_S, [_P]),
 }
 
 

@@ -657,6 +657,13 @@ extern "C" etcu_status etcu_context_destroy(etcu_context* ctx) {
 
 void etcu_set_context_free_error(const char* message) { g_create_error = message ? message : ""; }
 
+// Accessors for the library's other translation units (not exported).
+int etcu_context_device_index(const etcu_context* ctx) { return ctx ? ctx->device : 0; }
+void etcu_context_set_error(etcu_context* ctx, const char* message) {
+    if (ctx) ctx->err = message ? message : "";
+    else g_create_error = message ? message : "";
+}
+
 extern "C" const char* etcu_last_error(const etcu_context* ctx) {
     return ctx ? ctx->err.c_str() : g_create_error.c_str();
 }

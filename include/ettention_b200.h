@@ -460,6 +460,45 @@ ETCU_API etcu_status etcu_sart_view_update_noalloc(const etcu_volume_desc* desc,
                                                    uint32_t fp_samples, uint32_t bp_samples, float lambda,
                                                    void* cuda_stream, double* residual_sq);
 
+/* ---------------------------------------------------------------- learned warm start
+ * A 3-level 3-D convolutional encoder-decoder (3x3x3 convolutions, 16 / 32 / 64
+ * channels, BF16 weights and activations, FP32 accumulation on the tensor cores) that
+ * maps a few-iteration SART volume to a warm start from which plain SART continues,
+ * trained on pairs the method itself generates.  The reference has no learned part; its
+ * result enters the reference's loop where `volume.initFile` does
+ * (LR/algorithm/reconstruction/blockiterative/BlockIterativeConfiguration.cpp:36-41).
+ * Volumes are FP32 [batch][z][y][x] device arrays with x, y, z multiples of 4; every
+ * call is ordered on the context's stream.  Parameters are one FP32 vector: per layer
+ * W[27][cout][cin] (tap dz*9 + dy*3 + dx reads voxel (x+dx-1, y+dy-1, z+dz-1)), then
+ * b[cout]; `scale` divides the input volume (and multiplies the residual output). */
+typedef struct etcu_warmstart etcu_warmstart;
+/* Number of FP32 parameters of the network. */
+ETCU_API uint32_t etcu_warmstart_param_count(void);
+/* Layer l (0..10): out[0..5] = real input channels of source 0, channels of source 1
+ * (the skip connection, or 0), output channels, resolution level (1..3), offset of W and
+ * offset of b in the parameter vector. */
+ETCU_API etcu_status etcu_warmstart_layer_info(uint32_t layer, uint32_t out[6]);
+ETCU_API etcu_status etcu_warmstart_create(etcu_context* ctx, const uint32_t resolution[3], uint32_t max_batch,
+                                           etcu_warmstart** out);
+ETCU_API etcu_status etcu_warmstart_destroy(etcu_warmstart* ws);
+/* Replaces the parameters (host FP32, etcu_warmstart_param_count() values) and the input
+ * scale; resets the optimiser state. */
+ETCU_API etcu_status etcu_warmstart_set_params(etcu_warmstart* ws, const float* host_params, float scale);
+ETCU_API etcu_status etcu_warmstart_get_params(etcu_warmstart* ws, float* host_params, float* scale);
+/* d_out = d_in + scale * net(d_in / scale) for `batch` volumes (device pointers). */
+ETCU_API etcu_status etcu_warmstart_infer(etcu_warmstart* ws, const float* d_in, float* d_out, uint32_t batch);
+/* One Adam step (lr; beta 0.9 / 0.999, eps 1e-8) on the mean squared error between the
+ * network's output and d_target, in units of the scale.  loss (optional, host) receives
+ * the loss before the step and synchronises the stream. */
+ETCU_API etcu_status etcu_warmstart_train_step(etcu_warmstart* ws, const float* d_in, const float* d_target,
+                                               uint32_t batch, float lr, double* loss);
+/* The loss and its gradient with respect to every parameter (host FP32 vector), without
+ * an update; synchronises the stream. */
+ETCU_API etcu_status etcu_warmstart_gradients(etcu_warmstart* ws, const float* d_in, const float* d_target,
+                                              uint32_t batch, float* host_grads, double* loss);
+/* Synchronises and reports a convolution that gave up waiting for its operands. */
+ETCU_API etcu_status etcu_warmstart_check(etcu_warmstart* ws);
+
 /* Projection orderings on their own (LR/model/projectionset/ProjectionSet*.cpp), for callers
  * that keep their own driver loop. */
 ETCU_API etcu_status etcu_projection_order(etcu_order order, uint32_t n, const uint32_t* skip, uint32_t skip_count,

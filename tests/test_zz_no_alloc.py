@@ -74,7 +74,10 @@ def test_noalloc_view_update_matches_allocating_path(kind, fp_samples, bp_sample
             got = na_vol.download()
             d = np.linalg.norm((got - ref).ravel()) / np.linalg.norm((ref - init).ravel())
             assert d <= TOL, f"{kind} call {call}: rel-L2 {d}"
-            assert abs(r2.value - ref_r2) <= 1e-9 * ref_r2, (call, r2.value, ref_r2)
+            # the first call projects the same volume (same kernel, sums equal up to the FP64
+            # atomics' order); later calls project volumes that agree within TOL (the
+            # allocating path's single-view back projector may be another kernel)
+            assert abs(r2.value - ref_r2) <= (1e-9 if call == 0 else 1e-6) * ref_r2, (call, r2.value, ref_r2)
         # sizes beyond the static scratch are rejected before any launch: too many pixels,
         # and a narrow detector whose zero-bordered image does not fit (4100 x 260 texels)
         for w, h in ((2048, 1024), (4096, 256)):
