@@ -103,6 +103,8 @@ _SIG = {
     "etcu_volume_destroy": (_S, [_P]),
     "etcu_volume_upload": (_S, [_P, _P]),
     "etcu_volume_download": (_S, [_P, _P]),
+    "etcu_volume_upload_device": (_S, [_P, _P]),
+    "etcu_volume_download_device": (_S, [_P, _P]),
     "etcu_volume_set_mask": (_S, [_P, _P]),
     "etcu_volume_device_ptr": (_P, [_P]),
     "etcu_volume_set_intensity_clamp": (_S, [_P, _I, _F, _I, _F]),

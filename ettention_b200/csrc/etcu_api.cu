@@ -811,6 +811,25 @@ extern "C" etcu_status etcu_volume_upload(etcu_volume* vol, const float* host) {
     return s;
 }
 
+extern "C" etcu_status etcu_volume_upload_device(etcu_volume* vol, const float* d_src) {
+    if (!vol || !d_src) return fail(vol ? vol->ctx : nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    etcu_context* ctx = vol->ctx;
+    if (!vol->master) return fail(ctx, ETCU_ERR_UNSUPPORTED, "device-to-device upload needs an FP32 (master) volume");
+    CK(ctx, cudaMemcpyAsync(vol->master, d_src, voxel_count(vol->desc) * sizeof(float), cudaMemcpyDeviceToDevice,
+                            ctx->stream));
+    if (vol->type != ETCU_VOXEL_FLOAT32) return refresh_low_from_master(vol);
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_volume_download_device(etcu_volume* vol, float* d_dst) {
+    if (!vol || !d_dst) return fail(vol ? vol->ctx : nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    etcu_context* ctx = vol->ctx;
+    if (!vol->master) return fail(ctx, ETCU_ERR_UNSUPPORTED, "device-to-device download needs an FP32 (master) volume");
+    CK(ctx, cudaMemcpyAsync(d_dst, vol->master, voxel_count(vol->desc) * sizeof(float), cudaMemcpyDeviceToDevice,
+                            ctx->stream));
+    return ETCU_OK;
+}
+
 extern "C" etcu_status etcu_volume_download(etcu_volume* vol, float* host) {
     if (!vol || !host) return fail(vol ? vol->ctx : nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
     etcu_context* ctx = vol->ctx;

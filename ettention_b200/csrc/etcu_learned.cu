@@ -78,6 +78,9 @@ constexpr LayerDef kDefs[kLayers] = {
 };
 
 int cin_total(const LayerDef& d) { return d.cin_used0 + d.cin1; }
+// The input gradient of a layer runs as one convolution of cin_total outputs, or, when
+// that exceeds 64 (the 96-input decoder layer), as two: source 0's and source 1's.
+int dx_split(const LayerDef& d) { return cin_total(d) > 64 ? d.cin0 : cin_total(d); }
 size_t layer_params(const LayerDef& d) { return (size_t)27 * d.cout * cin_total(d) + d.cout; }
 
 size_t total_params() {
@@ -101,7 +104,8 @@ struct etcu_warmstart {
     // parameters
     float *params = nullptr, *grads = nullptr, *adam_m = nullptr, *adam_v = nullptr;
     __nv_bfloat16* wf[kLayers] = {};  // forward kernel layout
-    __nv_bfloat16* wb[kLayers] = {};  // input-gradient kernel layout
+    __nv_bfloat16* wb[kLayers] = {};  // input-gradient kernel layout (input channels [0, dx_split))
+    __nv_bfloat16* wb2[kLayers] = {}; // the rest of them, when the input gradient is split
     int adam_t = 0;
     // activations (level 1 / 2 / 3)
     Tensor x16, e1a, e1b, up1, d1a, d1b, dy16, gA1, gB1, gUp1, gSkip1;
@@ -175,32 +179,42 @@ etcu_status make_map(etcu_warmstart* w, CUtensorMap* m, const Tensor& t, int bat
     return ETCU_OK;
 }
 
-constexpr size_t kSmemBudget = 200 * 1024;
+constexpr size_t kSmemBudget = 200 * 1024;      // weight-gradient kernel
+constexpr size_t kConvSmemMax = 232448 - 1024 - 512;  // persistent convolution: stages + resident weights
+constexpr size_t kResidentMax = 64 * 1024;       // weights kept in shared memory for the whole launch
 
-template <int N>
-constexpr uint32_t conv_stage_bytes() {
-    return (ws::kHaloBytes + 27u * 2u * N * 16u + 1023u) & ~1023u;
-}
-
-template <int N>
+template <int N, int TY>
 etcu_status launch_conv_n(etcu_warmstart* w, const CUtensorMap& m0, const CUtensorMap& m1, ws::ConvArgs a,
                           int batch) {
-    const uint32_t stage = conv_stage_bytes<N>();
-    int S = (int)std::min<size_t>(std::max<size_t>(1, kSmemBudget / stage), (size_t)a.nsteps);
-    if (S < 1) S = 1;
+    using SH = ws::ConvShape<N, TY>;
+    const size_t wbytes = (size_t)a.nsteps * SH::kW;
+    a.resident = wbytes <= kResidentMax ? 1 : 0;
+    const size_t wres = a.resident ? (wbytes + 1023) & ~(size_t)1023 : 0;
+    const size_t stage = (SH::kHalo + (a.resident ? 0 : SH::kW) + 1023) & ~(size_t)1023;
+    int S = (int)std::min<size_t>(4, (kConvSmemMax - wres) / stage);
+    if (S < 1) return wfail(w, ETCU_ERR_UNSUPPORTED, "convolution stage of %zu bytes does not fit", stage);
     a.stages = S;
-    const size_t smem = (size_t)S * stage + (2 * S + 1) * 8 + 16 + 1024;
+    a.batch = batch;
+    // at least 120 KB, so that one CTA (and its tensor memory) owns each SM
+    const size_t smem = std::max<size_t>(wres + (size_t)S * stage + (2 * S + 5) * 8 + 16 + 1024, 120 * 1024);
     static std::atomic<unsigned long long> opted{0};
     if (w->device < 64 && !(opted.load() & (1ull << w->device))) {
-        WCK(w, cudaFuncSetAttribute(ws::conv_tc_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+        WCK(w, cudaFuncSetAttribute(ws::conv_tc_kernel<N, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    232448));
         opted.fetch_or(1ull << w->device);
     }
     const int ntx = (a.X + ws::kTileX - 1) / ws::kTileX;
-    const unsigned grid = (unsigned)ntx * a.Y * a.Z * batch;
-    ws::conv_tc_kernel<N><<<grid, 128, smem, w->stream>>>(m0, m1, a);
+    const int nty = (a.Y + TY - 1) / TY;
+    const long ntiles = (long)ntx * nty * a.Z * batch;
+    const unsigned grid = (unsigned)std::min<long>(ntiles, w->sms);
+    ws::conv_tc_kernel<N, TY><<<grid, 192, smem, w->stream>>>(m0, m1, a);
     WCK(w, cudaGetLastError());
     return ETCU_OK;
 }
+
+// Rows per tile of the persistent convolution by output width N (two accumulators of
+// TY * N tensor-memory columns; halo ring and weights within shared memory).
+int conv_rows(int n) { return n >= 64 ? 2 : 4; }
 
 // Convolution of one or two sources into `n` channels (forward: weights wf, bias and
 // ReLU; input gradient: weights wb, masks).
@@ -221,10 +235,11 @@ struct ConvCall {
 };
 
 etcu_status conv(etcu_warmstart* w, const ConvCall& c, int batch) {
+    const int TY = conv_rows(c.n);
     CUtensorMap m0, m1;
-    etcu_status s = make_map(w, &m0, *c.src0, batch, ws::kHaloX, 3, 3, 2);
+    etcu_status s = make_map(w, &m0, *c.src0, batch, ws::kHaloX, TY + 2, 3, 2);
     if (s != ETCU_OK) return s;
-    s = make_map(w, &m1, c.src1 ? *c.src1 : *c.src0, batch, ws::kHaloX, 3, 3, 2);
+    s = make_map(w, &m1, c.src1 ? *c.src1 : *c.src0, batch, ws::kHaloX, TY + 2, 3, 2);
     if (s != ETCU_OK) return s;
     ws::ConvArgs a{};
     const Grid& g = c.src0->g;
@@ -247,11 +262,10 @@ etcu_status conv(etcu_warmstart* w, const ConvCall& c, int batch) {
     a.head_scale = c.head_scale;
     a.err = w->d_err;
     switch (c.n) {
-    case 16: return launch_conv_n<16>(w, m0, m1, a, batch);
-    case 32: return launch_conv_n<32>(w, m0, m1, a, batch);
-    case 48: return launch_conv_n<48>(w, m0, m1, a, batch);
-    case 64: return launch_conv_n<64>(w, m0, m1, a, batch);
-    case 96: return launch_conv_n<96>(w, m0, m1, a, batch);
+    case 16: return launch_conv_n<16, 4>(w, m0, m1, a, batch);
+    case 32: return launch_conv_n<32, 4>(w, m0, m1, a, batch);
+    case 48: return launch_conv_n<48, 4>(w, m0, m1, a, batch);
+    case 64: return launch_conv_n<64, 2>(w, m0, m1, a, batch);
     default: return wfail(w, ETCU_ERR_UNSUPPORTED, "no convolution kernel for %d output channels", c.n);
     }
 }
@@ -350,9 +364,15 @@ etcu_status relayout(etcu_warmstart* w) {
                                                                        d.npad, nsteps_f, w->wf[l]);
         if (l > 0) {
             const int nsteps_b = (d.cout + 15) / 16;
-            const int nb = nsteps_b * 27 * 2 * cin_total(d) * 8;
-            ws::relayout_backward_kernel<<<blocks(nb), 256, 0, w->stream>>>(w->params + w->woff[l], d.cout,
-                                                                            cin_total(d), nsteps_b, w->wb[l]);
+            const int n0 = dx_split(d), n1 = cin_total(d) - n0;
+            const int nb0 = nsteps_b * 27 * 2 * n0 * 8;
+            ws::relayout_backward_kernel<<<blocks(nb0), 256, 0, w->stream>>>(w->params + w->woff[l], d.cout,
+                                                                             cin_total(d), 0, n0, nsteps_b, w->wb[l]);
+            if (n1 > 0) {
+                const int nb1 = nsteps_b * 27 * 2 * n1 * 8;
+                ws::relayout_backward_kernel<<<blocks(nb1), 256, 0, w->stream>>>(
+                    w->params + w->woff[l], d.cout, cin_total(d), n0, n1, nsteps_b, w->wb2[l]);
+            }
         }
     }
     WCK(w, cudaGetLastError());
@@ -438,13 +458,20 @@ etcu_status backward(etcu_warmstart* w, const float* d_in, const float* d_target
         c.w = w->wb[l];
         c.bias = nullptr;
         c.relu = false;
-        c.n = cin_total(d);
+        c.n = dx_split(d);
         c.dst0 = dst(out0, mask0);
-        if (out1) {
+        if (out1 && dx_split(d) == cin_total(d)) {  // both sources' gradients from one launch
             c.dst1 = dst(*out1);
             c.n0 = d.cin0;
+            c.n = cin_total(d);
         }
-        return conv(w, c, B);
+        etcu_status st = conv(w, c, B);
+        if (st != ETCU_OK || !out1 || dx_split(d) == cin_total(d)) return st;
+        ConvCall c2 = c;  // source 1's input gradient
+        c2.w = w->wb2[l];
+        c2.n = cin_total(d) - dx_split(d);
+        c2.dst0 = dst(*out1);
+        return conv(w, c2, B);
     };
     // head (layer 10): dPre(d1b) = conv^T(dy) * [d1b > 0]
     WTRY(wgrad(w, 10, w->d1b, 16, 0, w->dy16, B));
@@ -593,7 +620,11 @@ extern "C" etcu_status etcu_warmstart_create(etcu_context* ctx, const uint32_t r
     for (int l = 0; l < kLayers; ++l) {
         const LayerDef& d = kDefs[l];
         WTRY(walloc(p, (void**)&p->wf[l], (size_t)(d.cin0 + d.cin1) / 16 * 27 * 2 * d.npad * 8 * 2));
-        if (l > 0) WTRY(walloc(p, (void**)&p->wb[l], (size_t)((d.cout + 15) / 16) * 27 * 2 * cin_total(d) * 8 * 2));
+        if (l > 0) {
+            const size_t per = (size_t)((d.cout + 15) / 16) * 27 * 2 * 8 * 2;
+            WTRY(walloc(p, (void**)&p->wb[l], per * dx_split(d)));
+            if (cin_total(d) > dx_split(d)) WTRY(walloc(p, (void**)&p->wb2[l], per * (cin_total(d) - dx_split(d))));
+        }
         for (int cin : {d.cin0, d.cin1}) {
             if (cin == 0) continue;
             const int ngroups = cin == 16 ? 1 : (cin == 32 ? 3 : 9);

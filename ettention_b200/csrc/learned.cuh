@@ -52,6 +52,9 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                  : "memory");
 }
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
@@ -165,11 +168,12 @@ struct ConvDst {
 };
 
 struct ConvArgs {
-    int X, Y, Z;           // voxel grid of input and output (same-size convolution)
+    int X, Y, Z, batch;    // voxel grid of input and output (same-size convolution)
     int nsteps;            // K steps of 16 channels over both sources
     int nkp0;              // steps from source 0 (the rest from source 1)
     int c8_0, c8_1;        // chunks per batch item of source 0 / 1 (dim-4 coordinate n * c8 + 2 kp)
     const __nv_bfloat16* w;  // [step][27 taps][2 halves][N][8] bf16
+    int resident;          // 1: all steps' weights are loaded once into shared memory
     const float* bias;     // N values or NULL
     int relu;
     int head;              // 1: channel 0 only, out_f32 = in_f32 + scale * (acc + bias)
@@ -182,34 +186,45 @@ struct ConvArgs {
     unsigned* err;
 };
 
-// One CTA computes one row of 128 output voxels (x0 .. x0 + 127 at fixed y, z, batch item)
-// for all N output channels: warp 0 issues the halo and weight copies, warp 1 the MMAs
-// (27 per 16-channel step), all four warps then drain the accumulator.
-template <int N>
-__global__ void __launch_bounds__(128) conv_tc_kernel(const __grid_constant__ CUtensorMap src0,
-                                                      const __grid_constant__ CUtensorMap src1, ConvArgs a) {
+template <int N, int TY>
+struct ConvShape {
+    static constexpr uint32_t kHalo = (uint32_t)kHaloX * (TY + 2) * 3u * 16u * 2u;  // two chunks
+    static constexpr uint32_t kPlane = (uint32_t)kHaloX * (TY + 2) * 3u * 16u;      // one chunk
+    static constexpr uint32_t kW = 27u * 2u * N * 16u;                               // one step's weights
+    static constexpr uint32_t kAcc = (uint32_t)TY * N;                               // columns per accumulator
+    static constexpr uint32_t kCols = 2 * kAcc <= 32 ? 32 : 2 * kAcc <= 64 ? 64 : 2 * kAcc <= 128 ? 128
+                                      : 2 * kAcc <= 256 ? 256 : 512;
+    static_assert(2 * kAcc <= 512, "two accumulators must fit in tensor memory");
+};
+
+// Persistent convolution: a CTA takes tiles of 128 x-voxels by TY y-rows (one z, one batch
+// item) round-robin.  Warp 0 streams the 130 x (TY + 2) x 3 halo of every 16-channel step
+// (and, unless the weights are resident, the step's weights) through a ring of `stages`
+// buffers; warp 1 issues 27 x TY MMAs per step into one of two tensor-memory accumulators;
+// warps 2-5 drain the other accumulator (bias, ReLU, mask, BF16 store) meanwhile.
+template <int N, int TY>
+__global__ void __launch_bounds__(192, 1) conv_tc_kernel(const __grid_constant__ CUtensorMap src0,
+                                                         const __grid_constant__ CUtensorMap src1, ConvArgs a) {
+    using SH = ConvShape<N, TY>;
     static_assert(N % 16 == 0 && N >= 16 && N <= 256, "M = 128 needs N a multiple of 16");
-    constexpr uint32_t kWBytes = 27u * 2u * N * 16u;
-    constexpr uint32_t kStage = (kHaloBytes + kWBytes + 1023u) & ~1023u;
-    constexpr uint32_t kCols = N <= 32 ? 32 : (N <= 64 ? 64 : (N <= 128 ? 128 : 256));
     constexpr uint32_t kIdesc = idesc_bf16(128, N, 0, 0);
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     const int S = a.stages;
-    uint64_t* full = (uint64_t*)(smem + S * kStage);
+    const uint32_t wres = a.resident ? (uint32_t)a.nsteps * SH::kW : 0u;           // resident weights
+    const uint32_t stage = (SH::kHalo + (a.resident ? 0u : SH::kW) + 1023u) & ~1023u;
+    uint8_t* wsm = smem;                                                             // resident weights
+    uint8_t* ring = smem + ((wres + 1023u) & ~1023u);
+    uint64_t* full = (uint64_t*)(ring + (size_t)S * stage);
     uint64_t* empty = full + S;
-    uint64_t* done = empty + S;
-    uint32_t* tmem_slot = (uint32_t*)(done + 1);
+    uint64_t* accf = empty + S;  // [2] accumulator written (MMA -> epilogue)
+    uint64_t* acce = accf + 2;   // [2] accumulator drained (epilogue -> MMA)
+    uint64_t* wbar = acce + 2;
+    uint32_t* tmem_slot = (uint32_t*)(wbar + 1);
 
     const int ntx = (a.X + kTileX - 1) / kTileX;
-    int t = blockIdx.x;
-    const int xt = t % ntx;
-    t /= ntx;
-    const int y = t % a.Y;
-    t /= a.Y;
-    const int z = t % a.Z;
-    const int n = t / a.Z;
-    const int x0 = xt * kTileX;
+    const int nty = (a.Y + TY - 1) / TY;
+    const int ntiles = ntx * nty * a.Z * a.batch;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     if (threadIdx.x == 0) {
@@ -217,119 +232,178 @@ __global__ void __launch_bounds__(128) conv_tc_kernel(const __grid_constant__ CU
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
-        mbar_init(done, 1);
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(&accf[i], 1);
+            mbar_init(&acce[i], 4);
+        }
+        mbar_init(wbar, 1);
         mbar_fence_init();
     }
-    if (warp == 0) tmem_alloc(tmem_slot, kCols);
+    if (warp == 0) tmem_alloc(tmem_slot, SH::kCols);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
-    if (warp == 0 && lane == 0) {
-        // producer: halo of 16 channels + the step's weights, per stage
-        for (int s = 0; s < a.nsteps; ++s) {
-            const int st = s % S;
-            if (s >= S && !mbar_wait(&empty[st], ((s / S) - 1) & 1)) {
-                atomicOr(a.err, kErrWaitEmpty);
-                break;
+    if (warp == 0) {
+        if (lane == 0) {
+            if (a.resident) {
+                mbar_expect_tx(wbar, wres);
+                bulk_load(wsm, a.w, wres, wbar);
             }
-            uint8_t* halo = smem + st * kStage;
-            mbar_expect_tx(&full[st], kHaloBytes + kWBytes);
-            const bool second = s >= a.nkp0;
-            const int kp = second ? s - a.nkp0 : s;
-            const int c4 = n * (second ? a.c8_1 : a.c8_0) + 2 * kp;
-            tma_load_5d(halo, second ? &src1 : &src0, &full[st], 0, x0 - 1, y - 1, z - 1, c4);
-            bulk_load(halo + kHaloBytes, a.w + (size_t)s * (kWBytes / 2), kWBytes, &full[st]);
+            int q = 0;
+            bool ok = true;
+            for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+                int t = tile;
+                const int xt = t % ntx;
+                t /= ntx;
+                const int yt = t % nty;
+                t /= nty;
+                const int z = t % a.Z;
+                const int n = t / a.Z;
+                for (int s = 0; s < a.nsteps; ++s, ++q) {
+                    const int st = q % S;
+                    if (q >= S && !mbar_wait(&empty[st], ((q / S) - 1) & 1)) {
+                        atomicOr(a.err, kErrWaitEmpty);
+                        ok = false;
+                        break;
+                    }
+                    uint8_t* halo = ring + (size_t)st * stage;
+                    mbar_expect_tx(&full[st], SH::kHalo + (a.resident ? 0u : SH::kW));
+                    const bool second = s >= a.nkp0;
+                    const int kp = second ? s - a.nkp0 : s;
+                    const int c4 = n * (second ? a.c8_1 : a.c8_0) + 2 * kp;
+                    tma_load_5d(halo, second ? &src1 : &src0, &full[st], 0, xt * kTileX - 1, yt * TY - 1, z - 1, c4);
+                    if (!a.resident)
+                        bulk_load(halo + SH::kHalo, a.w + (size_t)s * (SH::kW / 2), SH::kW, &full[st]);
+                }
+            }
         }
-    } else if (warp == 1 && lane == 0) {
-        // MMA issuer
-        bool ok = true;
-        for (int s = 0; s < a.nsteps && ok; ++s) {
-            const int st = s % S;
-            if (!mbar_wait(&full[st], (s / S) & 1)) {
-                atomicOr(a.err, kErrWaitFull);
-                ok = false;
+    } else if (warp == 1) {
+        if (lane == 0) {
+            bool ok = !a.resident || mbar_wait(wbar, 0);
+            if (!ok) atomicOr(a.err, kErrWaitFull);
+            int q = 0, i = 0;
+            for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++i) {
+                const int acc = i & 1;
+                if (i >= 2 && !mbar_wait(&acce[acc], ((i >> 1) - 1) & 1)) {
+                    atomicOr(a.err, kErrWaitEmpty);
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t dacc = tmem + (uint32_t)acc * SH::kAcc;
+                for (int s = 0; s < a.nsteps; ++s, ++q) {
+                    const int st = q % S;
+                    if (!mbar_wait(&full[st], (q / S) & 1)) {
+                        atomicOr(a.err, kErrWaitFull);
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t hbase = smem_u32(ring + (size_t)st * stage);
+                    const uint32_t wbase = a.resident ? smem_u32(wsm) + (uint32_t)s * SH::kW : hbase + SH::kHalo;
+#pragma unroll 1
+                    for (int tap = 0; tap < 27; ++tap) {
+                        const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
+                        const uint64_t bd = sdesc(wbase + (uint32_t)tap * (2u * N * 16u), N * 16u, 128);
+#pragma unroll
+                        for (int ty = 0; ty < TY; ++ty) {
+                            const uint32_t aoff = (uint32_t)(((dz * (TY + 2) + ty + dy) * kHaloX + dx) * 16);
+                            umma_bf16(dacc + (uint32_t)(ty * N), sdesc(hbase + aoff, SH::kPlane, 128), bd, kIdesc,
+                                      (s > 0 || tap > 0) ? 1u : 0u);
+                        }
+                    }
+                    umma_commit(&empty[st]);
+                }
+                if (!ok) break;
+                umma_commit(&accf[acc]);
+            }
+        }
+    } else {
+        // epilogue: warp quarter (warp % 4) reads tensor-memory lanes 32 * (warp % 4) ...
+        const int quarter = warp & 3;
+        const int m = quarter * 32 + lane;
+        const size_t plane = (size_t)a.Z * a.Y * a.X;
+        int i = 0;
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i) {
+            const int acc = i & 1;
+            const bool got = mbar_wait(&accf[acc], (i >> 1) & 1);
+            __syncwarp();
+            if (!got) {
+                if (lane == 0) atomicOr(a.err, kErrWaitDone);
                 break;
             }
             tc_fence_after();
-            const uint32_t hbase = smem_u32(smem + st * kStage);
-            const uint32_t wbase = hbase + kHaloBytes;
+            int t = tile;
+            const int xt = t % ntx;
+            t /= ntx;
+            const int yt = t % nty;
+            t /= nty;
+            const int z = t % a.Z;
+            const int n = t / a.Z;
+            const int x = xt * kTileX + m;
+            const uint32_t dacc = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)acc * SH::kAcc;
 #pragma unroll 1
-            for (int tap = 0; tap < 27; ++tap) {
-                const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
-                const uint64_t ad = sdesc(hbase + (uint32_t)(((dz * 3 + dy) * kHaloX + dx) * 16), kHaloPlane, 128);
-                const uint64_t bd = sdesc(wbase + (uint32_t)tap * (2u * N * 16u), N * 16u, 128);
-                umma_bf16(tmem, ad, bd, kIdesc, (s > 0 || tap > 0) ? 1u : 0u);
-            }
-            umma_commit(&empty[st]);
-        }
-        if (ok) umma_commit(done);
-    }
-    __syncwarp();
-
-    // epilogue: thread = lane = output voxel x0 + 32 * warp + lane
-    const bool got = mbar_wait(done, 0);
-    if (!got && threadIdx.x == 0) atomicOr(a.err, kErrWaitDone);
-    __syncwarp();
-    tc_fence_after();
-    if (got) {
-        const int m = warp * 32 + lane;
-        const int x = x0 + m;
-        const bool valid = x < a.X;
-        const size_t plane = (size_t)a.Z * a.Y * a.X;
-        const size_t vox = ((size_t)z * a.Y + y) * a.X + x;
-        if (a.head) {
-            uint32_t r[16];
-            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16), r);
-            tmem_wait_ld();
-            if (valid) {
-                const size_t idx = (size_t)n * plane + vox;
-                float acc = __uint_as_float(r[0]) + (a.bias ? a.bias[0] : 0.f);
-                a.head_out[idx] = fmaf(a.head_scale, acc, a.head_in[idx]);
-            }
-        } else {
-#pragma unroll
-            for (int c = 0; c < N / 16; ++c) {
-                uint32_t r[16];
-                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c * 16), r);
-                tmem_wait_ld();
-                if (!valid) continue;
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int ch = c * 16 + h * 8;
-                    float v[8];
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) {
-                        v[j] = __uint_as_float(r[h * 8 + j]);
-                        if (a.bias) v[j] += a.bias[ch + j];
-                        if (a.relu) v[j] = fmaxf(v[j], 0.f);
+            for (int ty = 0; ty < TY; ++ty) {
+                const int y = yt * TY + ty;
+                const bool valid = x < a.X && y < a.Y;
+                const size_t vox = ((size_t)z * a.Y + y) * a.X + x;
+                if (a.head) {
+                    uint32_t r[16];
+                    tmem_ld16(dacc + (uint32_t)(ty * N), r);
+                    tmem_wait_ld();
+                    if (valid) {
+                        const size_t idx = (size_t)n * plane + vox;
+                        const float accv = __uint_as_float(r[0]) + (a.bias ? a.bias[0] : 0.f);
+                        a.head_out[idx] = fmaf(a.head_scale, accv, a.head_in[idx]);
                     }
-                    const bool first = ch < a.n0;
-                    const ConvDst& d = first ? a.dst0 : a.dst1;
-                    const int c8 = (first ? ch : ch - a.n0) >> 3;
-                    const size_t off = ((size_t)(n * (d.channels >> 3) + c8) * plane + vox) * 8;
-                    if (d.mask) {
-                        float mk[8];
-                        unpack_bf16x8(*reinterpret_cast<const uint4*>(d.mask + off), mk);
+                    continue;
+                }
 #pragma unroll
-                        for (int j = 0; j < 8; ++j) v[j] = mk[j] > 0.f ? v[j] : 0.f;
+                for (int c = 0; c < N / 16; ++c) {
+                    uint32_t r[16];
+                    tmem_ld16(dacc + (uint32_t)(ty * N + c * 16), r);
+                    tmem_wait_ld();
+                    if (!valid) continue;
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int ch = c * 16 + h * 8;
+                        float v[8];
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            v[j] = __uint_as_float(r[h * 8 + j]);
+                            if (a.bias) v[j] += a.bias[ch + j];
+                            if (a.relu) v[j] = fmaxf(v[j], 0.f);
+                        }
+                        const bool first = ch < a.n0;
+                        const ConvDst& d = first ? a.dst0 : a.dst1;
+                        const int c8 = (first ? ch : ch - a.n0) >> 3;
+                        const size_t off = ((size_t)(n * (d.channels >> 3) + c8) * plane + vox) * 8;
+                        if (d.mask) {
+                            float mk[8];
+                            unpack_bf16x8(*reinterpret_cast<const uint4*>(d.mask + off), mk);
+#pragma unroll
+                            for (int j = 0; j < 8; ++j) v[j] = mk[j] > 0.f ? v[j] : 0.f;
+                        }
+                        uint4 o;
+                        o.x = pack_bf16x2(v[0], v[1]);
+                        o.y = pack_bf16x2(v[2], v[3]);
+                        o.z = pack_bf16x2(v[4], v[5]);
+                        o.w = pack_bf16x2(v[6], v[7]);
+                        *reinterpret_cast<uint4*>(d.ptr + off) = o;
                     }
-                    uint4 o;
-                    o.x = pack_bf16x2(v[0], v[1]);
-                    o.y = pack_bf16x2(v[2], v[3]);
-                    o.z = pack_bf16x2(v[4], v[5]);
-                    o.w = pack_bf16x2(v[6], v[7]);
-                    *reinterpret_cast<uint4*>(d.ptr + off) = o;
                 }
             }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acce[acc]);
         }
     }
     tc_fence_before();
     __syncthreads();
     if (warp == 0) {
         tc_fence_after();
-        tmem_dealloc(tmem, kCols);
+        tmem_dealloc(tmem, SH::kCols);
     }
 }
 
@@ -696,8 +770,9 @@ __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, 
 // Kernel weight layouts from the FP32 master W[27][cout][cin_total]:
 //  forward: [step][tap][half][N][8] with N = n_pad (>= cout), input channel
 //           ci = step * 16 + half * 8 + j (zero beyond cin_total);
-//  input gradient: [step][tap'][half][N'][8] with N' = cin_total, output-gradient channel
-//           co = step * 16 + half * 8 + j (zero beyond cout), W' = W[26 - tap'] transposed.
+//  input gradient: [step][tap'][half][N'][8] for input channels ci0 .. ci0 + N' - 1,
+//           output-gradient channel co = step * 16 + half * 8 + j (zero beyond cout),
+//           W' = W[26 - tap'] transposed.
 __global__ void relayout_forward_kernel(const float* __restrict__ W, int cout, int cin_total, int n_pad, int nsteps,
                                         __nv_bfloat16* __restrict__ out) {
     const int total = nsteps * 27 * 2 * n_pad * 8;
@@ -716,21 +791,22 @@ __global__ void relayout_forward_kernel(const float* __restrict__ W, int cout, i
     const float w = (nn < cout && ci < cin_total) ? W[((size_t)tap * cout + nn) * cin_total + ci] : 0.f;
     out[i] = __float2bfloat16_rn(w);
 }
-__global__ void relayout_backward_kernel(const float* __restrict__ W, int cout, int cin_total, int nsteps,
-                                         __nv_bfloat16* __restrict__ out) {
-    const int total = nsteps * 27 * 2 * cin_total * 8;
+__global__ void relayout_backward_kernel(const float* __restrict__ W, int cout, int cin_total, int ci0, int n_part,
+                                         int nsteps, __nv_bfloat16* __restrict__ out) {
+    const int total = nsteps * 27 * 2 * n_part * 8;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= total) return;
     int t = i;
     const int j = t % 8;
     t /= 8;
-    const int ci = t % cin_total;
-    t /= cin_total;
+    const int nn = t % n_part;
+    t /= n_part;
     const int half = t % 2;
     t /= 2;
     const int tap = t % 27;
     const int step = t / 27;
     const int co = step * 16 + half * 8 + j;
+    const int ci = ci0 + nn;
     const float w = co < cout ? W[((size_t)(26 - tap) * cout + co) * cin_total + ci] : 0.f;
     out[i] = __float2bfloat16_rn(w);
 }

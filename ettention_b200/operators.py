@@ -578,6 +578,15 @@ class GPUMappedVolume:
     def device_ptr(self) -> int:
         return int(lib().etcu_volume_device_ptr(self.handle) or 0)
 
+    def upload_device(self, t) -> None:
+        """Copies a CUDA float32 tensor (z, y, x) into the volume on the library's stream."""
+        self.ctx.check(lib().etcu_volume_upload_device(self.handle, _dptr(t)))
+
+    def download_device(self, t) -> None:
+        """Copies the volume into a CUDA float32 tensor (z, y, x) on the library's stream
+        (synchronise the context before reading it on another stream)."""
+        self.ctx.check(lib().etcu_volume_download_device(self.handle, _dptr(t)))
+
 
 # ----------------------------------------------------------------------------- operators
 class ForwardProjectionOperator:

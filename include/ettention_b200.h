@@ -147,6 +147,12 @@ ETCU_API etcu_status etcu_volume_destroy(etcu_volume* vol);
 /* Host float32 volume (x fastest, z slowest) <-> device; converts to / from the storage type. */
 ETCU_API etcu_status etcu_volume_upload(etcu_volume* vol, const float* host);
 ETCU_API etcu_status etcu_volume_download(etcu_volume* vol, float* host);
+/* Stream-ordered device-to-device copies of the FP32 volume (FLOAT32 and *_MASTER types;
+ * an upload refreshes the 16-bit shadow): the device-memory counterpart of the
+ * reference's `volume.initFile` (BlockIterativeConfiguration.cpp:36-41), used to start a
+ * reconstruction from a warm start without a host round trip. */
+ETCU_API etcu_status etcu_volume_upload_device(etcu_volume* vol, const float* d_src);
+ETCU_API etcu_status etcu_volume_download_device(etcu_volume* vol, float* d_dst);
 /* Prior-knowledge mask (UCHAR_8 volume, value/255 weights; LR/algorithm/projections/
  * forward/ForwardProjectionKernel.cpp:21 USE_PRIOR_KNOWLEDGE_MASK).  NULL removes it. */
 ETCU_API etcu_status etcu_volume_set_mask(etcu_volume* vol, const uint8_t* host_mask);

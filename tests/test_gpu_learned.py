@@ -5,8 +5,8 @@ the FP64 CPU oracle of the network (oracle/warmstart_oracle.py):
   CUDA path does (rel-L2 of the network's correction <= 1e-2) and exactly in FP64;
 * the loss and the gradient of every layer's weights and biases (rel-L2 <= 2e-2 against
   the BF16-emulating oracle, <= 1e-1 against the exact FP64 network);
-* rows wider than one 128-voxel tile, a batch of two volumes, and a few Adam steps that
-  lower the loss.
+* rows wider than one 128-voxel tile, y extents that leave a tile's last rows outside the
+  volume, batches of two and three volumes, and a few Adam steps that lower the loss.
 """
 import numpy as np
 import pytest
@@ -52,7 +52,7 @@ def _rel(a, b):
     return float(np.linalg.norm((np.asarray(a, np.float64) - b).ravel()) / np.linalg.norm(np.asarray(b).ravel()))
 
 
-@pytest.mark.parametrize("res,batch", [((16, 16, 8), 2), ((160, 8, 4), 1)])
+@pytest.mark.parametrize("res,batch", [((16, 16, 8), 2), ((160, 8, 4), 1), ((32, 12, 8), 3)])
 def test_forward_matches_oracle(ctx, res, batch):
     import torch
     from oracle import warmstart_oracle as W
