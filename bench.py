@@ -56,9 +56,12 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-reps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--c4-f32", action="store_true", help="--workload c4 with FP32 volumes (default: FP16 shadow)")
+    ap.add_argument("--no-autotune", action="store_true", help="built-in launch shapes instead of the autotuner's")
     ap.add_argument("--no-c3", action="store_true",
                     help="leave out the perspective (C3) record that the default 1-GPU run adds to its line")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "blobs"],
+    ap.add_argument("--c5-seeds", type=int, default=100, help="held-out series of --workload c5")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5", "blobs"],
                     help="c2: the headline SART workload (default); c3: 2048^2 x 512 perspective, block 8, "
                          "bf16 shadow; c4: 64 batched series of uneven sizes")
     ap.add_argument("--c3-res", default="2048,2048,512",
@@ -600,9 +603,11 @@ def c4_shapes(seed: int = 4000):
 
 
 def run_c4(args):
-    """Batched SART of the 64 C4 series (one forward and one back-projection launch per
-    step over all series, one graph per iteration) against the same series one after
-    another (one graph per series)."""
+    """Batched SART of the 64 C4 series (the whole iteration of every series in one
+    persistent launch, its launch shape from the autotuner) against the same series one
+    after another (one graph per series).  Volumes are FP32 masters with an FP16 shadow
+    (the forward projections read FP16 values, updates accumulate in FP32); --c4-f32
+    keeps plain FP32 volumes."""
     import torch
     from ettention_b200 import _abi
     from ettention_b200.operators import (AlgebraicParameterSet, BatchReconstructionOperator,
@@ -627,6 +632,7 @@ def run_c4(args):
         problems.append(((X, Y, Z), geoms, projs.cpu().numpy()))
     p = AlgebraicParameterSet(algorithm="sart", block_size=1, iterations=1, lam=LAMBDA, order=_abi.ORDER_IDENTITY)
     stream = torch.cuda.ExternalStream(ctx.stream_handle)
+    voxel_type = _abi.VOXEL_FLOAT32 if args.c4_f32 else _abi.VOXEL_F16_MASTER
 
     def timed(run, reps):
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -638,8 +644,10 @@ def run_c4(args):
         ev1.synchronize()
         return ev0.elapsed_time(ev1) / reps
 
-    vols = [GPUMappedVolume(ctx, shape) for shape, _, _ in problems]
+    vols = [GPUMappedVolume(ctx, shape, voxel_type=voxel_type) for shape, _, _ in problems]
+    ctx.set_autotune(0 if args.no_autotune else 1)
     batch = BatchReconstructionOperator([(v, g, pr) for v, (_, g, pr) in zip(vols, problems)], p)
+    tuned = ctx.tune_report()
     for _ in range(args.warmup):
         batch.runNiterations(1)
     with ClockSampler(0) as clk:
@@ -649,8 +657,9 @@ def run_c4(args):
     for v in vols:
         v.close()
     seq = []
+    ctx.set_autotune(0)
     for shape, geoms, projs in problems:
-        vol = GPUMappedVolume(ctx, shape)
+        vol = GPUMappedVolume(ctx, shape, voxel_type=voxel_type)
         rec = BlockIterativeReconstructionOperator(vol, geoms, projs, p)
         seq.append((vol, rec))
     def run_seq():
@@ -673,7 +682,9 @@ def run_c4(args):
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     print(json.dumps({
         "metric": "C4 batched SART ms per iteration (64 series)", "value": batch_ms, "unit": "ms",
-        "higher_is_better": False, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "dtype": "f32",
+        "higher_is_better": False, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "dtype": "f32" if args.c4_f32 else "f32 math, f16 shadow, f32 master",
+        "tuned_launch_shape": tuned.strip().splitlines(),
         "data": "synthetic (seeded 40-ellipsoid phantoms per series, CUDA-forward-projected, noise-free)",
         "config": {"workload": "C4: 64 SART series, 96^3 to 256x256x128, 41 to 81 views over +-50..70 deg",
                    "series": C4_SERIES, "voxel_view_updates_per_iteration": updates},
@@ -823,6 +834,112 @@ def c3_cpu_seconds_per_view(phantom, res, view, threads: int):
     return time.perf_counter() - t0
 
 
+# ------------------------------------------------------------------ C5: learned warm start vs plain SART
+def warmstart_flops(res):
+    """Multiply-adds x 2 of one inference of the warm-start network (3x3x3 convolutions)."""
+    from ettention_b200.learned import LAYERS
+    X, Y, Z = res
+    level_vox = {1: X * Y * Z, 2: X * Y * Z // 8, 3: X * Y * Z // 64}
+    levels = [1, 1, 2, 2, 3, 3, 2, 2, 1, 1, 1]
+    return sum(2 * 27 * (c0 + c1) * co * level_vox[l] for (c0, c1, co), l in zip(LAYERS, levels))
+
+
+def run_c5(args):
+    """Held-out series of the learned warm start's workload (256^3/2 volumes, 61 views,
+    Poisson 100, SART lambda 0.03): the time plain SART takes to first reach its own
+    30-iteration residual ||Ax - b||^2, against 3 plain iterations + the network + the
+    residual judge + the plain iterations that then reach the same residual; both timed
+    with CUDA events on the library stream (the per-iteration residual checks that find
+    the iteration counts run untimed, before the timed runs)."""
+    import torch
+    from ettention_b200 import warmstart as W
+    from ettention_b200.learned import DEFAULT_WEIGHTS, WarmStartNet, load_weights
+    from ettention_b200.operators import Context
+    if not os.path.exists(DEFAULT_WEIGHTS):
+        return {"metric": "C5 learned warm start", "unavailable": "no trained weights file"}
+    params, scale, meta = load_weights(DEFAULT_WEIGHTS)
+    ctx = Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream_handle)
+    net = WarmStartNet(ctx, W.RES, params=params, scale=scale)
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ctx.synchronize()
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    per = []
+    cap = 3 * W.TARGET_ITERS
+    with ClockSampler(0) as clk:
+        for j in range(args.c5_seeds):
+            s = W.make_series(ctx, W.HELDOUT_SEED0 + j)
+            plain = W.PlainSart(ctx, s)
+            plain.set_volume(None)
+            r = []
+            for _ in range(W.TARGET_ITERS):
+                plain.iterate(1)
+                r.append(plain.residual())
+            target = r[-1]
+            k_plain = next(i + 1 for i, x in enumerate(r) if x <= target)
+            for _ in range(args.warmup if j == 0 else 0):
+                plain.set_volume(None)
+                plain.iterate(k_plain)
+            plain.set_volume(None)
+            t_plain = timed(lambda: plain.iterate(k_plain))
+            plain.close()
+            solver = W.WarmStartSolver(ctx, net, s)
+            kept = solver.start()
+            k_ws = 0
+            r_ws = solver.residual()
+            while r_ws > target and k_ws < cap:
+                solver.iterate(1)
+                k_ws += 1
+                r_ws = solver.residual()
+            reached = r_ws <= target
+            t_ws = timed(lambda: (solver.start(), solver.iterate(k_ws)))
+            t_net = timed(lambda: net.infer(solver.v_in, solver.v_ws, 1))
+            per.append({"seed": s.seed, "plain_iters": k_plain, "plain_ms": t_plain, "kept": bool(kept),
+                        "judge": [float(x) for x in solver.judge], "extra_iters": k_ws, "reached": bool(reached),
+                        "warm_ms": t_ws, "net_ms": t_net, "speedup": t_plain / t_ws,
+                        "r3": r[W.INPUT_ITERS - 1], "r30": target})
+            solver.close()
+            del s
+    net.close()
+    ctx.close()
+    sp = np.array([p["speedup"] for p in per])
+    flops = warmstart_flops(W.RES)
+    net_ms = float(np.median([p["net_ms"] for p in per]))
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    tf_peak = float(peaks.get("bf16_tflops", 1590.0))
+    return {
+        "metric": "C5 SART s to reach plain 30-iter residual, learned vs plain",
+        "value": float(np.median([p["warm_ms"] for p in per])) / 1e3, "unit": "s", "higher_is_better": False,
+        "plain_s": float(np.median([p["plain_ms"] for p in per])) / 1e3,
+        "speedup_median": float(np.median(sp)), "speedup_mean": float(np.mean(sp)),
+        "speedup_min": float(np.min(sp)), "kept_fraction": float(np.mean([p["kept"] for p in per])),
+        "reached_fraction": float(np.mean([p["reached"] for p in per])),
+        "extra_iters_median": float(np.median([p["extra_iters"] for p in per])),
+        "plain_iters_median": float(np.median([p["plain_iters"] for p in per])),
+        "n_seeds": len(per), "warmup": args.warmup,
+        "config": {"workload": "C5: 256x256x128 ellipsoid phantoms (40, semi-axes 8-64, density 0.05-1 x 0.02), "
+                               "61 parallel views -60..60, Poisson I0=100, SART lambda 0.03, identity order; "
+                               f"held-out seeds {W.HELDOUT_SEED0}..{W.HELDOUT_SEED0 + len(per) - 1}",
+                   "network": "3-level 3-D conv encoder-decoder 16/32/64, BF16, FP32 accumulate",
+                   "trained": {k: (v.tolist() if hasattr(v, "tolist") else v) for k, v in meta.items()
+                               if k in ("series", "epochs", "lr", "train_seed0")}},
+        "roofline": {"bound": "tensor", "kernel": "conv_tc_kernel (network inference)", "flops_per_inference": flops,
+                     "achieved": flops / (net_ms * 1e-3) / 1e12, "peak": tf_peak, "unit": "TFLOP/s",
+                     "frac": flops / (net_ms * 1e-3) / 1e12 / tf_peak, "net_ms": net_ms},
+        "clocks": clk.summary(), "per_seed": per[:8]}
+
+
 # ------------------------------------------------------------------ blob basis functions
 BLOB_RES = (256, 256, 256)
 BLOB_VIEWS = 61
@@ -910,6 +1027,9 @@ def main():
         return
     if args.workload == "c3":
         print(json.dumps(run_c3(args)), flush=True)
+        return
+    if args.workload == "c5":
+        print(json.dumps(run_c5(args)), flush=True)
         return
     if args.workload == "blobs":
         run_blobs(args)

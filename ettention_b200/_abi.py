@@ -94,6 +94,8 @@ _SIG = {
     "etcu_synchronize": (_S, [_P]),
     "etcu_set_stream": (_S, [_P, _P]),
     "etcu_device_bytes": (ctypes.c_size_t, [_P]),
+    "etcu_context_set_autotune": (_S, [_P, _I]),
+    "etcu_context_tune_report": (_S, [_P, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
     "etcu_context_stream": (_P, [_P]),
     "etcu_view_rotate": (_S, [ctypes.POINTER(View), _F, _F, ctypes.POINTER(View)]),
     "etcu_view_projection_matrix": (_S, [ctypes.POINTER(View), _P]),

@@ -17,7 +17,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libettention_b200.so")
 SOURCES = ["etcu_api.cu", "etcu_learned.cu", "etcu_io.cpp", "etcu_tiff.cpp", "etcu_stack.cpp"]
-HEADERS = ["geometry.hpp", "kernels.cuh", "io_util.hpp", "blobs.cuh", "learned.cuh"]
+HEADERS = ["geometry.hpp", "kernels.cuh", "io_util.hpp", "blobs.cuh", "learned.cuh", "tune.hpp"]
 
 # -fmad=false: no multiply-add is formed implicitly.  The kernels follow the
 # reference's operation order step by step and write every intended fused

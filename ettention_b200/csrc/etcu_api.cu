@@ -7,6 +7,7 @@
 //   LR/algorithm/projections/back/BackProjectionKernel.cpp         -> etcu_back_project
 //   LR/algorithm/reconstruction/blockiterative/*.cpp               -> etcu_recon_*
 #include <cuda_runtime.h>
+#include <sys/stat.h>
 
 #include <algorithm>
 #include <atomic>
@@ -14,6 +15,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <fstream>
+#include <functional>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -23,6 +27,9 @@
 #include "geometry.hpp"
 #include "kernels.cuh"
 #include "blobs.cuh"
+#include "tune.hpp"
+
+etcu_status check_fused_waits(etcu_recon* r);
 
 using namespace etcu;
 
@@ -44,6 +51,8 @@ struct etcu_context {
     bool fused_step = true; // fused SART step BP(p) + FP(p + 1) (ETCU_FUSED=0 disables)
     bool fused_persist = true; // all fused steps of an iteration in one launch (ETCU_PERSIST=0 disables)
     int fuse_withhold_row = -1; // tests of the bounded waits (ETCU_TEST_WITHHOLD_ROW)
+    int autotune = 0;           // 1: launch shapes from the tuner's cache, timed on a miss (ETCU_AUTOTUNE)
+    std::string tune_log;       // the choices made on this context, one line each
 };
 
 struct etcu_volume {
@@ -96,6 +105,7 @@ struct etcu_recon {
     // every fused step of an iteration in one launch (sart_fused_persistent_kernel)
     bool fuse_persist = false;
     int fuse_window = 0, fuse_grid = 0;
+    int fuse_per_sm = 0, fuse_sms = 0;  // resident blocks per SM of the persistent launch, SMs
     int2* d_tapwin = nullptr;     // per view id
     uint32_t* d_fuse_ctl = nullptr;  // unit counter + steps finished per row, then the error word
 };
@@ -362,6 +372,7 @@ void launch_bp_sart_m(const BpArgs& a, etcu_voxel_type t, etcu_sampling sm, cuda
 
 struct BpColPlan {
     int groups = 0;  // 4-voxel x groups per thread (1 or 2)
+    int shadow = 0;  // the master's 16-bit shadow written beside it (1: FP16, 2: BF16)
     int x0lo = 0, ntaps = 0;
     int zper = 0, zchunks = 0, grid = 0;
     size_t smem = 0;
@@ -376,16 +387,21 @@ void bp_col_limits(int dev, size_t smem, int& per_sm) {
         if ((int)opted.size() <= dev) opted.resize(dev + 1, 0);
         if (!opted[dev]) {
             cudaDeviceProp prop;
-            if (cudaGetDeviceProperties(&prop, dev) == cudaSuccess)
-                cudaFuncSetAttribute(bp_sart_column_kernel<kGroups>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            if (cudaGetDeviceProperties(&prop, dev) == cudaSuccess) {
+                cudaFuncSetAttribute(bp_sart_column_kernel<kGroups, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)prop.sharedMemPerBlockOptin);
+                cudaFuncSetAttribute(bp_sart_column_kernel<kGroups, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)prop.sharedMemPerBlockOptin);
+                cudaFuncSetAttribute(bp_sart_column_kernel<kGroups, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)prop.sharedMemPerBlockOptin);
+            }
             cudaGetLastError();
             opted[dev] = 1;
         }
     }
     per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_sart_column_kernel<kGroups>, kBpColThreads, smem) !=
-        cudaSuccess) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_sart_column_kernel<kGroups, 0>, kBpColThreads,
+                                                      smem) != cudaSuccess) {
         cudaGetLastError();
         per_sm = 0;
     }
@@ -405,14 +421,16 @@ int device_sms(int dev) {
 }
 
 // Whether the column-pipelined back projector applies to this view and
-// sub-volume, and its tap window, item and grid sizes.  It needs an FP32 volume
+// sub-volume, and its tap window, item and grid sizes.  It needs an FP32 volume (or FP32 master)
 // without mask and x rows of a multiple of 4 and at most 2048 voxels.  The tap window spans the
 // columns floor(u - 0.5) of every voxel centre with two columns of margin on each
 // side (the kernel's float coordinate is within a few ulps of the double
 // evaluated here at the sub-volume's corners; u is affine in the voxel indices).
+// FP32 volumes and FP32 masters with a 16-bit shadow (written beside the master).
 bool plan_bp_col(const etcu_volume* vol, const SlabConst& g, const ViewConst& vc, const float4& smp, BpColPlan& p) {
     etcu_context* ctx = vol->ctx;
-    if (!ctx->bp_column || vol->type != ETCU_VOXEL_FLOAT32 || vol->mask) return false;
+    if (!ctx->bp_column || vol->type == ETCU_VOXEL_HALF16 || vol->mask) return false;
+    p.shadow = vol->type == ETCU_VOXEL_F16_MASTER ? 1 : (vol->type == ETCU_VOXEL_BF16_MASTER ? 2 : 0);
     if (g.rx <= 0 || g.ry <= 0 || g.rz <= 0 || g.rx % 4 != 0 || g.rx > 8 * kBpColThreads) return false;
     double umin = 1e300, umax = -1e300;
     for (int c = 0; c < 8; ++c) {
@@ -477,9 +495,18 @@ void launch_bp_col(const BpArgs& a0, const BpColPlan& p, cudaStream_t st) {
     a.ntaps = p.ntaps;
     a.zper = p.zper;
     a.zchunks = p.zchunks;
+    a.shadow = a0.shadow;
     const dim3 grid(p.grid), block(kBpColThreads);
-    if (p.groups == 1) bp_sart_column_kernel<1><<<grid, block, p.smem, st>>>(a);
-    else bp_sart_column_kernel<2><<<grid, block, p.smem, st>>>(a);
+    const int sh = p.shadow;
+    if (p.groups == 1) {
+        if (sh == 1) bp_sart_column_kernel<1, 1><<<grid, block, p.smem, st>>>(a);
+        else if (sh == 2) bp_sart_column_kernel<1, 2><<<grid, block, p.smem, st>>>(a);
+        else bp_sart_column_kernel<1, 0><<<grid, block, p.smem, st>>>(a);
+    } else {
+        if (sh == 1) bp_sart_column_kernel<2, 1><<<grid, block, p.smem, st>>>(a);
+        else if (sh == 2) bp_sart_column_kernel<2, 2><<<grid, block, p.smem, st>>>(a);
+        else bp_sart_column_kernel<2, 0><<<grid, block, p.smem, st>>>(a);
+    }
 }
 
 // Back projection of a.nviews views; when their staged constants exceed the
@@ -640,6 +667,7 @@ extern "C" etcu_status etcu_context_create(int device, etcu_context** out) {
     if (const char* env = getenv("ETCU_FUSED")) c->fused_step = atoi(env) != 0;
     if (const char* env = getenv("ETCU_PERSIST")) c->fused_persist = atoi(env) != 0;
     if (const char* env = getenv("ETCU_TEST_WITHHOLD_ROW")) c->fuse_withhold_row = atoi(env);
+    if (const char* env = getenv("ETCU_AUTOTUNE")) c->autotune = atoi(env) != 0;
     *out = c.release();
     return ETCU_OK;
 }
@@ -659,6 +687,10 @@ void etcu_set_context_free_error(const char* message) { g_create_error = message
 
 // Accessors for the library's other translation units (not exported).
 int etcu_context_device_index(const etcu_context* ctx) { return ctx ? ctx->device : 0; }
+int etcu_context_autotune(const etcu_context* ctx) { return ctx ? ctx->autotune : 0; }
+void etcu_context_tune_note(etcu_context* ctx, const std::string& line) {
+    if (ctx) ctx->tune_log += line + "\n";
+}
 void etcu_context_set_error(etcu_context* ctx, const char* message) {
     if (ctx) ctx->err = message ? message : "";
     else g_create_error = message ? message : "";
@@ -684,6 +716,121 @@ extern "C" etcu_status etcu_set_stream(etcu_context* ctx, void* stream) {
 extern "C" size_t etcu_device_bytes(const etcu_context* ctx) { return ctx ? ctx->bytes : 0; }
 
 extern "C" void* etcu_context_stream(const etcu_context* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+// =============================================================== launch-shape autotuner
+namespace etcu_tune {
+namespace {
+std::mutex g_mu;
+std::map<std::string, int> g_table;
+bool g_loaded = false;
+
+std::string cache_path() {
+    if (const char* p = getenv("ETCU_TUNE_CACHE")) return p;
+    const char* home = getenv("HOME");
+    return std::string(home ? home : "/tmp") + "/.cache/ettention_b200/launch_shapes.txt";
+}
+
+void load_locked() {
+    if (g_loaded) return;
+    g_loaded = true;
+    std::ifstream f(cache_path());
+    std::string key;
+    int value;
+    while (f >> key >> value) g_table[key] = value;
+}
+}  // namespace
+
+int lookup(const std::string& key) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    load_locked();
+    auto it = g_table.find(key);
+    return it == g_table.end() ? -1 : it->second;
+}
+
+void store(const std::string& key, int value) {
+    std::lock_guard<std::mutex> lock(g_mu);
+    load_locked();
+    g_table[key] = value;
+    const std::string path = cache_path();
+    const size_t slash = path.find_last_of('/');
+    if (slash != std::string::npos) {  // create the directory chain
+        for (size_t i = 1; i <= slash; ++i)
+            if (path[i] == '/' || i == slash) {
+                const std::string d = path.substr(0, i == slash ? slash : i);
+                if (!d.empty()) mkdir(d.c_str(), 0755);
+            }
+    }
+    std::ofstream f(path, std::ios::app);
+    if (f) f << key << ' ' << value << '\n';
+}
+
+std::string device_tag(int device) {
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+        cudaGetLastError();
+        return "unknown";
+    }
+    std::string name(prop.name);
+    for (char& c : name)
+        if (c == ' ' || c == '|') c = '_';
+    return name + "|sm" + std::to_string(prop.major) + std::to_string(prop.minor) + "|" +
+           std::to_string(prop.multiProcessorCount);
+}
+
+int search(cudaStream_t st, const std::vector<int>& candidates, const std::function<bool(int)>& run, int reps,
+           std::string* log) {
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    int best = -1;
+    float best_ms = 0.f;
+    for (int c : candidates) {
+        if (!run(c) || cudaStreamSynchronize(st) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        float ms = 1e30f;
+        bool ok = true;
+        for (int i = 0; i < reps && ok; ++i) {
+            cudaEventRecord(e0, st);
+            ok = run(c);
+            cudaEventRecord(e1, st);
+            if (cudaEventSynchronize(e1) != cudaSuccess) ok = false;
+            float t = 0.f;
+            if (ok && cudaEventElapsedTime(&t, e0, e1) == cudaSuccess) ms = std::min(ms, t);
+        }
+        cudaGetLastError();
+        if (!ok) continue;
+        if (log) *log += " " + std::to_string(c) + "=" + std::to_string(ms) + "ms";
+        if (best < 0 || ms < best_ms) {
+            best = c;
+            best_ms = ms;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return best;
+}
+}  // namespace etcu_tune
+
+extern "C" etcu_status etcu_context_set_autotune(etcu_context* ctx, int mode) {
+    if (!ctx) return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    ctx->autotune = mode != 0;
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_context_tune_report(const etcu_context* ctx, char* out, size_t capacity, size_t* needed) {
+    if (!ctx) return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    if (needed) *needed = ctx->tune_log.size() + 1;
+    if (out && capacity) {
+        const size_t n = std::min(capacity - 1, ctx->tune_log.size());
+        memcpy(out, ctx->tune_log.data(), n);
+        out[n] = 0;
+    }
+    return ETCU_OK;
+}
 
 // =============================================================== geometry
 extern "C" etcu_status etcu_view_rotate(const etcu_view* base, float tilt, float xtilt, etcu_view* out) {
@@ -1159,7 +1306,12 @@ void launch_fused_step(etcu_recon* r, uint32_t p, cudaStream_t st) {
     a.real = r->d_proj;
     a.resid_sq = r->d_resid;
     a.loc = r->params.use_long_object_compensation ? 1 : 0;
-    sart_fused_kernel<<<g.ry, kFuseThreads, fuse_smem_bytes(g.rx, g.rz, a.ntaps), st>>>(a);
+    const size_t smem = fuse_smem_bytes(g.rx, g.rz, a.ntaps);
+    switch (vol->type) {
+    case ETCU_VOXEL_F16_MASTER: sart_fused_kernel<1><<<g.ry, kFuseThreads, smem, st>>>(a); break;
+    case ETCU_VOXEL_BF16_MASTER: sart_fused_kernel<2><<<g.ry, kFuseThreads, smem, st>>>(a); break;
+    default: sart_fused_kernel<0><<<g.ry, kFuseThreads, smem, st>>>(a); break;
+    }
 }
 
 // All M - 1 fused steps in one launch; the row counters are cleared first.
@@ -1191,7 +1343,15 @@ void launch_fused_persistent(etcu_recon* r, cudaStream_t st) {
     q.error = r->d_fuse_ctl + g.ry + 1;
     q.window = r->fuse_window;
     q.withhold_row = r->ctx->fuse_withhold_row;
-    sart_fused_persistent_kernel<<<r->fuse_grid, kFuseThreads, r->fuse_smem, st>>>(a, q);
+    switch (vol->type) {
+    case ETCU_VOXEL_F16_MASTER:
+        sart_fused_persistent_kernel<1><<<r->fuse_grid, kFuseThreads, r->fuse_smem, st>>>(a, q);
+        break;
+    case ETCU_VOXEL_BF16_MASTER:
+        sart_fused_persistent_kernel<2><<<r->fuse_grid, kFuseThreads, r->fuse_smem, st>>>(a, q);
+        break;
+    default: sart_fused_persistent_kernel<0><<<r->fuse_grid, kFuseThreads, r->fuse_smem, st>>>(a, q); break;
+    }
 }
 
 uint32_t issue_fused_iteration(etcu_recon* r, cudaStream_t st) {
@@ -1223,10 +1383,16 @@ void fuse_limits(int dev, size_t smem, int& per_sm, int& persist_per_sm, int& sm
         if ((int)opted.size() <= dev) opted.resize(dev + 1, 0);
         if (!opted[dev]) {
             if (have_prop) {
-                cudaFuncSetAttribute(sart_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)prop.sharedMemPerBlockOptin);
-                cudaFuncSetAttribute(sart_fused_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)prop.sharedMemPerBlockOptin - 16);
+                const int full = (int)prop.sharedMemPerBlockOptin, persist = full - 16;
+                cudaFuncSetAttribute(sart_fused_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, full);
+                cudaFuncSetAttribute(sart_fused_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, full);
+                cudaFuncSetAttribute(sart_fused_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, full);
+                cudaFuncSetAttribute(sart_fused_persistent_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     persist);
+                cudaFuncSetAttribute(sart_fused_persistent_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     persist);
+                cudaFuncSetAttribute(sart_fused_persistent_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     persist);
             }
             cudaGetLastError();
             opted[dev] = 1;
@@ -1234,11 +1400,12 @@ void fuse_limits(int dev, size_t smem, int& per_sm, int& persist_per_sm, int& sm
     }
     sms = have_prop ? prop.multiProcessorCount : 0;
     per_sm = persist_per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sart_fused_kernel, kFuseThreads, smem) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sart_fused_kernel<0>, kFuseThreads, smem) !=
+        cudaSuccess) {
         cudaGetLastError();
         per_sm = 0;
     }
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&persist_per_sm, sart_fused_persistent_kernel, kFuseThreads,
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&persist_per_sm, sart_fused_persistent_kernel<0>, kFuseThreads,
                                                       smem) != cudaSuccess) {
         cudaGetLastError();
         persist_per_sm = 0;
@@ -1327,7 +1494,8 @@ etcu_status fuse_row_table(etcu_context* ctx, const ViewConst* d_views, const Sl
 }
 
 // Whether every SART step of this reconstruction can run fused (sart_fused_kernel):
-// SART on one FP32 sub-volume without mask, one sample each way, 1/256 sampling,
+// SART on one sub-volume (FP32, or an FP32 master with a 16-bit shadow) without mask,
+// one sample each way, 1/256 sampling,
 // parallel views tilted about y (ray.y == 0, hpitch.y == 0, detector row constant
 // in y), x rows of an even number of at most 2 * kFuseThreads voxels, walks that
 // cannot reach the step cap, at most kFuseRays * kFuseThreads rays per volume row,
@@ -1339,7 +1507,9 @@ etcu_status plan_fused(etcu_recon* r, const std::vector<ViewConst>& vc, bool& ok
     etcu_context* ctx = r->ctx;
     const uint32_t N = r->n_input;
     if (!ctx->fused_step || r->persp || vol->slabs.size() != 1 || r->block != 1 || r->order.size() < 2) return ETCU_OK;
-    if (vol->type != ETCU_VOXEL_FLOAT32 || vol->mask || r->params.sampling != ETCU_SAMPLING_Q8) return ETCU_OK;
+    // FP32 volumes, and FP32 masters with a 16-bit shadow (the fused walk reads the chunk
+    // rounded as the shadow holds it; the shadow is written by the last back projection)
+    if (vol->type == ETCU_VOXEL_HALF16 || vol->mask || r->params.sampling != ETCU_SAMPLING_Q8) return ETCU_OK;
     if (r->params.fp_samples > 1 || r->params.bp_samples != 1 || r->hsamples.size() < N) return ETCU_OK;
     const SlabConst& g = vol->slabs[0];
     if (g.rx % 2 != 0 || g.rx > 2 * kFuseThreads || g.rx + g.rz - 1 > kMaxDdaIterations) return ETCU_OK;
@@ -1381,12 +1551,58 @@ etcu_status plan_fused(etcu_recon* r, const std::vector<ViewConst>& vc, bool& ok
             r->fuse_window = window;
             r->fuse_grid = (int)std::min<long long>((long long)persist_per_sm * sms,
                                                     (long long)(r->order.size() - 1) * g.ry);
+            r->fuse_per_sm = persist_per_sm;
+            r->fuse_sms = sms;
             r->fuse_persist = true;
         }
     }
     r->fuse_x0lo = std::move(x0lo);
     r->fuse_ntaps = std::move(ntaps);
     return ETCU_OK;
+}
+
+etcu_status issue_iteration(etcu_recon* r, cudaStream_t st, uint32_t* launches);
+
+// Autotuner: resident blocks per SM of the persistent fused launch (1 .. the occupancy
+// limit), timed on whole iterations of this reconstruction; the volume (master and
+// shadow) is saved before and restored after the timing runs.
+etcu_status tune_fused_grid(etcu_recon* r) {
+    etcu_context* ctx = r->ctx;
+    etcu_volume* vol = r->vol;
+    const SlabConst& g = vol->slabs[0];
+    const long long units = (long long)(r->order.size() - 1) * g.ry;
+    char key[512];
+    snprintf(key, sizeof(key), "sart_fused_persistent|%dx%dx%d|views%zu|det%ux%u|type%d|%s", g.rx, g.ry, g.rz,
+             r->order.size(), r->W, r->H, (int)vol->type, etcu_tune::device_tag(ctx->device).c_str());
+    int choice = etcu_tune::lookup(key);
+    std::string log;
+    if (choice < 1 || choice > r->fuse_per_sm) {
+        const size_t n = voxel_count(vol->desc);
+        const size_t lowb = vol->low ? n * 2 : 0;
+        void* save = nullptr;
+        etcu_status s = dalloc(ctx, &save, n * 4 + lowb);
+        if (s != ETCU_OK) return s;
+        CK(ctx, cudaMemcpyAsync(save, vol->master, n * 4, cudaMemcpyDeviceToDevice, ctx->stream));
+        if (lowb) CK(ctx, cudaMemcpyAsync((char*)save + n * 4, vol->low, lowb, cudaMemcpyDeviceToDevice, ctx->stream));
+        std::vector<int> cands;
+        for (int b = 1; b <= r->fuse_per_sm; ++b) cands.push_back(b);
+        choice = etcu_tune::search(ctx->stream, cands, [&](int b) {
+            r->fuse_grid = (int)std::min<long long>((long long)b * r->fuse_sms, units);
+            return issue_iteration(r, ctx->stream, nullptr) == ETCU_OK;
+        }, 2, &log);
+        CK(ctx, cudaMemcpyAsync(vol->master, save, n * 4, cudaMemcpyDeviceToDevice, ctx->stream));
+        if (lowb) CK(ctx, cudaMemcpyAsync(vol->low, (char*)save + n * 4, lowb, cudaMemcpyDeviceToDevice, ctx->stream));
+        CK(ctx, cudaStreamSynchronize(ctx->stream));
+        dfree(ctx, save, n * 4 + lowb);
+        if (choice < 1) choice = r->fuse_per_sm;
+        etcu_tune::store(key, choice);
+    } else {
+        log = " cached";
+    }
+    r->fuse_grid = (int)std::min<long long>((long long)choice * r->fuse_sms, units);
+    ctx->tune_log += std::string(key) + " " + std::to_string(choice) + log + "\n";
+    CK(ctx, cudaMemsetAsync(r->d_resid, 0, sizeof(double), ctx->stream));
+    return check_fused_waits(r);
 }
 
 // One iteration (BlockIterativeReconstructionOperator.cpp:92-103).
@@ -1533,6 +1749,7 @@ etcu_status recon_build(etcu_volume* vol, const etcu_view* views, uint32_t n_vie
                             ctx->stream));
     if ((s = dalloc(ctx, (void**)&r->d_resid, sizeof(double))) != ETCU_OK) return s;
     CK(ctx, cudaMemsetAsync(r->d_resid, 0, sizeof(double), ctx->stream));
+    if (r->fuse_persist && ctx->autotune && (s = tune_fused_grid(r.get())) != ETCU_OK) return s;
     CK(ctx, cudaStreamSynchronize(ctx->stream));
     if (params->use_graph) {
         // The launch sequence of one iteration never changes: capture it once.
@@ -2499,6 +2716,9 @@ struct etcu_batch {
     uint32_t* d_ctl = nullptr;  // [0] unit counter, then every series' row counters, then the error word
     int grid = 0, threads = 0;
     size_t smem = 0;
+    int shadow = 0;  // 1 / 2: every series is an FP32 master with an FP16 / BF16 shadow
+    int per_sm128 = 0, per_sm512 = 0, sms = 0;  // occupancy of the persistent variants (autotuner)
+    std::string shape_key;                       // the series' shapes, for the autotuner's cache
 };
 
 namespace {
@@ -2546,12 +2766,21 @@ etcu_status issue_batch_iteration(etcu_batch* b, cudaStream_t st) {
         CK(ctx, cudaMemsetAsync(b->d_ctl, 0, (size_t)(b->ctl_words - 1) * sizeof(uint32_t), st));
         uint32_t* err = b->d_ctl + b->ctl_words - 1;
         const int withhold = ctx->fuse_withhold_row;
-        if (b->threads == 128)
-            sart_fused_batch_kernel<128><<<b->grid, 128, b->smem, st>>>(b->d_series, b->d_segs, b->nsegs,
-                                                                        b->total_units, b->d_ctl, err, withhold);
-        else
-            sart_fused_batch_kernel<kFuseThreads><<<b->grid, kFuseThreads, b->smem, st>>>(
-                b->d_series, b->d_segs, b->nsegs, b->total_units, b->d_ctl, err, withhold);
+        const bool narrow = b->threads == 128;
+#define ETCU_BATCH_LAUNCH(T, SH)                                                                                   \
+    sart_fused_batch_kernel<T, SH><<<b->grid, T, b->smem, st>>>(b->d_series, b->d_segs, b->nsegs, b->total_units, \
+                                                                 b->d_ctl, err, withhold)
+        if (b->shadow == 1) {
+            if (narrow) ETCU_BATCH_LAUNCH(128, 1);
+            else ETCU_BATCH_LAUNCH(kFuseThreads, 1);
+        } else if (b->shadow == 2) {
+            if (narrow) ETCU_BATCH_LAUNCH(128, 2);
+            else ETCU_BATCH_LAUNCH(kFuseThreads, 2);
+        } else {
+            if (narrow) ETCU_BATCH_LAUNCH(128, 0);
+            else ETCU_BATCH_LAUNCH(kFuseThreads, 0);
+        }
+#undef ETCU_BATCH_LAUNCH
         CKL(ctx);
         return ETCU_OK;
     }
@@ -2621,22 +2850,36 @@ etcu_status plan_batch_persistent(etcu_batch* b, const std::vector<BatchSeriesRe
         return ETCU_OK;
     }
     const int threads = narrow ? 128 : kFuseThreads;
-    const void* kern = narrow ? (const void*)sart_fused_batch_kernel<128>
-                              : (const void*)sart_fused_batch_kernel<kFuseThreads>;
-    cudaFuncAttributes fa;
-    if (cudaFuncGetAttributes(&fa, kern) != cudaSuccess) {
+    const void* variants[3] = {
+        narrow ? (const void*)sart_fused_batch_kernel<128, 0> : (const void*)sart_fused_batch_kernel<kFuseThreads, 0>,
+        narrow ? (const void*)sart_fused_batch_kernel<128, 1> : (const void*)sart_fused_batch_kernel<kFuseThreads, 1>,
+        narrow ? (const void*)sart_fused_batch_kernel<128, 2> : (const void*)sart_fused_batch_kernel<kFuseThreads, 2>};
+    const void* kern = variants[b->shadow];
+    // resident blocks per SM of the 512-thread variant and (narrow batches) the 128-thread one
+    auto occupancy = [&](const void* k, int t) {
+        cudaFuncAttributes fa;
+        if (cudaFuncGetAttributes(&fa, k) != cudaSuccess) {
+            cudaGetLastError();
+            return 0;
+        }
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(prop.sharedMemPerBlockOptin - fa.sharedSizeBytes));
         cudaGetLastError();
-        return ETCU_OK;
-    }
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)(prop.sharedMemPerBlockOptin - fa.sharedSizeBytes));
-    cudaGetLastError();
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess) {
-        cudaGetLastError();
-        return ETCU_OK;
-    }
+        int per = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, t, smem) != cudaSuccess) {
+            cudaGetLastError();
+            return 0;
+        }
+        return per;
+    };
+    const void* wide_variants[3] = {(const void*)sart_fused_batch_kernel<kFuseThreads, 0>,
+                                    (const void*)sart_fused_batch_kernel<kFuseThreads, 1>,
+                                    (const void*)sart_fused_batch_kernel<kFuseThreads, 2>};
+    const int per_sm = occupancy(kern, threads);
     if (per_sm < 1) return ETCU_OK;
+    b->per_sm512 = narrow ? occupancy(wide_variants[b->shadow], kFuseThreads) : per_sm;
+    b->per_sm128 = narrow ? per_sm : 0;
+    b->sms = prop.multiProcessorCount;
     // segments: unit steps 0 .. M of every series, step-major
     uint32_t max_m = 0;
     for (const auto& rc : recs) max_m = std::max(max_m, rc.M);
@@ -2726,6 +2969,66 @@ etcu_status check_batch_waits(etcu_batch* b) {
     return ETCU_OK;
 }
 
+etcu_status issue_batch_iteration(etcu_batch* b, cudaStream_t st);
+
+// Autotuner: threads per block (128 for batches whose rows fit, 512) and resident blocks
+// per SM of the persistent batched iteration, timed on whole iterations; every series'
+// volume (master and shadow) is saved before and restored after the timing runs.
+etcu_status tune_batch(etcu_batch* b) {
+    etcu_context* ctx = b->ctx;
+    uint64_t h = 1469598103934665603ull;  // FNV-1a of the series' shapes
+    for (etcu_volume* v : b->vols)
+        for (int i = 0; i < 3; ++i) h = (h ^ v->desc.resolution[i]) * 1099511628211ull;
+    for (int m : b->steps) h = (h ^ (uint64_t)m) * 1099511628211ull;
+    char key[512];
+    snprintf(key, sizeof(key), "sart_fused_batch|n%u|%016llx%s|type%d|%s", b->n, (unsigned long long)h,
+             b->shape_key.c_str(), b->shadow, etcu_tune::device_tag(ctx->device).c_str());
+    auto apply = [&](int c) {
+        b->threads = c / 100;
+        b->grid = (int)std::min<long long>((long long)(c % 100) * b->sms, (long long)b->total_units);
+    };
+    std::vector<int> cands;
+    for (int bps = 1; bps <= std::min(b->per_sm512, 99); ++bps) cands.push_back(kFuseThreads * 100 + bps);
+    for (int bps = 1; bps <= std::min(b->per_sm128, 99); ++bps) cands.push_back(128 * 100 + bps);
+    int choice = etcu_tune::lookup(key);
+    std::string log;
+    if (std::find(cands.begin(), cands.end(), choice) == cands.end()) {
+        std::vector<std::pair<void*, size_t>> saved;
+        etcu_status s = ETCU_OK;
+        for (etcu_volume* v : b->vols) {
+            const size_t n = voxel_count(v->desc), bytes = n * 4 + (v->low ? n * 2 : 0);
+            void* p = nullptr;
+            if ((s = dalloc(ctx, &p, bytes)) != ETCU_OK) break;
+            saved.emplace_back(p, bytes);
+            CK(ctx, cudaMemcpyAsync(p, v->master, n * 4, cudaMemcpyDeviceToDevice, ctx->stream));
+            if (v->low) CK(ctx, cudaMemcpyAsync((char*)p + n * 4, v->low, n * 2, cudaMemcpyDeviceToDevice, ctx->stream));
+        }
+        const int def_threads = b->threads, def_grid = b->grid;
+        if (s == ETCU_OK)
+            choice = etcu_tune::search(ctx->stream, cands, [&](int c) {
+                apply(c);
+                return issue_batch_iteration(b, ctx->stream) == ETCU_OK;
+            }, 2, &log);
+        for (size_t i = 0; i < saved.size(); ++i) {
+            etcu_volume* v = b->vols[i];
+            const size_t n = voxel_count(v->desc);
+            cudaMemcpyAsync(v->master, saved[i].first, n * 4, cudaMemcpyDeviceToDevice, ctx->stream);
+            if (v->low) cudaMemcpyAsync(v->low, (char*)saved[i].first + n * 4, n * 2, cudaMemcpyDeviceToDevice, ctx->stream);
+        }
+        CK(ctx, cudaStreamSynchronize(ctx->stream));
+        for (auto& p : saved) dfree(ctx, p.first, p.second);
+        if (s != ETCU_OK) return s;
+        if (choice < 0) choice = def_threads * 100 + std::max(1, def_grid / std::max(1, b->sms));
+        etcu_tune::store(key, choice);
+    } else {
+        log = " cached";
+    }
+    apply(choice);
+    ctx->tune_log += std::string(key) + " " + std::to_string(choice) + log + "\n";
+    CK(ctx, cudaMemsetAsync(b->d_resid, 0, sizeof(double) * b->n, ctx->stream));
+    return check_batch_waits(b);
+}
+
 etcu_status batch_build(etcu_context* ctx, const etcu_batch_series* series, uint32_t n,
                         const etcu_recon_params* params, etcu_batch* b) {
     if (params->block_size != 1)
@@ -2749,9 +3052,13 @@ etcu_status batch_build(etcu_context* ctx, const etcu_batch_series* series, uint
         if (!vol || !sr.views || !sr.host_projections || sr.n_views == 0)
             return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "series %u: NULL volume, views or projections", i);
         if (vol->ctx != ctx) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "series %u: volume of another context", i);
-        if (vol->type != ETCU_VOXEL_FLOAT32 || vol->mask || vol->slabs.size() != 1)
-            return fail(ctx, ETCU_ERR_UNSUPPORTED, "series %u: batched series need an FP32 volume, one sub-volume, no mask",
-                        i);
+        if (vol->type == ETCU_VOXEL_HALF16 || vol->mask || vol->slabs.size() != 1)
+            return fail(ctx, ETCU_ERR_UNSUPPORTED,
+                        "series %u: batched series need an FP32 volume (or FP32 master), one sub-volume, no mask", i);
+        const int shadow = vol->type == ETCU_VOXEL_F16_MASTER ? 1 : (vol->type == ETCU_VOXEL_BF16_MASTER ? 2 : 0);
+        if (i > 0 && shadow != b->shadow)
+            return fail(ctx, ETCU_ERR_UNSUPPORTED, "series %u: every series of a batch has the same voxel type", i);
+        b->shadow = shadow;
         const SlabConst& slab = vol->slabs[0];
         const uint32_t W = sr.views[0].width, H = sr.views[0].height;
         for (uint32_t v = 0; v < sr.n_views; ++v) {
@@ -2861,6 +3168,11 @@ etcu_status batch_build(etcu_context* ctx, const etcu_batch_series* series, uint
     CK(ctx, cudaMemsetAsync(b->d_resid, 0, sizeof(double) * n, ctx->stream));
     CK(ctx, cudaStreamSynchronize(ctx->stream));
     if ((s = plan_batch_persistent(b, recs, params)) != ETCU_OK) return s;
+    if (b->shadow && !b->persist)
+        return fail(ctx, ETCU_ERR_UNSUPPORTED,
+                    "batched series with a 16-bit shadow run the persistent fused iteration only (SART, one sample, "
+                    "1/256 sampling, rows of an even number of voxels)");
+    if (b->persist && ctx->autotune && (s = tune_batch(b)) != ETCU_OK) return s;
     b->launches = b->persist ? 1u : 2u * (uint32_t)b->max_steps;
     if (params->use_graph) {
         cudaStream_t cs = ctx->stream;
@@ -2918,7 +3230,12 @@ extern "C" etcu_status etcu_batch_run(etcu_batch* b, uint32_t iterations) {
         }
     }
     CKL(ctx);
-    return check_batch_waits(b);
+    etcu_status s = check_batch_waits(b);
+    // the fused iteration updates the FP32 masters only: bring the shadows up to date
+    if (s == ETCU_OK && b->shadow && iterations > 0)
+        for (etcu_volume* v : b->vols)
+            if ((s = refresh_low_from_master(v)) != ETCU_OK) return s;
+    return s;
 }
 
 extern "C" etcu_status etcu_batch_last_residual_sq(etcu_batch* b, double* out) {

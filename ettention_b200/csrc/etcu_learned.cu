@@ -26,9 +26,12 @@
 
 #include "ettention_b200.h"
 #include "learned.cuh"
+#include "tune.hpp"
 
 int etcu_context_device_index(const etcu_context* ctx);
 void etcu_context_set_error(etcu_context* ctx, const char* message);
+int etcu_context_autotune(const etcu_context* ctx);
+void etcu_context_tune_note(etcu_context* ctx, const std::string& line);
 
 namespace {
 
@@ -191,12 +194,9 @@ etcu_status launch_conv_n(etcu_warmstart* w, const CUtensorMap& m0, const CUtens
     a.resident = wbytes <= kResidentMax ? 1 : 0;
     const size_t wres = a.resident ? (wbytes + 1023) & ~(size_t)1023 : 0;
     const size_t stage = (SH::kHalo + (a.resident ? 0 : SH::kW) + 1023) & ~(size_t)1023;
-    int S = (int)std::min<size_t>(4, (kConvSmemMax - wres) / stage);
-    if (S < 1) return wfail(w, ETCU_ERR_UNSUPPORTED, "convolution stage of %zu bytes does not fit", stage);
-    a.stages = S;
+    const int smax = (int)std::min<size_t>(4, (kConvSmemMax - wres) / stage);
+    if (smax < 1) return wfail(w, ETCU_ERR_UNSUPPORTED, "convolution stage of %zu bytes does not fit", stage);
     a.batch = batch;
-    // at least 120 KB, so that one CTA (and its tensor memory) owns each SM
-    const size_t smem = std::max<size_t>(wres + (size_t)S * stage + (2 * S + 5) * 8 + 16 + 1024, 120 * 1024);
     static std::atomic<unsigned long long> opted{0};
     if (w->device < 64 && !(opted.load() & (1ull << w->device))) {
         WCK(w, cudaFuncSetAttribute(ws::conv_tc_kernel<N, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -207,8 +207,36 @@ etcu_status launch_conv_n(etcu_warmstart* w, const CUtensorMap& m0, const CUtens
     const int nty = (a.Y + TY - 1) / TY;
     const long ntiles = (long)ntx * nty * a.Z * batch;
     const unsigned grid = (unsigned)std::min<long>(ntiles, w->sms);
-    ws::conv_tc_kernel<N, TY><<<grid, 192, smem, w->stream>>>(m0, m1, a);
-    WCK(w, cudaGetLastError());
+    cudaError_t last = cudaSuccess;
+    auto launch = [&](int S) {
+        a.stages = S;
+        // at least 120 KB, so that one CTA (and its tensor memory) owns each SM
+        const size_t smem = std::max<size_t>(wres + (size_t)S * stage + (2 * S + 5) * 8 + 16 + 1024, 120 * 1024);
+        ws::conv_tc_kernel<N, TY><<<grid, 192, smem, w->stream>>>(m0, m1, a);
+        last = cudaGetLastError();
+        return last == cudaSuccess;
+    };
+    int S = smax;
+    if (etcu_context_autotune(w->ctx) && smax > 1) {
+        // autotuner: ring stages of this convolution (the launch is idempotent)
+        char key[256];
+        snprintf(key, sizeof(key), "warmstart_conv|n%d|rows%d|%dx%dx%d|b%d|steps%d|res%d|%s", N, TY, a.X, a.Y, a.Z,
+                 batch, a.nsteps, a.resident, etcu_tune::device_tag(w->device).c_str());
+        int c = etcu_tune::lookup(key);
+        std::string log = " cached";
+        if (c < 1 || c > smax) {
+            std::vector<int> cands;
+            for (int k = 1; k <= smax; ++k) cands.push_back(k);
+            log.clear();
+            c = etcu_tune::search(w->stream, cands, launch, 3, &log);
+            if (c < 1) c = smax;
+            etcu_tune::store(key, c);
+            etcu_context_tune_note(w->ctx, std::string(key) + " " + std::to_string(c) + log);
+        }
+        S = c;
+    }
+    if (!launch(S))
+        return wfail(w, ETCU_ERR_CUDA, "convolution launch failed: %s", cudaGetErrorString(last));
     return ETCU_OK;
 }
 

@@ -988,7 +988,8 @@ __global__ void __launch_bounds__(256, 8)
 // the column coordinate is integer work on the bits of fl_down(t + 1.5 * 2^23),
 // which is 1.5 * 2^23 + floor(t) for |t| < 2^22.
 struct BpColArgs {
-    float* vol;                 // sub-volume base, x-fastest [z][y][x]
+    float* vol;                 // sub-volume base, x-fastest [z][y][x] (FP32, or the FP32 master)
+    void* shadow;               // the 16-bit shadow of the master (kShadow 1: FP16, 2: BF16), same indexing
     SlabConst slab;
     const ViewConst* views;     // view table by view id (nullptr: inline_view)
     const uint32_t* order;
@@ -1044,7 +1045,7 @@ __device__ __forceinline__ void q8_tap_bits(float f, int x0lo, int& e, float& a1
 
 // kFull: every thread owns all kCols columns (rx == kCols * kBpColThreads).
 // kGroups: 4-voxel x groups per thread (rx <= 4 * kGroups * kBpColThreads, rx % 4 == 0).
-template <int kGroups>
+template <int kGroups, int kShadow = 0>
 __global__ void __launch_bounds__(kBpColThreads, 4) bp_sart_column_kernel(const __grid_constant__ BpColArgs a) {
     extern __shared__ __align__(16) unsigned char bp_col_smem[];
     const SlabConst& g = a.slab;
@@ -1178,6 +1179,19 @@ __global__ void __launch_bounds__(kBpColThreads, 4) bp_sart_column_kernel(const 
                     }
                 }
                 *reinterpret_cast<float4*>(dst + 4 * k * kBpColThreads) = make_float4(vout[0], vout[1], vout[2], vout[3]);
+                if (kShadow) {  // the master's 16-bit shadow, as bp_store writes it
+                    const size_t e = (size_t)(dst - a.vol) + 4 * k * kBpColThreads;
+                    uint2 h;
+                    if (kShadow == 1) {
+                        const __half2 lo = __floats2half2_rn(vout[0], vout[1]), hi = __floats2half2_rn(vout[2], vout[3]);
+                        h = make_uint2(*reinterpret_cast<const uint32_t*>(&lo), *reinterpret_cast<const uint32_t*>(&hi));
+                    } else {
+                        const __nv_bfloat162 lo = __floats2bfloat162_rn(vout[0], vout[1]),
+                                             hi = __floats2bfloat162_rn(vout[2], vout[3]);
+                        h = make_uint2(*reinterpret_cast<const uint32_t*>(&lo), *reinterpret_cast<const uint32_t*>(&hi));
+                    }
+                    *reinterpret_cast<uint2*>((uint16_t*)a.shadow + e) = h;
+                }
             }
             rs = (rs + 1) & (kBpColDepth - 1);
             dst += plane;
@@ -1250,7 +1264,20 @@ constexpr int kUnitFused = 0, kUnitForward = 1, kUnitBack = 2;
 // kUnitForward skips the back projection (the volume is only read; p + 1 is the view),
 // kUnitBack the forward projection; each half performs the same operations as in the
 // fused step.
-template <bool kCoherent, int kKind = kUnitFused, int kThreads = kFuseThreads>
+// Value of the 16-bit shadow a forward projection reads for an FP32 master voxel
+// (kShadow 1: FP16, 2: BF16, 0: no shadow, the FP32 value itself).
+template <int kShadow>
+__device__ __forceinline__ float shadow_value(float v) {
+    if (kShadow == 1) return __half2float(__float2half_rn(v));
+    if (kShadow == 2) return __bfloat162float(__float2bfloat16_rn(v));
+    return v;
+}
+
+// kShadow (1: FP16, 2: BF16 shadow of an FP32 master): the walk reads the chunk rounded as
+// the shadow stores it, so the forward projection sees what the separate forward
+// projector reads from the shadow; the master is updated in FP32 (the shadow itself is
+// refreshed by the last back projection of the iteration).
+template <bool kCoherent, int kKind = kUnitFused, int kThreads = kFuseThreads, int kShadow = 0>
 __device__ __forceinline__ void fused_row_step(const FuseArgs& a, uint32_t p, int y, int x0lo, int ntaps,
                                                const float2* rl_in, float2* rl_out,
                                                unsigned char* fuse_smem) {
@@ -1363,6 +1390,15 @@ __device__ __forceinline__ void fused_row_step(const FuseArgs& a, uint32_t p, in
     };
     // BP update of chunk c in place (this thread's two columns), written back to the volume
     auto update = [&](int c) {
+        if (!kBP && kShadow && c < nchunks && on) {  // the walk reads the shadow's values
+            const int z0 = chunk_z0(c), z1 = min(rz, z0 + kFuseZc);
+            float* cb = buf + (size_t)(c & 1) * chunk_elems;
+            for (int z = z0; z < z1; ++z) {
+                float2* slot = reinterpret_cast<float2*>(cb + (size_t)(z - z0) * rx + x2);
+                const float2 v = *slot;
+                *slot = make_float2(shadow_value<kShadow>(v.x), shadow_value<kShadow>(v.y));
+            }
+        }
         if (!kBP || c >= nchunks || !on) return;
         const int z0 = chunk_z0(c), z1 = min(rz, z0 + kFuseZc);
         float* cb = buf + (size_t)(c & 1) * chunk_elems;
@@ -1392,7 +1428,7 @@ __device__ __forceinline__ void fused_row_step(const FuseArgs& a, uint32_t p, in
             }
             const float2 o = make_float2(vout[0], vout[1]);
             *reinterpret_cast<float2*>(dst) = o;
-            *slot = o;
+            *slot = kShadow ? make_float2(shadow_value<kShadow>(o.x), shadow_value<kShadow>(o.y)) : o;
         }
     };
     // FP walk of the rays through the updated chunk c (dda_walk_xz's steps, chunk-local
@@ -1492,9 +1528,11 @@ __device__ __forceinline__ void fused_row_step(const FuseArgs& a, uint32_t p, in
     }
 }
 
+template <int kShadow>
 __global__ void __launch_bounds__(kFuseThreads, 2) sart_fused_kernel(const __grid_constant__ FuseArgs a) {
     extern __shared__ __align__(16) unsigned char fuse_smem[];
-    fused_row_step<false>(a, a.p, (int)blockIdx.x, a.x0lo, a.ntaps, a.rl_in, a.rl_out, fuse_smem);
+    fused_row_step<false, kUnitFused, kFuseThreads, kShadow>(a, a.p, (int)blockIdx.x, a.x0lo, a.ntaps, a.rl_in,
+                                                             a.rl_out, fuse_smem);
 }
 
 // All fused steps of one SART iteration in one launch.  With parallel views tilted about
@@ -1535,6 +1573,7 @@ __device__ __forceinline__ unsigned long long global_ns() {
     return t;
 }
 
+template <int kShadow>
 __global__ void __launch_bounds__(kFuseThreads, 2)
     sart_fused_persistent_kernel(const __grid_constant__ FuseArgs a, const __grid_constant__ FusePersist q) {
     extern __shared__ __align__(16) unsigned char fuse_smem[];
@@ -1579,8 +1618,8 @@ __global__ void __launch_bounds__(kFuseThreads, 2)
         const uint32_t p = u / ry;
         const int y = (int)(u - p * ry);
         const int2 tw = q.tapwin[a.order[p]];
-        fused_row_step<true>(a, p, y, tw.x, tw.y, q.rl0 + (size_t)(p & 1) * q.rl_slot,
-                             q.rl0 + (size_t)((p + 1) & 1) * q.rl_slot, fuse_smem);
+        fused_row_step<true, kUnitFused, kFuseThreads, kShadow>(a, p, y, tw.x, tw.y, q.rl0 + (size_t)(p & 1) * q.rl_slot,
+                                                                q.rl0 + (size_t)((p + 1) & 1) * q.rl_slot, fuse_smem);
         __syncthreads();  // the unit's stores are issued and its shared memory is free
         if (threadIdx.x == 0 && !(p == 0 && y == q.withhold_row)) {
             __threadfence();
@@ -1612,7 +1651,9 @@ struct FuseSegment {
 
 // kThreads = 512 for rows of up to 1024 voxels, 128 for batches whose rows are at most 256
 // voxels wide with at most 256 rays each (two voxels and two rays per thread either way).
-template <int kThreads>
+// kShadow: every series holds an FP32 master with a 16-bit shadow of that kind
+// (fused_row_step); the shadows are refreshed from the masters after the launch.
+template <int kThreads, int kShadow = 0>
 __global__ void __launch_bounds__(kThreads, 1024 / kThreads)
     sart_fused_batch_kernel(const FuseSeries* series, const FuseSegment* segs, uint32_t nsegs, uint32_t total,
                             uint32_t* counter, uint32_t* error, int withhold_row) {
@@ -1674,16 +1715,17 @@ __global__ void __launch_bounds__(kThreads, 1024 / kThreads)
         }
         __syncthreads();
         if (st == 0) {
-            fused_row_step<true, kUnitForward, kThreads>(cur.a, 0xffffffffu, y, 0, 0, cur.rl0, cur.rl0, fuse_smem);
+            fused_row_step<true, kUnitForward, kThreads, kShadow>(cur.a, 0xffffffffu, y, 0, 0, cur.rl0, cur.rl0,
+                                                                  fuse_smem);
         } else {
             const uint32_t p = st - 1;
             const int2 tw = cur.tapwin[cur.a.order[p]];
             const float2* rin = cur.rl0 + (size_t)(p & 1) * cur.rl_slot;
             float2* rout = cur.rl0 + (size_t)((p + 1) & 1) * cur.rl_slot;
             if (st < cur.views)
-                fused_row_step<true, kUnitFused, kThreads>(cur.a, p, y, tw.x, tw.y, rin, rout, fuse_smem);
+                fused_row_step<true, kUnitFused, kThreads, kShadow>(cur.a, p, y, tw.x, tw.y, rin, rout, fuse_smem);
             else
-                fused_row_step<true, kUnitBack, kThreads>(cur.a, p, y, tw.x, tw.y, rin, rout, fuse_smem);
+                fused_row_step<true, kUnitBack, kThreads, kShadow>(cur.a, p, y, tw.x, tw.y, rin, rout, fuse_smem);
         }
         __syncthreads();  // the unit's stores are issued; its shared memory is free
         // withhold_row (tests of the bounded waits): series 0 never reports that row's step 0

@@ -490,6 +490,19 @@ class Context:
     def device_bytes(self) -> int:
         return int(lib().etcu_device_bytes(self.handle))
 
+    def set_autotune(self, mode: int = 1) -> None:
+        """Launch shapes from the autotuner's cache, timed on the real problem on a miss
+        (etcu_context_set_autotune); results do not depend on the choice."""
+        check(lib().etcu_context_set_autotune(self.handle, int(mode)), self.handle)
+
+    def tune_report(self) -> str:
+        """The autotuner's choices on this context, one line each."""
+        n = ctypes.c_size_t()
+        check(lib().etcu_context_tune_report(self.handle, None, 0, ctypes.byref(n)), self.handle)
+        buf = ctypes.create_string_buffer(n.value)
+        check(lib().etcu_context_tune_report(self.handle, buf, n.value, None), self.handle)
+        return buf.value.decode()
+
     def check(self, status: int) -> None:
         check(status, self.handle)
 

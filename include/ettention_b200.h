@@ -119,6 +119,17 @@ ETCU_API etcu_status etcu_set_stream(etcu_context* ctx, void* cuda_stream);
 ETCU_API void* etcu_context_stream(const etcu_context* ctx);
 /* Sum of device bytes the context currently holds. */
 ETCU_API size_t etcu_device_bytes(const etcu_context* ctx);
+/* Launch-shape autotuner (no counterpart in the reference): with mode 1, reconstructions,
+ * batches and the warm-start network created on this context take their launch shapes
+ * (resident blocks per multiprocessor, threads per block, pipeline stages) from a cache
+ * file ($ETCU_TUNE_CACHE, else ~/.cache/ettention_b200/launch_shapes.txt) and time the
+ * candidates with CUDA events on the real problem when the cache has no entry; results
+ * do not depend on the choice.  Mode 0 (default; ETCU_AUTOTUNE=1 in the environment of
+ * etcu_context_create sets 1) keeps the built-in shapes. */
+ETCU_API etcu_status etcu_context_set_autotune(etcu_context* ctx, int mode);
+/* The tuner's choices on this context so far, one "key choice [cached | candidate=ms ...]"
+ * line each; *needed receives the length including the terminating zero. */
+ETCU_API etcu_status etcu_context_tune_report(const etcu_context* ctx, char* out, size_t capacity, size_t* needed);
 
 /* ---------------------------------------------------------------- geometry */
 /* SingleAxisTiltRotator::createRotatedScannerGeometry

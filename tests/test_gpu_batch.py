@@ -223,3 +223,41 @@ def test_persistent_batch_wait_gives_up_and_context_survives():
     finally:
         ctx2.close()
     assert np.abs(fresh).max() > 0 and np.array_equal(after, fresh)
+
+
+@pytest.mark.parametrize("vt", [2, 3])
+def test_persistent_batch_with_16bit_shadow(vt):
+    """Series held as FP32 masters with FP16 (2) / BF16 (3) shadows run the persistent
+    batched iteration (one launch) and equal the single-series persistent reconstruction
+    bit for bit; after the run the shadows are refreshed from the masters, so a further
+    single-series iteration on a batched volume equals three single-series iterations."""
+    from ettention_b200 import _abi
+    from ettention_b200.operators import (AlgebraicParameterSet, BatchReconstructionOperator,
+                                          BlockIterativeReconstructionOperator, Context, GPUMappedVolume)
+    series = make_series(600)
+    ctx = Context(0)
+    try:
+        p = AlgebraicParameterSet(algorithm="sart", block_size=1, iterations=2, lam=0.3, order=_abi.ORDER_IDENTITY)
+        vols = [GPUMappedVolume(ctx, shape, voxel_type=vt) for shape, _, _ in series]
+        batch = BatchReconstructionOperator([(v, g, pr) for v, (_, g, pr) in zip(vols, series)], p)
+        assert batch.launches_per_iteration == 1
+        batch.runNiterations(2)
+        got = batch.getReconstructedVolumes()
+        batch.close()
+        for i, (shape, geoms, projs) in enumerate(series):
+            vol = GPUMappedVolume(ctx, shape, voxel_type=vt)
+            rec = BlockIterativeReconstructionOperator(vol, geoms, projs, p)
+            rec.runNiterations(2)
+            assert np.abs(got[i]).max() > 0 and np.array_equal(got[i], rec.getReconstructedVolume()), i
+            rec.runNiterations(1)
+            want3 = rec.getReconstructedVolume()
+            rec.close()
+            vol.close()
+            cont = BlockIterativeReconstructionOperator(vols[i], geoms, projs, p)
+            cont.runNiterations(1)
+            assert np.array_equal(cont.getReconstructedVolume(), want3), i
+            cont.close()
+        for v in vols:
+            v.close()
+    finally:
+        ctx.close()

@@ -176,3 +176,47 @@ def test_persistent_wait_gives_up_and_context_survives():
         ctx.close()
     fresh, _, _ = _run("unfused", res, geoms, projs, q, 2)
     assert np.abs(fresh).max() > 0 and np.array_equal(after, fresh)
+
+
+@pytest.mark.parametrize("vt", [2, 3])
+def test_fused_steps_with_16bit_shadow(vt):
+    """FP32 master with an FP16 (2) / BF16 (3) shadow on the fused paths: the walk reads
+    each updated chunk rounded as the shadow holds it, so the persistent and per-step
+    launches and the unfused kernels (the column back projector writing master and shadow,
+    the forward projector reading the shadow) give the same volume bit for bit; the FP64
+    oracle is met at the storage bound."""
+    from oracle import oracle as O
+    from ettention_b200 import _abi
+    from ettention_b200.operators import (AlgebraicParameterSet, BlockIterativeReconstructionOperator,
+                                          GPUMappedVolume)
+    from tests.helpers import oracle_geometry
+    res, det = (128, 64, 48), (128, 64)
+    angles = list(np.linspace(-70, 70, 15))
+    geoms, projs = _problem(res, det, angles, seed=31)
+    p = AlgebraicParameterSet(algorithm="sart", block_size=1, iterations=2, lam=0.3, order=_abi.ORDER_IDENTITY)
+
+    def run(mode):
+        ctx = _context(mode)
+        try:
+            vol = GPUMappedVolume(ctx, res, voxel_type=vt)
+            rec = BlockIterativeReconstructionOperator(vol, geoms, projs, p)
+            n = rec.launches_per_iteration
+            rec.runNiterations(2)
+            v = rec.getReconstructedVolume()
+            rec.close()
+            vol.close()
+        finally:
+            ctx.close()
+        return v, n
+
+    vp, np_ = run("persistent")
+    vs, ns = run("step")
+    vu, nu = run("unfused")
+    M = len(angles)
+    assert (np_, ns, nu) == (3, M + 1, 2 * M)
+    assert np.abs(vp).max() > 0 and np.array_equal(vp, vs) and np.array_equal(vp, vu)
+    vg = O.VolumeGeometry.centered(res)
+    setup = O.ReconstructionSetup(vg, [oracle_geometry(g) for g in geoms], projs, 0.3, 1, 1, 1)
+    v64 = np.zeros((res[2], res[1], res[0]), np.float32)
+    O.block_iterative(setup, v64, 2, 64)
+    assert O.rel_l2(vp, v64) <= (1e-2 if vt == 2 else 3e-2)
