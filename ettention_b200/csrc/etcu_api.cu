@@ -765,6 +765,11 @@ void store(const std::string& key, int value) {
 }
 
 std::string device_tag(int device) {
+    static std::mutex mu;
+    static std::map<int, std::string> tags;  // device properties are slow to query: once per device
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = tags.find(device);
+    if (it != tags.end()) return it->second;
     cudaDeviceProp prop;
     if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
         cudaGetLastError();
@@ -773,8 +778,8 @@ std::string device_tag(int device) {
     std::string name(prop.name);
     for (char& c : name)
         if (c == ' ' || c == '|') c = '_';
-    return name + "|sm" + std::to_string(prop.major) + std::to_string(prop.minor) + "|" +
-           std::to_string(prop.multiProcessorCount);
+    return tags[device] = name + "|sm" + std::to_string(prop.major) + std::to_string(prop.minor) + "|" +
+                          std::to_string(prop.multiProcessorCount);
 }
 
 int search(cudaStream_t st, const std::vector<int>& candidates, const std::function<bool(int)>& run, int reps,

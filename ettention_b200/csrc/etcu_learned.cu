@@ -19,6 +19,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -120,6 +121,7 @@ struct etcu_warmstart {
     unsigned* d_err = nullptr;
     double* d_loss = nullptr;
     std::string err;
+    int loader = -1;  // convolution operand loads: -1 default (tensor copies), 0 tensor copies, 1 cp.async (ETCU_CONV_LOADER)
 };
 
 namespace {
@@ -199,7 +201,9 @@ etcu_status launch_conv_n(etcu_warmstart* w, const CUtensorMap& m0, const CUtens
     a.batch = batch;
     static std::atomic<unsigned long long> opted{0};
     if (w->device < 64 && !(opted.load() & (1ull << w->device))) {
-        WCK(w, cudaFuncSetAttribute(ws::conv_tc_kernel<N, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        WCK(w, cudaFuncSetAttribute(ws::conv_tc_kernel<N, TY, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    232448));
+        WCK(w, cudaFuncSetAttribute(ws::conv_tc_kernel<N, TY, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     232448));
         opted.fetch_or(1ull << w->device);
     }
@@ -208,34 +212,37 @@ etcu_status launch_conv_n(etcu_warmstart* w, const CUtensorMap& m0, const CUtens
     const long ntiles = (long)ntx * nty * a.Z * batch;
     const unsigned grid = (unsigned)std::min<long>(ntiles, w->sms);
     cudaError_t last = cudaSuccess;
-    auto launch = [&](int S) {
+    // choice = loader * 10 + stages (loader 0: one tensor copy per halo, 1: cp.async warps)
+    auto launch = [&](int choice) {
+        const int S = choice % 10, load = choice / 10;
         a.stages = S;
         // at least 120 KB, so that one CTA (and its tensor memory) owns each SM
         const size_t smem = std::max<size_t>(wres + (size_t)S * stage + (2 * S + 5) * 8 + 16 + 1024, 120 * 1024);
-        ws::conv_tc_kernel<N, TY><<<grid, 192, smem, w->stream>>>(m0, m1, a);
+        if (load) ws::conv_tc_kernel<N, TY, 1><<<grid, ws::conv_threads<1>(), smem, w->stream>>>(m0, m1, a);
+        else ws::conv_tc_kernel<N, TY, 0><<<grid, ws::conv_threads<0>(), smem, w->stream>>>(m0, m1, a);
         last = cudaGetLastError();
         return last == cudaSuccess;
     };
-    int S = smax;
-    if (etcu_context_autotune(w->ctx) && smax > 1) {
-        // autotuner: ring stages of this convolution (the launch is idempotent)
+    int choice = (w->loader == 1 ? 10 : 0) + smax;
+    if (w->loader < 0 && etcu_context_autotune(w->ctx)) {
+        // autotuner: loader and ring stages of this convolution (the launch is idempotent)
         char key[256];
         snprintf(key, sizeof(key), "warmstart_conv|n%d|rows%d|%dx%dx%d|b%d|steps%d|res%d|%s", N, TY, a.X, a.Y, a.Z,
                  batch, a.nsteps, a.resident, etcu_tune::device_tag(w->device).c_str());
         int c = etcu_tune::lookup(key);
-        std::string log = " cached";
-        if (c < 1 || c > smax) {
+        if (c < 1 || c % 10 < 1 || c % 10 > smax || c / 10 > 1) {
             std::vector<int> cands;
-            for (int k = 1; k <= smax; ++k) cands.push_back(k);
-            log.clear();
+            for (int load = 0; load <= 1; ++load)
+                for (int k = 1; k <= smax; ++k) cands.push_back(load * 10 + k);
+            std::string log;
             c = etcu_tune::search(w->stream, cands, launch, 3, &log);
-            if (c < 1) c = smax;
+            if (c < 1) c = choice;
             etcu_tune::store(key, c);
             etcu_context_tune_note(w->ctx, std::string(key) + " " + std::to_string(c) + log);
         }
-        S = c;
+        choice = c;
     }
-    if (!launch(S))
+    if (!launch(choice))
         return wfail(w, ETCU_ERR_CUDA, "convolution launch failed: %s", cudaGetErrorString(last));
     return ETCU_OK;
 }
@@ -278,6 +285,8 @@ etcu_status conv(etcu_warmstart* w, const ConvCall& c, int batch) {
     a.nkp0 = c.nsteps0;
     a.c8_0 = c.src0->C / 8;
     a.c8_1 = c.src1 ? c.src1->C / 8 : 0;
+    a.p0 = c.src0->p;
+    a.p1 = c.src1 ? c.src1->p : c.src0->p;
     a.w = c.w;
     a.bias = c.bias;
     a.relu = c.relu ? 1 : 0;
@@ -413,10 +422,14 @@ etcu_status relayout(etcu_warmstart* w) {
         if (s_ != ETCU_OK) return s_;     \
     } while (0)
 
-etcu_status forward(etcu_warmstart* w, const float* d_in, float* d_out, int B) {
+// training: also store the BF16 input tensor the first layer's weight gradient reads.
+etcu_status forward(etcu_warmstart* w, const float* d_in, float* d_out, int B, bool training = false) {
     const size_t p1n = w->g1.plane();
-    ws::prep_input_kernel<<<blocks((size_t)B * p1n), 256, 0, w->stream>>>(d_in, 1.f / w->scale, p1n, B, w->x16.p);
-    WCK(w, cudaGetLastError());
+    if (training) {
+        ws::prep_input_kernel<<<blocks((size_t)B * p1n), 256, 0, w->stream>>>(d_in, 1.f / w->scale, p1n, B,
+                                                                              w->x16.p);
+        WCK(w, cudaGetLastError());
+    }
     auto fwd = [&](int l, const Tensor& s0, const Tensor* s1, const Tensor& out) {
         const LayerDef& d = kDefs[l];
         ConvCall c{};
@@ -431,7 +444,12 @@ etcu_status forward(etcu_warmstart* w, const float* d_in, float* d_out, int B) {
         c.dst0 = dst(out);
         return conv(w, c, B);
     };
-    WTRY(fwd(0, w->x16, nullptr, w->e1a));
+    // first layer (one input channel) on the CUDA cores
+    const dim3 end_grid((w->g1.X + ws::kEndTx - 1) / ws::kEndTx, (w->g1.Y + ws::kEndTy - 1) / ws::kEndTy,
+                        w->g1.Z * B);
+    ws::conv_in_kernel<<<end_grid, 256, 0, w->stream>>>(d_in, 1.f / w->scale, w->g1.X, w->g1.Y, w->g1.Z, B,
+                                                        w->params + w->woff[0], w->params + w->boff[0], w->e1a.p);
+    WCK(w, cudaGetLastError());
     WTRY(fwd(1, w->e1a, nullptr, w->e1b));
     ws::pool_kernel<<<blocks((size_t)B * 2 * w->g2.plane()), 256, 0, w->stream>>>(w->e1b.p, w->g1.X, w->g1.Y,
                                                                                    w->g1.Z, B * 2, w->p1.p);
@@ -449,22 +467,12 @@ etcu_status forward(etcu_warmstart* w, const float* d_in, float* d_out, int B) {
                                                                                        w->g1.Z, B * 4, w->up1.p);
     WTRY(fwd(8, w->up1, &w->e1b, w->d1a));
     WTRY(fwd(9, w->d1a, nullptr, w->d1b));
-    // head: out = v + scale * (conv(d1b) + b), channel 0 of a 16-wide MMA
-    ConvCall h{};
-    h.src0 = &w->d1b;
-    h.src1 = nullptr;
-    h.nsteps0 = 1;
-    h.nsteps1 = 0;
-    h.w = w->wf[10];
-    h.bias = w->params + w->boff[10];
-    h.relu = false;
-    h.n = 16;
-    h.head = true;
-    h.head_in = d_in;
-    h.head_out = d_out;
-    h.head_scale = w->scale;
+    // head (one output channel) on the CUDA cores: out = v + scale * (conv(d1b) + b)
+    ws::conv_head_kernel<<<end_grid, 256, 0, w->stream>>>(w->d1b.p, w->g1.X, w->g1.Y, w->g1.Z, B,
+                                                          w->params + w->woff[10], w->params + w->boff[10], d_in,
+                                                          w->scale, d_out);
     WCK(w, cudaGetLastError());
-    return conv(w, h, B);
+    return ETCU_OK;
 }
 
 etcu_status backward(etcu_warmstart* w, const float* d_in, const float* d_target, int B) {
@@ -626,6 +634,7 @@ extern "C" etcu_status etcu_warmstart_create(etcu_context* ctx, const uint32_t r
     WCK(w.get(), cudaSetDevice(w->device));
     WCK(w.get(), cudaDeviceGetAttribute(&w->sms, cudaDevAttrMultiProcessorCount, w->device));
     w->max_batch = (int)max_batch;
+    if (const char* env = getenv("ETCU_CONV_LOADER")) w->loader = atoi(env) ? 1 : 0;
     w->g1 = Grid{(int)resolution[0], (int)resolution[1], (int)resolution[2]};
     w->g2 = Grid{w->g1.X / 2, w->g1.Y / 2, w->g1.Z / 2};
     w->g3 = Grid{w->g2.X / 2, w->g2.Y / 2, w->g2.Z / 2};
@@ -740,7 +749,7 @@ extern "C" etcu_status etcu_warmstart_gradients(etcu_warmstart* w, const float* 
                                                 uint32_t batch, float* host_grads, double* loss) {
     if (!w || !d_in || !d_target) return wfail(w, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
     WTRY(check_batch(w, batch));
-    WTRY(forward(w, d_in, w->out, (int)batch));
+    WTRY(forward(w, d_in, w->out, (int)batch, true));
     WTRY(backward(w, d_in, d_target, (int)batch));
     if (host_grads)
         WCK(w, cudaMemcpyAsync(host_grads, w->grads, w->nparams * 4, cudaMemcpyDeviceToHost, w->stream));
@@ -755,7 +764,7 @@ extern "C" etcu_status etcu_warmstart_train_step(etcu_warmstart* w, const float*
                                                  uint32_t batch, float lr, double* loss) {
     if (!w || !d_in || !d_target) return wfail(w, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
     WTRY(check_batch(w, batch));
-    WTRY(forward(w, d_in, w->out, (int)batch));
+    WTRY(forward(w, d_in, w->out, (int)batch, true));
     WTRY(backward(w, d_in, d_target, (int)batch));
     w->adam_t += 1;
     const float b1 = 0.9f, b2 = 0.999f;

@@ -84,6 +84,20 @@ __device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* map, u
         "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(bar))
         : "memory");
 }
+// 16-byte copy global -> shared; src_bytes 0 writes 16 zero bytes (no global read).
+__device__ __forceinline__ void cp_async16z(uint32_t dst, const void* src, uint32_t src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_group() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+// Generic-proxy shared-memory writes (cp.async) made visible to the async proxy (the
+// tensor cores' operand reads).
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
 __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                      smem_u32(dst)),
@@ -172,6 +186,8 @@ struct ConvArgs {
     int nsteps;            // K steps of 16 channels over both sources
     int nkp0;              // steps from source 0 (the rest from source 1)
     int c8_0, c8_1;        // chunks per batch item of source 0 / 1 (dim-4 coordinate n * c8 + 2 kp)
+    const __nv_bfloat16* p0;  // the sources as NC8 tensors (cp.async loaders)
+    const __nv_bfloat16* p1;
     const __nv_bfloat16* w;  // [step][27 taps][2 halves][N][8] bf16
     int resident;          // 1: all steps' weights are loaded once into shared memory
     const float* bias;     // N values or NULL
@@ -202,9 +218,17 @@ struct ConvShape {
 // (and, unless the weights are resident, the step's weights) through a ring of `stages`
 // buffers; warp 1 issues 27 x TY MMAs per step into one of two tensor-memory accumulators;
 // warps 2-5 drain the other accumulator (bias, ReLU, mask, BF16 store) meanwhile.
-template <int N, int TY>
-__global__ void __launch_bounds__(192, 1) conv_tc_kernel(const __grid_constant__ CUtensorMap src0,
-                                                         const __grid_constant__ CUtensorMap src1, ConvArgs a) {
+// kLoad 0 (default): warp 0 brings every halo with one tensor copy (cp.async.bulk.tensor);
+// kLoad 1: warps 0-3 copy it with 16-byte cp.async (rows of 512 bytes per warp
+// instruction), the MMA and epilogue warps follow.  The autotuner times both (on B200 the
+// tensor copy was 1.6x faster on every layer of the 256 x 256 x 128 network).
+template <int kLoad>
+constexpr int conv_threads() { return kLoad ? 288 : 192; }
+
+template <int N, int TY, int kLoad>
+__global__ void __launch_bounds__(conv_threads<kLoad>(), 1) conv_tc_kernel(const __grid_constant__ CUtensorMap src0,
+                                                                          const __grid_constant__ CUtensorMap src1,
+                                                                          ConvArgs a) {
     using SH = ConvShape<N, TY>;
     static_assert(N % 16 == 0 && N >= 16 && N <= 256, "M = 128 needs N a multiple of 16");
     constexpr uint32_t kIdesc = idesc_bf16(128, N, 0, 0);
@@ -226,10 +250,12 @@ __global__ void __launch_bounds__(192, 1) conv_tc_kernel(const __grid_constant__
     const int nty = (a.Y + TY - 1) / TY;
     const int ntiles = ntx * nty * a.Z * a.batch;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr int kLoaders = kLoad ? 128 : 1;        // arrivals that complete a stage
+    constexpr int kMmaWarp = kLoad ? 4 : 1, kEpiWarp = kLoad ? 5 : 2;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < S; ++s) {
-            mbar_init(&full[s], 1);
+            mbar_init(&full[s], kLoaders);
             mbar_init(&empty[s], 1);
         }
         for (int i = 0; i < 2; ++i) {
@@ -245,7 +271,78 @@ __global__ void __launch_bounds__(192, 1) conv_tc_kernel(const __grid_constant__
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
-    if (warp == 0) {
+    if (kLoad && warp < 4) {
+        // cp.async loaders: stage q's copies are issued, then stage q - (S - 1)'s are
+        // waited for, fenced for the tensor cores and announced
+        const int tid = threadIdx.x;
+        if (tid == 0 && a.resident) {
+            mbar_expect_tx(wbar, wres);
+            bulk_load(wsm, a.w, wres, wbar);
+        }
+        const size_t plane = (size_t)a.Z * a.Y * a.X;
+        constexpr int kRows = 2 * 3 * (TY + 2);
+        constexpr int kElems = kRows * kHaloX;
+        int q = 0;
+        bool ok = true;
+        auto announce = [&](int k) {  // stage of load k is in shared memory
+            fence_proxy_async_smem();
+            mbar_arrive(&full[k % S]);
+        };
+        auto drain_to = [&](int pending) {  // wait until at most `pending` groups are in flight
+            switch (pending) {
+            case 0: cp_async_wait_group<0>(); break;
+            case 1: cp_async_wait_group<1>(); break;
+            case 2: cp_async_wait_group<2>(); break;
+            default: cp_async_wait_group<3>(); break;
+            }
+        };
+        for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+            int t = tile;
+            const int xt = t % ntx;
+            t /= ntx;
+            const int yt = t % nty;
+            t /= nty;
+            const int z = t % a.Z;
+            const int n = t / a.Z;
+            for (int s = 0; s < a.nsteps; ++s, ++q) {
+                const int st = q % S;
+                if (q >= S && !mbar_wait(&empty[st], ((q / S) - 1) & 1)) {
+                    if (tid == 0) atomicOr(a.err, kErrWaitEmpty);
+                    ok = false;
+                    break;
+                }
+                const uint32_t halo = smem_u32(ring + (size_t)st * stage);
+                const bool second = s >= a.nkp0;
+                const int kp = second ? s - a.nkp0 : s;
+                const __nv_bfloat16* src = second ? a.p1 : a.p0;
+                const int cbase = n * (second ? a.c8_1 : a.c8_0) + 2 * kp;
+                for (int e = tid; e < kElems; e += 128) {
+                    const int row = e / kHaloX, xi = e - row * kHaloX;
+                    const int c = row / (3 * (TY + 2)), rem = row - c * (3 * (TY + 2));
+                    const int dz = rem / (TY + 2), dy = rem - dz * (TY + 2);
+                    const int xx = xt * kTileX - 1 + xi, yy = yt * TY - 1 + dy, zz = z - 1 + dz;
+                    const bool in = xx >= 0 && xx < a.X && yy >= 0 && yy < a.Y && zz >= 0 && zz < a.Z;
+                    const __nv_bfloat16* g =
+                        in ? src + ((((size_t)(cbase + c) * a.Z + zz) * a.Y + yy) * a.X + xx) * 8 : src;
+                    cp_async16z(halo + (uint32_t)e * 16u, g, in ? 16u : 0u);
+                }
+                if (!a.resident) {
+                    const __nv_bfloat16* wsrc = a.w + (size_t)s * (SH::kW / 2);
+                    for (int e = tid; e < (int)(SH::kW / 16); e += 128)
+                        cp_async16z(halo + SH::kHalo + (uint32_t)e * 16u, wsrc + (size_t)e * 8, 16u);
+                }
+                cp_async_commit_group();
+                if (q >= S - 1) {
+                    drain_to(S - 1);
+                    announce(q - (S - 1));
+                }
+            }
+        }
+        // the last stages: announce what this thread issued and has not announced yet
+        const int first_open = q - (S - 1) < 0 ? 0 : q - (S - 1);
+        cp_async_wait_group<0>();
+        for (int k = first_open; k < q; ++k) announce(k);
+    } else if (!kLoad && warp == 0) {
         if (lane == 0) {
             if (a.resident) {
                 mbar_expect_tx(wbar, wres);
@@ -279,7 +376,7 @@ __global__ void __launch_bounds__(192, 1) conv_tc_kernel(const __grid_constant__
                 }
             }
         }
-    } else if (warp == 1) {
+    } else if (warp == kMmaWarp) {
         if (lane == 0) {
             bool ok = !a.resident || mbar_wait(wbar, 0);
             if (!ok) atomicOr(a.err, kErrWaitFull);
@@ -319,7 +416,7 @@ __global__ void __launch_bounds__(192, 1) conv_tc_kernel(const __grid_constant__
                 umma_commit(&accf[acc]);
             }
         }
-    } else {
+    } else if (warp >= kEpiWarp) {
         // epilogue: warp quarter (warp % 4) reads tensor-memory lanes 32 * (warp % 4) ...
         const int quarter = warp & 3;
         const int m = quarter * 32 + lane;
@@ -595,6 +692,105 @@ __global__ void channel_sum_kernel(const __nv_bfloat16* __restrict__ t, int c8, 
         for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
         if ((threadIdx.x & 31) == 0 && chunk * 8 + j < cout) atomicAdd(&db[chunk * 8 + j], s);
     }
+}
+
+// First layer and head (one input / one output channel: no GEMM shape) on the CUDA
+// cores.  A block of 256 threads computes a 32 x 8 tile of output voxels at one z; the
+// 34 x 10 x 3 input halo is staged in shared memory first.  Weights rounded to BF16 as
+// the tensor path holds them, FP32 accumulation.
+constexpr int kEndTx = 32, kEndTy = 8, kEndHx = kEndTx + 2, kEndHy = kEndTy + 2;
+constexpr int kEndHalo = kEndHx * kEndHy * 3;
+
+// e1a[co] = relu(b[co] + sum_t x(v + off(t)) W[t][co]), x = bf16(v / scale); 16 output
+// channels stored as the two chunks of an NC8 tensor.  W: FP32 master [27][16].
+// Grid: (ceil(X / 32), ceil(Y / 8), Z * batch).
+__global__ void __launch_bounds__(256) conv_in_kernel(const float* __restrict__ vin, float inv_scale, int X, int Y,
+                                                       int Z, int batch, const float* __restrict__ W,
+                                                       const float* __restrict__ bias, __nv_bfloat16* __restrict__ out) {
+    __shared__ float ws_[27 * 16];
+    __shared__ float bs_[16];
+    __shared__ float halo[kEndHalo];
+    const int tid = threadIdx.x;
+    for (int i = tid; i < 27 * 16; i += 256) ws_[i] = __bfloat162float(__float2bfloat16_rn(W[i]));
+    if (tid < 16) bs_[tid] = bias[tid];
+    const int x0 = blockIdx.x * kEndTx, y0 = blockIdx.y * kEndTy;
+    const int z = blockIdx.z % Z, n = blockIdx.z / Z;
+    const size_t plane = (size_t)X * Y * Z;
+    const float* src = vin + (size_t)n * plane;
+    for (int i = tid; i < kEndHalo; i += 256) {
+        const int hx = i % kEndHx, hy = (i / kEndHx) % kEndHy, hz = i / (kEndHx * kEndHy);
+        const int xx = x0 - 1 + hx, yy = y0 - 1 + hy, zz = z - 1 + hz;
+        float v = 0.f;
+        if (xx >= 0 && xx < X && yy >= 0 && yy < Y && zz >= 0 && zz < Z)
+            v = __bfloat162float(__float2bfloat16_rn(src[((size_t)zz * Y + yy) * X + xx] * inv_scale));
+        halo[i] = v;
+    }
+    __syncthreads();
+    const int tx = tid % kEndTx, ty = tid / kEndTx;
+    const int x = x0 + tx, y = y0 + ty;
+    if (x >= X || y >= Y) return;
+    float acc[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) acc[c] = bs_[c];
+#pragma unroll
+    for (int t = 0; t < 27; ++t) {
+        const float xv = halo[((t / 9) * kEndHy + ty + (t / 3) % 3) * kEndHx + tx + t % 3];
+#pragma unroll
+        for (int c = 0; c < 16; ++c) acc[c] = fmaf(xv, ws_[t * 16 + c], acc[c]);
+    }
+    const size_t v = ((size_t)z * Y + y) * X + x;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        uint4 o;
+        o.x = pack_bf16x2(fmaxf(acc[8 * h + 0], 0.f), fmaxf(acc[8 * h + 1], 0.f));
+        o.y = pack_bf16x2(fmaxf(acc[8 * h + 2], 0.f), fmaxf(acc[8 * h + 3], 0.f));
+        o.z = pack_bf16x2(fmaxf(acc[8 * h + 4], 0.f), fmaxf(acc[8 * h + 5], 0.f));
+        o.w = pack_bf16x2(fmaxf(acc[8 * h + 6], 0.f), fmaxf(acc[8 * h + 7], 0.f));
+        *reinterpret_cast<uint4*>(out + (((size_t)n * 2 + h) * plane + v) * 8) = o;
+    }
+}
+
+// out = vin + scale * (b + sum_t sum_ci d1b(v + off(t))[ci] W[t][ci]) from a 16-channel NC8
+// tensor.  W: FP32 master [27][1][16].  Grid as conv_in_kernel.
+__global__ void __launch_bounds__(256) conv_head_kernel(const __nv_bfloat16* __restrict__ in, int X, int Y, int Z,
+                                                         int batch, const float* __restrict__ W,
+                                                         const float* __restrict__ bias,
+                                                         const float* __restrict__ vin, float scale,
+                                                         float* __restrict__ out) {
+    __shared__ float ws_[27 * 16];
+    __shared__ __align__(16) uint4 halo[2][kEndHalo];  // the two 8-channel chunks
+    const int tid = threadIdx.x;
+    for (int i = tid; i < 27 * 16; i += 256) ws_[i] = __bfloat162float(__float2bfloat16_rn(W[i]));
+    const int x0 = blockIdx.x * kEndTx, y0 = blockIdx.y * kEndTy;
+    const int z = blockIdx.z % Z, n = blockIdx.z / Z;
+    const size_t plane = (size_t)X * Y * Z;
+    for (int i = tid; i < 2 * kEndHalo; i += 256) {
+        const int h = i / kEndHalo, j = i % kEndHalo;
+        const int hx = j % kEndHx, hy = (j / kEndHx) % kEndHy, hz = j / (kEndHx * kEndHy);
+        const int xx = x0 - 1 + hx, yy = y0 - 1 + hy, zz = z - 1 + hz;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if (xx >= 0 && xx < X && yy >= 0 && yy < Y && zz >= 0 && zz < Z)
+            v = *reinterpret_cast<const uint4*>(in + (((size_t)n * 2 + h) * plane + ((size_t)zz * Y + yy) * X + xx) * 8);
+        halo[h][j] = v;
+    }
+    __syncthreads();
+    const int tx = tid % kEndTx, ty = tid / kEndTx;
+    const int x = x0 + tx, y = y0 + ty;
+    if (x >= X || y >= Y) return;
+    float acc = bias[0];
+#pragma unroll 3
+    for (int t = 0; t < 27; ++t) {
+        const int j = ((t / 9) * kEndHy + ty + (t / 3) % 3) * kEndHx + tx + t % 3;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            float f[8];
+            unpack_bf16x8(halo[h][j], f);
+#pragma unroll
+            for (int c = 0; c < 8; ++c) acc = fmaf(f[c], ws_[t * 16 + 8 * h + c], acc);
+        }
+    }
+    const size_t i = (size_t)n * plane + ((size_t)z * Y + y) * X + x;
+    out[i] = fmaf(scale, acc, vin[i]);
 }
 
 // Network input: chunk 0 of a 16-channel NC8 tensor = (v / scale, 0, ..., 0); chunk 1

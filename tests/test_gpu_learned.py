@@ -18,6 +18,19 @@ GRAD_TOL = 2e-2
 FP64_TOL = 1e-1
 
 
+@pytest.fixture(scope="module", params=["tensor_copy", "cp_async"])
+def loader(request):
+    """The convolutions' two operand loaders (ETCU_CONV_LOADER 0: one tensor copy per
+    halo, 1: cp.async warps); every result must hold for both."""
+    return request.param
+
+
+@pytest.fixture()
+def net_env(loader, monkeypatch):
+    monkeypatch.setenv("ETCU_CONV_LOADER", "0" if loader == "tensor_copy" else "1")
+    return loader
+
+
 @pytest.fixture(scope="module")
 def ctx():
     import torch
@@ -53,7 +66,7 @@ def _rel(a, b):
 
 
 @pytest.mark.parametrize("res,batch", [((16, 16, 8), 2), ((160, 8, 4), 1), ((32, 12, 8), 3)])
-def test_forward_matches_oracle(ctx, res, batch):
+def test_forward_matches_oracle(ctx, net_env, res, batch):
     import torch
     from oracle import warmstart_oracle as W
     from ettention_b200.learned import WarmStartNet
@@ -72,7 +85,7 @@ def test_forward_matches_oracle(ctx, res, batch):
     assert _rel(got - v, ref64 - v) <= FP64_TOL
 
 
-def test_gradients_match_oracle(ctx):
+def test_gradients_match_oracle(ctx, net_env):
     import torch
     from oracle import warmstart_oracle as W
     from ettention_b200.learned import WarmStartNet
@@ -102,6 +115,6 @@ def test_adam_steps_lower_the_loss(ctx):
     t = (v * np.float32(0.8) + np.float32(0.1)).astype(np.float32)  # a mapping the network can learn
     with WarmStartNet(ctx, res, params=init_params(4), scale=1.0) as net:
         d_in, d_t = torch.as_tensor(v).cuda(), torch.as_tensor(t).cuda()
-        losses = [net.train_step(d_in, d_t, 1, lr=2e-3) for _ in range(40)]
+        losses = [net.train_step(d_in, d_t, 1, lr=2e-3) for _ in range(60)]
     assert np.all(np.isfinite(losses))
-    assert losses[-1] < 0.5 * losses[0], losses[::8]
+    assert losses[-1] < 0.5 * losses[0], losses[::10]
