@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--c4-f32", action="store_true", help="--workload c4 with FP32 volumes (default: FP16 shadow)")
     ap.add_argument("--no-autotune", action="store_true", help="built-in launch shapes instead of the autotuner's")
+    ap.add_argument("--no-c5", action="store_true",
+                    help="leave out the learned-warm-start (C5) record that the default 1-GPU run adds to its line")
     ap.add_argument("--no-c3", action="store_true",
                     help="leave out the perspective (C3) record that the default 1-GPU run adds to its line")
     ap.add_argument("--c5-seeds", type=int, default=100, help="held-out series of --workload c5")
@@ -69,6 +71,9 @@ def parse():
     ap.add_argument("--ncu-case", action="store_true",
                     help="small profiling case for ncu: 512x512x256 volume, 8 views, one SART iteration "
                          "launched kernel by kernel, then per-kernel times of the unfused kernels")
+    ap.add_argument("--warmstart-case", action="store_true",
+                    help="profiling case of the learned warm start: three inferences of the trained network on a "
+                         "256x256x128 volume (one 3-iteration SART volume of a held-out series)")
     ap.add_argument("--ncu-res", default="512,512,256",
                     help="volume of the --ncu-case (x,y,z; the detector is x by y)")
     return ap.parse_args()
@@ -240,13 +245,13 @@ def fused_moved_bytes():
 
 
 def source_key() -> str:
-    """Hash of the CUDA sources that define the kernels: a DRAM-traffic figure recorded
-    from an ncu capture is used only while the library is built from the same sources."""
+    """Hash of the CUDA source that defines the reconstruction kernels: a DRAM-traffic
+    figure recorded from an ncu capture is used only while the kernels are built from the
+    same source."""
     import hashlib
     h = hashlib.sha256()
-    for f in ("kernels.cuh", "etcu_api.cu"):
-        with open(os.path.join(ROOT, "ettention_b200", "csrc", f), "rb") as fh:
-            h.update(fh.read())
+    with open(os.path.join(ROOT, "ettention_b200", "csrc", "kernels.cuh"), "rb") as fh:
+        h.update(fh.read())
     return h.hexdigest()[:16]
 
 
@@ -532,6 +537,15 @@ def run_ours(args, rank, world, local):
     # ---- the perspective workload's record (1 GPU only): its own clocks, roofline and
     # CPU sample, in the same line ----
     ctx.close()
+    # ---- the learned warm start against plain SART (1 GPU only): 20 held-out series ----
+    c5 = None
+    if rank == 0 and world == 1 and not args.no_c5:
+        torch.cuda.empty_cache()
+        try:
+            c5 = run_c5(argparse.Namespace(**{**vars(args), "c5_seeds": min(args.c5_seeds, 20), "warmup": 3}))
+            c5.pop("per_seed", None)
+        except Exception as exc:  # the headline line is printed either way
+            c5 = {"error": f"{type(exc).__name__}: {exc}"}
     c3 = None
     if rank == 0 and world == 1 and not args.no_c3:
         torch.cuda.empty_cache()
@@ -557,7 +571,7 @@ def run_ours(args, rank, world, local):
                          "fp_steps_source": "entry and exit voxels of every ray of the 61 views"},
                 "residual_sq": {"before": d0, "after_warmup_and_timed": d1},
                 "c3": c3,
-                "learned_warm_start": "not built: plain SART only"}
+                "c5": c5}
         print(json.dumps(line), flush=True)
 
 
@@ -1017,8 +1031,40 @@ def run_blobs(args):
         "residual_sq_last_iteration": rsq, "clocks": clk.summary()}))
 
 
+def run_warmstart_case():
+    """Three inferences of the trained warm-start network on one held-out 3-iteration SART
+    volume (the case the convolution kernels are profiled on)."""
+    import torch
+    from ettention_b200 import warmstart as W
+    from ettention_b200.learned import WarmStartNet, load_weights
+    from ettention_b200.operators import Context
+    params, scale, _ = load_weights()
+    ctx = Context(0)
+    s = W.make_series(ctx, W.HELDOUT_SEED0)
+    v3, = W.sart_pair(ctx, s, stops=(W.INPUT_ITERS,))
+    net = WarmStartNet(ctx, W.RES, params=params, scale=scale)
+    x = v3[None].contiguous()
+    y = torch.empty_like(x)
+    stream = torch.cuda.ExternalStream(ctx.stream_handle)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for i in range(3):
+        if i == 2:
+            e0.record(stream)
+        net.infer(x, y)
+    e1.record(stream)
+    e1.synchronize()
+    net.check()
+    print(json.dumps({"warmstart_case": "256x256x128, one held-out 3-iteration SART volume",
+                      "infer_ms": e0.elapsed_time(e1), "flops": warmstart_flops(W.RES)}))
+    net.close()
+    ctx.close()
+
+
 def main():
     args = parse()
+    if args.warmstart_case:
+        run_warmstart_case()
+        return
     if args.ncu_case:
         run_ncu_case(tuple(int(v) for v in args.ncu_res.split(",")))
         return
