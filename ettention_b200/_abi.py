@@ -124,6 +124,10 @@ _SIG = {
     "etcu_recon_data_residual_sq": (_S, [_P, ctypes.POINTER(ctypes.c_double)]),
     "etcu_recon_view_order": (_S, [_P, _P, _U, ctypes.POINTER(_U)]),
     "etcu_recon_launches_per_iteration": (_U, [_P]),
+    "etcu_recon_block_count": (_S, [_P, ctypes.POINTER(_U), ctypes.POINTER(_U)]),
+    "etcu_recon_set_complete_bbox": (_S, [_P, _P, _P]),
+    "etcu_recon_slab_forward": (_S, [_P, _U, _P]),
+    "etcu_recon_slab_backward": (_S, [_P, _U, _P]),
     "etcu_recon_profile_iteration": (_S, [_P, ctypes.POINTER(_F), ctypes.POINTER(_F), ctypes.POINTER(_U),
                                          ctypes.POINTER(_U)]),
     "etcu_recon_profile_steps": (_S, [_P, _P, _P, _P, _U, ctypes.POINTER(_U)]),

@@ -72,6 +72,7 @@ struct etcu_recon {
     etcu_context* ctx = nullptr;
     etcu_recon_params params{};
     uint32_t n_input = 0, W = 0, H = 0;
+    std::vector<etcu_view> hviews;  // the input views (the slab decomposition recomputes their LOC length)
     std::vector<uint32_t> order;
     uint32_t block = 1, nblocks = 0;
     float* d_proj = nullptr;
@@ -1695,6 +1696,7 @@ etcu_status recon_build(etcu_volume* vol, const etcu_view* views, uint32_t n_vie
             vc[sl * n_views + i] = make_view_const(views[i], vol->slabs[sl], loc);
         }
     r->hvc = vc;
+    r->hviews.assign(views, views + n_views);
     r->row_const.resize(n_views);
     for (uint32_t i = 0; i < n_views; ++i) r->row_const[i] = row_constant(vc[i]) ? 1 : 0;
     r->fp_paths.resize(S);
@@ -1830,6 +1832,103 @@ extern "C" etcu_status etcu_recon_run(etcu_recon* r, uint32_t iterations) {
     }
     CKL(ctx);
     return check_fused_waits(r);
+}
+
+// =============================================================== z-slab decomposition over ranks
+// Residual of one block from the all-reduced (virtual, traversal) images: the epilogue of
+// the final sub-volume's forward projection (fp_store, kFpPairResidual: long-object
+// compensation over the complete volume, r = b - Ax) written as (r, L) pairs into the
+// block's slot images, and sum r^2 (FP64, one atomic per warp).
+__global__ void slab_residual_kernel(const float* __restrict__ complete, float2* rl, size_t rl_pitch, size_t rl_slot,
+                                     const float* __restrict__ real, const ViewConst* __restrict__ views,
+                                     const uint32_t* __restrict__ order, uint32_t first, int W, int H, int loc,
+                                     double* resid_sq) {
+    const int p = blockIdx.z, gy = blockIdx.y, gx = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t vid = order[first + p];
+    double r2 = 0.0;
+    if (gx < W) {
+        const size_t P = (size_t)W * H, i = (size_t)gy * W + gx;
+        float vv = complete[(size_t)p * 2 * P + i], ll = complete[((size_t)p * 2 + 1) * P + i];
+        if (loc) {  // VirtualProjection.cl:8-9
+            const float c = views[vid].loc_length;
+            vv = ll > kEps ? fdiv(fmul(vv, c), ll) : 0.f;
+            ll = c;
+        }
+        const float r = fsub(real[(size_t)vid * P + i], vv);  // Compare.cl:8
+        rl[(size_t)p * rl_slot + (size_t)gy * rl_pitch + gx] = make_float2(r, ll);
+        r2 = (double)r * (double)r;
+    }
+    for (int o = 16; o > 0; o >>= 1) r2 += __shfl_down_sync(0xffffffffu, r2, o);
+    if ((threadIdx.x & 31) == 0 && r2 != 0.0) atomicAdd(resid_sq, r2);
+}
+
+extern "C" etcu_status etcu_recon_block_count(const etcu_recon* r, uint32_t* blocks, uint32_t* block_size) {
+    if (!r || !blocks) return fail(nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    *blocks = r->nblocks;
+    if (block_size) *block_size = r->block;
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_recon_set_complete_bbox(etcu_recon* r, const float bbox_min[3], const float bbox_max[3]) {
+    if (!r || !bbox_min || !bbox_max) return fail(r ? r->ctx : nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    etcu_context* ctx = r->ctx;
+    if (!r->params.use_long_object_compensation) return ETCU_OK;
+    const uint32_t S = (uint32_t)r->vol->slabs.size();
+    for (uint32_t sl = 0; sl < S; ++sl)
+        for (uint32_t i = 0; i < r->n_input; ++i)
+            r->hvc[(size_t)sl * r->n_input + i].loc_length = traversal_length(r->hviews[i], bbox_min, bbox_max);
+    CK(ctx, cudaMemcpyAsync(r->d_views, r->hvc.data(), r->hvc.size() * sizeof(ViewConst), cudaMemcpyHostToDevice,
+                            ctx->stream));
+    CK(ctx, cudaStreamSynchronize(ctx->stream));
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_recon_slab_forward(etcu_recon* r, uint32_t block, float* d_partial) {
+    if (!r || !d_partial) return fail(r ? r->ctx : nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    etcu_context* ctx = r->ctx;
+    if (block >= r->nblocks) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "block %u of %u", block, r->nblocks);
+    const uint32_t M = (uint32_t)r->order.size(), first = block * r->block;
+    const uint32_t count = std::min(r->block, M - first);
+    const size_t P = (size_t)r->W * r->H;
+    cudaStream_t st = ctx->stream;
+    if (block == 0) CK(ctx, cudaMemsetAsync(r->d_resid, 0, sizeof(double), st));
+    CK(ctx, cudaMemsetAsync(d_partial, 0, (size_t)count * 2 * P * sizeof(float), st));
+    etcu_volume* vol = r->vol;
+    for (uint32_t k = 0; k < count; ++k)
+        for (uint32_t sl = 0; sl < (uint32_t)vol->slabs.size(); ++sl) {
+            const SlabConst& slab = vol->slabs[sl];
+            FpArgs a{};
+            fill_fp_volume_ptrs(vol, slab, a);
+            a.slab = slab;
+            a.views = r->d_views + (size_t)sl * r->n_input;
+            a.order = r->d_order;
+            a.first = first + k;
+            a.W = (int)r->W;
+            a.H = (int)r->H;
+            a.samples = r->params.fp_samples == 0 ? 1 : (int)r->params.fp_samples;
+            a.mode = kFpSeparateAccumulate;  // partial line integrals of this rank's slab, added (+=)
+            a.out_v = d_partial + (size_t)k * 2 * P;
+            a.out_l = d_partial + ((size_t)k * 2 + 1) * P;
+            launch_fp(vol, a, r->fp_paths[sl], 1, st);
+        }
+    CKL(ctx);
+    return ETCU_OK;
+}
+
+extern "C" etcu_status etcu_recon_slab_backward(etcu_recon* r, uint32_t block, const float* d_complete) {
+    if (!r || !d_complete) return fail(r ? r->ctx : nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    etcu_context* ctx = r->ctx;
+    if (block >= r->nblocks) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "block %u of %u", block, r->nblocks);
+    const uint32_t M = (uint32_t)r->order.size(), first = block * r->block;
+    const uint32_t count = std::min(r->block, M - first);
+    cudaStream_t st = ctx->stream;
+    const dim3 grid((r->W + 127) / 128, r->H, count);
+    slab_residual_kernel<<<grid, 128, 0, st>>>(d_complete, r->rl, r->rl_pitch, r->rl_slot, r->d_proj, r->d_views,
+                                               r->d_order, first, (int)r->W, (int)r->H,
+                                               r->params.use_long_object_compensation ? 1 : 0, r->d_resid);
+    issue_backward(r, first, count, st);
+    CKL(ctx);
+    return ETCU_OK;
 }
 
 extern "C" etcu_status etcu_recon_last_residual_sq(etcu_recon* r, double* out) {

@@ -10,9 +10,14 @@ forms the residual b - Ax (with long-object compensation when enabled), and each
 back projects its own slab with lambda / blockSize.  The only data exchange is that
 all-reduce: B x 2 x H x W floats per block.
 
-The driver is written against an engine (a rank's slab and its operators) so that the
-same loop runs on CUDA (`CudaSlabEngine`, one GPU per rank, NCCL) and, in tests, on a
-CPU restatement with the gloo backend.
+`CudaSlabReconstruction` runs this on the GPU through the block-step C ABI
+(etcu_recon_slab_forward / etcu_recon_slab_backward): per block one stream-ordered forward
+projection of the slab into a device buffer, the NCCL all-reduce of that buffer enqueued
+on the library's stream, and one stream-ordered residual + back projection -- no host
+synchronisation inside an iteration.  `SlabDecomposedReconstruction` is the same loop
+written against an engine (a rank's slab and its operators), which runs on CUDA
+(`CudaSlabEngine`, operator by operator) and, in tests, on a CPU restatement with the gloo
+backend.
 """
 from typing import List, Optional, Sequence, Tuple
 
@@ -156,3 +161,73 @@ class SlabDecomposedReconstruction:
     def runNiterations(self, n: int) -> None:
         for _ in range(int(n)):
             self.runSingleIteration()
+
+
+class CudaSlabReconstruction:
+    """This rank's z-slab of one volume, reconstructed with the block-step C ABI.
+
+    Every rank holds the whole tilt series; rank r owns slab r of the reference's split.
+    Per block: etcu_recon_slab_forward adds the slab's line integrals and ray lengths of
+    the block's views into a (B, 2, H, W) device buffer, `torch.distributed.all_reduce`
+    sums it over the ranks on the library's stream (NCCL when the process group uses it),
+    and etcu_recon_slab_backward forms b - Ax (long-object compensation over the complete
+    volume) and back projects the block into the slab with lambda / B."""
+
+    def __init__(self, ctx, resolution, bbox_min, bbox_max, rank: int, world: int, geometries,
+                 projections: np.ndarray, params, voxel_type: int = 0):
+        import ctypes
+        import torch
+        from .operators import BlockIterativeReconstructionOperator, GPUMappedVolume
+        self.torch = torch
+        self.ctx = ctx
+        self.rank, self.world = rank, world
+        z0, rz, lo, hi = slab_split(resolution, bbox_min, bbox_max, world)[rank]
+        self.z0, self.rz = z0, rz
+        self.volume = GPUMappedVolume(ctx, (int(resolution[0]), int(resolution[1]), rz), lo, hi, voxel_type=voxel_type)
+        self.rec = BlockIterativeReconstructionOperator(self.volume, geometries, projections, params, use_graph=False)
+        h = self.rec.handle
+        bmin = (ctypes.c_float * 3)(*[float(v) for v in bbox_min])
+        bmax = (ctypes.c_float * 3)(*[float(v) for v in bbox_max])
+        ctx.check(_abi.lib().etcu_recon_set_complete_bbox(h, bmin, bmax))
+        nb, bs = ctypes.c_uint32(), ctypes.c_uint32()
+        ctx.check(_abi.lib().etcu_recon_block_count(h, ctypes.byref(nb), ctypes.byref(bs)))
+        self.blocks, self.block_size = nb.value, bs.value
+        self.views = len(self.rec.view_order())
+        H, W = int(projections.shape[1]), int(projections.shape[2])
+        self.buf = torch.zeros((self.block_size, 2, H, W), dtype=torch.float32, device=torch.device("cuda", ctx.device))
+        torch.cuda.synchronize(self.buf.device)
+        self.stream = torch.cuda.ExternalStream(ctx.stream_handle)
+
+    def block_views(self, b: int) -> int:
+        return min(self.block_size, self.views - b * self.block_size)
+
+    def block_forward(self, b: int) -> None:
+        """This slab's partial (virtual, traversal) images of block b into ``buf``."""
+        self.ctx.check(_abi.lib().etcu_recon_slab_forward(self.rec.handle, int(b), self.buf.data_ptr()))
+
+    def block_backward(self, b: int) -> None:
+        """Residual from the complete images in ``buf`` and back projection into the slab."""
+        self.ctx.check(_abi.lib().etcu_recon_slab_backward(self.rec.handle, int(b), self.buf.data_ptr()))
+
+    def runSingleIteration(self) -> None:
+        for b in range(self.blocks):
+            self.block_forward(b)
+            if self.world > 1:
+                import torch.distributed as dist
+                with self.torch.cuda.stream(self.stream):
+                    dist.all_reduce(self.buf[:self.block_views(b)], op=dist.ReduceOp.SUM)
+            self.block_backward(b)
+
+    def runNiterations(self, n: int) -> None:
+        for _ in range(int(n)):
+            self.runSingleIteration()
+
+    def last_residual_sq(self) -> float:
+        return self.rec.last_residual_sq()
+
+    def download(self) -> np.ndarray:
+        return self.volume.download()
+
+    def close(self) -> None:
+        self.rec.close()
+        self.volume.close()

@@ -252,6 +252,25 @@ ETCU_API etcu_status etcu_recon_profile_steps(etcu_recon* rec, float* ms, uint32
 /* Kernel launches one iteration issues (graph nodes when captured). */
 ETCU_API uint32_t etcu_recon_launches_per_iteration(const etcu_recon* rec);
 
+/* One volume over several GPUs by z-slabs (one process per GPU; the reference's
+ * sub-volume split, LR/model/volume/VolumeProperties.cpp:74-98, with one slab per rank):
+ * `rec` reconstructs this rank's slab (a volume of the slab's resolution and bounding
+ * box).  Per block b of etcu_recon_block_count():
+ *   etcu_recon_slab_forward(rec, b, d_partial)   this slab's line integrals and lengths of
+ *       the block's views, added into zeroed d_partial: count x 2 x height x width floats
+ *       ((virtual, traversal) per view; the forward projections' += of
+ *       ParallelBeamsForwardProjection.cl:56-57 across slabs)
+ *   all-reduce (sum) of d_partial over the ranks, on the context's stream
+ *   etcu_recon_slab_backward(rec, b, d_complete) residual b - Ax (long-object compensation
+ *       over the complete volume, etcu_recon_set_complete_bbox) and the back projection of
+ *       the block on this slab with lambda / block size.
+ * Stream-ordered, no host synchronisation; the residual sum of the sweep is
+ * etcu_recon_last_residual_sq (reset by block 0's forward call). */
+ETCU_API etcu_status etcu_recon_block_count(const etcu_recon* rec, uint32_t* blocks, uint32_t* block_size);
+ETCU_API etcu_status etcu_recon_set_complete_bbox(etcu_recon* rec, const float bbox_min[3], const float bbox_max[3]);
+ETCU_API etcu_status etcu_recon_slab_forward(etcu_recon* rec, uint32_t block, float* d_partial);
+ETCU_API etcu_status etcu_recon_slab_backward(etcu_recon* rec, uint32_t block, const float* d_complete);
+
 /* One-call host-buffer reconstruction: upload projections and initial volume,
  * run `iterations`, download the result (the path a frontend's "ettention --config" run takes). */
 ETCU_API etcu_status etcu_reconstruct(etcu_context* ctx, const etcu_volume_desc* desc, etcu_voxel_type type,
