@@ -138,6 +138,7 @@ _SIG = {
     "etcu_mrc_read_stack": (_S, [ctypes.c_char_p, _I, _P, ctypes.c_size_t]),
     "etcu_read_tilt_angles": (_S, [ctypes.c_char_p, _P, _U, ctypes.POINTER(_U)]),
     "etcu_mrc_write_volume": (_S, [ctypes.c_char_p, _P, _P, _I]),
+    "etcu_mrc_write_volume_typed": (_S, [ctypes.c_char_p, _P, _P, _I, _I, _I]),
     "etcu_tiff_read_info": (_S, [ctypes.c_char_p, _U, ctypes.POINTER(ImageInfo)]),
     "etcu_tiff_read": (_S, [ctypes.c_char_p, _U, _P, ctypes.c_size_t]),
     "etcu_tiff_write": (_S, [ctypes.c_char_p, _P, _U, _U]),

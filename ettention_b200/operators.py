@@ -163,13 +163,22 @@ def read_tilt_angles(path: str) -> List[float]:
     return [float(a) for a in out[: n.value]]
 
 
-def write_mrc_volume(path: str, volume: np.ndarray, orientation: str = "xzy") -> None:
-    """VolumeFileFormatWriter + MRCWriter, float32: ``volume`` is (z, y, x); orientation
-    'xzy' (the reference's default output.options.orientation) or 'xyz'."""
+OUTPUT_VOXEL_TYPES = {"unsigned8": 0, "signed16": 1, "float32": 2, "unsigned16": 6}
+
+
+def write_mrc_volume(path: str, volume: np.ndarray, orientation: str = "xzy", voxel_type: str = "float32",
+                     invert: bool = False) -> None:
+    """VolumeFileFormatWriter + MRCWriter: ``volume`` is (z, y, x); orientation 'xzy' (the
+    reference's default output.options.orientation) or 'xyz'; voxel_type one of
+    output.options.voxelType's values (IOEnumerations.cpp:39-61: unsigned8, unsigned16,
+    signed16, float32); invert = output.options.invert."""
+    if voxel_type not in OUTPUT_VOXEL_TYPES:
+        raise EttentionError(_abi.ERR_INVALID_ARGUMENT, "ParseVoxelValueType: Unknown file mode ")
     v = np.ascontiguousarray(volume, np.float32)
     res = np.array([v.shape[2], v.shape[1], v.shape[0]], np.uint32)
     axes = {"xyz": _abi.AXES_XYZ, "xzy": _abi.AXES_XZY}[orientation.lower()]
-    _check_free(lib().etcu_mrc_write_volume(str(path).encode(), v.ctypes.data, res.ctypes.data, axes))
+    _check_free(lib().etcu_mrc_write_volume_typed(str(path).encode(), v.ctypes.data, res.ctypes.data, axes,
+                                                  OUTPUT_VOXEL_TYPES[voxel_type], int(bool(invert))))
 
 
 def read_tiff(path: str, page: int = 0) -> np.ndarray:
@@ -386,8 +395,9 @@ def reconstruct_from_config(config, device: int = 0, write_output: bool = True) 
     volume.initFileOrientation, XZY by default; BlockIterativeConfiguration.cpp:36-40,
     :155-198) and priorknowledge.maskVolumeFilename (MRC read in file order, values
     cast to 8 bits; :46-50), the iterations of BlockIterativeReconstructionOperator
-    on the GPU (or, for algorithm "wbp", the WBP plugin's weighted back projection), and Framework::writeFinalVolume to output.filename (float32 MRC,
-    output.options.orientation xyz_order or xzy_order, XZY by default).  Returns the
+    on the GPU (or, for algorithm "wbp", the WBP plugin's weighted back projection), and Framework::writeFinalVolume to output.filename (MRC of output.options.voxelType with
+    output.options.invert, output.options.orientation xyz_order or xzy_order, XZY by
+    default).  Returns the
     (z, y, x) volume."""
     cfg = config.config() if isinstance(config, XMLParameterSource) else dict(config)
     p = AlgebraicParameterSet.from_config(cfg)
@@ -396,10 +406,9 @@ def reconstruct_from_config(config, device: int = 0, write_output: bool = True) 
     if "input.projections" not in cfg:
         raise EttentionError(_abi.ERR_INVALID_ARGUMENT, "xml config file entry does not exist: input.projections")
     vt = cfg.get("output.options.voxelType", "float32")
-    if write_output and "output.filename" in cfg and vt != "float32":
-        raise EttentionError(_abi.ERR_UNSUPPORTED, f"output.options.voxelType {vt}: only float32 is written")
-    if _true(cfg.get("output.options.invert", "false")):
-        raise EttentionError(_abi.ERR_UNSUPPORTED, "output.options.invert is not supported")
+    if vt not in OUTPUT_VOXEL_TYPES:  # OutputParameterSet.cpp:29-33
+        raise EttentionError(_abi.ERR_INVALID_ARGUMENT, "ParseVoxelValueType: Unknown file mode ")
+    invert = _true(cfg.get("output.options.invert", "false"))
     out_order = _coordinate_order(cfg.get("output.options.orientation", "xzy_order"))
     if write_output and "output.filename" in cfg and out_order not in ("xyz", "xzy"):
         raise EttentionError(_abi.ERR_UNSUPPORTED, f"output orientation {out_order}: XYZ and XZY are written")
@@ -435,7 +444,7 @@ def reconstruct_from_config(config, device: int = 0, write_output: bool = True) 
         if isinstance(stack, ImageStackDirectoryDatasource):
             stack.close()
     if write_output and "output.filename" in cfg:
-        write_mrc_volume(cfg["output.filename"], v, out_order)
+        write_mrc_volume(cfg["output.filename"], v, out_order, vt, invert)
     return v
 
 

@@ -301,9 +301,25 @@ ETCU_API etcu_status etcu_read_tilt_angles(const char* path, float* out, uint32_
  * stores y as the file's sections and z as its rows. */
 typedef enum { ETCU_AXES_XYZ = 0, ETCU_AXES_XZY = 1 } etcu_orientation;
 /* VolumeFileFormatWriter / MRCWriter with output.options.voxelType float32: mode-2 MRC
- * with min / max / mean in the header; volume is x fastest, then y, then z. */
+ * with min / max / mean in the header (VolumeStatistics::compute); volume is x fastest,
+ * then y, then z. */
 ETCU_API etcu_status etcu_mrc_write_volume(const char* path, const float* volume, const uint32_t resolution[3],
                                            etcu_orientation orientation);
+/* output.options.voxelType (LR/setup/parameterset/IOEnumerations.h:8-13, the MRC mode). */
+typedef enum {
+    ETCU_OUT_UNSIGNED_8 = 0,
+    ETCU_OUT_SIGNED_16 = 1,
+    ETCU_OUT_FLOAT_32 = 2,
+    ETCU_OUT_UNSIGNED_16 = 6
+} etcu_output_voxel_type;
+/* VolumeFileFormatWriter::write with output.options.voxelType and output.options.invert
+ * (LR/io/serializer/VolumeFileFormatWriter.cpp:11-140, LinearRangeTransformation.cpp):
+ * integer types map [min, max] of the volume linearly onto the type's range (reversed
+ * with invert) and are C-cast; float32 is written as is (with invert the header's
+ * min / max / mean are mapped onto [max, min], the data are not). */
+ETCU_API etcu_status etcu_mrc_write_volume_typed(const char* path, const float* volume, const uint32_t resolution[3],
+                                                 etcu_orientation orientation, etcu_output_voxel_type voxel_type,
+                                                 int invert);
 
 /* TIFF images (LR/io/deserializer/ImageDeserializer.cpp:10-62, replacing FreeImage):
  * grey, one sample per pixel, 8 / 16-bit unsigned or 32-bit float samples, converted

@@ -553,11 +553,13 @@ private:
     std::vector<float> angles_;
 };
 
-// VolumeFileFormatWriter + MRCWriter, float32 (x fastest, then y, then z); XZY is the
-// reference's default output.options.orientation.
+// VolumeFileFormatWriter + MRCWriter (x fastest, then y, then z); XZY is the reference's
+// default output.options.orientation, float32 its default output.options.voxelType.
 inline void writeMrcVolume(const std::string& path, const float* volume, const std::array<uint32_t, 3>& resolution,
-                           etcu_orientation orientation = ETCU_AXES_XZY) {
-    check(etcu_mrc_write_volume(path.c_str(), volume, resolution.data(), orientation), nullptr);
+                           etcu_orientation orientation = ETCU_AXES_XZY,
+                           etcu_output_voxel_type voxelType = ETCU_OUT_FLOAT_32, bool invert = false) {
+    check(etcu_mrc_write_volume_typed(path.c_str(), volume, resolution.data(), orientation, voxelType, invert ? 1 : 0),
+          nullptr);
 }
 
 // ImageDeserializer::readImage / readImageFromStack: one page as height x width floats.

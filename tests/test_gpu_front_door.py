@@ -82,3 +82,30 @@ def test_reference_parameter_files_reconstruct_within_bounds(dataset, name):
     assert np.array_equal(written, np.transpose(v, (1, 0, 2)))  # XZY: sections are y
     rms = O.max_slice_rms(written, truth)
     assert rms <= limit, rms
+
+
+@pytest.mark.parametrize("vt,invert,dtype", [("unsigned16", "true", np.uint16), ("unsigned8", "false", np.uint8)])
+def test_parameter_file_output_voxel_type_and_invert(dataset, vt, invert, dtype):
+    """output.options.voxelType / invert through the front door: the written file is the
+    reconstruction mapped onto the type's range (reversed with invert) in XZY order."""
+    from ettention_b200.operators import XMLParameterSource, reconstruct_from_config
+    body, _ = CONFIGS["sart"]
+    xml = dataset / f"out_{vt}.xml"
+    xml.write_text('<?xml version="1.0"?>\n' + body + '<input><projections value="."/></input>'
+                   f'<output><filename value="out/typed_{vt}.mrc"/>'
+                   f'<options><voxelType value="{vt}"/><invert value="{invert}"/></options></output>'
+                   '<volume><dimension value="64 64 64"/><initValue value="0.0"/></volume>')
+    (dataset / "out").mkdir(exist_ok=True)
+    v = reconstruct_from_config(XMLParameterSource(str(xml)))
+    with open(dataset / "out" / f"typed_{vt}.mrc", "rb") as fh:
+        raw = fh.read()
+    mode = int(np.frombuffer(raw[12:16], np.int32)[0])
+    data = np.frombuffer(raw[1024:], dtype).reshape(64, 64, 64)
+    assert mode == {"unsigned16": 6, "unsigned8": 0}[vt]
+    top = int(np.iinfo(dtype).max)
+    lo_voxel, hi_voxel = np.unravel_index(np.argmin(v), v.shape), np.unravel_index(np.argmax(v), v.shape)
+    xzy = lambda i: (i[1], i[0], i[2])  # noqa: E731 (z, y, x) index -> file (y, z, x)
+    if invert == "true":
+        assert data[xzy(lo_voxel)] == top and data[xzy(hi_voxel)] == 0
+    else:
+        assert data[xzy(lo_voxel)] == 0 and data[xzy(hi_voxel)] == top

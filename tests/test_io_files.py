@@ -126,3 +126,92 @@ def test_reference_jason64_stack_and_tilt_file():
         f.seek(1024 + 11520)
         raw = np.frombuffer(f.read(64 * 64 * 90 * 2), np.int16).reshape(90, 64, 64)
     np.testing.assert_allclose(st.load_projections(), log_transform(raw, 1), rtol=2e-7, atol=1e-7)
+
+
+def _reference_statistics(v):
+    """VolumeStatistics::compute (VolumeStatistics.cpp:17-48) in float32: min from FLT_MAX,
+    max from FLT_MIN (the smallest positive normal), NaN skipped, float sum in voxel order
+    times 1 / (float)count."""
+    f = np.float32
+    mn, mx, s = f(np.finfo(np.float32).max), f(np.finfo(np.float32).tiny), f(0.0)
+    for x in v.reshape(-1):
+        if np.isnan(x):
+            continue
+        mn = min(mn, x)
+        mx = max(mx, x)
+        s = f(s + x)
+    return mn, mx, f(s * f(f(1.0) / f(v.size)))
+
+
+def _linear(v, smin, smax, lo, hi):
+    """LinearRangeTransformation::transformRange, float32 step by step."""
+    f = np.float32
+    a = (np.asarray(v, f) - f(smin)).astype(f)
+    b = (a / f(f(smax) - f(smin))).astype(f)
+    c = (b * f(f(hi) - f(lo))).astype(f)
+    return (c + f(lo)).astype(f)
+
+
+def _mrc_writer_volume():
+    """MRCWriterTest's volume (test/src/unit/io/MRCWriterTest.cpp:35-42): 16^3 zeros with
+    four voxels set, (z, y, x)."""
+    v = np.zeros((16, 16, 16), np.float32)
+    v[0, 0, 0], v[0, 0, 15], v[0, 15, 0], v[15, 0, 0] = 1.0, 2.0, 3.0, 4.0
+    return v
+
+
+def _read_mrc(path):
+    with open(path, "rb") as fh:
+        raw = fh.read()
+    hdr = np.frombuffer(raw[:1024], np.uint8)
+    nx, ny, nz, mode = np.frombuffer(hdr[:16].tobytes(), np.int32)
+    dmin, dmax, dmean = np.frombuffer(hdr[76:88].tobytes(), np.float32)
+    dt = {0: np.uint8, 1: np.int16, 2: np.float32, 6: np.uint16}[int(mode)]
+    data = np.frombuffer(raw[1024:], dt).reshape(nz, ny, nx)
+    return int(mode), (dmin, dmax, dmean), data, raw[208:212]
+
+
+@pytest.mark.parametrize("vt,mode,lo,hi,dtype", [("unsigned8", 0, 0.0, 255.0, np.uint8),
+                                                 ("unsigned16", 6, 0.0, 65535.0, np.uint16),
+                                                 ("signed16", 1, -32768.0, 32767.0, np.int16)])
+@pytest.mark.parametrize("invert", [False, True])
+def test_volume_writer_integer_types_follow_range_transformation(tmp_path, vt, mode, lo, hi, dtype, invert):
+    """The MRCWriterTest cases (unsigned 8 / 16, signed 16, inverted): the volume's
+    [min, max] mapped linearly onto the type's range (reversed with invert), C-cast, and
+    the header's min / max / mean transformed the same way."""
+    from ettention_b200.operators import write_mrc_volume
+    v = _mrc_writer_volume()
+    v[3, 4, 5] = -1.5  # a negative voxel so that the range does not start at zero
+    path = tmp_path / "t.mrc"
+    write_mrc_volume(str(path), v, "xyz", vt, invert)
+    got_mode, hdr, data, tag = _read_mrc(path)
+    mn, mx, mean = _reference_statistics(v)
+    out_lo, out_hi = (hi, lo) if invert else (lo, hi)
+    want = np.trunc(_linear(v, mn, mx, out_lo, out_hi)).astype(dtype)
+    assert got_mode == mode and tag == b"MAP "
+    assert np.array_equal(data, want)
+    assert hdr == tuple(_linear(np.array([mn, mx, mean]), mn, mx, out_lo, out_hi))
+    assert data.max() == int(hi) and data.min() == int(lo)
+
+
+def test_volume_writer_float32_statistics_and_inverted_header(tmp_path):
+    """float32 (MRCWriterTest Test_Float32 / Test_Float_32_Inverted): data as is; the
+    header carries the reference's statistics -- with invert mapped onto [max, min] while
+    the data stay untransformed -- and the XZY order puts y in the sections."""
+    from ettention_b200.operators import write_mrc_volume
+    v = -np.abs(_mrc_writer_volume()) - 0.25  # all negative: max stays FLT_MIN in the reference
+    for invert in (False, True):
+        path = tmp_path / f"f{int(invert)}.mrc"
+        write_mrc_volume(str(path), v, "xzy", "float32", invert)
+        mode, hdr, data, _ = _read_mrc(path)
+        mn, mx, mean = _reference_statistics(v)
+        assert mode == 2 and np.array_equal(data, np.transpose(v, (1, 0, 2)))
+        assert mx == np.finfo(np.float32).tiny
+        want = (mn, mx, mean) if not invert else tuple(_linear(np.array([mn, mx, mean]), mn, mx, mx, mn))
+        assert hdr == want
+
+
+def test_volume_writer_rejects_unknown_voxel_type(tmp_path):
+    from ettention_b200.operators import EttentionError, write_mrc_volume
+    with pytest.raises(EttentionError, match="Unknown file mode"):
+        write_mrc_volume(str(tmp_path / "x.mrc"), np.zeros((2, 2, 2), np.float32), "xyz", "float64")
