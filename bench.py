@@ -57,6 +57,9 @@ def parse():
     ap.add_argument("--e2e-reps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--c4-f32", action="store_true", help="--workload c4 with FP32 volumes (default: FP16 shadow)")
+    ap.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"],
+                    help="headline workload's storage: f32, or an FP32 master volume with an FP16 / BF16 shadow and "
+                         "the tilt series stored in the same 16-bit format")
     ap.add_argument("--no-autotune", action="store_true", help="built-in launch shapes instead of the autotuner's")
     ap.add_argument("--no-c5", action="store_true",
                     help="leave out the learned-warm-start (C5) record that the default 1-GPU run adds to its line")
@@ -377,7 +380,7 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def run_e2e(args, ctx, geoms, b, params, world, lib_stream):
+def run_e2e(args, ctx, geoms, b, params, world, lib_stream, vol_type=0):
     """30 iterations through etcu_reconstruct with pinned host buffers (in and out)."""
     import torch
     from ettention_b200 import _abi
@@ -403,7 +406,7 @@ def run_e2e(args, ctx, geoms, b, params, world, lib_stream):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(lib_stream)
-        ctx.check(lib().etcu_reconstruct(ctx.handle, ctypes.byref(desc), _abi.VOXEL_FLOAT32, views, N_VIEWS,
+        ctx.check(lib().etcu_reconstruct(ctx.handle, ctypes.byref(desc), vol_type, views, N_VIEWS,
                                          host_proj.data_ptr(), ctypes.byref(rp), TARGET_ITERS, host_vol.data_ptr()))
         e1.record(lib_stream)
         torch.cuda.synchronize()
@@ -443,9 +446,11 @@ def run_ours(args, rank, world, local):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu_problem = cpu_sample_problem(phantom)
     del phantom
+    vt, ps = {"f32": (_abi.VOXEL_FLOAT32, _abi.PROJ_F32), "f16": (_abi.VOXEL_F16_MASTER, _abi.PROJ_F16),
+              "bf16": (_abi.VOXEL_BF16_MASTER, _abi.PROJ_BF16)}[args.storage]
     params = AlgebraicParameterSet(algorithm="sart", block_size=1, iterations=TARGET_ITERS, lam=LAMBDA,
-                                   order=_abi.ORDER_IDENTITY)
-    vol = GPUMappedVolume(ctx, RES)
+                                   order=_abi.ORDER_IDENTITY, projection_storage=ps)
+    vol = GPUMappedVolume(ctx, RES, voxel_type=vt)
     rec = BlockIterativeReconstructionOperator(vol, geoms, b, params, use_graph=True)
     launches_per_iter = rec.launches_per_iteration
     d0 = rec.data_residual_sq()
@@ -526,7 +531,7 @@ def run_ours(args, rank, world, local):
     # ---- e2e: one-call host-buffer reconstruction through the C ABI ----
     e2e = None
     if args.e2e_reps > 0:
-        e2e = run_e2e(args, ctx, geoms, b, params, world, lib_stream)
+        e2e = run_e2e(args, ctx, geoms, b, params, world, lib_stream, vt)
     del b
     # ---- CPU baseline (rank 0, N = 1 only) ----
     cpu = None
@@ -562,7 +567,9 @@ def run_ours(args, rank, world, local):
                 "data": "synthetic (seeded ellipsoid phantom, CUDA-forward-projected, Poisson noise)",
                 "config": {"workload": WORKLOAD, "step": "one SART iteration (61 views, one CUDA graph)",
                            "volume": list(RES), "views": N_VIEWS, "detector": list(DET), "lambda": LAMBDA,
-                           "storage": "f32", "l2": "inputs larger than L2 (1 GiB volume)",
+                           "storage": args.storage if args.storage == "f32" else
+                           f"f32 master + {args.storage} shadow, {args.storage} tilt series",
+                           "l2": "inputs larger than L2 (1 GiB volume)",
                            "parallelism": f"independent series per GPU x{world}"},
                 "e2e": e2e,
                 "gpu_launches": launches_per_iter * args.steps,

@@ -46,7 +46,10 @@ class ReconParams(ctypes.Structure):
     _fields_ = [("lam", ctypes.c_float), ("block_size", ctypes.c_uint32), ("fp_samples", ctypes.c_uint32),
                 ("bp_samples", ctypes.c_uint32), ("use_long_object_compensation", ctypes.c_int32),
                 ("order", ctypes.c_int), ("sampling", ctypes.c_int), ("skip", ctypes.POINTER(ctypes.c_uint32)),
-                ("skip_count", ctypes.c_uint32), ("use_graph", ctypes.c_int32)]
+                ("skip_count", ctypes.c_uint32), ("use_graph", ctypes.c_int32), ("projection_storage", ctypes.c_int)]
+
+
+PROJ_F32, PROJ_F16, PROJ_BF16 = 0, 1, 2
 
 
 class MrcInfo(ctypes.Structure):

@@ -75,8 +75,9 @@ struct etcu_recon {
     std::vector<etcu_view> hviews;  // the input views (the slab decomposition recomputes their LOC length)
     std::vector<uint32_t> order;
     uint32_t block = 1, nblocks = 0;
-    float* d_proj = nullptr;
+    float* d_proj = nullptr;  // measured projections, element type proj_kind (load_real)
     bool own_proj = false;
+    int proj_kind = 0;         // etcu_projection_storage
     ViewConst* d_views = nullptr;
     uint32_t* d_order = nullptr;
     float4* d_samples = nullptr;
@@ -1197,6 +1198,53 @@ extern "C" etcu_status etcu_compute_ray_length(etcu_volume* vol, const etcu_view
 // =============================================================== reconstruction
 namespace {
 
+size_t proj_elem_bytes(int kind) { return kind == ETCU_PROJ_F32 ? sizeof(float) : 2; }
+
+// The tilt series (n floats, from the host or the device) in the given storage: FP32
+// copied as is (or, from the device, used in place when `in_place`), FP16 / BF16 rounded
+// to nearest on the device.  *out receives the buffer (allocated with alloc), *owned
+// whether it must be freed.
+template <typename Alloc>
+etcu_status stage_projections(etcu_context* ctx, const float* host, const float* dev, size_t n, int kind,
+                              bool in_place, Alloc alloc, float** out, bool* owned) {
+    *owned = false;
+    if (kind != ETCU_PROJ_F32 && kind != ETCU_PROJ_F16 && kind != ETCU_PROJ_BF16)
+        return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "unknown projection storage %d", kind);
+    if (kind == ETCU_PROJ_F32 && dev && in_place) {
+        *out = const_cast<float*>(dev);
+        return ETCU_OK;
+    }
+    etcu_status s;
+    void* buf = nullptr;
+    if ((s = alloc(&buf, n * proj_elem_bytes(kind))) != ETCU_OK) return s;
+    *owned = true;
+    *out = (float*)buf;
+    if (kind == ETCU_PROJ_F32) {
+        CK(ctx, cudaMemcpyAsync(buf, host ? (const void*)host : (const void*)dev, n * sizeof(float),
+                                host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, ctx->stream));
+        return ETCU_OK;
+    }
+    const float* src = dev;
+    float* tmp = nullptr;
+    if (host) {
+        if ((s = dalloc(ctx, (void**)&tmp, n * sizeof(float))) != ETCU_OK) return s;
+        CK(ctx, cudaMemcpyAsync(tmp, host, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+        src = tmp;
+    }
+    dim3 g, b;
+    launch_1d_dims(n, g, b);
+    if (kind == ETCU_PROJ_F16)
+        convert_from_float_kernel<__half><<<g, b, 0, ctx->stream>>>(src, (__half*)buf, n);
+    else
+        convert_from_float_kernel<__nv_bfloat16><<<g, b, 0, ctx->stream>>>(src, (__nv_bfloat16*)buf, n);
+    CKL(ctx);
+    if (tmp) {
+        CK(ctx, cudaStreamSynchronize(ctx->stream));
+        dfree(ctx, tmp, n * sizeof(float));
+    }
+    return ETCU_OK;
+}
+
 void recon_free(etcu_recon* r) {
     etcu_context* ctx = r->ctx;
     cudaStreamSynchronize(ctx->stream);
@@ -1204,7 +1252,7 @@ void recon_free(etcu_recon* r) {
     if (r->graph) cudaGraphDestroy(r->graph);
     for (auto t : r->texs) cudaDestroyTextureObject(t);
     size_t N = r->n_input;
-    if (r->own_proj) dfree(ctx, r->d_proj, N * (size_t)r->W * r->H * sizeof(float));
+    if (r->own_proj) dfree(ctx, r->d_proj, N * (size_t)r->W * r->H * proj_elem_bytes(r->proj_kind));
     dfree(ctx, r->d_views, N * sizeof(ViewConst) * r->vol->slabs.size());
     dfree(ctx, r->d_order, r->order.size() * sizeof(uint32_t));
     dfree(ctx, r->d_samples, N * r->nsamples * sizeof(float4));
@@ -1241,6 +1289,7 @@ uint32_t issue_forward(etcu_recon* r, uint32_t first, uint32_t count, cudaStream
         a.rl_pitch = r->rl_pitch;
         a.rl_slot = r->rl_slot;
         a.real = r->d_proj;
+        a.real_kind = r->proj_kind;
         a.resid_sq = r->d_resid;
         launch_fp(vol, a, r->fp_paths[s], count, st);
     }
@@ -1310,6 +1359,7 @@ void launch_fused_step(etcu_recon* r, uint32_t p, cudaStream_t st) {
     a.ntaps = r->fuse_ntaps[vb];
     a.jrange = r->d_jrange;
     a.real = r->d_proj;
+    a.real_kind = r->proj_kind;
     a.resid_sq = r->d_resid;
     a.loc = r->params.use_long_object_compensation ? 1 : 0;
     const size_t smem = fuse_smem_bytes(g.rx, g.rz, a.ntaps);
@@ -1338,6 +1388,7 @@ void launch_fused_persistent(etcu_recon* r, cudaStream_t st) {
     a.lambda = r->params.lambda;
     a.jrange = r->d_jrange;
     a.real = r->d_proj;
+    a.real_kind = r->proj_kind;
     a.resid_sq = r->d_resid;
     a.loc = r->params.use_long_object_compensation ? 1 : 0;
     FusePersist q{};
@@ -1676,15 +1727,12 @@ etcu_status recon_build(etcu_volume* vol, const etcu_view* views, uint32_t n_vie
     r->slots = r->block;
     etcu_status s;
     const size_t P = (size_t)W * H;
-    // tilt series, device-resident for the whole reconstruction
-    if (dev_proj) {
-        r->d_proj = const_cast<float*>(dev_proj);
-    } else {
-        if ((s = dalloc(ctx, (void**)&r->d_proj, P * n_views * sizeof(float))) != ETCU_OK) return s;
-        r->own_proj = true;
-        CK(ctx, cudaMemcpyAsync(r->d_proj, host_proj, P * n_views * sizeof(float), cudaMemcpyHostToDevice,
-                                ctx->stream));
-    }
+    // tilt series, device-resident for the whole reconstruction (FP32 device input is used in place)
+    r->proj_kind = params->projection_storage;
+    if ((s = stage_projections(ctx, host_proj, dev_proj, P * n_views, r->proj_kind, true,
+                               [&](void** p, size_t bytes) { return dalloc(ctx, p, bytes); }, &r->d_proj,
+                               &r->own_proj)) != ETCU_OK)
+        return s;
     // view constants per slab (fast-path flags depend on the voxel size)
     const size_t S = vol->slabs.size();
     std::vector<ViewConst> vc(S * n_views);
@@ -1840,7 +1888,7 @@ extern "C" etcu_status etcu_recon_run(etcu_recon* r, uint32_t iterations) {
 // compensation over the complete volume, r = b - Ax) written as (r, L) pairs into the
 // block's slot images, and sum r^2 (FP64, one atomic per warp).
 __global__ void slab_residual_kernel(const float* __restrict__ complete, float2* rl, size_t rl_pitch, size_t rl_slot,
-                                     const float* __restrict__ real, const ViewConst* __restrict__ views,
+                                     const float* __restrict__ real, int real_kind, const ViewConst* __restrict__ views,
                                      const uint32_t* __restrict__ order, uint32_t first, int W, int H, int loc,
                                      double* resid_sq) {
     const int p = blockIdx.z, gy = blockIdx.y, gx = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1854,7 +1902,7 @@ __global__ void slab_residual_kernel(const float* __restrict__ complete, float2*
             vv = ll > kEps ? fdiv(fmul(vv, c), ll) : 0.f;
             ll = c;
         }
-        const float r = fsub(real[(size_t)vid * P + i], vv);  // Compare.cl:8
+        const float r = fsub(load_real(real, real_kind, (size_t)vid * P + i), vv);  // Compare.cl:8
         rl[(size_t)p * rl_slot + (size_t)gy * rl_pitch + gx] = make_float2(r, ll);
         r2 = (double)r * (double)r;
     }
@@ -1923,7 +1971,8 @@ extern "C" etcu_status etcu_recon_slab_backward(etcu_recon* r, uint32_t block, c
     const uint32_t count = std::min(r->block, M - first);
     cudaStream_t st = ctx->stream;
     const dim3 grid((r->W + 127) / 128, r->H, count);
-    slab_residual_kernel<<<grid, 128, 0, st>>>(d_complete, r->rl, r->rl_pitch, r->rl_slot, r->d_proj, r->d_views,
+    slab_residual_kernel<<<grid, 128, 0, st>>>(d_complete, r->rl, r->rl_pitch, r->rl_slot, r->d_proj, r->proj_kind,
+                                               r->d_views,
                                                r->d_order, first, (int)r->W, (int)r->H,
                                                r->params.use_long_object_compensation ? 1 : 0, r->d_resid);
     issue_backward(r, first, count, st);
@@ -2582,6 +2631,8 @@ etcu_status blob_recon_build(etcu_volume* vol, const etcu_view* views, uint32_t 
     if (params->use_long_object_compensation)
         return fail(ctx, ETCU_ERR_INVALID_ARGUMENT,
                     "Calculation of traversal length is only supported for parallel scanner geometry!");
+    if (params->projection_storage != ETCU_PROJ_F32)
+        return fail(ctx, ETCU_ERR_UNSUPPORTED, "blob reconstructions keep the projections in FP32");
     BlobP p;
     etcu_status s;
     if ((s = blob_volume_ok(ctx, vol)) != ETCU_OK || (s = blob_params(ctx, blob, p)) != ETCU_OK) return s;
@@ -3033,6 +3084,7 @@ etcu_status plan_batch_persistent(etcu_batch* b, const std::vector<BatchSeriesRe
         f.a.lambda = params->lambda;  // block size 1
         f.a.jrange = d_jr;
         f.a.real = rc.d_proj;
+        f.a.real_kind = params->projection_storage;
         f.a.resid_sq = b->d_resid + i;
         f.a.loc = params->use_long_object_compensation ? 1 : 0;
         f.tapwin = d_tw;
@@ -3195,12 +3247,14 @@ etcu_status batch_build(etcu_context* ctx, const etcu_batch_series* series, uint
         uint32_t* d_order;
         float4* d_samples;
         const size_t P = (size_t)W * H;
-        if ((s = batch_alloc(b, (void**)&d_proj, P * sr.n_views * sizeof(float))) != ETCU_OK) return s;
+        bool proj_owned;
+        if ((s = stage_projections(ctx, sr.host_projections, nullptr, P * sr.n_views, params->projection_storage, false,
+                                   [&](void** p, size_t bytes) { return batch_alloc(b, p, bytes); }, &d_proj,
+                                   &proj_owned)) != ETCU_OK)
+            return s;
         if ((s = batch_alloc(b, (void**)&d_views, vc.size() * sizeof(ViewConst))) != ETCU_OK) return s;
         if ((s = batch_alloc(b, (void**)&d_order, order.size() * sizeof(uint32_t))) != ETCU_OK) return s;
         if ((s = batch_alloc(b, (void**)&d_samples, pat.size() * sizeof(float))) != ETCU_OK) return s;
-        CK(ctx, cudaMemcpyAsync(d_proj, sr.host_projections, P * sr.n_views * sizeof(float), cudaMemcpyHostToDevice,
-                                ctx->stream));
         CK(ctx, cudaMemcpyAsync(d_views, vc.data(), vc.size() * sizeof(ViewConst), cudaMemcpyHostToDevice, ctx->stream));
         CK(ctx, cudaMemcpyAsync(d_order, order.data(), order.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
                                 ctx->stream));
@@ -3228,6 +3282,7 @@ etcu_status batch_build(etcu_context* ctx, const etcu_batch_series* series, uint
         f.rl_pitch = pitch;
         f.rl_slot = slot;
         f.real = d_proj;
+        f.real_kind = params->projection_storage;
         f.resid_sq = nullptr;  // set below (per-series element of d_resid)
         BpArgs& g = bp[i];
         g = BpArgs{};

@@ -342,6 +342,13 @@ __device__ __forceinline__ void trace_ray(float3 src, float3 ray, float3 inv, bo
     }
 }
 
+// Measured projection i stored as FP32 (kind 0), FP16 (1) or BF16 (2), widened exactly to float.
+__device__ __forceinline__ float load_real(const float* base, int kind, size_t i) {
+    if (kind == 1) return __half2float(reinterpret_cast<const __half*>(base)[i]);
+    if (kind == 2) return __bfloat162float(reinterpret_cast<const __nv_bfloat16*>(base)[i]);
+    return base[i];
+}
+
 // ---------------------------------------------------------------- forward projection
 enum FpMode : int {
     kFpSeparateAccumulate = 0,  // d_virtual += ..., d_traversal += ...   (ForwardProjectionKernel semantics)
@@ -363,7 +370,8 @@ struct FpArgs {
     float* out_l;
     float2* rl;                 // modes 1/2: slot p at rl + p * rl_slot, row pitch rl_pitch (float2 units)
     size_t rl_pitch, rl_slot;
-    const float* real;          // mode 2: measured projections, view id * W * H
+    const float* real;          // mode 2: measured projections, view id * W * H (element type real_kind)
+    int real_kind;              // 0 FP32, 1 FP16, 2 BF16 (load_real)
     double* resid_sq;           // mode 2: optional sum of residual^2 (FP64)
 };
 
@@ -395,7 +403,7 @@ __device__ __forceinline__ double fp_store(const FpArgs& a, const ViewConst& vc,
         vv = ll > kEps ? fdiv(fmul(vv, vc.loc_length), ll) : 0.f;
         ll = vc.loc_length;
     }
-    float r = fsub(a.real[(size_t)vid * (size_t)a.W * (size_t)a.H + i], vv);  // Compare.cl:8
+    float r = fsub(load_real(a.real, a.real_kind, (size_t)vid * (size_t)a.W * (size_t)a.H + i), vv);  // Compare.cl:8
     *slot = make_float2(r, ll);
     return (double)r * (double)r;
 }
@@ -1233,7 +1241,8 @@ struct FuseArgs {
     float lambda;
     int x0lo, ntaps;            // view p's tap window (plan_bp_col)
     const int2* jrange;         // [view id * ry + y]: detector rows [x, y) whose rays lie in volume row y
-    const float* real;          // measured projections, view id * W * H
+    const float* real;          // measured projections, view id * W * H (element type real_kind)
+    int real_kind;              // 0 FP32, 1 FP16, 2 BF16 (load_real)
     double* resid_sq;           // sum of residual^2 (FP64), or nullptr
     int loc;                    // long-object compensation
 };
@@ -1517,7 +1526,7 @@ __device__ __forceinline__ void fused_row_step(const FuseArgs& a, uint32_t p, in
                 ll = fc.loc_length;
             }
             const size_t pix = (size_t)gy * (size_t)a.W + (size_t)gx;
-            const float r = fsub(a.real[(size_t)vf * (size_t)a.W * (size_t)a.H + pix], vv);
+            const float r = fsub(load_real(a.real, a.real_kind, (size_t)vf * (size_t)a.W * (size_t)a.H + pix), vv);
             rl_out[(size_t)gy * a.rl_pitch + (size_t)gx] = make_float2(r, ll);
             r2 += (double)r * (double)r;
         }

@@ -279,7 +279,6 @@ __global__ void __launch_bounds__(conv_threads<kLoad>(), 1) conv_tc_kernel(const
             mbar_expect_tx(wbar, wres);
             bulk_load(wsm, a.w, wres, wbar);
         }
-        const size_t plane = (size_t)a.Z * a.Y * a.X;
         constexpr int kRows = 2 * 3 * (TY + 2);
         constexpr int kElems = kRows * kHaloX;
         int q = 0;

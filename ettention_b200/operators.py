@@ -935,6 +935,7 @@ class AlgebraicParameterSet:
     basis_functions: str = "voxels"
     blob: BlobParameters = field(default_factory=BlobParameters)
     enable_voxelization: bool = False
+    projection_storage: int = _abi.PROJ_F32  # device storage of the tilt series (FP32, FP16 or BF16)
 
     @classmethod
     def from_config(cls, cfg: Dict[str, str]) -> "AlgebraicParameterSet":
@@ -1011,6 +1012,7 @@ class AlgebraicParameterSet:
         rp.order = int(self.order)
         rp.sampling = int(self.sampling)
         rp.use_graph = int(bool(use_graph))
+        rp.projection_storage = int(self.projection_storage)
         return rp
 
 

@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define ETCU_ABI_VERSION 1
+#define ETCU_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define ETCU_API __attribute__((visibility("default")))
@@ -205,6 +205,11 @@ ETCU_API etcu_status etcu_compute_ray_length(etcu_volume* vol, const etcu_view* 
  * OptimizationParameterSet semantics (LR/setup/parameterset/AlgorithmParameterSet.cpp:8-53).
  * block_size: 1 = SART, ETCU_BLOCK_ALL = SIRT, else algorithm.blockSize. */
 #define ETCU_BLOCK_ALL 0xffffffffu
+/* Storage of the measured projections on the device (HalfFloatSupport.hl:6-14 applies the
+ * reference's half storage to volumes; the same 16-bit storage is offered for the tilt
+ * series): FP32 as given, or rounded to nearest FP16 / BF16 once when the reconstruction
+ * is created and widened exactly where the residual is formed. */
+typedef enum { ETCU_PROJ_F32 = 0, ETCU_PROJ_F16 = 1, ETCU_PROJ_BF16 = 2 } etcu_projection_storage;
 typedef struct {
     float lambda;                 /* algorithm.lambda */
     uint32_t block_size;          /* algorithm.blockSize (1 SART, ETCU_BLOCK_ALL SIRT) */
@@ -216,6 +221,7 @@ typedef struct {
     const uint32_t* skip;         /* input.skipProjections (may be NULL) */
     uint32_t skip_count;
     int32_t use_graph;            /* capture each iteration in a CUDA graph */
+    etcu_projection_storage projection_storage; /* element type the measured projections are kept in */
 } etcu_recon_params;
 
 /* Uploads the tilt series (n_views x height x width floats, host memory) once

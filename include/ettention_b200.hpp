@@ -326,6 +326,7 @@ struct AlgebraicParameterSet {
     etcu_voxel_type voxelType = ETCU_VOXEL_FLOAT32;
     etcu_order order = ETCU_ORDER_RANDOM;  // optimization.projectionIteration default
     etcu_sampling sampling = ETCU_SAMPLING_Q8;
+    etcu_projection_storage projectionStorage = ETCU_PROJ_F32;  // device storage of the tilt series
     std::string basisFunctions = "voxels";  // algorithm.basisFunctions
     BlobParameters blob;                    // blobs.*
     bool enableVoxelization = false;        // output.options.enableVoxelization
@@ -428,6 +429,7 @@ struct AlgebraicParameterSet {
         r.skip = skip.empty() ? nullptr : skip.data();
         r.skip_count = (uint32_t)skip.size();
         r.use_graph = use_graph ? 1 : 0;
+        r.projection_storage = projectionStorage;
         return r;
     }
 };

@@ -39,7 +39,7 @@ def test_library_exports_every_declared_symbol():
     for s in syms:
         assert getattr(L, s) is not None
     assert set(_abi._SIG) == set(syms)
-    assert L.etcu_abi_version() == 1
+    assert L.etcu_abi_version() == 2
 
 
 def test_no_device_fails_loudly():

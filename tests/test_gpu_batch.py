@@ -261,3 +261,35 @@ def test_persistent_batch_with_16bit_shadow(vt):
             v.close()
     finally:
         ctx.close()
+
+
+@pytest.mark.parametrize("kind", [1, 2])
+def test_persistent_batch_with_16bit_projections(kind):
+    """Tilt series stored in FP16 (1) / BF16 (2) on the persistent batched path (FP16-shadow
+    volumes): every series equals its single-series reconstruction with the same storage,
+    bit for bit."""
+    from ettention_b200 import _abi
+    from ettention_b200.operators import (AlgebraicParameterSet, BatchReconstructionOperator,
+                                          BlockIterativeReconstructionOperator, Context, GPUMappedVolume)
+    series = make_series(700)
+    ctx = Context(0)
+    try:
+        p = AlgebraicParameterSet(algorithm="sart", block_size=1, iterations=2, lam=0.3, order=_abi.ORDER_IDENTITY,
+                                  projection_storage=kind)
+        vols = [GPUMappedVolume(ctx, shape, voxel_type=2) for shape, _, _ in series]
+        batch = BatchReconstructionOperator([(v, g, pr) for v, (_, g, pr) in zip(vols, series)], p)
+        assert batch.launches_per_iteration == 1
+        batch.runNiterations(2)
+        got = batch.getReconstructedVolumes()
+        batch.close()
+        for v in vols:
+            v.close()
+        for i, (shape, geoms, projs) in enumerate(series):
+            vol = GPUMappedVolume(ctx, shape, voxel_type=2)
+            rec = BlockIterativeReconstructionOperator(vol, geoms, projs, p)
+            rec.runNiterations(2)
+            assert np.abs(got[i]).max() > 0 and np.array_equal(got[i], rec.getReconstructedVolume()), i
+            rec.close()
+            vol.close()
+    finally:
+        ctx.close()

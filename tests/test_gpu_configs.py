@@ -142,3 +142,65 @@ def test_parallel_sirt_sart_storage(ctx, parallel_problem, algo, block, iters, v
     else:
         v64 = oracle_recon(geoms, projs, PAR_RES, p.lam, nblock, iters, order, 64)
         assert O.rel_l2(v, v64) <= F16_TOL
+
+
+def round_projections(projs, kind):
+    """The tilt series as 16-bit storage keeps it: round to nearest even FP16 (numpy) or
+    BF16 (the upper 16 bits after adding 0x7fff plus the kept bit's parity), widened back."""
+    if kind == 1:
+        return projs.astype(np.float16).astype(np.float32)
+    bits = projs.astype(np.float32).view(np.uint32).astype(np.uint64)
+    bits = (bits + 0x7FFF + ((bits >> 16) & 1)) & 0xFFFF0000
+    return bits.astype(np.uint32).view(np.float32)
+
+
+@pytest.mark.parametrize("kind", [1, 2])
+@pytest.mark.parametrize("algo,fused", [("sart", "1"), ("sart", "0"), ("sirt", "1")])
+def test_projection_storage_equals_prerounded_series(ctx, parallel_problem, kind, algo, fused, monkeypatch):
+    """FP16 / BF16 storage of the tilt series: the reconstruction equals, bit for bit, the
+    FP32-storage reconstruction of the series rounded to that format on the host -- on the
+    fused persistent SART path, the unfused one, and SIRT -- with an FP16-shadow volume
+    for SART (the C2 low-precision storage) and FP32 for SIRT."""
+    from ettention_b200 import _abi
+    from ettention_b200.operators import AlgebraicParameterSet, Context
+    monkeypatch.setenv("ETCU_FUSED", fused)
+    geoms, projs = parallel_problem
+    vt = 2 if algo == "sart" else 0
+    lam, block = (0.3, 1) if algo == "sart" else (1.0, 0xFFFFFFFF)
+    c = Context(0)  # the environment is read when a context is created
+    try:
+        p16 = AlgebraicParameterSet(algorithm=algo, block_size=block, iterations=2, lam=lam,
+                                    order=_abi.ORDER_IDENTITY, projection_storage=kind)
+        v16, _ = cuda_recon(c, geoms, projs, PAR_RES, p16, 2, voxel_type=vt)
+        p32 = AlgebraicParameterSet(algorithm=algo, block_size=block, iterations=2, lam=lam,
+                                    order=_abi.ORDER_IDENTITY)
+        vr, _ = cuda_recon(c, geoms, round_projections(projs, kind), PAR_RES, p32, 2, voxel_type=vt)
+    finally:
+        c.close()
+    assert np.abs(v16).max() > 0
+    assert np.array_equal(v16, vr)
+
+
+@pytest.mark.parametrize("kind,tol", [(1, F16_TOL), (2, BF16_TOL)])
+def test_projection_and_volume_16bit_storage_against_fp64_oracle(ctx, parallel_problem, kind, tol):
+    """The C2 low-precision configuration: volume with a 16-bit shadow (FP16 or BF16) over
+    an FP32 master and the tilt series stored in the same 16-bit format, SART, against the
+    FP64 oracle on the FP32 series, at that format's storage bound."""
+    from oracle import oracle as O
+    from ettention_b200 import _abi
+    from ettention_b200.operators import AlgebraicParameterSet
+    geoms, projs = parallel_problem
+    p = AlgebraicParameterSet(algorithm="sart", block_size=1, iterations=2, lam=0.3, order=_abi.ORDER_IDENTITY,
+                              projection_storage=kind)
+    v, order = cuda_recon(ctx, geoms, projs, PAR_RES, p, 2, voxel_type={1: 2, 2: 3}[kind])
+    v64 = oracle_recon(geoms, projs, PAR_RES, 0.3, 1, 2, order, 64)
+    assert O.rel_l2(v, v64) <= tol
+
+
+def test_unknown_projection_storage_is_rejected(ctx, parallel_problem):
+    from ettention_b200._abi import EttentionError
+    from ettention_b200.operators import AlgebraicParameterSet
+    geoms, projs = parallel_problem
+    p = AlgebraicParameterSet(algorithm="sart", iterations=1, lam=0.3, projection_storage=7)
+    with pytest.raises(EttentionError, match="unknown projection storage"):
+        cuda_recon(ctx, geoms, projs, PAR_RES, p, 1)
