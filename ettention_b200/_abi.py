@@ -131,6 +131,7 @@ _SIG = {
     "etcu_recon_set_complete_bbox": (_S, [_P, _P, _P]),
     "etcu_recon_slab_forward": (_S, [_P, _U, _P]),
     "etcu_recon_slab_backward": (_S, [_P, _U, _P]),
+    "etcu_recon_slab_step": (_S, [_P, _U, _P, _P]),
     "etcu_recon_profile_iteration": (_S, [_P, ctypes.POINTER(_F), ctypes.POINTER(_F), ctypes.POINTER(_U),
                                          ctypes.POINTER(_U)]),
     "etcu_recon_profile_steps": (_S, [_P, _P, _P, _P, _U, ctypes.POINTER(_U)]),

@@ -318,9 +318,19 @@ void launch_bp_t(const BpArgs& a, int device, cudaStream_t st) {
     // Host threads driving different devices may get here together: the set of opted-in
     // devices is one atomic word (setting the attribute twice is harmless).
     static std::atomic<unsigned long long> opted{0};
-    auto kern = kPersp ? bp_perspective_kernel<kMask, kStore, kSampling> : bp_parallel_kernel<kMask, kStore, kSampling>;
+    // the perspective kernel with the intensity clamps compiled in only when a clamp is set
+    auto persp = (a.use_min || a.use_max) ? bp_perspective_kernel<kMask, kStore, kSampling, true>
+                                          : bp_perspective_kernel<kMask, kStore, kSampling, false>;
+    auto kern = kPersp ? persp : bp_parallel_kernel<kMask, kStore, kSampling>;
     if (device < 64 && !(opted.load(std::memory_order_acquire) & (1ull << device))) {
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBpSmemBudget);
+        if (kPersp) {
+            cudaFuncSetAttribute(bp_perspective_kernel<kMask, kStore, kSampling, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBpSmemBudget);
+            cudaFuncSetAttribute(bp_perspective_kernel<kMask, kStore, kSampling, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBpSmemBudget);
+        } else {
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBpSmemBudget);
+        }
         opted.fetch_or(1ull << device, std::memory_order_acq_rel);
     }
     const size_t smem = bp_smem_bytes(a.nviews, kPersp ? 0 : a.nsamples);
@@ -1338,7 +1348,8 @@ uint32_t issue_backward(etcu_recon* r, uint32_t first, uint32_t count, cudaStrea
 // SART with the fused step: FP of the first view into slot 0, then for every order
 // position p the fused BP(p) + FP(p + 1) (slots alternate), then the BP of the last
 // view.  Same operations in the same order as the unfused sequence.
-void launch_fused_step(etcu_recon* r, uint32_t p, cudaStream_t st) {
+void launch_fused_step(etcu_recon* r, uint32_t p, cudaStream_t st, const float2* rl_in = nullptr,
+                       float* part = nullptr) {
     etcu_volume* vol = r->vol;
     const SlabConst& g = vol->slabs[0];
     const uint32_t vb = r->order[p];
@@ -1349,7 +1360,7 @@ void launch_fused_step(etcu_recon* r, uint32_t p, cudaStream_t st) {
     a.order = r->d_order;
     a.p = p;
     a.samples = r->d_samples;
-    a.rl_in = r->rl + (size_t)(p & 1) * r->rl_slot;
+    a.rl_in = rl_in ? rl_in : r->rl + (size_t)(p & 1) * r->rl_slot;
     a.rl_out = r->rl + (size_t)((p + 1) & 1) * r->rl_slot;
     a.rl_pitch = r->rl_pitch;
     a.W = (int)r->W;
@@ -1360,8 +1371,9 @@ void launch_fused_step(etcu_recon* r, uint32_t p, cudaStream_t st) {
     a.jrange = r->d_jrange;
     a.real = r->d_proj;
     a.real_kind = r->proj_kind;
-    a.resid_sq = r->d_resid;
+    a.resid_sq = part ? nullptr : r->d_resid;
     a.loc = r->params.use_long_object_compensation ? 1 : 0;
+    a.part = part;
     const size_t smem = fuse_smem_bytes(g.rx, g.rz, a.ntaps);
     switch (vol->type) {
     case ETCU_VOXEL_F16_MASTER: sart_fused_kernel<1><<<g.ry, kFuseThreads, smem, st>>>(a); break;
@@ -1976,6 +1988,32 @@ extern "C" etcu_status etcu_recon_slab_backward(etcu_recon* r, uint32_t block, c
                                                r->d_order, first, (int)r->W, (int)r->H,
                                                r->params.use_long_object_compensation ? 1 : 0, r->d_resid);
     issue_backward(r, first, count, st);
+    CKL(ctx);
+    return ETCU_OK;
+}
+
+// Residual of block `block` from the complete images, then its back projection and the
+// forward projection of block + 1 into d_next: for SART on the fused path one fused step
+// (sart_fused_kernel writing the slab's partial images of view p + 1), otherwise the
+// two calls above.
+extern "C" etcu_status etcu_recon_slab_step(etcu_recon* r, uint32_t block, const float* d_complete, float* d_next) {
+    if (!r || !d_complete || !d_next) return fail(r ? r->ctx : nullptr, ETCU_ERR_INVALID_ARGUMENT, "NULL argument");
+    etcu_context* ctx = r->ctx;
+    if (block + 1 >= r->nblocks)
+        return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "block %u has no next block (%u blocks)", block, r->nblocks);
+    if (d_next == d_complete) return fail(ctx, ETCU_ERR_INVALID_ARGUMENT, "the next block needs its own buffer");
+    if (!r->fused) {
+        etcu_status s = etcu_recon_slab_backward(r, block, d_complete);
+        return s != ETCU_OK ? s : etcu_recon_slab_forward(r, block + 1, d_next);
+    }
+    cudaStream_t st = ctx->stream;
+    const size_t P = (size_t)r->W * r->H;
+    const dim3 grid((r->W + 127) / 128, r->H, 1);
+    slab_residual_kernel<<<grid, 128, 0, st>>>(d_complete, r->rl, r->rl_pitch, r->rl_slot, r->d_proj, r->proj_kind,
+                                               r->d_views, r->d_order, block, (int)r->W, (int)r->H,
+                                               r->params.use_long_object_compensation ? 1 : 0, r->d_resid);
+    CK(ctx, cudaMemsetAsync(d_next, 0, 2 * P * sizeof(float), st));
+    launch_fused_step(r, block, st, r->rl, d_next);
     CKL(ctx);
     return ETCU_OK;
 }

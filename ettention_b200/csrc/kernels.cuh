@@ -273,8 +273,9 @@ __device__ __forceinline__ void dda_walk3_fast(const DdaStart& st, const SlabCon
 #pragma unroll
             for (int j = 0; j < kUnroll; ++j) {
                 const float dt = fminf(fminf(rx, ry), rz);
-                const bool bx = rx <= ry && rx <= rz;
-                const bool by = ry < rx && ry <= rz;
+                // rx <= ry && rx <= rz, and ry < rx && ry <= rz, from the minimum
+                const bool bx = rx == dt;
+                const bool by = !bx && ry == dt;
                 const bool bz = !bx && !by;
                 dts[j] = dt;
                 vals[j] = load_voxel(vol + off);
@@ -294,8 +295,8 @@ __device__ __forceinline__ void dda_walk3_fast(const DdaStart& st, const SlabCon
             for (int j = 0; j < kUnroll; ++j) {
                 const bool live = (nx > 0) & (ny > 0) & (nz > 0) & (left > 0);
                 const float dt = fminf(fminf(rx, ry), rz);
-                const bool bx = rx <= ry && rx <= rz;
-                const bool by = ry < rx && ry <= rz;
+                const bool bx = rx == dt;
+                const bool by = !bx && ry == dt;
                 const bool bz = !bx && !by;  // rz < rx && rz < ry for finite values
                 dts[j] = live ? dt : 0.f;
                 vals[j] = 0.f;
@@ -1245,6 +1246,9 @@ struct FuseArgs {
     int real_kind;              // 0 FP32, 1 FP16, 2 BF16 (load_real)
     double* resid_sq;           // sum of residual^2 (FP64), or nullptr
     int loc;                    // long-object compensation
+    float* part;                // non-null: view p + 1's (projection, ray length) of this sub-volume go to
+                                // part[pixel] and part[W * H + pixel] (kFpSeparateAccumulate into
+                                // zeros) instead of the residual (the z-slab block step)
 };
 
 __host__ __device__ constexpr size_t fuse_smem_bytes(int rx, int rz, int ntaps) {
@@ -1521,6 +1525,12 @@ __device__ __forceinline__ void fused_row_step(const FuseArgs& a, uint32_t p, in
             // fp_pixel sums its one sub-ray into zero, fp_store divides by the count
             const float pv = fdiv(fadd(0.f, acc[i]), 1.f), pl = fdiv(fadd(0.f, accl[i]), 1.f);
             float vv = fadd(0.f, pv), ll = fadd(0.f, pl);
+            if (a.part) {
+                const size_t pix = (size_t)gy * (size_t)a.W + (size_t)gx;
+                a.part[pix] = vv;
+                a.part[(size_t)a.W * (size_t)a.H + pix] = ll;
+                continue;
+            }
             if (a.loc) {
                 vv = ll > kEps ? fdiv(fmul(vv, fc.loc_length), ll) : 0.f;
                 ll = fc.loc_length;
@@ -1793,7 +1803,7 @@ __device__ __forceinline__ float chord_in_voxel(float3 o, float3 dir, float3 c, 
 
 // PerspectiveBeamsBackProjection.cl:28-71: n^3 sub-voxel samples, each weighted by
 // its own chord through the voxel; optional intensity clamps.
-template <bool kMask, int kStore, int kSampling>
+template <bool kMask, int kStore, int kSampling, bool kClamp>
 __global__ void __launch_bounds__(256) bp_perspective_kernel(const __grid_constant__ BpArgs a) {
     extern __shared__ __align__(16) unsigned char bp_smem[];
     BpView* sv = (BpView*)bp_smem;
@@ -1844,53 +1854,62 @@ __global__ void __launch_bounds__(256) bp_perspective_kernel(const __grid_consta
             for (int p = 0; p < a.nviews; ++p) {
                 const BpView& V = sv[p];
                 const float2* img = a.rl + (size_t)p * a.rl_slot;
-                const float cu = fadd(fmul(V.mu[0], px), fmul(V.mu[1], py));
-                const float cv = fadd(fmul(V.mv[0], px), fmul(V.mv[1], py));
+                const float2 cuv = f2(fadd(fmul(V.mu[0], px), fmul(V.mu[1], py)), fadd(fmul(V.mv[0], px), fmul(V.mv[1], py)));
+                const float2 m2 = f2(V.mu[2], V.mv[2]), m3 = f2(V.mu[3], V.mv[3]);
                 const float cw = fadd(fmul(V.mw[0], px), fmul(V.mw[1], py));
                 const float dx = fsub(px, V.src[0]), dy = fsub(py, V.src[1]);
                 const float dxy = fadd(fmul(dx, dx), fmul(dy, dy));
-                const float lxy = fminf(fmul(g.vs.x, rcp_approx(fabsf(dx))), fmul(g.vs.y, rcp_approx(fabsf(dy))));
+                // chord of the ray through the centre: |d| / max_i(|d_i| / vs_i)
+                const float mxy = fmaxf(fmul(fabsf(dx), g.ivs.x), fmul(fabsf(dy), g.ivs.y));
+                // the coordinate clamps keep the taps inside the padded image (texels -2 .. W + 1);
+                // out there every texel is a zero pad, as it is for the unclamped coordinate
+                const float2 lo = splat(-1.5f), hi = f2((float)a.W + 1.49609375f, (float)a.H + 1.49609375f);
 #pragma unroll
                 for (int j = 0; j < kBpZPersp; ++j) {
                     if (!kFull && j >= nzc) continue;
-                    float u = fadd(fadd(cu, fmul(V.mu[2], pz[j])), V.mu[3]);
-                    float v = fadd(fadd(cv, fmul(V.mv[2], pz[j])), V.mv[3]);
+                    // u and v as paired operations (each lane the same operations as alone)
+                    float2 uv = add2(add2(cuv, __fmul2_rn(m2, splat(pz[j]))), m3);
                     const float w = fadd(fadd(cw, fmul(V.mw[2], pz[j])), V.mw[3]);
                     float rw = rcp_approx(w);
                     rw = fmaf(rw, fmaf(-w, rw, 1.f), rw);
-                    u = fmul(u, rw);
-                    v = fmul(v, rw);
+                    uv = __fmul2_rn(uv, splat(rw));
                     float2 rl;
                     if (kSampling == kSampleQ8) {
-                        // the bilinear blend of (r, L) as paired FMAs: both channels per
-                        // instruction (weights as the 1/256 texture filter rounds them)
-                        int x0, y0;
-                        float wa, wb;
-                        split_coord<kSampling>(u, a.W, x0, wa);
-                        split_coord<kSampling>(v, a.H, y0, wb);
+                        // q = floor(256 c - 127.5) in the mantissa of 1.5 * 2^23 + q (exact for
+                        // the clamped coordinates): texel floor(q / 256), weight (q & 255) / 256,
+                        // the split of split_coord with its 1/256 weights (a weight that rounds
+                        // up to 1 is weight 0 on the next texel, the same blend)
+                        const float2 uc = f2(fminf(fmaxf(uv.x, lo.x), hi.x), fminf(fmaxf(uv.y, lo.y), hi.y));
+                        const float2 fq = __fadd2_rd(fma2(uc, splat(256.f), splat(-127.5f)), splat(12582912.0f));
+                        const int bu = __float_as_int(fq.x), bv = __float_as_int(fq.y);
+                        const int x0 = (bu - 0x4B400000) >> 8, y0 = (bv - 0x4B400000) >> 8;
+                        const float2 wab = add2(f2(__int_as_float(((bu << 15) & 0x007F8000) | 0x3F800000),
+                                                   __int_as_float(((bv << 15) & 0x007F8000) | 0x3F800000)),
+                                                splat(-1.f));
                         float2 t00, t10, t01, t11;
                         taps(img + (ptrdiff_t)y0 * (ptrdiff_t)a.rl_pitch, a.rl_pitch, x0, t00, t10, t01, t11);
-                        const float ob = fsub(1.f, wb), oa = fsub(1.f, wa);
-                        rl = __fmul2_rn(splat(fmul(oa, ob)), t00);
-                        rl = fma2(splat(fmul(wa, ob)), t10, rl);
-                        rl = fma2(splat(fmul(oa, wb)), t01, rl);
-                        rl = fma2(splat(fmul(wa, wb)), t11, rl);
+                        // bilinear blend of (r, L) as two lerps along x and one along y, both
+                        // channels per instruction
+                        const float2 p0 = fma2(splat(wab.x), fma2(t00, splat(-1.f), t10), t00);
+                        const float2 p1 = fma2(splat(wab.x), fma2(t01, splat(-1.f), t11), t01);
+                        rl = fma2(splat(wab.y), fma2(p0, splat(-1.f), p1), p0);
                     } else {
-                        rl = sample_pair<kSampling>(img, a.rl_pitch, a.W, a.H, V.tex, u, v);
+                        rl = sample_pair<kSampling>(img, a.rl_pitch, a.W, a.H, V.tex, uv.x, uv.y);
                     }
                     float value = 0.f;
                     if (rl.y >= kEps) {
+                        // r * chord / L with chord = |d| / m: r * nd2 * rsqrt(nd2 * (m L)^2),
+                        // one reciprocal square root for the chord and the division by L
                         const float dz = fsub(pz[j], V.src[2]);
-                        // |d| by reciprocal square root (within 2 ulp; the IEEE square root
-                        // cost 4 % of the kernel)
                         const float nd2 = fadd(dxy, fmul(dz, dz));
-                        const float nd = fmul(nd2, rsqrtf(nd2));
-                        const float l = fmul(nd, fminf(lxy, fmul(g.vs.z, rcp_approx(fabsf(dz)))));
-                        value = fmul(fmul(rl.x, l), rcp_approx(rl.y));
+                        const float mL = fmul(fmaxf(mxy, fmul(fabsf(dz), g.ivs.z)), rl.y);
+                        value = fmul(rl.x, fmul(nd2, rsqrtf(fmul(nd2, fmul(mL, mL)))));
                     }
                     float vj = fadd(val[j], fmul(fmul(a.lambda, value), mw[j]));
-                    if (a.use_min) vj = fmaxf(a.vmin, vj);
-                    if (a.use_max) vj = fminf(a.vmax, vj);
+                    if (kClamp) {
+                        if (a.use_min) vj = fmaxf(a.vmin, vj);
+                        if (a.use_max) vj = fminf(a.vmax, vj);
+                    }
                     if (kStore == 1) vj = __half2float(__float2half_rn(vj));
                     val[j] = vj;
                 }

@@ -11,10 +11,11 @@ back projects its own slab with lambda / blockSize.  The only data exchange is t
 all-reduce: B x 2 x H x W floats per block.
 
 `CudaSlabReconstruction` runs this on the GPU through the block-step C ABI
-(etcu_recon_slab_forward / etcu_recon_slab_backward): per block one stream-ordered forward
-projection of the slab into a device buffer, the NCCL all-reduce of that buffer enqueued
-on the library's stream, and one stream-ordered residual + back projection -- no host
-synchronisation inside an iteration.  `SlabDecomposedReconstruction` is the same loop
+(etcu_recon_slab_forward / _step / _backward): the first block's forward projection of the
+slab into a device buffer, then per block the NCCL all-reduce of its buffer enqueued on the
+library's stream and one stream-ordered step -- its residual and back projection and the
+next block's forward projection, for SART one fused step -- with no host synchronisation
+inside an iteration.  `SlabDecomposedReconstruction` is the same loop
 written against an engine (a rank's slab and its operators), which runs on CUDA
 (`CudaSlabEngine`, operator by operator) and, in tests, on a CPU restatement with the gloo
 backend.
@@ -167,11 +168,13 @@ class CudaSlabReconstruction:
     """This rank's z-slab of one volume, reconstructed with the block-step C ABI.
 
     Every rank holds the whole tilt series; rank r owns slab r of the reference's split.
-    Per block: etcu_recon_slab_forward adds the slab's line integrals and ray lengths of
-    the block's views into a (B, 2, H, W) device buffer, `torch.distributed.all_reduce`
-    sums it over the ranks on the library's stream (NCCL when the process group uses it),
-    and etcu_recon_slab_backward forms b - Ax (long-object compensation over the complete
-    volume) and back projects the block into the slab with lambda / B."""
+    Block b's (B, 2, H, W) buffer receives the slab's line integrals and ray lengths of the
+    block's views (etcu_recon_slab_forward for the first block, the previous step for the
+    others), `torch.distributed.all_reduce` sums it over the ranks on the library's stream
+    (NCCL when the process group uses it), and etcu_recon_slab_step forms b - Ax
+    (long-object compensation over the complete volume), back projects the block into the
+    slab with lambda / B and forward projects block b + 1 into the other buffer
+    (etcu_recon_slab_backward for the last block)."""
 
     def __init__(self, ctx, resolution, bbox_min, bbox_max, rank: int, world: int, geometries,
                  projections: np.ndarray, params, voxel_type: int = 0):
@@ -194,29 +197,48 @@ class CudaSlabReconstruction:
         self.blocks, self.block_size = nb.value, bs.value
         self.views = len(self.rec.view_order())
         H, W = int(projections.shape[1]), int(projections.shape[2])
-        self.buf = torch.zeros((self.block_size, 2, H, W), dtype=torch.float32, device=torch.device("cuda", ctx.device))
-        torch.cuda.synchronize(self.buf.device)
+        dev = torch.device("cuda", ctx.device)
+        # blocks alternate between two (B, 2, H, W) buffers: a step reads block b's complete
+        # images while it writes block b + 1's partial ones
+        self.bufs = [torch.zeros((self.block_size, 2, H, W), dtype=torch.float32, device=dev) for _ in range(2)]
+        torch.cuda.synchronize(dev)
         self.stream = torch.cuda.ExternalStream(ctx.stream_handle)
 
     def block_views(self, b: int) -> int:
         return min(self.block_size, self.views - b * self.block_size)
 
+    def buffer(self, b: int):
+        """Block b's (virtual, traversal) images."""
+        return self.bufs[b % 2]
+
     def block_forward(self, b: int) -> None:
-        """This slab's partial (virtual, traversal) images of block b into ``buf``."""
-        self.ctx.check(_abi.lib().etcu_recon_slab_forward(self.rec.handle, int(b), self.buf.data_ptr()))
+        """This slab's partial images of block b into buffer(b)."""
+        self.ctx.check(_abi.lib().etcu_recon_slab_forward(self.rec.handle, int(b), self.buffer(b).data_ptr()))
+
+    def block_step(self, b: int) -> None:
+        """Block b's residual and back projection (from the complete images in buffer(b)) and
+        block b + 1's partial images into buffer(b + 1); one fused step for SART."""
+        self.ctx.check(_abi.lib().etcu_recon_slab_step(self.rec.handle, int(b), self.buffer(b).data_ptr(),
+                                                       self.buffer(b + 1).data_ptr()))
 
     def block_backward(self, b: int) -> None:
-        """Residual from the complete images in ``buf`` and back projection into the slab."""
-        self.ctx.check(_abi.lib().etcu_recon_slab_backward(self.rec.handle, int(b), self.buf.data_ptr()))
+        """Residual from the complete images in buffer(b) and back projection into the slab."""
+        self.ctx.check(_abi.lib().etcu_recon_slab_backward(self.rec.handle, int(b), self.buffer(b).data_ptr()))
+
+    def all_reduce(self, b: int) -> None:
+        if self.world > 1:
+            import torch.distributed as dist
+            with self.torch.cuda.stream(self.stream):
+                dist.all_reduce(self.buffer(b)[:self.block_views(b)], op=dist.ReduceOp.SUM)
 
     def runSingleIteration(self) -> None:
+        self.block_forward(0)
         for b in range(self.blocks):
-            self.block_forward(b)
-            if self.world > 1:
-                import torch.distributed as dist
-                with self.torch.cuda.stream(self.stream):
-                    dist.all_reduce(self.buf[:self.block_views(b)], op=dist.ReduceOp.SUM)
-            self.block_backward(b)
+            self.all_reduce(b)
+            if b + 1 < self.blocks:
+                self.block_step(b)
+            else:
+                self.block_backward(b)
 
     def runNiterations(self, n: int) -> None:
         for _ in range(int(n)):

@@ -276,6 +276,11 @@ ETCU_API etcu_status etcu_recon_block_count(const etcu_recon* rec, uint32_t* blo
 ETCU_API etcu_status etcu_recon_set_complete_bbox(etcu_recon* rec, const float bbox_min[3], const float bbox_max[3]);
 ETCU_API etcu_status etcu_recon_slab_forward(etcu_recon* rec, uint32_t block, float* d_partial);
 ETCU_API etcu_status etcu_recon_slab_backward(etcu_recon* rec, uint32_t block, const float* d_complete);
+/* etcu_recon_slab_backward(block) then etcu_recon_slab_forward(block + 1, d_next) in one
+ * call (block + 1 < blocks; d_next a second count x 2 x height x width buffer).  For SART
+ * on the fused path this is one fused step: the back projection of view p and the forward
+ * projection of view p + 1 in one pass over the slab. */
+ETCU_API etcu_status etcu_recon_slab_step(etcu_recon* rec, uint32_t block, const float* d_complete, float* d_next);
 
 /* One-call host-buffer reconstruction: upload projections and initial volume,
  * run `iterations`, download the result (the path a frontend's "ettention --config" run takes). */

@@ -100,17 +100,22 @@ def test_block_step_abi_two_slabs_equal_subvolume_reconstruction(block, loc):
     try:
         lo, hi = [-0.5 * X, -0.5 * Y, -0.5 * Z], [0.5 * X, 0.5 * Y, 0.5 * Z]
         ranks = [CudaSlabReconstruction(ctx, (X, Y, Z), lo, hi, k, 2, geoms, projs, p) for k in range(2)]
-        for _ in range(2):
+        for it in range(2):
+            for s in ranks:
+                s.block_forward(0)
             for b in range(ranks[0].blocks):
                 n = ranks[0].block_views(b)
-                for s in ranks:
-                    s.block_forward(b)
                 with torch.cuda.stream(ranks[0].stream):
-                    tot = ranks[0].buf[:n] + ranks[1].buf[:n]
+                    tot = ranks[0].buffer(b)[:n] + ranks[1].buffer(b)[:n]
                     for s in ranks:
-                        s.buf[:n].copy_(tot)
+                        s.buffer(b)[:n].copy_(tot)
                 for s in ranks:
-                    s.block_backward(b)
+                    if b + 1 < s.blocks and (it == 0 or b % 2):  # both the step and the split calls
+                        s.block_step(b)
+                    else:
+                        s.block_backward(b)
+                        if b + 1 < s.blocks:
+                            s.block_forward(b + 1)
         ctx.synchronize()
         v = np.zeros((Z, Y, X), np.float32)
         for s in ranks:
