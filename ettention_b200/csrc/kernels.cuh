@@ -268,29 +268,45 @@ __device__ __forceinline__ void dda_walk3_fast(const DdaStart& st, const SlabCon
     const float sdx = st.sd.x, sdy = st.sd.y, sdz = st.sd.z;
     for (;;) {
         float dts[kUnroll], vals[kUnroll], mws[kUnroll];
-        if (min(min(nx, ny), min(nz, left)) >= kUnroll) {
-            // no axis can run out within the next kUnroll steps: every step is live
+        const int budget = min(min(nx, ny), min(nz, left));
+        if (budget > kUnroll) {
+            // Each step spends one step of one axis, so no axis can run out within
+            // budget - 1 steps: walk a multiple of kUnroll of them without step budgets,
+            // then recover the indices from the offset and renew the budgets.
+            const int run = (budget - 1) / kUnroll * kUnroll;
+            for (int s = 0; s < run; s += kUnroll) {
 #pragma unroll
-            for (int j = 0; j < kUnroll; ++j) {
-                const float dt = fminf(fminf(rx, ry), rz);
-                // rx <= ry && rx <= rz, and ry < rx && ry <= rz, from the minimum
-                const bool bx = rx == dt;
-                const bool by = !bx && ry == dt;
-                const bool bz = !bx && !by;
-                dts[j] = dt;
-                vals[j] = load_voxel(vol + off);
-                mws[j] = 0.f;
-                if (kMask) mws[j] = mask_weight(mask + off);
-                rx = bx ? sdx : fsub(rx, dt);
-                ry = by ? sdy : fsub(ry, dt);
-                rz = bz ? sdz : fsub(rz, dt);
-                off += bx ? dx : (by ? dy : dz);
-                nx -= bx ? 1 : 0;
-                ny -= by ? 1 : 0;
-                nz -= bz ? 1 : 0;
+                for (int j = 0; j < kUnroll; ++j) {
+                    const float dt = fminf(fminf(rx, ry), rz);
+                    // rx <= ry && rx <= rz, and ry < rx && ry <= rz, from the minimum
+                    const bool bx = rx == dt;
+                    const bool by = !bx && ry == dt;
+                    const bool bz = !bx && !by;
+                    dts[j] = dt;
+                    vals[j] = load_voxel(vol + off);
+                    mws[j] = 0.f;
+                    if (kMask) mws[j] = mask_weight(mask + off);
+                    rx = bx ? sdx : fsub(rx, dt);
+                    ry = by ? sdy : fsub(ry, dt);
+                    rz = bz ? sdz : fsub(rz, dt);
+                    off += bx ? dx : (by ? dy : dz);
+                }
+#pragma unroll
+                for (int j = 0; j < kUnroll; ++j) {
+                    acc = fmaf(dts[j], vals[j], acc);
+                    if (kMask) accl = fmaf(dts[j], mws[j], accl);
+                    else accl += dts[j];
+                }
             }
-            left -= kUnroll;
-        } else {
+            left -= run;
+            const Idx iz = off / plane, rem = off - iz * plane, iy = rem / rowlen;
+            const int ix = (int)(rem - iy * rowlen);
+            nx = st.sx > 0 ? g.rx - ix : (st.sx < 0 ? ix + 1 : 0x7fffffff);
+            ny = st.sy > 0 ? g.ry - (int)iy : (st.sy < 0 ? (int)iy + 1 : 0x7fffffff);
+            nz = st.sz > 0 ? g.rz - (int)iz : (st.sz < 0 ? (int)iz + 1 : 0x7fffffff);
+            continue;
+        }
+        {
 #pragma unroll
             for (int j = 0; j < kUnroll; ++j) {
                 const bool live = (nx > 0) & (ny > 0) & (nz > 0) & (left > 0);
