@@ -1880,6 +1880,7 @@ __global__ void __launch_bounds__(256) bp_perspective_kernel(const __grid_consta
                 // the coordinate clamps keep the taps inside the padded image (texels -2 .. W + 1);
                 // out there every texel is a zero pad, as it is for the unclamped coordinate
                 const float2 lo = splat(-1.5f), hi = f2((float)a.W + 1.49609375f, (float)a.H + 1.49609375f);
+                const int pitch = (int)a.rl_pitch;
 #pragma unroll
                 for (int j = 0; j < kBpZPersp; ++j) {
                     if (!kFull && j >= nzc) continue;
@@ -1902,8 +1903,10 @@ __global__ void __launch_bounds__(256) bp_perspective_kernel(const __grid_consta
                         const float2 wab = add2(f2(__int_as_float(((bu << 15) & 0x007F8000) | 0x3F800000),
                                                    __int_as_float(((bv << 15) & 0x007F8000) | 0x3F800000)),
                                                 splat(-1.f));
-                        float2 t00, t10, t01, t11;
-                        taps(img + (ptrdiff_t)y0 * (ptrdiff_t)a.rl_pitch, a.rl_pitch, x0, t00, t10, t01, t11);
+                        // texel index in 32 bits (a slot holds fewer than 2^31 texels)
+                        const int t = y0 * pitch + x0;
+                        const float2 t00 = __ldg(img + t), t10 = __ldg(img + t + 1);
+                        const float2 t01 = __ldg(img + (t + pitch)), t11 = __ldg(img + (t + pitch + 1));
                         // bilinear blend of (r, L) as two lerps along x and one along y, both
                         // channels per instruction
                         const float2 p0 = fma2(splat(wab.x), fma2(t00, splat(-1.f), t10), t00);
