@@ -569,6 +569,8 @@ struct BpView {
     float mu[4], mv[4], mw[4];     // matrix rows: (m0, m4, m8, m12), (m1, m5, m9, m13), (m3, m7, m11, m15)
     float src[3];
     int affine;                    // mw == (0, 0, 0, 1): the divide by w is the identity
+    int inside;                    // perspective back projection: every voxel centre of the block's
+                                   // brick projects well inside the padded image (no clamps needed)
     cudaTextureObject_t tex;
 };
 
@@ -654,6 +656,7 @@ __device__ __forceinline__ void bp_stage(const BpArgs& a, BpView* sv, float4* ss
         v.mw[0] = vc.mat[3]; v.mw[1] = vc.mat[7]; v.mw[2] = vc.mat[11]; v.mw[3] = vc.mat[15];
         v.src[0] = vc.source.x; v.src[1] = vc.source.y; v.src[2] = vc.source.z;
         v.affine = (v.mw[0] == 0.f && v.mw[1] == 0.f && v.mw[2] == 0.f && v.mw[3] == 1.f) ? 1 : 0;
+        v.inside = 0;
         v.tex = a.texs ? a.texs[p] : a.inline_tex;
         sv[p] = v;
     }
@@ -1817,6 +1820,34 @@ __device__ __forceinline__ float chord_in_voxel(float3 o, float3 dir, float3 c, 
     return fmaxf(0.f, fsub(tout, tin));
 }
 
+// Whether every voxel centre of the brick [x0, x1] x [y0, y1] x [z0, z1] projects with
+// w > 0 and (u, v) at least 1/64 texel inside [ulo, uhi] x [vlo, vhi]: w is affine in the
+// position, so its minimum over the brick is at a corner, and with w > 0 on the brick the
+// projected brick is the convex hull of the projected corners.  The margin covers the
+// rounding of the per-voxel evaluation.
+__device__ __forceinline__ int brick_projects_inside(const BpView& V, const SlabConst& g, int x0, int x1, int y0,
+                                                     int y1, int z0, int z1, float ulo, float uhi, float vlo,
+                                                     float vhi) {
+    float wmin = FLT_MAX, wmax = 0.f, umin = FLT_MAX, umax = -FLT_MAX, vmin = FLT_MAX, vmax = -FLT_MAX;
+    for (int c = 0; c < 8; ++c) {
+        const float px = g.bmin.x + ((float)((c & 1) ? x1 : x0) + 0.5f) * g.vs.x;
+        const float py = g.bmin.y + ((float)((c & 2) ? y1 : y0) + 0.5f) * g.vs.y;
+        const float pz = g.bmin.z + ((float)((c & 4) ? z1 : z0) + 0.5f) * g.vs.z;
+        const float w = V.mw[0] * px + V.mw[1] * py + V.mw[2] * pz + V.mw[3];
+        if (!(w > 0.f)) return 0;
+        const float u = (V.mu[0] * px + V.mu[1] * py + V.mu[2] * pz + V.mu[3]) / w;
+        const float v = (V.mv[0] * px + V.mv[1] * py + V.mv[2] * pz + V.mv[3]) / w;
+        wmin = fminf(wmin, w);
+        wmax = fmaxf(wmax, w);
+        umin = fminf(umin, u);
+        umax = fmaxf(umax, u);
+        vmin = fminf(vmin, v);
+        vmax = fmaxf(vmax, v);
+    }
+    const float m = 1.f / 64.f;
+    return (wmin > 1e-5f * wmax && umin >= ulo + m && umax <= uhi - m && vmin >= vlo + m && vmax <= vhi - m) ? 1 : 0;
+}
+
 // PerspectiveBeamsBackProjection.cl:28-71: n^3 sub-voxel samples, each weighted by
 // its own chord through the voxel; optional intensity clamps.
 template <bool kMask, int kStore, int kSampling, bool kClamp>
@@ -1830,6 +1861,17 @@ __global__ void __launch_bounds__(256) bp_perspective_kernel(const __grid_consta
     const int x = blockIdx.y * blockDim.x + threadIdx.x;
     const int y = blockIdx.z * blockDim.y + threadIdx.y;
     const int z0 = blockIdx.x * kBpZPersp;
+    if (a.persp_n == 1 && kSampling == kSampleQ8) {
+        // per view, whether the block's voxels can skip the texel-coordinate clamps
+        const int tid = threadIdx.y * blockDim.x + threadIdx.x, nt = blockDim.x * blockDim.y;
+        const int bx0 = blockIdx.y * blockDim.x, by0 = blockIdx.z * blockDim.y;
+        const int bx1 = min(g.rx, bx0 + (int)blockDim.x) - 1, by1 = min(g.ry, by0 + (int)blockDim.y) - 1;
+        const int bz1 = min(g.rz, z0 + kBpZPersp) - 1;
+        for (int p = tid; p < a.nviews; p += nt)
+            sv[p].inside = brick_projects_inside(sv[p], g, bx0, bx1, by0, by1, z0, bz1, -1.5f,
+                                                 (float)a.W + 1.49609375f, -1.5f, (float)a.H + 1.49609375f);
+        __syncthreads();
+    }
     if (x >= g.rx || y >= g.ry) return;
     const int nzc = min(kBpZPersp, g.rz - z0);
     const size_t plane = (size_t)g.rx * (size_t)g.ry;
@@ -1881,6 +1923,10 @@ __global__ void __launch_bounds__(256) bp_perspective_kernel(const __grid_consta
                 // out there every texel is a zero pad, as it is for the unclamped coordinate
                 const float2 lo = splat(-1.5f), hi = f2((float)a.W + 1.49609375f, (float)a.H + 1.49609375f);
                 const int pitch = (int)a.rl_pitch;
+                // kCoordClamp false when the whole brick projects inside (V.inside): the clamps
+                // would change no coordinate
+                auto zloop = [&](auto clamp_tag) {
+                constexpr bool kCoordClamp = decltype(clamp_tag)::value;
 #pragma unroll
                 for (int j = 0; j < kBpZPersp; ++j) {
                     if (!kFull && j >= nzc) continue;
@@ -1896,7 +1942,8 @@ __global__ void __launch_bounds__(256) bp_perspective_kernel(const __grid_consta
                         // the clamped coordinates): texel floor(q / 256), weight (q & 255) / 256,
                         // the split of split_coord with its 1/256 weights (a weight that rounds
                         // up to 1 is weight 0 on the next texel, the same blend)
-                        const float2 uc = f2(fminf(fmaxf(uv.x, lo.x), hi.x), fminf(fmaxf(uv.y, lo.y), hi.y));
+                        const float2 uc =
+                            kCoordClamp ? f2(fminf(fmaxf(uv.x, lo.x), hi.x), fminf(fmaxf(uv.y, lo.y), hi.y)) : uv;
                         const float2 fq = __fadd2_rd(fma2(uc, splat(256.f), splat(-127.5f)), splat(12582912.0f));
                         const int bu = __float_as_int(fq.x), bv = __float_as_int(fq.y);
                         const int x0 = (bu - 0x4B400000) >> 8, y0 = (bv - 0x4B400000) >> 8;
@@ -1932,6 +1979,9 @@ __global__ void __launch_bounds__(256) bp_perspective_kernel(const __grid_consta
                     if (kStore == 1) vj = __half2float(__float2half_rn(vj));
                     val[j] = vj;
                 }
+                };
+                if (kSampling == kSampleQ8 && V.inside) zloop(std::false_type{});
+                else zloop(std::true_type{});
             }
         };
         if (nzc == kBpZPersp) views(std::true_type{});
