@@ -676,21 +676,42 @@ def c4_shapes(seed: int = 4000):
     return out
 
 
-def run_c4(args):
+def c4_shard(shapes, rank: int, world: int):
+    """The series (indices into `shapes`) rank `rank` of `world` reconstructs: the series
+    are independent, so they are dealt out with no exchange between ranks -- largest work
+    first (voxel-view updates of one iteration) to the rank with the least work so far,
+    ties to the lower rank.  Every rank computes the same deal."""
+    work = [s[0][0] * s[0][1] * s[0][2] * s[1] for s in shapes]
+    load = [0] * world
+    owner = [0] * len(shapes)
+    for i in sorted(range(len(shapes)), key=lambda i: (-work[i], i)):
+        r = min(range(world), key=lambda k: (load[k], k))
+        owner[i] = r
+        load[r] += work[i]
+    return [i for i in range(len(shapes)) if owner[i] == rank]
+
+
+def run_c4(args, rank: int = 0, world: int = 1, local: int = 0):
     """Batched SART of the 64 C4 series (the whole iteration of every series in one
     persistent launch, its launch shape from the autotuner) against the same series one
     after another (one graph per series).  Volumes are FP32 masters with an FP16 shadow
     (the forward projections read FP16 values, updates accumulate in FP32); --c4-f32
-    keeps plain FP32 volumes."""
+    keeps plain FP32 volumes.  Under torchrun each rank batches its share of the 64
+    series (c4_shard; strong scaling of the fixed job, no data exchange) and the times are
+    the max over ranks."""
     import torch
     from ettention_b200 import _abi
     from ettention_b200.operators import (AlgebraicParameterSet, BatchReconstructionOperator,
                                           BlockIterativeReconstructionOperator, Context,
                                           ForwardProjectionOperator, GPUMappedVolume, mrc_base_geometry)
-    ctx = Context(0)
-    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(local)
+    ctx = Context(local)
+    dev = torch.device("cuda", local)
     problems = []
-    for i, ((X, Y, Z), nv, tmax) in enumerate(c4_shapes()):
+    shapes = c4_shapes()
+    mine = c4_shard(shapes, rank, world)
+    for i in mine:
+        (X, Y, Z), nv, tmax = shapes[i]
         ph = make_phantom_torch(4100 + i, dev, (X, Y, Z), count=40, axes=(4.0, 48.0))
         geoms = [mrc_base_geometry(X, Y).rotated(float(a)) for a in np.linspace(-tmax, tmax, nv)]
         vol = GPUMappedVolume(ctx, (X, Y, Z))
@@ -724,8 +745,10 @@ def run_c4(args):
     tuned = ctx.tune_report()
     for _ in range(args.warmup):
         batch.runNiterations(1)
-    with ClockSampler(0) as clk:
+    barrier(world)
+    with ClockSampler(local) as clk:
         batch_ms = timed(lambda: batch.runNiterations(1), args.steps)
+    batch_ms = max_over_ranks(batch_ms, world)
     launches = batch.launches_per_iteration
     batch.close()
     for v in vols:
@@ -741,22 +764,28 @@ def run_c4(args):
             rec.runNiterations(1)
     for _ in range(args.warmup):
         run_seq()
-    seq_ms = timed(run_seq, args.steps)
+    barrier(world)
+    seq_ms = max_over_ranks(timed(run_seq, args.steps), world)
     seq_launches = sum(r.launches_per_iteration for _, r in seq)
     for vol, rec in seq:
         rec.close()
         vol.close()
-    updates = sum(s[0] * s[1] * s[2] * len(g) for s, g, _ in problems)
-    byts = sum(len(g) * (3 * s[0] * s[1] * s[2] * 4 + 20 * s[0] * s[1]) for s, g, _ in problems)
+    # work of the whole job (every rank's series)
+    updates = sum(s[0][0] * s[0][1] * s[0][2] * s[1] for s in shapes)
+    byts = sum(s[1] * (3 * s[0][0] * s[0][1] * s[0][2] * 4 + 20 * s[0][0] * s[0][1]) for s in shapes)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except OSError:
         pass
-    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    hbm = float(peaks.get("hbm_gbs", 6650.0)) * world  # the job's bytes over every rank's HBM
+    if rank != 0:
+        ctx.close()
+        return
     print(json.dumps({
         "metric": "C4 batched SART ms per iteration (64 series)", "value": batch_ms, "unit": "ms",
-        "higher_is_better": False, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": False, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "scaling": "strong", "series_of_rank0": len(mine),
         "dtype": "f32" if args.c4_f32 else "f32 math, f16 shadow, f32 master",
         "tuned_launch_shape": tuned.strip().splitlines(),
         "data": "synthetic (seeded 40-ellipsoid phantoms per series, CUDA-forward-projected, noise-free)",
@@ -767,7 +796,7 @@ def run_c4(args):
         "voxel_updates_per_s": updates / (batch_ms * 1e-3),
         "roofline": {"bound": "hbm", "achieved": byts / (batch_ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
                      "frac": byts / (batch_ms * 1e-3) / 1e9 / hbm,
-                     "bytes": "per view: 4V forward read + 8V back read+write + 20P"},
+                     "bytes": "per view: 4V forward read + 8V back read+write + 20P", "gpus": world},
         "clocks": clk.summary()}))
     ctx.close()
 
@@ -1128,9 +1157,7 @@ def main():
     if args.ncu_case:
         run_ncu_case(tuple(int(v) for v in args.ncu_res.split(",")))
         return
-    if args.workload == "c4":
-        run_c4(args)
-        return
+
     if args.workload == "c3":
         print(json.dumps(run_c3(args)), flush=True)
         return
@@ -1146,6 +1173,8 @@ def main():
             run_reference(args, rank, world)
         elif args.workload == "slabs":
             run_slabs(args, rank, world, local)
+        elif args.workload == "c4":
+            run_c4(args, rank, world, local)
         else:
             run_ours(args, rank, world, local)
     finally:

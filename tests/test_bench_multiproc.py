@@ -81,3 +81,19 @@ def test_single_process_needs_no_process_group(monkeypatch):
     assert bench.dist_init() == (0, 1, 0)
     assert not dist.is_initialized()
     assert bench.max_over_ranks(7.0, 1) == 7.0
+
+
+@pytest.mark.parametrize("world", [1, 2, 3, 8])
+def test_c4_series_are_dealt_out_once_and_evenly(world):
+    """bench.py --workload c4 under torchrun: every one of the 64 independent series goes to
+    exactly one rank, every rank computes the same deal, and the ranks' work (voxel-view
+    updates per iteration) stays within the largest series of the mean."""
+    import bench
+    shapes = bench.c4_shapes()
+    deal = [bench.c4_shard(shapes, r, world) for r in range(world)]
+    flat = sorted(i for d in deal for i in d)
+    assert flat == list(range(len(shapes)))
+    assert deal == [bench.c4_shard(shapes, r, world) for r in range(world)]
+    work = [s[0][0] * s[0][1] * s[0][2] * s[1] for s in shapes]
+    loads = [sum(work[i] for i in d) for d in deal]
+    assert max(loads) - min(loads) <= max(work)
