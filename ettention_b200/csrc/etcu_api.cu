@@ -1802,6 +1802,10 @@ etcu_status recon_build(etcu_volume* vol, const etcu_view* views, uint32_t n_vie
     size_t slot_bytes = round_up(pitch_bytes * ph, std::max<size_t>(ctx->tex_align, 256));
     r->rl_pitch = pitch_bytes / sizeof(float2);
     r->rl_slot = slot_bytes / sizeof(float2);
+    // the data-residual pass (etcu_recon_data_residual_sq) projects as many views per
+    // launch as there are slots: add slots up to all views while they fit in 64 MiB
+    r->slots = std::max<uint32_t>(
+        r->slots, std::min<uint32_t>(M, (uint32_t)std::max<size_t>(1, ((size_t)64 << 20) / slot_bytes)));
     if ((s = dalloc_aligned(ctx, &r->rl_raw, (void**)&r->rl_base, slot_bytes * r->slots, ctx->tex_align)) != ETCU_OK)
         return s;
     CK(ctx, cudaMemsetAsync(r->rl_base, 0, slot_bytes * r->slots, ctx->stream));

@@ -92,16 +92,18 @@ class PlainSart:
     series, with the volume exchangeable through device memory."""
 
     def __init__(self, ctx: Context, series: Series, lam: float = LAMBDA):
+        import torch
         self.ctx = ctx
         self.vol = GPUMappedVolume(ctx, series.res)
+        X, Y, Z = series.res
+        self._zeros = torch.zeros((Z, Y, X), dtype=torch.float32, device=torch.device("cuda", ctx.device))
+        torch.cuda.synchronize(self._zeros.device)  # filled on torch's stream, read on the library's
         p = AlgebraicParameterSet(algorithm="sart", block_size=1, iterations=1, lam=lam, order=_abi.ORDER_IDENTITY)
         self.rec = BlockIterativeReconstructionOperator(self.vol, series.geoms, series.b, p, use_graph=True)
 
     def set_volume(self, t=None) -> None:
-        if t is None:
-            self.vol.upload(np.zeros(self.vol.resolution[::-1], np.float32))
-        else:
-            self.vol.upload_device(t)
+        """The volume from device tensor t, or zero (a device-to-device copy of zeros)."""
+        self.vol.upload_device(self._zeros if t is None else t)
 
     def get_volume(self, t) -> None:
         self.vol.download_device(t)
