@@ -1435,7 +1435,7 @@ __device__ __forceinline__ void fused_row_step(const FuseArgs& a, uint32_t p, in
         const int z0 = chunk_z0(c), z1 = min(rz, z0 + kFuseZc);
         float* cb = buf + (size_t)(c & 1) * chunk_elems;
         float* dst = a.vol + ((size_t)z0 * ry + y) * rx + x2;
-        for (int z = z0; z < z1; ++z, dst += plane) {
+        auto voxel = [&](int z, float* d) {
             float2* slot = reinterpret_cast<float2*>(cb + (size_t)(z - z0) * rx + x2);
             const float2 v = *slot;
             const float vin[2] = {v.x, v.y};
@@ -1459,8 +1459,14 @@ __device__ __forceinline__ void fused_row_step(const FuseArgs& a, uint32_t p, in
                 vout[q] = RL.y > kEps ? fadd(vin[q], cc) : vin[q];
             }
             const float2 o = make_float2(vout[0], vout[1]);
-            *reinterpret_cast<float2*>(dst) = o;
+            *reinterpret_cast<float2*>(d) = o;
             *slot = kShadow ? make_float2(shadow_value<kShadow>(o.x), shadow_value<kShadow>(o.y)) : o;
+        };
+        if (z1 - z0 == kFuseZc) {  // a whole chunk: its rows unrolled
+#pragma unroll
+            for (int k = 0; k < kFuseZc; ++k) voxel(z0 + k, dst + (size_t)k * plane);
+        } else {
+            for (int z = z0; z < z1; ++z, dst += plane) voxel(z, dst);
         }
     };
     // FP walk of the rays through the updated chunk c (dda_walk_xz's steps, chunk-local
