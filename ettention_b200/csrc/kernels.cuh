@@ -1416,7 +1416,13 @@ __device__ __forceinline__ void fused_row_step(const FuseArgs& a, uint32_t p, in
             const int z0 = chunk_z0(c), z1 = min(rz, z0 + kFuseZc);
             float* dst = buf + (size_t)(c & 1) * chunk_elems + x2;
             const float* src = a.vol + ((size_t)z0 * ry + y) * rx + x2;
-            for (int z = z0; z < z1; ++z, dst += rx, src += plane) cp_async8(smem_addr(dst), src);
+            if (z1 - z0 == kFuseZc) {  // a whole chunk: its rows unrolled
+                const uint32_t d0 = smem_addr(dst);
+#pragma unroll
+                for (int k = 0; k < kFuseZc; ++k) cp_async8(d0 + 4u * (uint32_t)(k * rx), src + (size_t)k * plane);
+            } else {
+                for (int z = z0; z < z1; ++z, dst += rx, src += plane) cp_async8(smem_addr(dst), src);
+            }
         }
         cp_async_commit();
     };
