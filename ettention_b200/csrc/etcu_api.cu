@@ -53,6 +53,10 @@ struct etcu_context {
     int fuse_withhold_row = -1; // tests of the bounded waits (ETCU_TEST_WITHHOLD_ROW)
     int autotune = 0;           // 1: launch shapes from the tuner's cache, timed on a miss (ETCU_AUTOTUNE)
     std::string tune_log;       // the choices made on this context, one line each
+    // device memory of the context's objects: a stream-ordered pool that keeps freed memory
+    // for the next allocation (volumes and reconstructions created and destroyed call after
+    // call then cost no driver allocation or release); trimmed when the context is destroyed
+    cudaMemPool_t pool = nullptr;
 };
 
 struct etcu_volume {
@@ -140,7 +144,7 @@ etcu_status fail(etcu_context* ctx, etcu_status st, const char* fmt, ...) {
 etcu_status dalloc(etcu_context* ctx, void** p, size_t bytes) {
     *p = nullptr;
     if (bytes == 0) return ETCU_OK;
-    cudaError_t e = cudaMalloc(p, bytes);
+    cudaError_t e = ctx && ctx->pool ? cudaMallocFromPoolAsync(p, bytes, ctx->pool, ctx->stream) : cudaMalloc(p, bytes);
     if (e != cudaSuccess) {
         cudaGetLastError();
         return fail(ctx, ETCU_ERR_OUT_OF_MEMORY, "device allocation of %zu bytes failed: %s", bytes,
@@ -162,7 +166,8 @@ etcu_status dalloc_aligned(etcu_context* ctx, void** raw, void** aligned, size_t
 
 void dfree(etcu_context* ctx, void* p, size_t bytes) {
     if (p) {
-        cudaFree(p);
+        if (ctx->pool) cudaFreeAsync(p, ctx->stream);
+        else cudaFree(p);
         ctx->bytes -= std::min(ctx->bytes, bytes);
     }
 }
@@ -675,6 +680,20 @@ extern "C" etcu_status etcu_context_create(int device, etcu_context** out) {
     if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamDefault) != cudaSuccess)
         return fail(nullptr, ETCU_ERR_CUDA, "cudaStreamCreate failed");
     c->stream = c->own_stream;
+    {
+        cudaMemPoolProps pp{};
+        pp.allocType = cudaMemAllocationTypePinned;
+        pp.handleTypes = cudaMemHandleTypeNone;
+        pp.location.type = cudaMemLocationTypeDevice;
+        pp.location.id = device;
+        if (cudaMemPoolCreate(&c->pool, &pp) == cudaSuccess) {
+            uint64_t keep = ~0ull;  // never release freed memory while the context lives
+            cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        } else {
+            cudaGetLastError();
+            c->pool = nullptr;  // plain cudaMalloc / cudaFree
+        }
+    }
     if (const char* env = getenv("ETCU_BP_COLUMN")) c->bp_column = atoi(env) != 0;
     if (const char* env = getenv("ETCU_FUSED")) c->fused_step = atoi(env) != 0;
     if (const char* env = getenv("ETCU_PERSIST")) c->fused_persist = atoi(env) != 0;
@@ -689,7 +708,12 @@ extern "C" etcu_status etcu_context_destroy(etcu_context* ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     if (ctx->pair_tex) cudaDestroyTextureObject(ctx->pair_tex);
-    if (ctx->pair_raw) cudaFree(ctx->pair_raw);
+    if (ctx->pair_raw) dfree(ctx, ctx->pair_raw, 0);
+    cudaStreamSynchronize(ctx->stream);
+    if (ctx->pool) {
+        cudaMemPoolTrimTo(ctx->pool, 0);
+        cudaMemPoolDestroy(ctx->pool);  // released once every allocation from it is freed
+    }
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return ETCU_OK;
