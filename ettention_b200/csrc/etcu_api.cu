@@ -1468,15 +1468,17 @@ uint32_t issue_fused_iteration(etcu_recon* r, cudaStream_t st) {
 void fuse_limits(int dev, size_t smem, int& per_sm, int& persist_per_sm, int& sms) {
     static std::mutex mu;
     static std::vector<char> opted;
-    cudaDeviceProp prop;
-    const bool have_prop = cudaGetDeviceProperties(&prop, dev) == cudaSuccess;
+    // two attributes, not cudaGetDeviceProperties (milliseconds per call, once per reconstruction)
+    int optin = 0, nsm = 0;
+    const bool have_prop = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess &&
+                           cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess;
     if (!have_prop) cudaGetLastError();
     {
         std::lock_guard<std::mutex> lock(mu);
         if ((int)opted.size() <= dev) opted.resize(dev + 1, 0);
         if (!opted[dev]) {
             if (have_prop) {
-                const int full = (int)prop.sharedMemPerBlockOptin, persist = full - 16;
+                const int full = optin, persist = full - 16;
                 cudaFuncSetAttribute(sart_fused_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, full);
                 cudaFuncSetAttribute(sart_fused_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, full);
                 cudaFuncSetAttribute(sart_fused_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, full);
@@ -1491,7 +1493,7 @@ void fuse_limits(int dev, size_t smem, int& per_sm, int& persist_per_sm, int& sm
             opted[dev] = 1;
         }
     }
-    sms = have_prop ? prop.multiProcessorCount : 0;
+    sms = have_prop ? nsm : 0;
     per_sm = persist_per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sart_fused_kernel<0>, kFuseThreads, smem) !=
         cudaSuccess) {
