@@ -86,6 +86,8 @@ int cin_total(const LayerDef& d) { return d.cin_used0 + d.cin1; }
 // that exceeds 64 (the 96-input decoder layer), as two: source 0's and source 1's.
 int dx_split(const LayerDef& d) { return cin_total(d) > 64 ? d.cin0 : cin_total(d); }
 size_t layer_params(const LayerDef& d) { return (size_t)27 * d.cout * cin_total(d) + d.cout; }
+// Tensor-core forward layers of 16 outputs (not the first and the last, which run on the CUDA cores).
+bool zfold_layer(int l) { return l > 0 && l < kLayers - 1 && kDefs[l].npad == 16; }
 
 size_t total_params() {
     size_t n = 0;
@@ -122,6 +124,10 @@ struct etcu_warmstart {
     double* d_loss = nullptr;
     std::string err;
     int loader = -1;  // convolution operand loads: -1 default (tensor copies), 0 tensor copies, 1 cp.async (ETCU_CONV_LOADER)
+    // forward convolutions of 16 outputs as the z-streamed kernel with dz folded into N
+    // (ws::conv_zfold_kernel; ETCU_CONV_ZFOLD=0 keeps them on conv_tc_kernel)
+    int zfold = 1;
+    __nv_bfloat16* wz[kLayers] = {};  // its weight layout
 };
 
 namespace {
@@ -244,6 +250,38 @@ etcu_status launch_conv_n(etcu_warmstart* w, const CUtensorMap& m0, const CUtens
     }
     if (!launch(choice))
         return wfail(w, ETCU_ERR_CUDA, "convolution launch failed: %s", cudaGetErrorString(last));
+    return ETCU_OK;
+}
+
+// The z-streamed 16-output convolution: TY = 2 rows per tile (four 96-column slices of
+// tensor memory), work units of one (x tile, y tile) column over kZseg output slices.
+constexpr int kZfoldRows = 2, kZseg = 32;
+
+etcu_status launch_zfold(etcu_warmstart* w, const CUtensorMap& m0, const CUtensorMap& m1, ws::ZfoldArgs a,
+                         int batch) {
+    using SH = ws::ZfoldShape<kZfoldRows>;
+    const size_t wbytes = (size_t)a.nsteps * SH::kW;
+    a.resident = wbytes <= kResidentMax ? 1 : 0;
+    const size_t wres = a.resident ? (wbytes + 1023) & ~(size_t)1023 : 0;
+    const size_t stage = (SH::kHalo + (a.resident ? 0 : SH::kW) + 1023) & ~(size_t)1023;
+    const int S = (int)std::min<size_t>(4, (kConvSmemMax - wres) / stage);
+    if (S < 2) return wfail(w, ETCU_ERR_UNSUPPORTED, "z-streamed convolution stage of %zu bytes does not fit", stage);
+    a.batch = batch;
+    a.stages = S;
+    a.zseg = kZseg;
+    static std::atomic<unsigned long long> opted{0};
+    if (w->device < 64 && !(opted.load() & (1ull << w->device))) {
+        WCK(w, cudaFuncSetAttribute(ws::conv_zfold_kernel<kZfoldRows>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    232448));
+        opted.fetch_or(1ull << w->device);
+    }
+    const long units = (long)((a.X + ws::kTileX - 1) / ws::kTileX) * ((a.Y + kZfoldRows - 1) / kZfoldRows) *
+                       ((a.Z + kZseg - 1) / kZseg) * batch;
+    const unsigned grid = (unsigned)std::min<long>(units, w->sms);
+    // at least 120 KB, so that one CTA (and its 512 tensor-memory columns) owns each SM
+    const size_t smem = std::max<size_t>(wres + (size_t)S * stage + (2 * S + 9) * 8 + 16 + 1024, 120 * 1024);
+    ws::conv_zfold_kernel<kZfoldRows><<<grid, 192, smem, w->stream>>>(m0, m1, a);
+    WCK(w, cudaGetLastError());
     return ETCU_OK;
 }
 
@@ -399,6 +437,11 @@ etcu_status relayout(etcu_warmstart* w) {
         const int nf = nsteps_f * 27 * 2 * d.npad * 8;
         ws::relayout_forward_kernel<<<blocks(nf), 256, 0, w->stream>>>(w->params + w->woff[l], d.cout, cin_total(d),
                                                                        d.npad, nsteps_f, w->wf[l]);
+        if (w->wz[l]) {
+            const int nz = nsteps_f * 9 * 2 * 48 * 8;
+            ws::relayout_zfold_kernel<<<blocks(nz), 256, 0, w->stream>>>(w->params + w->woff[l], d.cout, cin_total(d),
+                                                                         nsteps_f, w->wz[l]);
+        }
         if (l > 0) {
             const int nsteps_b = (d.cout + 15) / 16;
             const int n0 = dx_split(d), n1 = cin_total(d) - n0;
@@ -442,6 +485,25 @@ etcu_status forward(etcu_warmstart* w, const float* d_in, float* d_out, int B, b
         c.relu = true;
         c.n = d.npad;
         c.dst0 = dst(out);
+        if (w->zfold && w->wz[l]) {  // 16 outputs: the z-streamed kernel
+            CUtensorMap m0, m1;
+            WTRY(make_map(w, &m0, s0, B, ws::kHaloX, kZfoldRows + 2, 1, 2));
+            WTRY(make_map(w, &m1, s1 ? *s1 : s0, B, ws::kHaloX, kZfoldRows + 2, 1, 2));
+            ws::ZfoldArgs z{};
+            z.X = s0.g.X;
+            z.Y = s0.g.Y;
+            z.Z = s0.g.Z;
+            z.nsteps = c.nsteps0 + c.nsteps1;
+            z.nkp0 = c.nsteps0;
+            z.c8_0 = s0.C / 8;
+            z.c8_1 = s1 ? s1->C / 8 : 0;
+            z.w = w->wz[l];
+            z.bias = c.bias;
+            z.relu = 1;
+            z.dst = c.dst0;
+            z.err = w->d_err;
+            return launch_zfold(w, m0, m1, z, B);
+        }
         return conv(w, c, B);
     };
     // first layer (one input channel) on the CUDA cores
@@ -635,6 +697,7 @@ extern "C" etcu_status etcu_warmstart_create(etcu_context* ctx, const uint32_t r
     WCK(w.get(), cudaDeviceGetAttribute(&w->sms, cudaDevAttrMultiProcessorCount, w->device));
     w->max_batch = (int)max_batch;
     if (const char* env = getenv("ETCU_CONV_LOADER")) w->loader = atoi(env) ? 1 : 0;
+    if (const char* env = getenv("ETCU_CONV_ZFOLD")) w->zfold = atoi(env) ? 1 : 0;
     w->g1 = Grid{(int)resolution[0], (int)resolution[1], (int)resolution[2]};
     w->g2 = Grid{w->g1.X / 2, w->g1.Y / 2, w->g1.Z / 2};
     w->g3 = Grid{w->g2.X / 2, w->g2.Y / 2, w->g2.Z / 2};
@@ -657,6 +720,7 @@ extern "C" etcu_status etcu_warmstart_create(etcu_context* ctx, const uint32_t r
     for (int l = 0; l < kLayers; ++l) {
         const LayerDef& d = kDefs[l];
         WTRY(walloc(p, (void**)&p->wf[l], (size_t)(d.cin0 + d.cin1) / 16 * 27 * 2 * d.npad * 8 * 2));
+        if (zfold_layer(l)) WTRY(walloc(p, (void**)&p->wz[l], (size_t)(d.cin0 + d.cin1) / 16 * 9 * 2 * 48 * 8 * 2));
         if (l > 0) {
             const size_t per = (size_t)((d.cout + 15) / 16) * 27 * 2 * 8 * 2;
             WTRY(walloc(p, (void**)&p->wb[l], per * dx_split(d)));

@@ -503,6 +503,276 @@ __global__ void __launch_bounds__(conv_threads<kLoad>(), 1) conv_tc_kernel(const
     }
 }
 
+// ---------------------------------------------------------------- z-streamed convolution, 16 outputs
+// For the 16-output-channel layers the MMAs above are N = 16 wide and re-read their 128-row
+// A operand from shared memory for each of the 27 taps.  Here a CTA walks a column of
+// tiles (128 x-voxels by TY y-rows) along z, one input z slice at a time, and folds the
+// three dz taps into N: for input slice zi and tap (dy, dx) one MMA of N = 48 computes
+// D[zi][g][o] = sum_{c, dy, dx} W[dz = g - 1][dy][dx][c][o] * In[zi][y + dy - 1][x + dx - 1][c]
+// for g = 0, 1, 2, and the epilogue forms out[z] = D[z - 1][0] + D[z][1] + D[z + 1][2]
+// (the 3x3x3 convolution; zero slices outside the volume come from the tensor copy's
+// out-of-range fill).  So 9 MMAs per K step and row instead of 27, and a 1-slice halo
+// instead of 3.  Slice j of a segment (zi = z0 - 1 + j) accumulates in tensor-memory slot
+// (global slice count) % 4 of TY x 48 columns; the epilogue of output z0 + j - 2 (after
+// slice j) reads slots of j - 2, j - 1, j and releases j - 2's (all three at the
+// segment's last output), so the MMAs run up to two slices ahead of the epilogue.
+template <int TY>
+struct ZfoldShape {
+    static constexpr uint32_t kPlane = (uint32_t)kHaloX * (TY + 2) * 16u;  // one 8-channel chunk, one z
+    static constexpr uint32_t kHalo = 2u * kPlane;                         // 16 channels = one K step
+    static constexpr uint32_t kW = 9u * 2u * 48u * 16u;                    // one step's weights
+    static constexpr uint32_t kSlot = (uint32_t)TY * 48u;                  // tensor-memory columns per slice
+    static_assert(4 * kSlot <= 512, "four slices must fit in tensor memory");
+};
+
+struct ZfoldArgs {
+    int X, Y, Z, batch;
+    int zseg;              // output z slices per work unit
+    int nsteps, nkp0, c8_0, c8_1;
+    const __nv_bfloat16* w;  // [step][9 taps (dy, dx)][2 halves][48 = 3 dz x 16][8] bf16
+    int resident;
+    const float* bias;     // 16 values
+    int relu;
+    ConvDst dst;           // 16 channels
+    int stages;
+    unsigned* err;
+};
+
+template <int TY>
+__global__ void __launch_bounds__(192, 1) conv_zfold_kernel(const __grid_constant__ CUtensorMap src0,
+                                                            const __grid_constant__ CUtensorMap src1, ZfoldArgs a) {
+    using SH = ZfoldShape<TY>;
+    constexpr uint32_t kIdesc = idesc_bf16(128, 48, 0, 0);
+    constexpr uint32_t kCols = 512;
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    const int S = a.stages;
+    const uint32_t wres = a.resident ? (uint32_t)a.nsteps * SH::kW : 0u;
+    const uint32_t stage = (SH::kHalo + (a.resident ? 0u : SH::kW) + 1023u) & ~1023u;
+    uint8_t* wsm = smem;
+    uint8_t* ring = smem + ((wres + 1023u) & ~1023u);
+    uint64_t* full = (uint64_t*)(ring + (size_t)S * stage);
+    uint64_t* empty = full + S;
+    uint64_t* accf = empty + S;  // [4] slice written (MMA -> epilogue)
+    uint64_t* acce = accf + 4;   // [4] slice released (epilogue -> MMA)
+    uint64_t* wbar = acce + 4;
+    uint32_t* tmem_slot = (uint32_t*)(wbar + 1);
+
+    const int ntx = (a.X + kTileX - 1) / kTileX;
+    const int nty = (a.Y + TY - 1) / TY;
+    const int nseg = (a.Z + a.zseg - 1) / a.zseg;
+    const int nunits = ntx * nty * nseg * a.batch;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    auto unit_of = [&](int u, int& xt, int& yt, int& z0, int& len, int& n) {
+        xt = u % ntx;
+        u /= ntx;
+        yt = u % nty;
+        u /= nty;
+        const int sg = u % nseg;
+        n = u / nseg;
+        z0 = sg * a.zseg;
+        len = min(a.zseg, a.Z - z0);
+    };
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int i = 0; i < 4; ++i) {
+            mbar_init(&accf[i], 1);
+            mbar_init(&acce[i], 4);
+        }
+        mbar_init(wbar, 1);
+        mbar_fence_init();
+    }
+    if (warp == 0) tmem_alloc(tmem_slot, kCols);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            if (a.resident) {
+                mbar_expect_tx(wbar, wres);
+                bulk_load(wsm, a.w, wres, wbar);
+            }
+            int q = 0;
+            bool ok = true;
+            for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+                int xt, yt, z0, len, n;
+                unit_of(u, xt, yt, z0, len, n);
+                for (int j = 0; j < len + 2 && ok; ++j)
+                    for (int s = 0; s < a.nsteps; ++s, ++q) {
+                        const int st = q % S;
+                        if (q >= S && !mbar_wait(&empty[st], ((q / S) - 1) & 1)) {
+                            atomicOr(a.err, kErrWaitEmpty);
+                            ok = false;
+                            break;
+                        }
+                        uint8_t* halo = ring + (size_t)st * stage;
+                        mbar_expect_tx(&full[st], SH::kHalo + (a.resident ? 0u : SH::kW));
+                        const bool second = s >= a.nkp0;
+                        const int kp = second ? s - a.nkp0 : s;
+                        const int c4 = n * (second ? a.c8_1 : a.c8_0) + 2 * kp;
+                        tma_load_5d(halo, second ? &src1 : &src0, &full[st], 0, xt * kTileX - 1, yt * TY - 1,
+                                    z0 - 1 + j, c4);
+                        if (!a.resident)
+                            bulk_load(halo + SH::kHalo, a.w + (size_t)s * (SH::kW / 2), SH::kW, &full[st]);
+                    }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            bool ok = !a.resident || mbar_wait(wbar, 0);
+            if (!ok) atomicOr(a.err, kErrWaitFull);
+            int q = 0, G = 0;
+            for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+                int xt, yt, z0, len, n;
+                unit_of(u, xt, yt, z0, len, n);
+                for (int j = 0; j < len + 2 && ok; ++j, ++G) {
+                    const int slot = G & 3;
+                    if (G >= 4 && !mbar_wait(&acce[slot], ((G >> 2) - 1) & 1)) {
+                        atomicOr(a.err, kErrWaitEmpty);
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t dslot = tmem + (uint32_t)slot * SH::kSlot;
+                    for (int s = 0; s < a.nsteps; ++s, ++q) {
+                        const int st = q % S;
+                        if (!mbar_wait(&full[st], (q / S) & 1)) {
+                            atomicOr(a.err, kErrWaitFull);
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                        const uint32_t hbase = smem_u32(ring + (size_t)st * stage);
+                        const uint32_t wbase =
+                            a.resident ? smem_u32(wsm) + (uint32_t)s * SH::kW : hbase + SH::kHalo;
+#pragma unroll 1
+                        for (int tap = 0; tap < 9; ++tap) {
+                            const int dy = tap / 3, dx = tap % 3;
+                            const uint64_t bd = sdesc(wbase + (uint32_t)tap * (2u * 48u * 16u), 48u * 16u, 128);
+#pragma unroll
+                            for (int ty = 0; ty < TY; ++ty) {
+                                const uint32_t aoff = (uint32_t)(((ty + dy) * kHaloX + dx) * 16);
+                                umma_bf16(dslot + (uint32_t)(ty * 48), sdesc(hbase + aoff, SH::kPlane, 128), bd,
+                                          kIdesc, (s > 0 || tap > 0) ? 1u : 0u);
+                            }
+                        }
+                        umma_commit(&empty[st]);
+                    }
+                    if (!ok) break;
+                    umma_commit(&accf[slot]);
+                }
+            }
+        }
+    } else {
+        // epilogue: warp quarter (warp % 4) reads tensor-memory lanes 32 * (warp % 4) ...
+        const int quarter = warp & 3;
+        const int m = quarter * 32 + lane;
+        const size_t plane = (size_t)a.Z * a.Y * a.X;
+        int G = 0;
+        bool ok = true;
+        for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+            int xt, yt, z0, len, n;
+            unit_of(u, xt, yt, z0, len, n);
+            const int x = xt * kTileX + m;
+            for (int j = 0; j < len + 2; ++j, ++G) {
+                if (j < 2) continue;  // output z0 + j - 2 needs slices j - 2, j - 1, j
+                const bool got = mbar_wait(&accf[G & 3], (G >> 2) & 1);
+                __syncwarp();
+                if (!got) {
+                    if (lane == 0) atomicOr(a.err, kErrWaitDone);
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const int z = z0 + j - 2;
+                const uint32_t lanes = (uint32_t)(quarter * 32) << 16;
+                const uint32_t s0 = tmem + lanes + (uint32_t)((G - 2) & 3) * SH::kSlot;
+                const uint32_t s1 = tmem + lanes + (uint32_t)((G - 1) & 3) * SH::kSlot;
+                const uint32_t s2 = tmem + lanes + (uint32_t)(G & 3) * SH::kSlot;
+#pragma unroll 1
+                for (int ty = 0; ty < TY; ++ty) {
+                    const int y = yt * TY + ty;
+                    uint32_t r0[16], r1[16], r2[16];
+                    tmem_ld16(s0 + (uint32_t)(ty * 48), r0);       // dz = -1 of slice z - 1
+                    tmem_ld16(s1 + (uint32_t)(ty * 48 + 16), r1);  // dz = 0 of slice z
+                    tmem_ld16(s2 + (uint32_t)(ty * 48 + 32), r2);  // dz = +1 of slice z + 1
+                    tmem_wait_ld();
+                    if (x >= a.X || y >= a.Y) continue;
+                    const size_t vox = ((size_t)z * a.Y + y) * a.X + x;
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        float v[8];
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) {
+                            const int c = h * 8 + k;
+                            v[k] = __uint_as_float(r0[c]) + __uint_as_float(r1[c]) + __uint_as_float(r2[c]);
+                            if (a.bias) v[k] += a.bias[c];
+                            if (a.relu) v[k] = fmaxf(v[k], 0.f);
+                        }
+                        const size_t off = ((size_t)(n * (a.dst.channels >> 3) + h) * plane + vox) * 8;
+                        if (a.dst.mask) {
+                            float mk[8];
+                            unpack_bf16x8(*reinterpret_cast<const uint4*>(a.dst.mask + off), mk);
+#pragma unroll
+                            for (int k = 0; k < 8; ++k) v[k] = mk[k] > 0.f ? v[k] : 0.f;
+                        }
+                        uint4 o;
+                        o.x = pack_bf16x2(v[0], v[1]);
+                        o.y = pack_bf16x2(v[2], v[3]);
+                        o.z = pack_bf16x2(v[4], v[5]);
+                        o.w = pack_bf16x2(v[6], v[7]);
+                        *reinterpret_cast<uint4*>(a.dst.ptr + off) = o;
+                    }
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) {
+                    mbar_arrive(&acce[(G - 2) & 3]);  // slice j - 2 is no longer needed
+                    if (j == len + 1) {               // the segment's last output: its last two slices too
+                        mbar_arrive(&acce[(G - 1) & 3]);
+                        mbar_arrive(&acce[G & 3]);
+                    }
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_dealloc(tmem, kCols);
+    }
+}
+
+// Forward weights of a 16-output layer for conv_zfold_kernel: [step][tap9 = dy * 3 + dx][half]
+// [r = g * 16 + o][8] = W[tap = (g) * 9 + tap9][o][ci] (dz = g - 1), bf16, zero past cout / cin.
+__global__ void relayout_zfold_kernel(const float* __restrict__ W, int cout, int cin_total, int nsteps,
+                                      __nv_bfloat16* __restrict__ out) {
+    const int total = nsteps * 9 * 2 * 48 * 8;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    int t = i;
+    const int j = t % 8;
+    t /= 8;
+    const int r = t % 48;
+    t /= 48;
+    const int half = t % 2;
+    t /= 2;
+    const int tap9 = t % 9;
+    const int step = t / 9;
+    const int g = r / 16, o = r % 16;
+    const int tap = g * 9 + tap9;
+    const int ci = step * 16 + half * 8 + j;
+    const float w = (o < cout && ci < cin_total) ? W[((size_t)tap * cout + o) * cin_total + ci] : 0.f;
+    out[i] = __float2bfloat16_rn(w);
+}
+
 // ---------------------------------------------------------------- weight gradient
 // dW[tap][co][ci] = sum over voxels v of dPre[v][co] * In[v + off(tap)][ci].  Per tile of
 // 128 voxels the K dimension of the MMA runs over voxels: A = dPre^T (M = co, padded to

@@ -118,3 +118,38 @@ def test_adam_steps_lower_the_loss(ctx):
         losses = [net.train_step(d_in, d_t, 1, lr=2e-3) for _ in range(60)]
     assert np.all(np.isfinite(losses))
     assert losses[-1] < 0.5 * losses[0], losses[::10]
+
+
+@pytest.mark.parametrize("res,batch", [((64, 40, 36), 2), ((160, 12, 68), 1)])
+def test_zstreamed_convolution_equals_per_tap_kernel(ctx, monkeypatch, res, batch):
+    """The 16-output layers as the z-streamed kernel (dz folded into N = 48, the three
+    partial sums added in the epilogue; ETCU_CONV_ZFOLD=1, the default) against the
+    per-tap kernel (ETCU_CONV_ZFOLD=0), on volumes whose last z segment is partial (36 and
+    68 slices over segments of 32), with rows of one partial and of one full plus one
+    partial x tile, and a batch of two.  Both stay within FWD_TOL of the BF16-emulating
+    oracle, and they agree with each other to 5e-3 of the correction: the two kernels sum
+    the same products in different orders, and every layer re-rounds its output to BF16, so
+    order-level differences flip a few BF16 roundings that the later layers carry on (the
+    difference is spread evenly over z, with no step at the segment boundary)."""
+    from oracle import warmstart_oracle as W
+    import torch
+    from ettention_b200.learned import WarmStartNet
+    p = _params(7)
+    v, _ = _volumes(res, batch, 8)
+    outs = {}
+    for mode in ("0", "1"):
+        monkeypatch.setenv("ETCU_CONV_ZFOLD", mode)
+        with WarmStartNet(ctx, res, max_batch=batch, params=p, scale=0.5) as net:
+            d_in = torch.as_tensor(v).cuda()
+            d_out = torch.zeros_like(d_in)
+            net.infer(d_in, d_out, batch)
+            ctx.synchronize()
+            net.check()
+            outs[mode] = d_out.cpu().numpy()
+    corr_ref = outs["0"] - v
+    assert np.abs(corr_ref).max() > 0
+    assert _rel(outs["1"] - v, corr_ref) <= 5e-3
+    if batch == 2:
+        ob, _ = W.forward(p, v, 0.5, bf16=True)
+        for mode in ("0", "1"):
+            assert _rel(outs[mode] - v, ob - v) <= FWD_TOL
