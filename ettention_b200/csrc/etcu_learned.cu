@@ -86,8 +86,9 @@ int cin_total(const LayerDef& d) { return d.cin_used0 + d.cin1; }
 // that exceeds 64 (the 96-input decoder layer), as two: source 0's and source 1's.
 int dx_split(const LayerDef& d) { return cin_total(d) > 64 ? d.cin0 : cin_total(d); }
 size_t layer_params(const LayerDef& d) { return (size_t)27 * d.cout * cin_total(d) + d.cout; }
-// Tensor-core forward layers of 16 outputs (not the first and the last, which run on the CUDA cores).
-bool zfold_layer(int l) { return l > 0 && l < kLayers - 1 && kDefs[l].npad == 16; }
+// Forward layers of 16 (padded) outputs that have a z-streamed form: all but the first,
+// whose one input channel runs on the CUDA cores (the head's one output is padded to 16).
+bool zfold_layer(int l) { return l > 0 && kDefs[l].npad == 16; }
 
 size_t total_params() {
     size_t n = 0;
@@ -529,7 +530,27 @@ etcu_status forward(etcu_warmstart* w, const float* d_in, float* d_out, int B, b
                                                                                        w->g1.Z, B * 4, w->up1.p);
     WTRY(fwd(8, w->up1, &w->e1b, w->d1a));
     WTRY(fwd(9, w->d1a, nullptr, w->d1b));
-    // head (one output channel) on the CUDA cores: out = v + scale * (conv(d1b) + b)
+    // head (one output channel): out = v + scale * (conv(d1b) + b), as the z-streamed
+    // tensor-core convolution (channel 0 of 16), or on the CUDA cores
+    if (w->zfold && w->wz[10]) {
+        CUtensorMap m0;
+        WTRY(make_map(w, &m0, w->d1b, B, ws::kHaloX, kZfoldRows + 2, 1, 2));
+        ws::ZfoldArgs z{};
+        z.X = w->g1.X;
+        z.Y = w->g1.Y;
+        z.Z = w->g1.Z;
+        z.nsteps = 1;
+        z.nkp0 = 1;
+        z.c8_0 = w->d1b.C / 8;
+        z.w = w->wz[10];
+        z.bias = w->params + w->boff[10];
+        z.head = 1;
+        z.head_in = d_in;
+        z.head_out = d_out;
+        z.head_scale = w->scale;
+        z.err = w->d_err;
+        return launch_zfold(w, m0, m0, z, B);
+    }
     ws::conv_head_kernel<<<end_grid, 256, 0, w->stream>>>(w->d1b.p, w->g1.X, w->g1.Y, w->g1.Z, B,
                                                           w->params + w->woff[10], w->params + w->boff[10], d_in,
                                                           w->scale, d_out);

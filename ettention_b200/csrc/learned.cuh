@@ -534,6 +534,10 @@ struct ZfoldArgs {
     const float* bias;     // 16 values
     int relu;
     ConvDst dst;           // 16 channels
+    int head;              // 1: channel 0 only, head_out = head_in + head_scale * (acc + bias) (FP32)
+    const float* head_in;
+    float* head_out;
+    float head_scale;
     int stages;
     unsigned* err;
 };
@@ -705,6 +709,13 @@ __global__ void __launch_bounds__(192, 1) conv_zfold_kernel(const __grid_constan
                     tmem_wait_ld();
                     if (x >= a.X || y >= a.Y) continue;
                     const size_t vox = ((size_t)z * a.Y + y) * a.X + x;
+                    if (a.head) {
+                        const size_t idx = (size_t)n * plane + vox;
+                        const float accv = __uint_as_float(r0[0]) + __uint_as_float(r1[0]) + __uint_as_float(r2[0]) +
+                                           (a.bias ? a.bias[0] : 0.f);
+                        a.head_out[idx] = fmaf(a.head_scale, accv, a.head_in[idx]);
+                        continue;
+                    }
 #pragma unroll
                     for (int h = 0; h < 2; ++h) {
                         float v[8];
