@@ -86,9 +86,10 @@ int cin_total(const LayerDef& d) { return d.cin_used0 + d.cin1; }
 // that exceeds 64 (the 96-input decoder layer), as two: source 0's and source 1's.
 int dx_split(const LayerDef& d) { return cin_total(d) > 64 ? d.cin0 : cin_total(d); }
 size_t layer_params(const LayerDef& d) { return (size_t)27 * d.cout * cin_total(d) + d.cout; }
-// Forward layers of 16 (padded) outputs that have a z-streamed form: all but the first,
-// whose one input channel runs on the CUDA cores (the head's one output is padded to 16).
-bool zfold_layer(int l) { return l > 0 && kDefs[l].npad == 16; }
+// Forward layers of 16 or 32 (padded) outputs that have a z-streamed form: all of those
+// but the first, whose one input channel runs on the CUDA cores (the head's one output is
+// padded to 16).
+bool zfold_layer(int l) { return l > 0 && (kDefs[l].npad == 16 || kDefs[l].npad == 32); }
 
 size_t total_params() {
     size_t n = 0;
@@ -254,13 +255,17 @@ etcu_status launch_conv_n(etcu_warmstart* w, const CUtensorMap& m0, const CUtens
     return ETCU_OK;
 }
 
-// The z-streamed 16-output convolution: TY = 2 rows per tile (four 96-column slices of
-// tensor memory), work units of one (x tile, y tile) column over kZseg output slices.
-constexpr int kZfoldRows = 2, kZseg = 32;
+// The z-streamed convolution: 16 outputs with TY = 2 rows per tile, 32 outputs with TY = 1
+// (four slices of 96 tensor-memory columns either way); work units of one (x tile, y tile)
+// column over kZseg output slices.
+constexpr int kZseg = 32;
+constexpr int zfold_rows(int nout) { return nout == 16 ? 2 : 1; }
 
+template <int NOUT>
 etcu_status launch_zfold(etcu_warmstart* w, const CUtensorMap& m0, const CUtensorMap& m1, ws::ZfoldArgs a,
                          int batch) {
-    using SH = ws::ZfoldShape<kZfoldRows>;
+    constexpr int kZfoldRows = zfold_rows(NOUT);
+    using SH = ws::ZfoldShape<NOUT, kZfoldRows>;
     const size_t wbytes = (size_t)a.nsteps * SH::kW;
     a.resident = wbytes <= kResidentMax ? 1 : 0;
     const size_t wres = a.resident ? (wbytes + 1023) & ~(size_t)1023 : 0;
@@ -272,8 +277,8 @@ etcu_status launch_zfold(etcu_warmstart* w, const CUtensorMap& m0, const CUtenso
     a.zseg = kZseg;
     static std::atomic<unsigned long long> opted{0};
     if (w->device < 64 && !(opted.load() & (1ull << w->device))) {
-        WCK(w, cudaFuncSetAttribute(ws::conv_zfold_kernel<kZfoldRows>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    232448));
+        WCK(w, cudaFuncSetAttribute(ws::conv_zfold_kernel<NOUT, kZfoldRows>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, 232448));
         opted.fetch_or(1ull << w->device);
     }
     const long units = (long)((a.X + ws::kTileX - 1) / ws::kTileX) * ((a.Y + kZfoldRows - 1) / kZfoldRows) *
@@ -281,7 +286,7 @@ etcu_status launch_zfold(etcu_warmstart* w, const CUtensorMap& m0, const CUtenso
     const unsigned grid = (unsigned)std::min<long>(units, w->sms);
     // at least 120 KB, so that one CTA (and its 512 tensor-memory columns) owns each SM
     const size_t smem = std::max<size_t>(wres + (size_t)S * stage + (2 * S + 9) * 8 + 16 + 1024, 120 * 1024);
-    ws::conv_zfold_kernel<kZfoldRows><<<grid, 192, smem, w->stream>>>(m0, m1, a);
+    ws::conv_zfold_kernel<NOUT, kZfoldRows><<<grid, 192, smem, w->stream>>>(m0, m1, a);
     WCK(w, cudaGetLastError());
     return ETCU_OK;
 }
@@ -439,9 +444,9 @@ etcu_status relayout(etcu_warmstart* w) {
         ws::relayout_forward_kernel<<<blocks(nf), 256, 0, w->stream>>>(w->params + w->woff[l], d.cout, cin_total(d),
                                                                        d.npad, nsteps_f, w->wf[l]);
         if (w->wz[l]) {
-            const int nz = nsteps_f * 9 * 2 * 48 * 8;
+            const int nz = nsteps_f * 9 * 2 * 3 * d.npad * 8;
             ws::relayout_zfold_kernel<<<blocks(nz), 256, 0, w->stream>>>(w->params + w->woff[l], d.cout, cin_total(d),
-                                                                         nsteps_f, w->wz[l]);
+                                                                         d.npad, nsteps_f, w->wz[l]);
         }
         if (l > 0) {
             const int nsteps_b = (d.cout + 15) / 16;
@@ -486,10 +491,11 @@ etcu_status forward(etcu_warmstart* w, const float* d_in, float* d_out, int B, b
         c.relu = true;
         c.n = d.npad;
         c.dst0 = dst(out);
-        if (w->zfold && w->wz[l]) {  // 16 outputs: the z-streamed kernel
+        if (w->zfold && w->wz[l]) {  // 16 or 32 outputs: the z-streamed kernel
+            const int rows = zfold_rows(d.npad);
             CUtensorMap m0, m1;
-            WTRY(make_map(w, &m0, s0, B, ws::kHaloX, kZfoldRows + 2, 1, 2));
-            WTRY(make_map(w, &m1, s1 ? *s1 : s0, B, ws::kHaloX, kZfoldRows + 2, 1, 2));
+            WTRY(make_map(w, &m0, s0, B, ws::kHaloX, rows + 2, 1, 2));
+            WTRY(make_map(w, &m1, s1 ? *s1 : s0, B, ws::kHaloX, rows + 2, 1, 2));
             ws::ZfoldArgs z{};
             z.X = s0.g.X;
             z.Y = s0.g.Y;
@@ -503,7 +509,7 @@ etcu_status forward(etcu_warmstart* w, const float* d_in, float* d_out, int B, b
             z.relu = 1;
             z.dst = c.dst0;
             z.err = w->d_err;
-            return launch_zfold(w, m0, m1, z, B);
+            return d.npad == 16 ? launch_zfold<16>(w, m0, m1, z, B) : launch_zfold<32>(w, m0, m1, z, B);
         }
         return conv(w, c, B);
     };
@@ -534,7 +540,7 @@ etcu_status forward(etcu_warmstart* w, const float* d_in, float* d_out, int B, b
     // tensor-core convolution (channel 0 of 16), or on the CUDA cores
     if (w->zfold && w->wz[10]) {
         CUtensorMap m0;
-        WTRY(make_map(w, &m0, w->d1b, B, ws::kHaloX, kZfoldRows + 2, 1, 2));
+        WTRY(make_map(w, &m0, w->d1b, B, ws::kHaloX, zfold_rows(16) + 2, 1, 2));
         ws::ZfoldArgs z{};
         z.X = w->g1.X;
         z.Y = w->g1.Y;
@@ -549,7 +555,7 @@ etcu_status forward(etcu_warmstart* w, const float* d_in, float* d_out, int B, b
         z.head_out = d_out;
         z.head_scale = w->scale;
         z.err = w->d_err;
-        return launch_zfold(w, m0, m0, z, B);
+        return launch_zfold<16>(w, m0, m0, z, B);
     }
     ws::conv_head_kernel<<<end_grid, 256, 0, w->stream>>>(w->d1b.p, w->g1.X, w->g1.Y, w->g1.Z, B,
                                                           w->params + w->woff[10], w->params + w->boff[10], d_in,
@@ -741,7 +747,8 @@ extern "C" etcu_status etcu_warmstart_create(etcu_context* ctx, const uint32_t r
     for (int l = 0; l < kLayers; ++l) {
         const LayerDef& d = kDefs[l];
         WTRY(walloc(p, (void**)&p->wf[l], (size_t)(d.cin0 + d.cin1) / 16 * 27 * 2 * d.npad * 8 * 2));
-        if (zfold_layer(l)) WTRY(walloc(p, (void**)&p->wz[l], (size_t)(d.cin0 + d.cin1) / 16 * 9 * 2 * 48 * 8 * 2));
+        if (zfold_layer(l))
+            WTRY(walloc(p, (void**)&p->wz[l], (size_t)(d.cin0 + d.cin1) / 16 * 9 * 2 * 3 * d.npad * 8 * 2));
         if (l > 0) {
             const size_t per = (size_t)((d.cout + 15) / 16) * 27 * 2 * 8 * 2;
             WTRY(walloc(p, (void**)&p->wb[l], per * dx_split(d)));

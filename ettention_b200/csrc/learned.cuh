@@ -516,12 +516,13 @@ __global__ void __launch_bounds__(conv_threads<kLoad>(), 1) conv_tc_kernel(const
 // (global slice count) % 4 of TY x 48 columns; the epilogue of output z0 + j - 2 (after
 // slice j) reads slots of j - 2, j - 1, j and releases j - 2's (all three at the
 // segment's last output), so the MMAs run up to two slices ahead of the epilogue.
-template <int TY>
+template <int NOUT, int TY>
 struct ZfoldShape {
+    static constexpr uint32_t kN = 3u * NOUT;                              // MMA N: three dz groups
     static constexpr uint32_t kPlane = (uint32_t)kHaloX * (TY + 2) * 16u;  // one 8-channel chunk, one z
     static constexpr uint32_t kHalo = 2u * kPlane;                         // 16 channels = one K step
-    static constexpr uint32_t kW = 9u * 2u * 48u * 16u;                    // one step's weights
-    static constexpr uint32_t kSlot = (uint32_t)TY * 48u;                  // tensor-memory columns per slice
+    static constexpr uint32_t kW = 9u * 2u * kN * 16u;                     // one step's weights
+    static constexpr uint32_t kSlot = (uint32_t)TY * kN;                   // tensor-memory columns per slice
     static_assert(4 * kSlot <= 512, "four slices must fit in tensor memory");
 };
 
@@ -529,11 +530,11 @@ struct ZfoldArgs {
     int X, Y, Z, batch;
     int zseg;              // output z slices per work unit
     int nsteps, nkp0, c8_0, c8_1;
-    const __nv_bfloat16* w;  // [step][9 taps (dy, dx)][2 halves][48 = 3 dz x 16][8] bf16
+    const __nv_bfloat16* w;  // [step][9 taps (dy, dx)][2 halves][3 dz x NOUT][8] bf16
     int resident;
-    const float* bias;     // 16 values
+    const float* bias;     // NOUT values
     int relu;
-    ConvDst dst;           // 16 channels
+    ConvDst dst;           // NOUT channels
     int head;              // 1: channel 0 only, head_out = head_in + head_scale * (acc + bias) (FP32)
     const float* head_in;
     float* head_out;
@@ -542,11 +543,11 @@ struct ZfoldArgs {
     unsigned* err;
 };
 
-template <int TY>
+template <int NOUT, int TY>
 __global__ void __launch_bounds__(192, 1) conv_zfold_kernel(const __grid_constant__ CUtensorMap src0,
                                                             const __grid_constant__ CUtensorMap src1, ZfoldArgs a) {
-    using SH = ZfoldShape<TY>;
-    constexpr uint32_t kIdesc = idesc_bf16(128, 48, 0, 0);
+    using SH = ZfoldShape<NOUT, TY>;
+    constexpr uint32_t kIdesc = idesc_bf16(128, SH::kN, 0, 0);
     constexpr uint32_t kCols = 512;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -658,11 +659,11 @@ __global__ void __launch_bounds__(192, 1) conv_zfold_kernel(const __grid_constan
 #pragma unroll 1
                         for (int tap = 0; tap < 9; ++tap) {
                             const int dy = tap / 3, dx = tap % 3;
-                            const uint64_t bd = sdesc(wbase + (uint32_t)tap * (2u * 48u * 16u), 48u * 16u, 128);
+                            const uint64_t bd = sdesc(wbase + (uint32_t)tap * (2u * SH::kN * 16u), SH::kN * 16u, 128);
 #pragma unroll
                             for (int ty = 0; ty < TY; ++ty) {
                                 const uint32_t aoff = (uint32_t)(((ty + dy) * kHaloX + dx) * 16);
-                                umma_bf16(dslot + (uint32_t)(ty * 48), sdesc(hbase + aoff, SH::kPlane, 128), bd,
+                                umma_bf16(dslot + (uint32_t)ty * SH::kN, sdesc(hbase + aoff, SH::kPlane, 128), bd,
                                           kIdesc, (s > 0 || tap > 0) ? 1u : 0u);
                             }
                         }
@@ -702,43 +703,49 @@ __global__ void __launch_bounds__(192, 1) conv_zfold_kernel(const __grid_constan
 #pragma unroll 1
                 for (int ty = 0; ty < TY; ++ty) {
                     const int y = yt * TY + ty;
-                    uint32_t r0[16], r1[16], r2[16];
-                    tmem_ld16(s0 + (uint32_t)(ty * 48), r0);       // dz = -1 of slice z - 1
-                    tmem_ld16(s1 + (uint32_t)(ty * 48 + 16), r1);  // dz = 0 of slice z
-                    tmem_ld16(s2 + (uint32_t)(ty * 48 + 32), r2);  // dz = +1 of slice z + 1
-                    tmem_wait_ld();
-                    if (x >= a.X || y >= a.Y) continue;
+                    const bool valid = x < a.X && y < a.Y;
                     const size_t vox = ((size_t)z * a.Y + y) * a.X + x;
-                    if (a.head) {
-                        const size_t idx = (size_t)n * plane + vox;
-                        const float accv = __uint_as_float(r0[0]) + __uint_as_float(r1[0]) + __uint_as_float(r2[0]) +
-                                           (a.bias ? a.bias[0] : 0.f);
-                        a.head_out[idx] = fmaf(a.head_scale, accv, a.head_in[idx]);
-                        continue;
-                    }
 #pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        float v[8];
-#pragma unroll
-                        for (int k = 0; k < 8; ++k) {
-                            const int c = h * 8 + k;
-                            v[k] = __uint_as_float(r0[c]) + __uint_as_float(r1[c]) + __uint_as_float(r2[c]);
-                            if (a.bias) v[k] += a.bias[c];
-                            if (a.relu) v[k] = fmaxf(v[k], 0.f);
+                    for (int c16 = 0; c16 < NOUT / 16; ++c16) {
+                        const uint32_t col = (uint32_t)ty * SH::kN + (uint32_t)c16 * 16u;
+                        uint32_t r0[16], r1[16], r2[16];
+                        tmem_ld16(s0 + col, r0);             // dz = -1 of slice z - 1
+                        tmem_ld16(s1 + col + NOUT, r1);      // dz = 0 of slice z
+                        tmem_ld16(s2 + col + 2 * NOUT, r2);  // dz = +1 of slice z + 1
+                        tmem_wait_ld();
+                        if (!valid) continue;
+                        if (a.head) {
+                            const size_t idx = (size_t)n * plane + vox;
+                            const float accv = __uint_as_float(r0[0]) + __uint_as_float(r1[0]) +
+                                               __uint_as_float(r2[0]) + (a.bias ? a.bias[0] : 0.f);
+                            a.head_out[idx] = fmaf(a.head_scale, accv, a.head_in[idx]);
+                            continue;
                         }
-                        const size_t off = ((size_t)(n * (a.dst.channels >> 3) + h) * plane + vox) * 8;
-                        if (a.dst.mask) {
-                            float mk[8];
-                            unpack_bf16x8(*reinterpret_cast<const uint4*>(a.dst.mask + off), mk);
 #pragma unroll
-                            for (int k = 0; k < 8; ++k) v[k] = mk[k] > 0.f ? v[k] : 0.f;
+                        for (int h = 0; h < 2; ++h) {
+                            float v[8];
+#pragma unroll
+                            for (int k = 0; k < 8; ++k) {
+                                const int c = h * 8 + k;
+                                v[k] = __uint_as_float(r0[c]) + __uint_as_float(r1[c]) + __uint_as_float(r2[c]);
+                                if (a.bias) v[k] += a.bias[c16 * 16 + c];
+                                if (a.relu) v[k] = fmaxf(v[k], 0.f);
+                            }
+                            const size_t off =
+                                ((size_t)(n * (a.dst.channels >> 3) + c16 * 2 + h) * plane + vox) * 8;
+                            if (a.dst.mask) {
+                                float mk[8];
+                                unpack_bf16x8(*reinterpret_cast<const uint4*>(a.dst.mask + off), mk);
+#pragma unroll
+                                for (int k = 0; k < 8; ++k) v[k] = mk[k] > 0.f ? v[k] : 0.f;
+                            }
+                            uint4 o;
+                            o.x = pack_bf16x2(v[0], v[1]);
+                            o.y = pack_bf16x2(v[2], v[3]);
+                            o.z = pack_bf16x2(v[4], v[5]);
+                            o.w = pack_bf16x2(v[6], v[7]);
+                            *reinterpret_cast<uint4*>(a.dst.ptr + off) = o;
                         }
-                        uint4 o;
-                        o.x = pack_bf16x2(v[0], v[1]);
-                        o.y = pack_bf16x2(v[2], v[3]);
-                        o.z = pack_bf16x2(v[4], v[5]);
-                        o.w = pack_bf16x2(v[6], v[7]);
-                        *reinterpret_cast<uint4*>(a.dst.ptr + off) = o;
                     }
                 }
                 tc_fence_before();
@@ -761,23 +768,25 @@ __global__ void __launch_bounds__(192, 1) conv_zfold_kernel(const __grid_constan
     }
 }
 
-// Forward weights of a 16-output layer for conv_zfold_kernel: [step][tap9 = dy * 3 + dx][half]
-// [r = g * 16 + o][8] = W[tap = (g) * 9 + tap9][o][ci] (dz = g - 1), bf16, zero past cout / cin.
-__global__ void relayout_zfold_kernel(const float* __restrict__ W, int cout, int cin_total, int nsteps,
+// Forward weights of an nout-output layer for conv_zfold_kernel: [step][tap9 = dy * 3 + dx]
+// [half][r = g * nout + o][8] = W[tap = g * 9 + tap9][o][ci] (input z offset g - 1), bf16,
+// zero past cout / cin.
+__global__ void relayout_zfold_kernel(const float* __restrict__ W, int cout, int cin_total, int nout, int nsteps,
                                       __nv_bfloat16* __restrict__ out) {
-    const int total = nsteps * 9 * 2 * 48 * 8;
+    const int nn = 3 * nout;
+    const int total = nsteps * 9 * 2 * nn * 8;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= total) return;
     int t = i;
     const int j = t % 8;
     t /= 8;
-    const int r = t % 48;
-    t /= 48;
+    const int r = t % nn;
+    t /= nn;
     const int half = t % 2;
     t /= 2;
     const int tap9 = t % 9;
     const int step = t / 9;
-    const int g = r / 16, o = r % 16;
+    const int g = r / nout, o = r % nout;
     const int tap = g * 9 + tap9;
     const int ci = step * 16 + half * 8 + j;
     const float w = (o < cout && ci < cin_total) ? W[((size_t)tap * cout + o) * cin_total + ci] : 0.f;
