@@ -286,7 +286,7 @@ etcu_status launch_zfold(etcu_warmstart* w, const CUtensorMap& m0, const CUtenso
     const unsigned grid = (unsigned)std::min<long>(units, w->sms);
     // at least 120 KB, so that one CTA (and its 512 tensor-memory columns) owns each SM
     const size_t smem = std::max<size_t>(wres + (size_t)S * stage + (2 * S + 9) * 8 + 16 + 1024, 120 * 1024);
-    ws::conv_zfold_kernel<NOUT, kZfoldRows><<<grid, 192, smem, w->stream>>>(m0, m1, a);
+    ws::conv_zfold_kernel<NOUT, kZfoldRows><<<grid, ws::kZfoldThreads, smem, w->stream>>>(m0, m1, a);
     WCK(w, cudaGetLastError());
     return ETCU_OK;
 }

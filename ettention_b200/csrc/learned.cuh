@@ -543,8 +543,10 @@ struct ZfoldArgs {
     unsigned* err;
 };
 
+constexpr int kZfoldThreads = 320;  // warp 0 loads, warp 1 issues the MMAs, warps 2-9 drain
+
 template <int NOUT, int TY>
-__global__ void __launch_bounds__(192, 1) conv_zfold_kernel(const __grid_constant__ CUtensorMap src0,
+__global__ void __launch_bounds__(kZfoldThreads, 1) conv_zfold_kernel(const __grid_constant__ CUtensorMap src0,
                                                             const __grid_constant__ CUtensorMap src1, ZfoldArgs a) {
     using SH = ZfoldShape<NOUT, TY>;
     constexpr uint32_t kIdesc = idesc_bf16(128, SH::kN, 0, 0);
@@ -586,7 +588,7 @@ __global__ void __launch_bounds__(192, 1) conv_zfold_kernel(const __grid_constan
         }
         for (int i = 0; i < 4; ++i) {
             mbar_init(&accf[i], 1);
-            mbar_init(&acce[i], 4);
+            mbar_init(&acce[i], 8);  // the eight epilogue warps
         }
         mbar_init(wbar, 1);
         mbar_fence_init();
@@ -656,15 +658,20 @@ __global__ void __launch_bounds__(192, 1) conv_zfold_kernel(const __grid_constan
                         const uint32_t hbase = smem_u32(ring + (size_t)st * stage);
                         const uint32_t wbase =
                             a.resident ? smem_u32(wsm) + (uint32_t)s * SH::kW : hbase + SH::kHalo;
-#pragma unroll 1
+                        // one descriptor per operand base; every tap's is the base plus a constant
+                        // (the start-address field is address / 16, and every address here is
+                        // below 256 KiB, so the add never leaves the field)
+                        const uint64_t a0 = sdesc(hbase, SH::kPlane, 128);
+                        const uint64_t b0 = sdesc(wbase, SH::kN * 16u, 128);
+#pragma unroll
                         for (int tap = 0; tap < 9; ++tap) {
                             const int dy = tap / 3, dx = tap % 3;
-                            const uint64_t bd = sdesc(wbase + (uint32_t)tap * (2u * SH::kN * 16u), SH::kN * 16u, 128);
+                            const uint64_t bd = b0 + (uint64_t)((tap * 2u * SH::kN * 16u) >> 4);
 #pragma unroll
                             for (int ty = 0; ty < TY; ++ty) {
                                 const uint32_t aoff = (uint32_t)(((ty + dy) * kHaloX + dx) * 16);
-                                umma_bf16(dslot + (uint32_t)ty * SH::kN, sdesc(hbase + aoff, SH::kPlane, 128), bd,
-                                          kIdesc, (s > 0 || tap > 0) ? 1u : 0u);
+                                umma_bf16(dslot + (uint32_t)ty * SH::kN, a0 + (uint64_t)(aoff >> 4), bd, kIdesc,
+                                          (s > 0 || tap > 0) ? 1u : 0u);
                             }
                         }
                         umma_commit(&empty[st]);
@@ -675,10 +682,14 @@ __global__ void __launch_bounds__(192, 1) conv_zfold_kernel(const __grid_constan
             }
         }
     } else {
-        // epilogue: warp quarter (warp % 4) reads tensor-memory lanes 32 * (warp % 4) ...
-        const int quarter = warp & 3;
+        // epilogue: warp quarter (warp % 4) reads tensor-memory lanes 32 * (warp % 4) ...;
+        // two warps per quarter, one per tile row (TY = 2) or per 16 channels (TY = 1)
+        const int quarter = warp & 3, part = (warp - 2) >> 2;
         const int m = quarter * 32 + lane;
         const size_t plane = (size_t)a.Z * a.Y * a.X;
+        float bias[NOUT];
+#pragma unroll
+        for (int c = 0; c < NOUT; ++c) bias[c] = a.bias ? a.bias[c] : 0.f;
         int G = 0;
         bool ok = true;
         for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
@@ -702,11 +713,13 @@ __global__ void __launch_bounds__(192, 1) conv_zfold_kernel(const __grid_constan
                 const uint32_t s2 = tmem + lanes + (uint32_t)(G & 3) * SH::kSlot;
 #pragma unroll 1
                 for (int ty = 0; ty < TY; ++ty) {
+                    if (TY == 2 && ty != part) continue;
                     const int y = yt * TY + ty;
                     const bool valid = x < a.X && y < a.Y;
                     const size_t vox = ((size_t)z * a.Y + y) * a.X + x;
 #pragma unroll
                     for (int c16 = 0; c16 < NOUT / 16; ++c16) {
+                        if (TY == 1 && NOUT == 32 && c16 != part) continue;
                         const uint32_t col = (uint32_t)ty * SH::kN + (uint32_t)c16 * 16u;
                         uint32_t r0[16], r1[16], r2[16];
                         tmem_ld16(s0 + col, r0);             // dz = -1 of slice z - 1
@@ -716,8 +729,8 @@ __global__ void __launch_bounds__(192, 1) conv_zfold_kernel(const __grid_constan
                         if (!valid) continue;
                         if (a.head) {
                             const size_t idx = (size_t)n * plane + vox;
-                            const float accv = __uint_as_float(r0[0]) + __uint_as_float(r1[0]) +
-                                               __uint_as_float(r2[0]) + (a.bias ? a.bias[0] : 0.f);
+                            const float accv =
+                                __uint_as_float(r0[0]) + __uint_as_float(r1[0]) + __uint_as_float(r2[0]) + bias[0];
                             a.head_out[idx] = fmaf(a.head_scale, accv, a.head_in[idx]);
                             continue;
                         }
@@ -728,7 +741,7 @@ __global__ void __launch_bounds__(192, 1) conv_zfold_kernel(const __grid_constan
                             for (int k = 0; k < 8; ++k) {
                                 const int c = h * 8 + k;
                                 v[k] = __uint_as_float(r0[c]) + __uint_as_float(r1[c]) + __uint_as_float(r2[c]);
-                                if (a.bias) v[k] += a.bias[c16 * 16 + c];
+                                v[k] += bias[c16 * 16 + c];
                                 if (a.relu) v[k] = fmaxf(v[k], 0.f);
                             }
                             const size_t off =
