@@ -398,14 +398,18 @@ __global__ void __launch_bounds__(conv_threads<kLoad>(), 1) conv_tc_kernel(const
                     tc_fence_after();
                     const uint32_t hbase = smem_u32(ring + (size_t)st * stage);
                     const uint32_t wbase = a.resident ? smem_u32(wsm) + (uint32_t)s * SH::kW : hbase + SH::kHalo;
-#pragma unroll 1
+                    // per-tap descriptors as the base descriptor plus a constant (address / 16
+                    // in the start-address field; shared-memory addresses stay below 256 KiB)
+                    const uint64_t a0 = sdesc(hbase, SH::kPlane, 128);
+                    const uint64_t b0 = sdesc(wbase, N * 16u, 128);
+#pragma unroll
                     for (int tap = 0; tap < 27; ++tap) {
                         const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
-                        const uint64_t bd = sdesc(wbase + (uint32_t)tap * (2u * N * 16u), N * 16u, 128);
+                        const uint64_t bd = b0 + (uint64_t)((tap * 2u * N * 16u) >> 4);
 #pragma unroll
                         for (int ty = 0; ty < TY; ++ty) {
                             const uint32_t aoff = (uint32_t)(((dz * (TY + 2) + ty + dy) * kHaloX + dx) * 16);
-                            umma_bf16(dacc + (uint32_t)(ty * N), sdesc(hbase + aoff, SH::kPlane, 128), bd, kIdesc,
+                            umma_bf16(dacc + (uint32_t)(ty * N), a0 + (uint64_t)(aoff >> 4), bd, kIdesc,
                                       (s > 0 || tap > 0) ? 1u : 0u);
                         }
                     }
