@@ -528,11 +528,11 @@ etcu_status forward(etcu_warmstart* w, const float* d_in, float* d_out, int B, b
                                                                                    w->g2.Z, B * 4, w->p2.p);
     WTRY(fwd(4, w->p2, nullptr, w->e3a));
     WTRY(fwd(5, w->e3a, nullptr, w->e3b));
-    ws::upsample_kernel<<<blocks((size_t)B * 8 * w->g2.plane()), 256, 0, w->stream>>>(w->e3b.p, w->g2.X, w->g2.Y,
+    ws::upsample_kernel<<<blocks((size_t)B * w->g2.plane()), 256, 0, w->stream>>>(w->e3b.p, w->g2.X, w->g2.Y,
                                                                                        w->g2.Z, B * 8, w->up2.p);
     WTRY(fwd(6, w->up2, &w->e2b, w->d2a));
     WTRY(fwd(7, w->d2a, nullptr, w->d2b));
-    ws::upsample_kernel<<<blocks((size_t)B * 4 * w->g1.plane()), 256, 0, w->stream>>>(w->d2b.p, w->g1.X, w->g1.Y,
+    ws::upsample_kernel<<<blocks((size_t)B * w->g1.plane() / 2), 256, 0, w->stream>>>(w->d2b.p, w->g1.X, w->g1.Y,
                                                                                        w->g1.Z, B * 4, w->up1.p);
     WTRY(fwd(8, w->up1, &w->e1b, w->d1a));
     WTRY(fwd(9, w->d1a, nullptr, w->d1b));

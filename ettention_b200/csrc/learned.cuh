@@ -1013,7 +1013,7 @@ constexpr int kEndHalo = kEndHx * kEndHy * 3;
 __global__ void __launch_bounds__(256) conv_in_kernel(const float* __restrict__ vin, float inv_scale, int X, int Y,
                                                        int Z, int batch, const float* __restrict__ W,
                                                        const float* __restrict__ bias, __nv_bfloat16* __restrict__ out) {
-    __shared__ float ws_[27 * 16];
+    __shared__ __align__(16) float ws_[27 * 16];
     __shared__ float bs_[16];
     __shared__ float halo[kEndHalo];
     const int tid = threadIdx.x;
@@ -1035,14 +1035,23 @@ __global__ void __launch_bounds__(256) conv_in_kernel(const float* __restrict__ 
     const int tx = tid % kEndTx, ty = tid / kEndTx;
     const int x = x0 + tx, y = y0 + ty;
     if (x >= X || y >= Y) return;
-    float acc[16];
+    // the 16 channels as 8 pairs: one paired FMA per pair (each lane the fmaf of one channel)
+    float2 acc2[8];
 #pragma unroll
-    for (int c = 0; c < 16; ++c) acc[c] = bs_[c];
+    for (int c = 0; c < 8; ++c) acc2[c] = make_float2(bs_[2 * c], bs_[2 * c + 1]);
+    const float2* w2 = reinterpret_cast<const float2*>(ws_);
 #pragma unroll
     for (int t = 0; t < 27; ++t) {
         const float xv = halo[((t / 9) * kEndHy + ty + (t / 3) % 3) * kEndHx + tx + t % 3];
+        const float2 xx = make_float2(xv, xv);
 #pragma unroll
-        for (int c = 0; c < 16; ++c) acc[c] = fmaf(xv, ws_[t * 16 + c], acc[c]);
+        for (int c = 0; c < 8; ++c) acc2[c] = __ffma2_rn(xx, w2[t * 8 + c], acc2[c]);
+    }
+    float acc[16];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        acc[2 * c] = acc2[c].x;
+        acc[2 * c + 1] = acc2[c].y;
     }
     const size_t v = ((size_t)z * Y + y) * X + x;
 #pragma unroll
@@ -1181,20 +1190,31 @@ __global__ void pool_backward_kernel(const __nv_bfloat16* __restrict__ coarse, c
 }
 
 // Nearest-neighbour upsampling by 2 of an NC8 tensor (coarse grid X/2, Y/2, Z/2).
+// One thread per coarse cell: it reads the cell once and writes its 2 x 2 x 2 fine copies
+// (X, Y, Z: the fine grid, even; the coarse grid has fewer than 2^32 cells).
 __global__ void upsample_kernel(const __nv_bfloat16* __restrict__ in, int X, int Y, int Z, int nchunks,
                                 __nv_bfloat16* __restrict__ out) {
-    const size_t total = (size_t)nchunks * Z * Y * X;
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t xc = (uint32_t)X / 2, yc = (uint32_t)Y / 2, zc = (uint32_t)Z / 2;
+    const uint32_t total = (uint32_t)nchunks * zc * yc * xc;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= total) return;
-    size_t t = i;
-    const int x = t % X;
-    t /= X;
-    const int y = t % Y;
-    t /= Y;
-    const int z = t % Z;
-    const size_t c = t / Z;
-    *reinterpret_cast<uint4*>(out + i * 8) = *reinterpret_cast<const uint4*>(
-        in + (((c * (Z / 2) + z / 2) * (Y / 2) + y / 2) * (X / 2) + x / 2) * 8);
+    uint32_t t = i;
+    const uint32_t x = t % xc;
+    t /= xc;
+    const uint32_t y = t % yc;
+    t /= yc;
+    const uint32_t z = t % zc;
+    const uint32_t c = t / zc;
+    const uint4 v = *reinterpret_cast<const uint4*>(in + (size_t)i * 8);
+#pragma unroll
+    for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
+        for (int dy = 0; dy < 2; ++dy) {
+            const size_t row = (((size_t)c * Z + 2 * z + dz) * Y + 2 * y + dy) * X + 2 * x;
+            uint4* o = reinterpret_cast<uint4*>(out + row * 8);
+            o[0] = v;
+            o[1] = v;
+        }
 }
 
 // Gradient through the upsampling (sum of the 8 children) times the ReLU mask of the
