@@ -686,7 +686,9 @@ __device__ __forceinline__ void bp_store(const BpArgs& a, size_t idx, float val)
 }
 
 constexpr int kBpZ = 8;  // voxels per thread along z (parallel)
-constexpr int kBpZPersp = 8;
+// perspective: 16 z voxels per thread, so a column's per-view terms (matrix rows, source
+// offsets, chord bounds) are formed once per 16 voxels; 64 registers at 4 blocks per SM
+constexpr int kBpZPersp = 16;
 
 // Row-constant view, one sample, 1/256 weights: the per-voxel sequence reduced to the
 // column coordinate.  q = floor((u - 0.5) * 256 + 0.5) is the 1/256-rounded texel
@@ -1863,7 +1865,7 @@ __device__ __forceinline__ int brick_projects_inside(const BpView& V, const Slab
 // PerspectiveBeamsBackProjection.cl:28-71: n^3 sub-voxel samples, each weighted by
 // its own chord through the voxel; optional intensity clamps.
 template <bool kMask, int kStore, int kSampling, bool kClamp>
-__global__ void __launch_bounds__(256) bp_perspective_kernel(const __grid_constant__ BpArgs a) {
+__global__ void __launch_bounds__(256, 4) bp_perspective_kernel(const __grid_constant__ BpArgs a) {
     extern __shared__ __align__(16) unsigned char bp_smem[];
     BpView* sv = (BpView*)bp_smem;
     bp_stage(a, sv, nullptr, false);
@@ -1974,15 +1976,14 @@ __global__ void __launch_bounds__(256) bp_perspective_kernel(const __grid_consta
                     } else {
                         rl = sample_pair<kSampling>(img, a.rl_pitch, a.W, a.H, V.tex, uv.x, uv.y);
                     }
-                    float value = 0.f;
-                    if (rl.y >= kEps) {
-                        // r * chord / L with chord = |d| / m: r * nd2 * rsqrt(nd2 * (m L)^2),
-                        // one reciprocal square root for the chord and the division by L
-                        const float dz = fsub(pz[j], V.src[2]);
-                        const float nd2 = fadd(dxy, fmul(dz, dz));
-                        const float mL = fmul(fmaxf(mxy, fmul(fabsf(dz), g.ivs.z)), rl.y);
-                        value = fmul(rl.x, fmul(nd2, rsqrtf(fmul(nd2, fmul(mL, mL)))));
-                    }
+                    // r * chord / L with chord = |d| / m: r * nd2 * rsqrt(nd2 * (m L)^2),
+                    // one reciprocal square root for the chord and the division by L; formed
+                    // for every sample and selected (0 where L < kEps, which the reference skips)
+                    const float dz = fsub(pz[j], V.src[2]);
+                    const float nd2 = fadd(dxy, fmul(dz, dz));
+                    const float mL = fmul(fmaxf(mxy, fmul(fabsf(dz), g.ivs.z)), rl.y);
+                    const float q = fmul(rl.x, fmul(nd2, rsqrtf(fmul(nd2, fmul(mL, mL)))));
+                    const float value = rl.y >= kEps ? q : 0.f;
                     float vj = fadd(val[j], fmul(fmul(a.lambda, value), mw[j]));
                     if (kClamp) {
                         if (a.use_min) vj = fmaxf(a.vmin, vj);
