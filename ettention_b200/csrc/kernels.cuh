@@ -1064,13 +1064,20 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// The float 1 + k 2^-15 for k = bits & 255: one byte permute puts k in bits 8..15 under
+// the exponent of 1 (bytes 3, 2, 0 from 0x3F800000).
+__device__ __forceinline__ float q8_k1(unsigned bits) { return __uint_as_float(__byte_perm(bits, 0x3F800000u, 0x7604)); }
+
+// The 1/256 weights k / 256 from two q8_k1 values: 128 (1 + k 2^-15) - 128, exact.
+__device__ __forceinline__ float2 q8_weight2(float2 k1) { return fma2(k1, splat(128.f), splat(-128.f)); }
+
 // Column tap of one voxel from f = fl_down(t + 1.5 * 2^23) = 1.5 * 2^23 + floor(t),
-// t = u * 256 - 127.5 (exact): tap-pair index x0 - x0lo and 1 + a, where
-// a = (floor(t) mod 256) / 256 is the 1/256 weight (exact).
-__device__ __forceinline__ void q8_tap_bits(float f, int x0lo, int& e, float& a1) {
-    const int bits = __float_as_int(f);
-    e = (bits >> 8) - ((0x4B400000 >> 8) + x0lo);
-    a1 = __int_as_float(((bits << 15) & 0x007F8000) | 0x3F800000);
+// t = u * 256 - 127.5 (exact): tap-pair index x0 - x0lo and q8_k1 of k = floor(t) mod 256,
+// whose weight k / 256 q8_weight2 forms.
+__device__ __forceinline__ void q8_tap_bits(float f, int x0lo, int& e, float& k1) {
+    const unsigned bits = __float_as_uint(f);
+    e = (int)(bits >> 8) - ((0x4B400000 >> 8) + x0lo);
+    k1 = q8_k1(bits);
 }
 
 // kFull: every thread owns all kCols columns (rx == kCols * kBpColThreads).
@@ -1192,10 +1199,10 @@ __global__ void __launch_bounds__(kBpColThreads, 4) bp_sart_column_kernel(const 
                     const float2 u = add2(add2(au[k][h], kz), m12);
                     const float2 f = __fadd2_rd(fma2(u, splat(256.f), splat(-127.5f)), splat(12582912.0f));
                     int e0, e1;
-                    float a0, a1;
-                    q8_tap_bits(f.x, x0lo, e0, a0);
-                    q8_tap_bits(f.y, x0lo, e1, a1);
-                    const float2 ax = add2(f2(a0, a1), splat(-1.f));
+                    float k0, k1;
+                    q8_tap_bits(f.x, x0lo, e0, k0);
+                    q8_tap_bits(f.y, x0lo, e1, k1);
+                    const float2 ax = q8_weight2(f2(k0, k1));
 #pragma unroll
                     for (int q = 0; q < 2; ++q) {
                         const int eq = q ? e1 : e0;
@@ -1452,10 +1459,10 @@ __device__ __forceinline__ void fused_row_step(const FuseArgs& a, uint32_t p, in
             const float2 u = add2(add2(au, splat(K[z])), m12);
             const float2 f = __fadd2_rd(fma2(u, splat(256.f), splat(-127.5f)), splat(12582912.0f));
             int e0, e1;
-            float a0, a1;
-            q8_tap_bits(f.x, x0lo, e0, a0);
-            q8_tap_bits(f.y, x0lo, e1, a1);
-            const float2 ax = add2(f2(a0, a1), splat(-1.f));
+            float k0, k1;
+            q8_tap_bits(f.x, x0lo, e0, k0);
+            q8_tap_bits(f.y, x0lo, e1, k1);
+            const float2 ax = q8_weight2(f2(k0, k1));
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
                 const int eq = q ? e1 : e0;
@@ -1937,6 +1944,7 @@ __global__ void __launch_bounds__(256, 4) bp_perspective_kernel(const __grid_con
                 // out there every texel is a zero pad, as it is for the unclamped coordinate
                 const float2 lo = splat(-1.5f), hi = f2((float)a.W + 1.49609375f, (float)a.H + 1.49609375f);
                 const int pitch = (int)a.rl_pitch;
+                const unsigned kq = 0x4B4000u * (unsigned)(pitch + 1);
                 // kCoordClamp false when the whole brick projects inside (V.inside): the clamps
                 // would change no coordinate
                 auto zloop = [&](auto clamp_tag) {
@@ -1959,13 +1967,13 @@ __global__ void __launch_bounds__(256, 4) bp_perspective_kernel(const __grid_con
                         const float2 uc =
                             kCoordClamp ? f2(fminf(fmaxf(uv.x, lo.x), hi.x), fminf(fmaxf(uv.y, lo.y), hi.y)) : uv;
                         const float2 fq = __fadd2_rd(fma2(uc, splat(256.f), splat(-127.5f)), splat(12582912.0f));
-                        const int bu = __float_as_int(fq.x), bv = __float_as_int(fq.y);
-                        const int x0 = (bu - 0x4B400000) >> 8, y0 = (bv - 0x4B400000) >> 8;
-                        const float2 wab = add2(f2(__int_as_float(((bu << 15) & 0x007F8000) | 0x3F800000),
-                                                   __int_as_float(((bv << 15) & 0x007F8000) | 0x3F800000)),
-                                                splat(-1.f));
-                        // texel index in 32 bits (a slot holds fewer than 2^31 texels)
-                        const int t = y0 * pitch + x0;
+                        const unsigned bu = __float_as_uint(fq.x), bv = __float_as_uint(fq.y);
+                        const float2 wab = q8_weight2(f2(q8_k1(bu), q8_k1(bv)));
+                        // texel index in 32 bits (a slot holds fewer than 2^31 texels):
+                        // bu >> 8 = 0x4B4000 + floor(q / 256), so y0 * pitch + x0 is
+                        // (bv >> 8) * pitch + (bu >> 8) - 0x4B4000 (pitch + 1), in wrapping
+                        // unsigned arithmetic
+                        const int t = (int)((bv >> 8) * (unsigned)pitch + (bu >> 8) - kq);
                         const float2 t00 = __ldg(img + t), t10 = __ldg(img + t + 1);
                         const float2 t01 = __ldg(img + (t + pitch)), t11 = __ldg(img + (t + pitch + 1));
                         // bilinear blend of (r, L) as two lerps along x and one along y, both
