@@ -338,7 +338,8 @@ void launch_bp_t(const BpArgs& a, int device, cudaStream_t st) {
         }
         opted.fetch_or(1ull << device, std::memory_order_acq_rel);
     }
-    const size_t smem = bp_smem_bytes(a.nviews, kPersp ? 0 : a.nsamples);
+    // perspective: the per-(view, z voxel) table of the one-sample path in the sample slots
+    const size_t smem = bp_smem_bytes(a.nviews, kPersp ? kBpZPersp : a.nsamples);
     const int zc = kPersp ? kBpZPersp : kBpZ;
     const int zchunks = (a.slab.rz + zc - 1) / zc;
     dim3 block(32, 8, 1);
@@ -544,7 +545,7 @@ uint32_t launch_bp(const etcu_volume* vol, const BpArgs& a0, bool persp, etcu_sa
         else launch_bp_sart_m<false>(a0, vol->type, sm, st);
         return 1;
     }
-    const size_t per_view = bp_smem_bytes(1, persp ? 0 : a0.nsamples);
+    const size_t per_view = bp_smem_bytes(1, persp ? kBpZPersp : a0.nsamples);
     const int max_views = (int)std::max<size_t>(1, (kBpSmemBudget - 16) / per_view);
     uint32_t launches = 0;
     for (int c0 = 0; c0 < a0.nviews; c0 += max_views) {

@@ -1065,19 +1065,20 @@ __device__ __forceinline__ void cp_async_wait() {
 }
 
 // The float 1 + k 2^-15 for k = bits & 255: one byte permute puts k in bits 8..15 under
-// the exponent of 1 (bytes 3, 2, 0 from 0x3F800000).
+// the exponent of 1 (bytes 3, 2, 0 from 0x3F800000).  The perspective back projector's
+// weights; in the fused SART step the shift and mask-or of q8_tap_bits measured faster.
 __device__ __forceinline__ float q8_k1(unsigned bits) { return __uint_as_float(__byte_perm(bits, 0x3F800000u, 0x7604)); }
 
 // The 1/256 weights k / 256 from two q8_k1 values: 128 (1 + k 2^-15) - 128, exact.
 __device__ __forceinline__ float2 q8_weight2(float2 k1) { return fma2(k1, splat(128.f), splat(-128.f)); }
 
 // Column tap of one voxel from f = fl_down(t + 1.5 * 2^23) = 1.5 * 2^23 + floor(t),
-// t = u * 256 - 127.5 (exact): tap-pair index x0 - x0lo and q8_k1 of k = floor(t) mod 256,
-// whose weight k / 256 q8_weight2 forms.
-__device__ __forceinline__ void q8_tap_bits(float f, int x0lo, int& e, float& k1) {
-    const unsigned bits = __float_as_uint(f);
-    e = (int)(bits >> 8) - ((0x4B400000 >> 8) + x0lo);
-    k1 = q8_k1(bits);
+// t = u * 256 - 127.5 (exact): tap-pair index x0 - x0lo and 1 + a, where
+// a = (floor(t) mod 256) / 256 is the 1/256 weight (exact).
+__device__ __forceinline__ void q8_tap_bits(float f, int x0lo, int& e, float& a1) {
+    const int bits = __float_as_int(f);
+    e = (bits >> 8) - ((0x4B400000 >> 8) + x0lo);
+    a1 = __int_as_float(((bits << 15) & 0x007F8000) | 0x3F800000);
 }
 
 // kFull: every thread owns all kCols columns (rx == kCols * kBpColThreads).
@@ -1199,10 +1200,10 @@ __global__ void __launch_bounds__(kBpColThreads, 4) bp_sart_column_kernel(const 
                     const float2 u = add2(add2(au[k][h], kz), m12);
                     const float2 f = __fadd2_rd(fma2(u, splat(256.f), splat(-127.5f)), splat(12582912.0f));
                     int e0, e1;
-                    float k0, k1;
-                    q8_tap_bits(f.x, x0lo, e0, k0);
-                    q8_tap_bits(f.y, x0lo, e1, k1);
-                    const float2 ax = q8_weight2(f2(k0, k1));
+                    float a0, a1;
+                    q8_tap_bits(f.x, x0lo, e0, a0);
+                    q8_tap_bits(f.y, x0lo, e1, a1);
+                    const float2 ax = add2(f2(a0, a1), splat(-1.f));
 #pragma unroll
                     for (int q = 0; q < 2; ++q) {
                         const int eq = q ? e1 : e0;
@@ -1459,10 +1460,10 @@ __device__ __forceinline__ void fused_row_step(const FuseArgs& a, uint32_t p, in
             const float2 u = add2(add2(au, splat(K[z])), m12);
             const float2 f = __fadd2_rd(fma2(u, splat(256.f), splat(-127.5f)), splat(12582912.0f));
             int e0, e1;
-            float k0, k1;
-            q8_tap_bits(f.x, x0lo, e0, k0);
-            q8_tap_bits(f.y, x0lo, e1, k1);
-            const float2 ax = q8_weight2(f2(k0, k1));
+            float a0, a1;
+            q8_tap_bits(f.x, x0lo, e0, a0);
+            q8_tap_bits(f.y, x0lo, e1, a1);
+            const float2 ax = add2(f2(a0, a1), splat(-1.f));
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
                 const int eq = q ? e1 : e0;
@@ -1882,15 +1883,32 @@ __global__ void __launch_bounds__(256, 4) bp_perspective_kernel(const __grid_con
     const int x = blockIdx.y * blockDim.x + threadIdx.x;
     const int y = blockIdx.z * blockDim.y + threadIdx.y;
     const int z0 = blockIdx.x * kBpZPersp;
-    if (a.persp_n == 1 && kSampling == kSampleQ8) {
-        // per view, whether the block's voxels can skip the texel-coordinate clamps
+    // one sample per voxel, 1/256 weights, no mask: per (view, z voxel of the chunk) the
+    // terms that depend on the view and z only, shared by the block's columns (a table after
+    // the views in shared memory; the other variants form them per voxel, where the table's
+    // registers would not fit the 64 of four blocks per SM)
+    constexpr bool kZTable = kSampling == kSampleQ8 && !kMask;
+    float4* zt = (float4*)(bp_smem + ((size_t)a.nviews * sizeof(BpView) + 15) / 16 * 16);
+    if (a.persp_n == 1) {
         const int tid = threadIdx.y * blockDim.x + threadIdx.x, nt = blockDim.x * blockDim.y;
-        const int bx0 = blockIdx.y * blockDim.x, by0 = blockIdx.z * blockDim.y;
-        const int bx1 = min(g.rx, bx0 + (int)blockDim.x) - 1, by1 = min(g.ry, by0 + (int)blockDim.y) - 1;
-        const int bz1 = min(g.rz, z0 + kBpZPersp) - 1;
-        for (int p = tid; p < a.nviews; p += nt)
-            sv[p].inside = brick_projects_inside(sv[p], g, bx0, bx1, by0, by1, z0, bz1, -1.5f,
-                                                 (float)a.W + 1.49609375f, -1.5f, (float)a.H + 1.49609375f);
+        if (kSampling == kSampleQ8) {
+            // per view, whether the block's voxels can skip the texel-coordinate clamps
+            const int bx0 = blockIdx.y * blockDim.x, by0 = blockIdx.z * blockDim.y;
+            const int bx1 = min(g.rx, bx0 + (int)blockDim.x) - 1, by1 = min(g.ry, by0 + (int)blockDim.y) - 1;
+            const int bz1 = min(g.rz, z0 + kBpZPersp) - 1;
+            for (int p = tid; p < a.nviews; p += nt)
+                sv[p].inside = brick_projects_inside(sv[p], g, bx0, bx1, by0, by1, z0, bz1, -1.5f,
+                                                     (float)a.W + 1.49609375f, -1.5f, (float)a.H + 1.49609375f);
+        }
+        // (m_w2 pz, dz^2, |dz| / vs_z, pz) with pz the voxel centre's z, dz = pz - source z:
+        // the same operations as at the voxel (z voxels past the slab get unused entries)
+        for (int i = tid; kZTable && i < a.nviews * kBpZPersp; i += nt) {
+            const int p = i / kBpZPersp, j = i - p * kBpZPersp;
+            const float cz = fadd(g.bmin.z, fmul(fadd((float)(z0 + j), 0.5f), g.vs.z));
+            const float pzj = fadd(fsub(cz, fmul(0.5f, g.vs.z)), fmul(g.vs.z, 0.5f));
+            const float dz = fsub(pzj, sv[p].src[2]);
+            zt[i] = make_float4(fmul(sv[p].mw[2], pzj), fmul(dz, dz), fmul(fabsf(dz), g.ivs.z), pzj);
+        }
         __syncthreads();
     }
     if (x >= g.rx || y >= g.ry) return;
@@ -1913,16 +1931,19 @@ __global__ void __launch_bounds__(256, 4) bp_perspective_kernel(const __grid_con
         // as evaluating everything per voxel.
         const float px = fadd(fsub(cx, fmul(0.5f, g.vs.x)), fmul(g.vs.x, 0.5f));
         const float py = fadd(fsub(cy, fmul(0.5f, g.vs.y)), fmul(g.vs.y, 0.5f));
-        float val[kBpZPersp], pz[kBpZPersp], mw[kBpZPersp];
+        // the voxel centres' z (pz): from the table, or in registers
+        float val[kBpZPersp], mw[kBpZPersp], pz[kZTable ? 1 : kBpZPersp];
 #pragma unroll
         for (int j = 0; j < kBpZPersp; ++j) {
             val[j] = 0.f;
-            pz[j] = 0.f;
             mw[j] = 1.f;
+            if constexpr (!kZTable) pz[j] = 0.f;
             if (j < nzc) {
                 const size_t idx = base + (size_t)j * plane;
-                const float cz = fadd(g.bmin.z, fmul(fadd((float)(z0 + j), 0.5f), g.vs.z));
-                pz[j] = fadd(fsub(cz, fmul(0.5f, g.vs.z)), fmul(g.vs.z, 0.5f));
+                if constexpr (!kZTable) {
+                    const float cz = fadd(g.bmin.z, fmul(fadd((float)(z0 + j), 0.5f), g.vs.z));
+                    pz[j] = fadd(fsub(cz, fmul(0.5f, g.vs.z)), fmul(g.vs.z, 0.5f));
+                }
                 val[j] = bp_load<kStore>(a, idx);
                 if (kMask) mw[j] = mask_weight(a.mask + idx);
             }
@@ -1932,6 +1953,7 @@ __global__ void __launch_bounds__(256, 4) bp_perspective_kernel(const __grid_con
             constexpr bool kFull = decltype(full_tag)::value;
             for (int p = 0; p < a.nviews; ++p) {
                 const BpView& V = sv[p];
+                [[maybe_unused]] const float4* zv = zt + p * kBpZPersp;
                 const float2* img = a.rl + (size_t)p * a.rl_slot;
                 const float2 cuv = f2(fadd(fmul(V.mu[0], px), fmul(V.mu[1], py)), fadd(fmul(V.mv[0], px), fmul(V.mv[1], py)));
                 const float2 m2 = f2(V.mu[2], V.mv[2]), m3 = f2(V.mu[3], V.mv[3]);
@@ -1952,9 +1974,17 @@ __global__ void __launch_bounds__(256, 4) bp_perspective_kernel(const __grid_con
 #pragma unroll
                 for (int j = 0; j < kBpZPersp; ++j) {
                     if (!kFull && j >= nzc) continue;
+                    // (m_w2 pz, dz^2, |dz| / vs_z, pz) of this view and z voxel
+                    float4 zq;
+                    if constexpr (kZTable) {
+                        zq = zv[j];
+                    } else {
+                        const float dz = fsub(pz[j], V.src[2]);
+                        zq = make_float4(fmul(V.mw[2], pz[j]), fmul(dz, dz), fmul(fabsf(dz), g.ivs.z), pz[j]);
+                    }
                     // u and v as paired operations (each lane the same operations as alone)
-                    float2 uv = add2(add2(cuv, __fmul2_rn(m2, splat(pz[j]))), m3);
-                    const float w = fadd(fadd(cw, fmul(V.mw[2], pz[j])), V.mw[3]);
+                    float2 uv = add2(add2(cuv, __fmul2_rn(m2, splat(zq.w))), m3);
+                    const float w = fadd(fadd(cw, zq.x), V.mw[3]);
                     float rw = rcp_approx(w);
                     rw = fmaf(rw, fmaf(-w, rw, 1.f), rw);
                     uv = __fmul2_rn(uv, splat(rw));
@@ -1987,9 +2017,8 @@ __global__ void __launch_bounds__(256, 4) bp_perspective_kernel(const __grid_con
                     // r * chord / L with chord = |d| / m: r * nd2 * rsqrt(nd2 * (m L)^2),
                     // one reciprocal square root for the chord and the division by L; formed
                     // for every sample and selected (0 where L < kEps, which the reference skips)
-                    const float dz = fsub(pz[j], V.src[2]);
-                    const float nd2 = fadd(dxy, fmul(dz, dz));
-                    const float mL = fmul(fmaxf(mxy, fmul(fabsf(dz), g.ivs.z)), rl.y);
+                    const float nd2 = fadd(dxy, zq.y);
+                    const float mL = fmul(fmaxf(mxy, zq.z), rl.y);
                     const float q = fmul(rl.x, fmul(nd2, rsqrtf(fmul(nd2, fmul(mL, mL)))));
                     const float value = rl.y >= kEps ? q : 0.f;
                     float vj = fadd(val[j], fmul(fmul(a.lambda, value), mw[j]));
