@@ -1159,7 +1159,7 @@ def main():
         return
 
     if args.workload == "c3":
-        print(json.dumps(run_c3(args)), flush=True)
+        print(json.dumps(run_c3(args, cpu_baseline=not args.no_cpu_baseline)), flush=True)
         return
     if args.workload == "c5":
         print(json.dumps(run_c5(args)), flush=True)
